@@ -1,0 +1,95 @@
+// Internal layouts of libimbart shared by the host-side builders/converters and the
+// sm_100a kernels. Nothing here is part of the C ABI.
+#pragma once
+
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/imbart.h"
+
+namespace imbart {
+
+// ---------------------------------------------------------------------------------------
+// Compressed 8-wide BVH node, 80 bytes = 5 x 16 B, read with five 128-bit loads.
+//
+//   q0: px, py, pz (float grid origin), w = ex | ey << 8 | ez << 16 | imask << 24
+//       (ex/ey/ez: signed 8-bit exponents, child box coordinate = p + q * 2^e;
+//        imask bit s: slot s holds an internal child)
+//   q1: child_base, prim_base, meta[0..3], meta[4..7]
+//       internal child in slot s -> node child_base + popc(imask & ((1 << s) - 1))
+//       leaf child in slot s     -> meta[s] = count << 5 | offset: primitives
+//                                   [prim_base + offset, prim_base + offset + count)
+//       empty slot               -> meta[s] = 0 and an inverted box
+//   q2: qlo_x[0..7] (bytes 0-7), qhi_x[0..7] (bytes 8-15)
+//   q3: qlo_y, qhi_y      q4: qlo_z, qhi_z
+//
+// Child slots are assigned at build time so that slot s holds the child lying towards
+// (s&1 ? +x : -x, s&2 ? +y : -y, s&4 ? +z : -z); a ray with direction octant `oct` (bit set
+// for a negative component) visits hit children in ascending order of (slot ^ oct),
+// which approximates front-to-back order without sorting.
+// ---------------------------------------------------------------------------------------
+struct alignas(16) WideNode {
+    float px, py, pz;
+    uint8_t ex, ey, ez, imask;
+    uint32_t child_base;
+    uint32_t prim_base;
+    uint8_t meta[8];
+    uint8_t qlo_x[8], qhi_x[8];
+    uint8_t qlo_y[8], qhi_y[8];
+    uint8_t qlo_z[8], qhi_z[8];
+};
+static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
+
+// Triangle record, 48 bytes: v0.xyz + global tri id (int bits) in v0.w, v1.xyz, v2.xyz.
+struct alignas(16) WideTri {
+    float v0[3]; int32_t id;
+    float v1[3]; int32_t pad0;
+    float v2[3]; int32_t pad1;
+};
+static_assert(sizeof(WideTri) == 48, "WideTri must be 48 bytes");
+
+// Instance record, 64 bytes: rows of the 3x4 world-to-object matrix, instance id and the
+// wide index of the instanced mesh's root node.
+struct alignas(16) WideInst {
+    float m[12];
+    int32_t id;
+    int32_t root;
+    int32_t pad[2];
+};
+static_assert(sizeof(WideInst) == 64, "WideInst must be 64 bytes");
+
+// Host-side result of converting a reference layout.
+struct HostWideScene {
+    std::vector<WideNode> nodes;
+    std::vector<WideTri> tris;
+    std::vector<WideInst> insts;
+    int root = 0;          // wide index of the top-level root
+    int top_nodes = 0;     // number of top-level wide nodes
+    bool masked = false;
+    std::vector<int> indices;
+    std::vector<imbart_vec2> texcoords;
+    std::vector<imbart_mask_desc> masks;
+    std::vector<uint8_t> mask_buffer;
+};
+
+// Converters (convert.cpp). Return empty string on success, else an error message.
+std::string convert_node2(int root, const imbart_node2* nodes, int n_nodes,
+                          const imbart_instance_node* insts, int n_insts,
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out);
+std::string convert_node4(int root, const imbart_node4* nodes, int n_nodes,
+                          const imbart_instance_node* insts, int n_insts,
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out);
+// Decides whether the masks are all opaque and copies them when they are not.
+void attach_masks(HostWideScene& out, const int* indices, int n_indices,
+                  const imbart_vec2* texcoords, int n_texcoords,
+                  const imbart_mask_desc* masks, int n_masks,
+                  const char* mask_buffer, int mask_buffer_size);
+
+// Thread-local error reporting (error.cpp).
+void set_error(int code, const std::string& msg);
+
+inline int float_bits(float f) { union { float f; int i; } u; u.f = f; return u.i; }
+inline float bits_float(int i) { union { float f; int i; } u; u.i = i; return u.f; }
+
+}  // namespace imbart

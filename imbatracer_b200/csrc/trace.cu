@@ -1,0 +1,440 @@
+// Host side of the traversal: scene preparation and upload, the stream-ordered trace entry
+// points and the four drop-in symbols of the reference boundary (ray_queue.h:247-343).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "imbart_internal.h"
+#include "trace_kernel.cuh"
+
+struct imbart_scene {
+    int device = 0;
+    imbart::WideNode* nodes = nullptr;
+    imbart::WideTri* tris = nullptr;
+    imbart::WideInst* insts = nullptr;
+    int* indices = nullptr;
+    float2* texcoords = nullptr;
+    int* masks = nullptr;
+    uint8_t* mask_buffer = nullptr;
+    int n_masks = 0;
+    int* error_flags = nullptr;
+    imbart_scene_info info{};
+};
+
+namespace imbart {
+namespace {
+
+std::atomic<int64_t> g_launches{0};
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? IMBART_ERR_OUT_OF_MEMORY : IMBART_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+template <typename T>
+bool upload(T** dst, const T* src, size_t n, int64_t* bytes) {
+    *dst = nullptr;
+    if (n == 0) return true;
+    if (!cuda_ok(cudaMalloc((void**)dst, n * sizeof(T)), "cudaMalloc")) return false;
+    *bytes += (int64_t)(n * sizeof(T));
+    return cuda_ok(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+}
+
+void free_scene(imbart_scene* s) {
+    if (!s) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->insts);
+    cudaFree(s->indices); cudaFree(s->texcoords); cudaFree(s->masks); cudaFree(s->mask_buffer);
+    cudaFree(s->error_flags);
+    cudaSetDevice(prev);
+    delete s;
+}
+
+imbart_scene* upload_scene(const HostWideScene& h, int device) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return nullptr;
+    std::unique_ptr<imbart_scene, void (*)(imbart_scene*)> s(new imbart_scene, free_scene);
+    s->device = device;
+    int64_t bytes = 0;
+    bool ok = upload(&s->nodes, h.nodes.data(), h.nodes.size(), &bytes) &&
+              upload(&s->tris, h.tris.data(), h.tris.size(), &bytes) &&
+              upload(&s->insts, h.insts.data(), h.insts.size(), &bytes);
+    if (ok && h.masked) {
+        std::vector<int> m(3 * h.masks.size());
+        for (size_t i = 0; i < h.masks.size(); ++i) {
+            m[3 * i] = h.masks[i].width; m[3 * i + 1] = h.masks[i].height; m[3 * i + 2] = h.masks[i].offset;
+        }
+        ok = upload(&s->indices, h.indices.data(), h.indices.size(), &bytes) &&
+             upload(&s->texcoords, reinterpret_cast<const float2*>(h.texcoords.data()), h.texcoords.size(), &bytes) &&
+             upload(&s->masks, m.data(), m.size(), &bytes) &&
+             upload(&s->mask_buffer, h.mask_buffer.data(), h.mask_buffer.size(), &bytes);
+        s->n_masks = (int)h.masks.size();
+    }
+    if (ok) ok = cuda_ok(cudaMalloc((void**)&s->error_flags, 4 * sizeof(int)), "cudaMalloc") &&
+                 cuda_ok(cudaMemset(s->error_flags, 0, 4 * sizeof(int)), "cudaMemset");
+    cudaSetDevice(prev);
+    if (!ok) return nullptr;
+    s->info.wide_nodes = (int64_t)h.nodes.size();
+    s->info.top_nodes = h.top_nodes;
+    s->info.triangles = (int64_t)h.tris.size();
+    s->info.instances = (int64_t)h.insts.size();
+    s->info.device_bytes = bytes;
+    s->info.root = h.root;
+    s->info.masked = h.masked ? 1 : 0;
+    return s.release();
+}
+
+template <typename Node, typename Convert>
+imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
+                      const imbart_instance_node* insts, int n_insts, const imbart_vec4* tris, int n_tri_vec4,
+                      const int* indices, int n_indices, const imbart_vec2* texcoords, int n_texcoords,
+                      const imbart_mask_desc* masks, int n_masks, const char* mask_buffer, int mask_buffer_size,
+                      int device) {
+    if (!nodes || !insts || !tris || n_nodes <= 0 || n_insts <= 0 || n_tri_vec4 <= 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "scene preparation: missing arrays");
+        return nullptr;
+    }
+    HostWideScene h;
+    const std::string err = convert(root, nodes, n_nodes, insts, n_insts, tris, n_tri_vec4, h);
+    if (!err.empty()) {
+        set_error(IMBART_ERR_BAD_SCENE, "scene preparation: " + err);
+        return nullptr;
+    }
+    attach_masks(h, indices, n_indices, texcoords, n_texcoords, masks, n_masks, mask_buffer, mask_buffer_size);
+    return upload_scene(h, device);
+}
+
+int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out,
+                 int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr) {
+    if (!s || (!rays && count > 0) || (!hits && count > 0) || count < 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (count == 0) return 0;
+    TraceParams p;
+    p.nodes = s->nodes; p.tris = s->tris; p.insts = s->insts; p.root = s->info.root;
+    p.indices = s->indices; p.texcoords = s->texcoords; p.masks = s->masks; p.mask_buffer = s->mask_buffer;
+    p.n_masks = s->n_masks;
+    p.rays = reinterpret_cast<const float4*>(rays);
+    p.hits = reinterpret_cast<int4*>(hits);
+    p.v_out = v_out;
+    p.count = count;
+    p.error_flags = s->error_flags;
+    p.stats = stats;
+    const int block = 128;
+    const int grid = (count + block - 1) / block;
+    const bool any = (flags & IMBART_TRACE_ANY) != 0;
+    const bool masked = s->info.masked != 0;
+    if (stats) {
+        if (any && masked) trace_kernel<true, true, true><<<grid, block, 0, stream>>>(p);
+        else if (any) trace_kernel<true, false, true><<<grid, block, 0, stream>>>(p);
+        else if (masked) trace_kernel<false, true, true><<<grid, block, 0, stream>>>(p);
+        else trace_kernel<false, false, true><<<grid, block, 0, stream>>>(p);
+    } else {
+        if (any && masked) trace_kernel<true, true, false><<<grid, block, 0, stream>>>(p);
+        else if (any) trace_kernel<true, false, false><<<grid, block, 0, stream>>>(p);
+        else if (masked) trace_kernel<false, true, false><<<grid, block, 0, stream>>>(p);
+        else trace_kernel<false, false, false><<<grid, block, 0, stream>>>(p);
+    }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!cuda_ok(cudaGetLastError(), "trace kernel launch")) return IMBART_ERR_CUDA;
+    return 0;
+}
+
+// Per-thread stream for the synchronous drop-in entry points: the reference calls them
+// concurrently from its tile-scheduler threads (tile_scheduler.h:120-130).
+cudaStream_t thread_stream() {
+    thread_local cudaStream_t st = nullptr;
+    if (!st) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    return st;
+}
+
+// ---------------------------------------------------------------------------------------
+// Drop-in scene cache. The reference passes raw pointers without sizes; device arrays are
+// sized through their allocation range, host arrays are walked from the root.
+// ---------------------------------------------------------------------------------------
+using CacheKey = std::tuple<const void*, int, const void*, const void*, const void*, const void*, int>;
+std::mutex g_cache_mutex;
+std::map<CacheKey, imbart_scene*> g_cache;
+
+void clear_cache() {
+    std::lock_guard<std::mutex> lk(g_cache_mutex);
+    for (auto& kv : g_cache) free_scene(kv.second);
+    g_cache.clear();
+}
+
+// cuMemGetAddressRange through the runtime's driver entry-point table, so that the library
+// loads on machines without a driver (the CPU-only build and test host).
+using MemGetAddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+MemGetAddressRangeFn mem_get_address_range() {
+    static MemGetAddressRangeFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<MemGetAddressRangeFn>(f);
+    }();
+    return fn;
+}
+
+// Copies the tail of the device allocation that starts at or before `ptr` to the host.
+template <typename T>
+bool fetch_device_array(const T* ptr, std::vector<T>& out) {
+    out.clear();
+    if (!ptr) return true;
+    cudaFree(0);  // make the primary context current for the driver call
+    MemGetAddressRangeFn range = mem_get_address_range();
+    if (!range) {
+        set_error(IMBART_ERR_CUDA, "drop-in traversal: cuMemGetAddressRange unavailable");
+        return false;
+    }
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (range(&base, &size, (CUdeviceptr)ptr) != CUDA_SUCCESS) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "drop-in traversal: pointer is not a device allocation");
+        return false;
+    }
+    const size_t off = (size_t)((CUdeviceptr)ptr - base);
+    const size_t n = (size - off) / sizeof(T);
+    out.resize(n);
+    return n == 0 || cuda_ok(cudaMemcpy(out.data(), ptr, n * sizeof(T), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+}
+
+imbart_scene* cached_device_scene(int root, const imbart_node2* nodes, const imbart_instance_node* insts,
+                                  const imbart_vec4* tris, const int* indices, const imbart_vec2* texcoords,
+                                  const imbart_mask_desc* masks, const char* mask_buffer) {
+    int device = 0;
+    cudaGetDevice(&device);
+    const CacheKey key{nodes, root, insts, tris, masks, mask_buffer, device};
+    std::lock_guard<std::mutex> lk(g_cache_mutex);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) return it->second;
+    std::vector<imbart_node2> hn;
+    std::vector<imbart_instance_node> hi;
+    std::vector<imbart_vec4> ht;
+    std::vector<int> hidx;
+    std::vector<imbart_vec2> htc;
+    std::vector<imbart_mask_desc> hm;
+    std::vector<char> hmb;
+    if (!fetch_device_array(nodes, hn) || !fetch_device_array(insts, hi) || !fetch_device_array(tris, ht) ||
+        !fetch_device_array(indices, hidx) || !fetch_device_array(texcoords, htc) ||
+        !fetch_device_array(masks, hm) || !fetch_device_array(mask_buffer, hmb))
+        return nullptr;
+    imbart_scene* s = prepare<imbart_node2>(convert_node2, root, hn.data(), (int)hn.size(), hi.data(), (int)hi.size(),
+                                            ht.data(), (int)ht.size(), hidx.data(), (int)hidx.size(),
+                                            htc.data(), (int)htc.size(), hm.data(), (int)hm.size(),
+                                            hmb.data(), (int)hmb.size(), device);
+    if (s) g_cache[key] = s;
+    return s;
+}
+
+imbart_scene* cached_host_scene(int root, const imbart_node4* nodes, const imbart_instance_node* insts,
+                                const imbart_vec4* tris, const int* indices, const imbart_vec2* texcoords,
+                                const imbart_mask_desc* masks, const char* mask_buffer) {
+    int device = 0;
+    cudaGetDevice(&device);
+    const CacheKey key{nodes, root, insts, tris, masks, mask_buffer, device};
+    std::lock_guard<std::mutex> lk(g_cache_mutex);
+    auto it = g_cache.find(key);
+    if (it != g_cache.end()) return it->second;
+    // Host arrays carry no size: the converter only touches what is reachable from the root.
+    // Index and texcoord arrays are only needed when masks are active; their extent is the
+    // largest index reachable through the triangles (computed by the converter's caller).
+    HostWideScene h;
+    const std::string err = convert_node4(root, nodes, INT_MAX, insts, INT_MAX, tris, INT_MAX, h);
+    if (!err.empty()) {
+        set_error(IMBART_ERR_BAD_SCENE, "scene preparation: " + err);
+        return nullptr;
+    }
+    if (masks && mask_buffer && indices) {
+        int max_tri = 0;
+        for (const WideTri& t : h.tris) max_tri = std::max(max_tri, t.id);
+        int n_idx = 4 * (max_tri + 1), max_mat = 0, max_tc = 0;
+        for (int i = 0; i < n_idx; ++i) {
+            if (i % 4 == 3) max_mat = std::max(max_mat, indices[i]);
+            else max_tc = std::max(max_tc, indices[i]);
+        }
+        int buf = 0;
+        for (int m = 0; m <= max_mat; ++m) buf = std::max(buf, masks[m].offset + masks[m].width * masks[m].height);
+        attach_masks(h, indices, n_idx, texcoords, texcoords ? max_tc + 1 : 0, masks, max_mat + 1, mask_buffer, buf);
+    }
+    imbart_scene* s = upload_scene(h, device);
+    if (s) g_cache[key] = s;
+    return s;
+}
+
+void dropin_device(bool any, int root, imbart_node2* nodes, imbart_instance_node* insts, imbart_vec4* tris,
+                   imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                   imbart_mask_desc* masks, char* mask_buffer, int count) {
+    imbart_scene* s = cached_device_scene(root, nodes, insts, tris, indices, texcoords, masks, mask_buffer);
+    if (!s) return;
+    cudaStream_t st = thread_stream();
+    if (launch_trace(s, rays, hits, nullptr, count, any ? IMBART_TRACE_ANY : IMBART_TRACE_CLOSEST, st) == 0)
+        cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+}
+
+void dropin_host(bool any, int root, imbart_node4* nodes, imbart_instance_node* insts, imbart_vec4* tris,
+                 imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                 imbart_mask_desc* masks, char* mask_buffer, int count) {
+    imbart_scene* s = cached_host_scene(root, nodes, insts, tris, indices, texcoords, masks, mask_buffer);
+    if (!s) return;
+    imbart_trace_host(s, rays, hits, count, any ? IMBART_TRACE_ANY : IMBART_TRACE_CLOSEST, thread_stream());
+}
+
+}  // namespace
+}  // namespace imbart
+
+using namespace imbart;
+
+extern "C" {
+
+imbart_scene* imbart_scene_from_node2(int root, const imbart_node2* nodes, int n_nodes,
+                                      const imbart_instance_node* instances, int n_instances,
+                                      const imbart_vec4* tris, int n_tri_vec4,
+                                      const int* indices, int n_indices,
+                                      const imbart_vec2* texcoords, int n_texcoords,
+                                      const imbart_mask_desc* masks, int n_masks,
+                                      const char* mask_buffer, int mask_buffer_size, int device) {
+    return prepare<imbart_node2>(convert_node2, root, nodes, n_nodes, instances, n_instances, tris, n_tri_vec4,
+                                 indices, n_indices, texcoords, n_texcoords, masks, n_masks, mask_buffer,
+                                 mask_buffer_size, device);
+}
+
+imbart_scene* imbart_scene_from_node4(int root, const imbart_node4* nodes, int n_nodes,
+                                      const imbart_instance_node* instances, int n_instances,
+                                      const imbart_vec4* tris, int n_tri_vec4,
+                                      const int* indices, int n_indices,
+                                      const imbart_vec2* texcoords, int n_texcoords,
+                                      const imbart_mask_desc* masks, int n_masks,
+                                      const char* mask_buffer, int mask_buffer_size, int device) {
+    return prepare<imbart_node4>(convert_node4, root, nodes, n_nodes, instances, n_instances, tris, n_tri_vec4,
+                                 indices, n_indices, texcoords, n_texcoords, masks, n_masks, mask_buffer,
+                                 mask_buffer_size, device);
+}
+
+void imbart_scene_destroy(imbart_scene* scene) { free_scene(scene); }
+
+int imbart_scene_get_info(const imbart_scene* scene, imbart_scene_info* out) {
+    if (!scene || !out) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_scene_get_info"); return IMBART_ERR_INVALID_ARGUMENT; }
+    *out = scene->info;
+    return 0;
+}
+
+int imbart_scene_get_device_arrays(const imbart_scene* scene, const void** nodes, const void** tris,
+                                   const void** instances) {
+    if (!scene) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_scene_get_device_arrays"); return IMBART_ERR_INVALID_ARGUMENT; }
+    if (nodes) *nodes = scene->nodes;
+    if (tris) *tris = scene->tris;
+    if (instances) *instances = scene->insts;
+    return 0;
+}
+
+int imbart_trace(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count, int flags,
+                 void* stream) {
+    return launch_trace(scene, rays, hits, nullptr, count, flags, (cudaStream_t)stream);
+}
+
+int imbart_trace_uv(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, float* v_out, int count,
+                    int flags, void* stream) {
+    return launch_trace(scene, rays, hits, v_out, count, flags, (cudaStream_t)stream);
+}
+
+int imbart_trace_host(const imbart_scene* scene, const imbart_ray* rays_host, imbart_hit* hits_host, int count,
+                      int flags, void* stream) {
+    if (!scene || count < 0 || (count > 0 && (!rays_host || !hits_host))) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace_host: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (count == 0) return 0;
+    // Per-thread device staging buffers, grown on demand.
+    thread_local imbart_ray* d_rays = nullptr;
+    thread_local imbart_hit* d_hits = nullptr;
+    thread_local int cap = 0;
+    thread_local int cap_device = -1;
+    if (cap < count || cap_device != scene->device) {
+        cudaFree(d_rays); cudaFree(d_hits);
+        d_rays = nullptr; d_hits = nullptr; cap = 0;
+        if (!cuda_ok(cudaMalloc((void**)&d_rays, sizeof(imbart_ray) * (size_t)count), "cudaMalloc") ||
+            !cuda_ok(cudaMalloc((void**)&d_hits, sizeof(imbart_hit) * (size_t)count), "cudaMalloc"))
+            return IMBART_ERR_OUT_OF_MEMORY;
+        cap = count;
+        cap_device = scene->device;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!cuda_ok(cudaMemcpyAsync(d_rays, rays_host, sizeof(imbart_ray) * (size_t)count, cudaMemcpyHostToDevice, st),
+                 "cudaMemcpyAsync H2D"))
+        return IMBART_ERR_CUDA;
+    const int rc = launch_trace(scene, d_rays, d_hits, nullptr, count, flags, st);
+    if (rc) return rc;
+    if (!cuda_ok(cudaMemcpyAsync(hits_host, d_hits, sizeof(imbart_hit) * (size_t)count, cudaMemcpyDeviceToHost, st),
+                 "cudaMemcpyAsync D2H"))
+        return IMBART_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize")) return IMBART_ERR_CUDA;
+    return 0;
+}
+
+int imbart_trace_stats(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count, int flags,
+                       unsigned long long* stats, void* stream) {
+    if (!stats) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace_stats: stats is NULL");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    return launch_trace(scene, rays, hits, nullptr, count, flags, (cudaStream_t)stream, stats);
+}
+
+int imbart_scene_error_count(const imbart_scene* scene) {
+    if (!scene) return -1;
+    int v = 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    const bool ok = cuda_ok(cudaMemcpy(&v, scene->error_flags, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    cudaSetDevice(prev);
+    return ok ? v : -1;
+}
+
+int64_t imbart_kernel_launch_count(void) { return g_launches.load(); }
+
+void imbart_invalidate_scenes(void) { clear_cache(); }
+
+void intersect_gpu_masked_instanced(int root, imbart_node2* nodes, imbart_instance_node* instances, imbart_vec4* tris,
+                                    imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                                    imbart_mask_desc* masks, char* mask_buffer, int count) {
+    dropin_device(false, root, nodes, instances, tris, rays, hits, indices, texcoords, masks, mask_buffer, count);
+}
+
+void occluded_gpu_masked_instanced(int root, imbart_node2* nodes, imbart_instance_node* instances, imbart_vec4* tris,
+                                   imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                                   imbart_mask_desc* masks, char* mask_buffer, int count) {
+    dropin_device(true, root, nodes, instances, tris, rays, hits, indices, texcoords, masks, mask_buffer, count);
+}
+
+void intersect_cpu_masked_instanced(int root, imbart_node4* nodes, imbart_instance_node* instances, imbart_vec4* tris,
+                                    imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                                    imbart_mask_desc* masks, char* mask_buffer, int count) {
+    dropin_host(false, root, nodes, instances, tris, rays, hits, indices, texcoords, masks, mask_buffer, count);
+}
+
+void occluded_cpu_masked_instanced(int root, imbart_node4* nodes, imbart_instance_node* instances, imbart_vec4* tris,
+                                   imbart_ray* rays, imbart_hit* hits, int* indices, imbart_vec2* texcoords,
+                                   imbart_mask_desc* masks, char* mask_buffer, int count) {
+    dropin_host(true, root, nodes, instances, tris, rays, hits, indices, texcoords, masks, mask_buffer, count);
+}
+
+}  // extern "C"

@@ -1,0 +1,373 @@
+// Device-side traversal of the compressed 8-wide two-level BVH (closest hit and any hit).
+//
+// Semantics follow the reference boundary: rays carry tmin in org.w and tmax in dir.w
+// (camera.h:61-64), hits report the global triangle id, the instance id, t and the
+// barycentric weight u of the triangle's second vertex (integrator.h:71-94). The triangle
+// test is the watertight test of Woop, Benthin and Wald (JCGT 2013) evaluated with explicit
+// round-to-nearest operations (no contraction), so that the CPU oracle computes bit-identical
+// t/u/v. Equal-t hits resolve to the smallest (inst_id, tri_id), which makes the result
+// independent of the traversal order and of the BVH.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "imbart_internal.h"
+
+namespace imbart {
+
+constexpr int kStackSize = 64;
+constexpr uint32_t kTypeShift = 30;
+constexpr uint32_t kIndexMask = (1u << kTypeShift) - 1u;
+constexpr uint32_t kEntryNode = 0u;     // node group: x = child base, y = hits << 8 | imask
+constexpr uint32_t kEntryInst = 1u;     // instance group: x = prim base, y = prim mask
+constexpr uint32_t kEntryMarker = 2u;   // return from an instance to the world-space ray
+
+// Relative slack applied to slab exits and to the current hit distance when culling
+// children; together with the build-time padding of quantized boxes it makes the box test
+// conservative under float rounding (cf. Ize, "Robust BVH Ray Traversal", JCGT 2013).
+#define IMBART_SLACK 1.00000095367431640625f  /* 1 + 2^-20 */
+
+struct TraceParams {
+    const WideNode* __restrict__ nodes;
+    const WideTri* __restrict__ tris;
+    const WideInst* __restrict__ insts;
+    int root;
+    // alpha masks (only when masked)
+    const int* __restrict__ indices;
+    const float2* __restrict__ texcoords;
+    const int* __restrict__ masks;          // 3 ints per descriptor
+    const uint8_t* __restrict__ mask_buffer;
+    int n_masks;
+    // rays/hits
+    const float4* __restrict__ rays;        // 2 float4 per ray
+    int4* __restrict__ hits;                // 1 int4 per hit (tri, inst, t bits, u bits)
+    float* __restrict__ v_out;              // optional
+    int count;
+    int* __restrict__ error_flags;          // [0]: stack overflow count
+    unsigned long long* __restrict__ stats; // statistics variant: nodes, triangles, instances
+};
+
+// Work counters of one ray, accumulated only by the statistics variant of the kernel.
+struct RayStats {
+    uint32_t nodes = 0, tris = 0, insts = 0;
+};
+
+__device__ __forceinline__ int max_dim3(float x, float y, float z) {
+    return (x > y) ? ((x > z) ? 0 : 2) : ((y > z) ? 1 : 2);
+}
+
+__device__ __forceinline__ float comp3(float x, float y, float z, int k) {
+    return k == 0 ? x : (k == 1 ? y : z);
+}
+
+// Per-space ray data: origin, direction, safe inverse direction, octant, shear constants,
+// and the slab padding `pad` (world units of the current space). The watertight test may
+// accept a hit a few ulps of |vertex - origin| outside the exact triangle; padding every
+// slab by 2^-20 * max|origin| (here) and every child box by 2^-20 of the node's coordinate
+// magnitude (at build time) keeps such hits inside the boxes that lead to them.
+struct SpaceRay {
+    float pad;
+    float ox, oy, oz;
+    float dx, dy, dz;
+    float ix, iy, iz;
+    uint32_t oct;
+    int kx, ky, kz;
+    float Sx, Sy, Sz;
+};
+
+__device__ __forceinline__ float safe_rcp(float d) {
+    // Zero components get a huge finite inverse of the right sign so that slab tests stay
+    // free of 0 * inf; the triangle test uses the true direction.
+    const float tiny = 1e-30f;
+    const float dd = fabsf(d) < tiny ? copysignf(tiny, d) : d;
+    return __frcp_rn(dd);
+}
+
+__device__ __forceinline__ void setup_space(SpaceRay& r) {
+    r.pad = fmaxf(fmaxf(fabsf(r.ox), fabsf(r.oy)), fabsf(r.oz)) * 9.5367431640625e-07f;
+    r.ix = safe_rcp(r.dx); r.iy = safe_rcp(r.dy); r.iz = safe_rcp(r.dz);
+    r.oct = (r.dx < 0.0f ? 1u : 0u) | (r.dy < 0.0f ? 2u : 0u) | (r.dz < 0.0f ? 4u : 0u);
+    const int kz = max_dim3(fabsf(r.dx), fabsf(r.dy), fabsf(r.dz));
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    const float dkz = comp3(r.dx, r.dy, r.dz, kz);
+    if (dkz < 0.0f) { const int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.Sx = __fdiv_rn(comp3(r.dx, r.dy, r.dz, kx), dkz);
+    r.Sy = __fdiv_rn(comp3(r.dx, r.dy, r.dz, ky), dkz);
+    r.Sz = __fdiv_rn(1.0f, dkz);
+}
+
+// Watertight ray/triangle test. Returns true and writes t/u/v when the ray's line hits the
+// triangle (edges and vertices included, both faces). u weights v1 and v weights v2.
+__device__ __forceinline__ bool tri_test(const SpaceRay& r, const float4 a, const float4 b, const float4 c,
+                                         float& t, float& u, float& v) {
+    const float Ax0 = __fsub_rn(a.x, r.ox), Ay0 = __fsub_rn(a.y, r.oy), Az0 = __fsub_rn(a.z, r.oz);
+    const float Bx0 = __fsub_rn(b.x, r.ox), By0 = __fsub_rn(b.y, r.oy), Bz0 = __fsub_rn(b.z, r.oz);
+    const float Cx0 = __fsub_rn(c.x, r.ox), Cy0 = __fsub_rn(c.y, r.oy), Cz0 = __fsub_rn(c.z, r.oz);
+    const float Akx = comp3(Ax0, Ay0, Az0, r.kx), Aky = comp3(Ax0, Ay0, Az0, r.ky), Akz = comp3(Ax0, Ay0, Az0, r.kz);
+    const float Bkx = comp3(Bx0, By0, Bz0, r.kx), Bky = comp3(Bx0, By0, Bz0, r.ky), Bkz = comp3(Bx0, By0, Bz0, r.kz);
+    const float Ckx = comp3(Cx0, Cy0, Cz0, r.kx), Cky = comp3(Cx0, Cy0, Cz0, r.ky), Ckz = comp3(Cx0, Cy0, Cz0, r.kz);
+    const float Ax = __fsub_rn(Akx, __fmul_rn(r.Sx, Akz));
+    const float Ay = __fsub_rn(Aky, __fmul_rn(r.Sy, Akz));
+    const float Bx = __fsub_rn(Bkx, __fmul_rn(r.Sx, Bkz));
+    const float By = __fsub_rn(Bky, __fmul_rn(r.Sy, Bkz));
+    const float Cx = __fsub_rn(Ckx, __fmul_rn(r.Sx, Ckz));
+    const float Cy = __fsub_rn(Cky, __fmul_rn(r.Sy, Ckz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // Edge case: recompute the edge functions in double precision (Woop et al., sec. 5).
+        U = __double2float_rn(__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx)));
+        V = __double2float_rn(__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx)));
+        W = __double2float_rn(__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax)));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.0f) return false;
+    const float Az = __fmul_rn(r.Sz, Akz);
+    const float Bz = __fmul_rn(r.Sz, Bkz);
+    const float Cz = __fmul_rn(r.Sz, Ckz);
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    const float rcp = __fdiv_rn(1.0f, det);
+    t = __fmul_rn(T, rcp);
+    u = __fmul_rn(V, rcp);
+    v = __fmul_rn(W, rcp);
+    return true;
+}
+
+// Transforms a world-space point/vector by the instance's 3x4 matrix, in the order of
+// float3x4 * float4 (float3x4.h:36-40): ((m0*x + m1*y) + m2*z) + m3*w.
+__device__ __forceinline__ float xform_row(const float4 m, float x, float y, float z, float w) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
+}
+
+__device__ __forceinline__ float byte_to_float(uint32_t w, int k) {
+    return __uint2float_rn((w >> (8 * k)) & 0xffu);
+}
+
+// Intersects the 8 child boxes of a node. Returns internal-child hits in octant order
+// (bit slot^oct) and the triangle/instance hit mask relative to prim_base.
+__device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node, const SpaceRay& r,
+                                               float tmin, float tlimit,
+                                               uint32_t& child_base, uint32_t& imask, uint32_t& hits8,
+                                               uint32_t& prim_base, uint32_t& prim_mask) {
+    const uint4* q = reinterpret_cast<const uint4*>(node);
+    const uint4 q0 = __ldg(q + 0);
+    const uint4 q1 = __ldg(q + 1);
+    uint4 qx = __ldg(q + 2);
+    uint4 qy = __ldg(q + 3);
+    uint4 qz = __ldg(q + 4);
+    const float sx = __uint_as_float((q0.w & 0xffu) << 23);
+    const float sy = __uint_as_float(((q0.w >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((q0.w >> 16) & 0xffu) << 23);
+    imask = q0.w >> 24;
+    child_base = q1.x;
+    prim_base = q1.y;
+    const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
+    // Slab offsets of the padded low (-pad) and high (+pad) planes; the near plane is the
+    // low one for positive directions.
+    const float px = __uint_as_float(q0.x), py = __uint_as_float(q0.y), pz = __uint_as_float(q0.z);
+    const float blx = (px - r.pad - r.ox) * r.ix, bhx = (px + r.pad - r.ox) * r.ix;
+    const float bly = (py - r.pad - r.oy) * r.iy, bhy = (py + r.pad - r.oy) * r.iy;
+    const float blz = (pz - r.pad - r.oz) * r.iz, bhz = (pz + r.pad - r.oz) * r.iz;
+    const float bnx = r.ix < 0.0f ? bhx : blx, bfx = r.ix < 0.0f ? blx : bhx;
+    const float bny = r.iy < 0.0f ? bhy : bly, bfy = r.iy < 0.0f ? bly : bhy;
+    const float bnz = r.iz < 0.0f ? bhz : blz, bfz = r.iz < 0.0f ? blz : bhz;
+    // Near plane uses the low bytes for positive directions, the high bytes otherwise.
+    if (r.ix < 0.0f) { uint32_t t0 = qx.x, t1 = qx.y; qx.x = qx.z; qx.y = qx.w; qx.z = t0; qx.w = t1; }
+    if (r.iy < 0.0f) { uint32_t t0 = qy.x, t1 = qy.y; qy.x = qy.z; qy.y = qy.w; qy.z = t0; qy.w = t1; }
+    if (r.iz < 0.0f) { uint32_t t0 = qz.x, t1 = qz.y; qz.x = qz.z; qz.y = qz.w; qz.z = t0; qz.w = t1; }
+    hits8 = 0;
+    prim_mask = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const uint32_t wn_x = s < 4 ? qx.x : qx.y, wf_x = s < 4 ? qx.z : qx.w;
+        const uint32_t wn_y = s < 4 ? qy.x : qy.y, wf_y = s < 4 ? qy.z : qy.w;
+        const uint32_t wn_z = s < 4 ? qz.x : qz.y, wf_z = s < 4 ? qz.z : qz.w;
+        const int k = s & 3;
+        const float tnx = fmaf(byte_to_float(wn_x, k), ax, bnx);
+        const float tfx = fmaf(byte_to_float(wf_x, k), ax, bfx);
+        const float tny = fmaf(byte_to_float(wn_y, k), ay, bny);
+        const float tfy = fmaf(byte_to_float(wf_y, k), ay, bfy);
+        const float tnz = fmaf(byte_to_float(wn_z, k), az, bnz);
+        const float tfz = fmaf(byte_to_float(wf_z, k), az, bfz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+        const float tf = fminf(fminf(tfx, tfy), tfz) * IMBART_SLACK;
+        const bool hit = tn <= fminf(tf, tlimit);
+        if (hit) {
+            if ((imask >> s) & 1u) {
+                hits8 |= 1u << (s ^ r.oct);
+            } else {
+                const uint32_t meta = ((s < 4 ? q1.z : q1.w) >> (8 * k)) & 0xffu;
+                const uint32_t cnt = meta >> 5;
+                const uint32_t off = meta & 31u;
+                prim_mask |= ((1u << cnt) - 1u) << off;
+            }
+        }
+    }
+}
+
+// Alpha-mask lookup for a candidate hit (mask.h:22-40): transparent texels reject the hit.
+__device__ __forceinline__ bool mask_opaque(const TraceParams& p, int tri, float u, float v) {
+    const int m = __ldg(p.indices + 4 * tri + 3);
+    if (m < 0 || m >= p.n_masks) return true;
+    const int w = __ldg(p.masks + 3 * m + 0);
+    const int h = __ldg(p.masks + 3 * m + 1);
+    const int off = __ldg(p.masks + 3 * m + 2);
+    int x = 0, y = 0;
+    if (w * h > 1) {
+        const float2 t0 = p.texcoords[__ldg(p.indices + 4 * tri + 0)];
+        const float2 t1 = p.texcoords[__ldg(p.indices + 4 * tri + 1)];
+        const float2 t2 = p.texcoords[__ldg(p.indices + 4 * tri + 2)];
+        const float w0 = __fsub_rn(__fsub_rn(1.0f, u), v);
+        const float tu = __fadd_rn(__fadd_rn(__fmul_rn(t0.x, w0), __fmul_rn(t1.x, u)), __fmul_rn(t2.x, v));
+        const float tv = __fadd_rn(__fadd_rn(__fmul_rn(t0.y, w0), __fmul_rn(t1.y, u)), __fmul_rn(t2.y, v));
+        x = (int)floorf(__fmul_rn(tu, (float)w)) % w; if (x < 0) x += w;
+        y = (int)floorf(__fmul_rn(tv, (float)h)) % h; if (y < 0) y += h;
+    }
+    return p.mask_buffer[off + y * w + x] != 0;
+}
+
+template <bool kAnyHit, bool kMasked, bool kStats>
+__device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, RayStats& st) {
+    const float4 ro = __ldg(p.rays + 2 * ray_index + 0);
+    const float4 rd = __ldg(p.rays + 2 * ray_index + 1);
+    const float tmin = ro.w;
+    const float tmax = rd.w;
+
+    int best_tri = -1, best_inst = -1;
+    float best_t = tmax, best_u = 0.0f, best_v = 0.0f;
+
+    const bool valid = (tmin <= tmax) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f);
+    if (valid) {
+        SpaceRay world;
+        world.ox = ro.x; world.oy = ro.y; world.oz = ro.z;
+        world.dx = rd.x; world.dy = rd.y; world.dz = rd.z;
+        setup_space(world);
+        SpaceRay r = world;
+        bool bottom = false;
+        int cur_inst = -1;
+        float tlimit = best_t * IMBART_SLACK;
+
+        uint2 stack[kStackSize];
+        int sp = 0;
+        // Root group: one internal child in slot 0.
+        uint32_t g_base = (uint32_t)p.root, g_imask = 1u, g_hits = 1u << (0u ^ r.oct);
+        uint32_t t_base = 0, t_mask = 0;
+        bool done = false;
+
+        while (!done) {
+            if (t_mask == 0 && g_hits != 0) {
+                const uint32_t bitpos = __ffs(g_hits) - 1;
+                g_hits &= g_hits - 1;
+                const uint32_t slot = bitpos ^ r.oct;
+                const uint32_t idx = g_base + __popc(g_imask & ((1u << slot) - 1u));
+                if (g_hits != 0) {
+                    if (sp == kStackSize) { atomicAdd(p.error_flags, 1); break; }
+                    stack[sp++] = make_uint2(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask);
+                }
+                intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+                if (kStats) st.nodes++;
+            }
+
+            if (t_mask != 0) {
+                if (bottom) {
+                    while (t_mask != 0) {
+                        const uint32_t i = __ffs(t_mask) - 1;
+                        t_mask &= t_mask - 1;
+                        const float4* tp = reinterpret_cast<const float4*>(p.tris + t_base + i);
+                        const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                        if (kStats) st.tris++;
+                        float t, u, v;
+                        if (!tri_test(r, a, b, c, t, u, v)) continue;
+                        if (!(t >= tmin)) continue;
+                        const int tri = __float_as_int(a.w);
+                        const bool closer = (t < best_t) ||
+                            (t == best_t && (best_tri < 0 || cur_inst < best_inst ||
+                                             (cur_inst == best_inst && tri < best_tri)));
+                        if (!closer) continue;
+                        if (kMasked && !mask_opaque(p, tri, u, v)) continue;
+                        best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
+                        tlimit = best_t * IMBART_SLACK;
+                        if (kAnyHit) { done = true; break; }
+                    }
+                    if (done) break;
+                } else {
+                    // Enter the next instance of the group.
+                    const uint32_t i = __ffs(t_mask) - 1;
+                    t_mask &= t_mask - 1;
+                    if (sp + 3 > kStackSize) { atomicAdd(p.error_flags, 1); break; }
+                    if (g_hits != 0)
+                        stack[sp++] = make_uint2(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask);
+                    if (t_mask != 0)
+                        stack[sp++] = make_uint2(t_base | (kEntryInst << kTypeShift), t_mask);
+                    stack[sp++] = make_uint2(kEntryMarker << kTypeShift, 0u);
+                    t_mask = 0;
+                    const float4* ip = reinterpret_cast<const float4*>(p.insts + t_base + i);
+                    const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+                    const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
+                    if (kStats) st.insts++;
+                    r.ox = xform_row(m0, world.ox, world.oy, world.oz, 1.0f);
+                    r.oy = xform_row(m1, world.ox, world.oy, world.oz, 1.0f);
+                    r.oz = xform_row(m2, world.ox, world.oy, world.oz, 1.0f);
+                    r.dx = xform_row(m0, world.dx, world.dy, world.dz, 0.0f);
+                    r.dy = xform_row(m1, world.dx, world.dy, world.dz, 0.0f);
+                    r.dz = xform_row(m2, world.dx, world.dy, world.dz, 0.0f);
+                    setup_space(r);
+                    cur_inst = meta.x;
+                    bottom = true;
+                    g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                    continue;
+                }
+            }
+
+            if (g_hits == 0 && t_mask == 0) {
+                // Pop the next group.
+                for (;;) {
+                    if (sp == 0) { done = true; break; }
+                    const uint2 e = stack[--sp];
+                    const uint32_t type = e.x >> kTypeShift;
+                    if (type == kEntryMarker) {
+                        r = world; bottom = false; cur_inst = -1;
+                        continue;
+                    }
+                    if (type == kEntryInst) { t_base = e.x & kIndexMask; t_mask = e.y; break; }
+                    g_base = e.x & kIndexMask; g_imask = e.y & 0xffu; g_hits = e.y >> 8;
+                    break;
+                }
+            }
+        }
+    }
+
+    int4 h;
+    h.x = best_tri;
+    h.y = best_tri >= 0 ? best_inst : -1;
+    h.z = __float_as_int(best_t);
+    h.w = __float_as_int(best_tri >= 0 ? best_u : 0.0f);
+    p.hits[ray_index] = h;
+    if (p.v_out) p.v_out[ray_index] = best_tri >= 0 ? best_v : 0.0f;
+}
+
+template <bool kAnyHit, bool kMasked, bool kStats>
+__global__ void __launch_bounds__(128) trace_kernel(TraceParams p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    RayStats st;
+    if (i < p.count) trace_one<kAnyHit, kMasked, kStats>(p, i, st);
+    if (kStats) {
+        // Warp-aggregated accumulation of the per-ray counters.
+        const unsigned m = __activemask();
+        const unsigned n = __reduce_add_sync(m, st.nodes);
+        const unsigned t = __reduce_add_sync(m, st.tris);
+        const unsigned k = __reduce_add_sync(m, st.insts);
+        if ((threadIdx.x & 31) == __ffs(m) - 1) {
+            atomicAdd(p.stats + 0, (unsigned long long)n);
+            atomicAdd(p.stats + 1, (unsigned long long)t);
+            atomicAdd(p.stats + 2, (unsigned long long)k);
+        }
+    }
+}
+
+}  // namespace imbart

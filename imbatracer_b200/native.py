@@ -1,0 +1,121 @@
+"""ctypes bindings of libimbart's C ABI (include/imbart.h).
+
+The library is the product; this module only loads it and declares the signatures. It
+raises immediately when the library is missing: there is no Python or CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+# --- numpy views of the boundary structs (byte layouts of include/imbart.h) -------------
+RAY_DTYPE = np.dtype([("org", "<f4", 4), ("dir", "<f4", 4)])
+HIT_DTYPE = np.dtype([("tri_id", "<i4"), ("inst_id", "<i4"), ("tmax", "<f4"), ("u", "<f4")])
+BBOX_DTYPE = np.dtype([("lo_x", "<f4"), ("hi_x", "<f4"), ("lo_y", "<f4"), ("hi_y", "<f4"),
+                       ("lo_z", "<f4"), ("hi_z", "<f4")])
+NODE2_DTYPE = np.dtype([("left_bb", BBOX_DTYPE), ("right_bb", BBOX_DTYPE), ("left", "<i4"),
+                        ("right", "<i4"), ("pad", "<i4", 2)])
+NODE4_DTYPE = np.dtype([("min_x", "<f4", 4), ("max_x", "<f4", 4), ("min_y", "<f4", 4),
+                        ("max_y", "<f4", 4), ("min_z", "<f4", 4), ("max_z", "<f4", 4),
+                        ("children", "<i4", 4)])
+INST_DTYPE = np.dtype([("transf", "<f4", 12), ("id", "<i4"), ("next", "<i4"), ("pad", "<i4", 2)])
+MASK_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("offset", "<i4")])
+assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
+assert NODE2_DTYPE.itemsize == 64 and NODE4_DTYPE.itemsize == 112 and INST_DTYPE.itemsize == 64
+
+TRACE_CLOSEST = 0
+TRACE_ANY = 1
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("wide_nodes", C.c_int64), ("top_nodes", C.c_int64), ("triangles", C.c_int64),
+                ("instances", C.c_int64), ("device_bytes", C.c_int64), ("root", C.c_int32),
+                ("masked", C.c_int32)]
+
+
+class ImbartError(RuntimeError):
+    pass
+
+
+_lib = None
+
+P = C.c_void_p
+I = C.c_int
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "imbart_last_error": (I, []),
+    "imbart_last_error_string": (C.c_char_p, []),
+    "imbart_clear_error": (None, []),
+    "imbart_version": (C.c_char_p, []),
+    "imbart_invalidate_scenes": (None, []),
+    "imbart_scene_from_node2": (P, [I, P, I, P, I, P, I, P, I, P, I, P, I, P, I, I]),
+    "imbart_scene_from_node4": (P, [I, P, I, P, I, P, I, P, I, P, I, P, I, P, I, I]),
+    "imbart_scene_destroy": (None, [P]),
+    "imbart_wide_from_node2": (I, [I, P, I, P, I, P, I, P, I, P, I, P, I, P]),
+    "imbart_scene_get_info": (I, [P, C.POINTER(SceneInfo)]),
+    "imbart_scene_get_device_arrays": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "imbart_trace": (I, [P, P, P, I, I, P]),
+    "imbart_trace_uv": (I, [P, P, P, P, I, I, P]),
+    "imbart_trace_host": (I, [P, P, P, I, I, P]),
+    "imbart_trace_stats": (I, [P, P, P, I, I, P, P]),
+    "imbart_scene_error_count": (I, [P]),
+    "imbart_kernel_launch_count": (C.c_int64, []),
+    "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
+    "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
+    "intersect_gpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
+    "occluded_gpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
+    "intersect_cpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
+    "occluded_cpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
+}
+
+
+def lib_path() -> str:
+    return _build.lib_path()
+
+
+def load() -> C.CDLL:
+    """Loads libimbart.so (built in-tree). Raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not os.path.exists(path):
+        raise ImbartError(f"libimbart is not built ({path} missing); run imbatracer_b200.build.build()")
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        lib = load()
+        msg = lib.imbart_last_error_string().decode(errors="replace")
+        raise ImbartError(f"{what}: error {rc}: {msg}")
+
+
+def last_error() -> tuple[int, str]:
+    lib = load()
+    return lib.imbart_last_error(), lib.imbart_last_error_string().decode(errors="replace")
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array or torch tensor (None for None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    return a.data_ptr()

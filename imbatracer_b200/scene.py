@@ -1,0 +1,212 @@
+"""Host-side scene: meshes, instances, materials and lights, and the traversal data.
+
+Mirrors the reference's Scene (src/imbatracer/render/scene.{h,cpp}): per-mesh bottom-level BVHs
+are laid out one after another in one node array (scene.cpp:37-72), global triangle ids are
+offset per mesh (tri_layout, scene.cpp:75-97), the top-level BVH follows at node index
+`node_count` which becomes the root (scene.cpp:103-117, 167-188). The BVHs are written by
+libimbart's binned-SAH builder in the reference two-wide GPU layout, then converted by
+libimbart into the compressed 8-wide layout resident on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import native as N
+
+
+@dataclass
+class Mesh:
+    """Triangle mesh: vertices (V,3), indices (T,4) = {i0, i1, i2, material} (mesh.h:103-114),
+    optional per-vertex normals (V,3) and texture coordinates (V,2)."""
+    vertices: np.ndarray
+    indices: np.ndarray
+    normals: np.ndarray | None = None
+    texcoords: np.ndarray | None = None
+    geom_normals: np.ndarray | None = None
+
+    def __post_init__(self):
+        self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float32).reshape(-1, 3)
+        self.indices = np.ascontiguousarray(self.indices, dtype=np.int32).reshape(-1, 4)
+        if self.texcoords is None:
+            self.texcoords = np.zeros((len(self.vertices), 2), np.float32)
+        self.texcoords = np.ascontiguousarray(self.texcoords, dtype=np.float32).reshape(-1, 2)
+        if self.geom_normals is None:
+            self.geom_normals = face_normals(self.vertices, self.indices)
+        if self.normals is None:
+            self.normals = vertex_normals(self.vertices, self.indices, self.geom_normals)
+        self.normals = np.ascontiguousarray(self.normals, dtype=np.float32).reshape(-1, 3)
+
+    @property
+    def triangle_count(self) -> int:
+        return len(self.indices)
+
+    def bounding_box(self) -> tuple[np.ndarray, np.ndarray]:
+        return self.vertices.min(0), self.vertices.max(0)
+
+
+def face_normals(v: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    """Normalized geometric normals cross(v1 - v0, v2 - v0) per face (mesh.cpp)."""
+    a, b, c = v[idx[:, 0]], v[idx[:, 1]], v[idx[:, 2]]
+    n = np.cross(b - a, c - a)
+    ln = np.linalg.norm(n, axis=1, keepdims=True)
+    ln[ln == 0] = 1.0
+    return (n / ln).astype(np.float32)
+
+
+def vertex_normals(v: np.ndarray, idx: np.ndarray, fn: np.ndarray) -> np.ndarray:
+    """Area-unweighted average of adjacent face normals, normalized."""
+    acc = np.zeros_like(v, dtype=np.float64)
+    for k in range(3):
+        np.add.at(acc, idx[:, k], fn)
+    ln = np.linalg.norm(acc, axis=1, keepdims=True)
+    ln[ln == 0] = 1.0
+    return (acc / ln).astype(np.float32)
+
+
+@dataclass
+class Instance:
+    """A mesh instance with its object-to-world matrix (mesh.h:19-27)."""
+    mesh_id: int
+    mat: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+
+    def __post_init__(self):
+        self.mat = np.asarray(self.mat, np.float32).reshape(4, 4)
+        self.inv_mat = np.linalg.inv(self.mat.astype(np.float64)).astype(np.float32)[:3].copy()
+
+
+class TraversalData:
+    """The reference-layout traversal arrays of a scene (ray_queue.h:42-54)."""
+
+    def __init__(self, root, nodes, instances, tris, indices, texcoords, masks, mask_buffer, layout, tri_layout):
+        self.root = root
+        self.nodes = nodes
+        self.instances = instances
+        self.tris = tris
+        self.indices = indices
+        self.texcoords = texcoords
+        self.masks = masks
+        self.mask_buffer = mask_buffer
+        self.layout = layout
+        self.tri_layout = tri_layout
+
+
+def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_size: int = 2,
+                         masks: np.ndarray | None = None, mask_buffer: np.ndarray | None = None) -> TraversalData:
+    """Builds all bottom-level BVHs and the top-level BVH in the reference two-wide layout."""
+    lib = N.load()
+    total_tris = sum(m.triangle_count for m in meshes)
+    node_cap = sum(m.triangle_count + 1 for m in meshes) + 2 * len(instances) + 1
+    nodes = np.zeros(node_cap, N.NODE2_DTYPE)
+    tris = np.zeros((3 * total_tris, 4), np.float32)
+    n_nodes = C.c_int(0)
+    n_tv = C.c_int(0)
+    layout, tri_layout = [], []
+    tri_off = 0
+    for m in meshes:
+        layout.append(n_nodes.value)
+        tri_layout.append(tri_off)
+        rc = lib.imbart_build_mesh_node2(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices),
+                                         m.triangle_count, tri_off, leaf_size, N.ptr(nodes), node_cap,
+                                         C.byref(n_nodes), N.ptr(tris), len(tris), C.byref(n_tv))
+        N.check(rc, "imbart_build_mesh_node2")
+        tri_off += m.triangle_count
+    node_count = n_nodes.value
+    # Instance world boxes: transformed mesh box centre +- |M| * half extent (gpu_adapter.cpp:171-179).
+    boxes = np.zeros((len(instances), 6), np.float32)
+    inv = np.zeros((len(instances), 12), np.float32)
+    roots = np.zeros(len(instances), np.int32)
+    mesh_boxes = [m.bounding_box() for m in meshes]
+    for i, inst in enumerate(instances):
+        lo, hi = mesh_boxes[inst.mesh_id]
+        c = (hi + lo) * np.float32(0.5)
+        e = (hi - lo) * np.float32(0.5)
+        wc = inst.mat[:3, :3] @ c + inst.mat[:3, 3]
+        we = np.abs(inst.mat[:3, :3]) @ e
+        boxes[i, :3] = wc - we
+        boxes[i, 3:] = wc + we
+        inv[i] = inst.inv_mat.reshape(-1)
+        roots[i] = layout[inst.mesh_id]
+    insts = np.zeros(len(instances), N.INST_DTYPE)
+    rc = lib.imbart_build_top_node2(N.ptr(boxes), N.ptr(inv), N.ptr(roots), len(instances), N.ptr(nodes),
+                                    node_cap, C.byref(n_nodes), N.ptr(insts))
+    N.check(rc, "imbart_build_top_node2")
+    nodes = nodes[: n_nodes.value].copy()
+    tris = tris[: n_tv.value].copy()
+    # Global index and texcoord buffers (scene.cpp:75-97): texcoord indices offset per mesh.
+    idx_parts, tc_parts = [], []
+    tc_off = 0
+    for m in meshes:
+        ii = m.indices.copy()
+        ii[:, :3] += tc_off
+        idx_parts.append(ii.reshape(-1))
+        tc_parts.append(m.texcoords)
+        tc_off += len(m.texcoords)
+    indices = np.ascontiguousarray(np.concatenate(idx_parts).astype(np.int32))
+    texcoords = np.ascontiguousarray(np.concatenate(tc_parts).astype(np.float32))
+    if masks is None:
+        n_mats = int(max(m.indices[:, 3].max() for m in meshes)) + 1
+        masks = np.zeros(n_mats, N.MASK_DTYPE)
+        masks["width"] = 1
+        masks["height"] = 1
+        mask_buffer = np.ones(4, np.uint8)  # MaskBuffer starts with 4 opaque texels (mask.h:24-28)
+    return TraversalData(node_count, nodes, insts, tris, indices, texcoords, masks,
+                         np.ascontiguousarray(mask_buffer, dtype=np.uint8), layout, tri_layout)
+
+
+class DeviceScene:
+    """A prepared scene resident on one GPU (imbart_scene)."""
+
+    def __init__(self, td: TraversalData, device: int = 0):
+        lib = N.load()
+        h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),
+                                        len(td.instances), N.ptr(td.tris), len(td.tris), N.ptr(td.indices),
+                                        len(td.indices), N.ptr(td.texcoords), len(td.texcoords), N.ptr(td.masks),
+                                        len(td.masks), N.ptr(td.mask_buffer), len(td.mask_buffer), device)
+        if not h:
+            code, msg = N.last_error()
+            raise N.ImbartError(f"imbart_scene_from_node2 failed ({code}): {msg}")
+        self.handle = h
+        self.device = device
+        self.td = td
+        info = N.SceneInfo()
+        N.check(lib.imbart_scene_get_info(h, C.byref(info)), "imbart_scene_get_info")
+        self.info = info
+
+    def trace(self, rays, hits, count: int | None = None, any_hit: bool = False, stream=None, v_out=None):
+        """Traces device tensors: rays (N,8) float32, hits (N,4) int32; stream-ordered."""
+        lib = N.load()
+        n = rays.shape[0] if count is None else count
+        st = None if stream is None else stream.cuda_stream
+        flags = N.TRACE_ANY if any_hit else N.TRACE_CLOSEST
+        if v_out is None:
+            rc = lib.imbart_trace(self.handle, N.ptr(rays), N.ptr(hits), n, flags, st)
+        else:
+            rc = lib.imbart_trace_uv(self.handle, N.ptr(rays), N.ptr(hits), N.ptr(v_out), n, flags, st)
+        N.check(rc, "imbart_trace")
+
+    def trace_host(self, rays: np.ndarray, hits: np.ndarray, any_hit: bool = False, stream=None):
+        lib = N.load()
+        st = None if stream is None else stream.cuda_stream
+        rc = lib.imbart_trace_host(self.handle, N.ptr(rays), N.ptr(hits), len(rays),
+                                   N.TRACE_ANY if any_hit else N.TRACE_CLOSEST, st)
+        N.check(rc, "imbart_trace_host")
+
+    def device_arrays(self):
+        lib = N.load()
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        N.check(lib.imbart_scene_get_device_arrays(self.handle, C.byref(a), C.byref(b), C.byref(c)), "arrays")
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self.handle:
+            N.load().imbart_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,258 @@
+/*
+ * imbart.h — C ABI of libimbart, the B200 (sm_100a) wavefront hot path of imbatracer.
+ *
+ * Two groups of entry points live here:
+ *
+ *  1. The four traversal symbols the reference links against (AnyDSL/traversal, which
+ *     the reference includes from outside its tree, src/imbatracer/core/traversal_interface.h:4-10).
+ *     They keep the reference's signatures and semantics exactly; see the comment on each.
+ *     The matching drop-in headers for the reference's `namespace traversal_gpu { #include
+ *     <traversal_gpu.h> }` pattern are include/traversal_gpu.h and include/traversal_cpu.h.
+ *
+ *  2. The extended imbart_* API: explicit scene preparation, asynchronous stream-ordered
+ *     tracing of device buffers, the photon hash grid and error reporting.
+ *
+ * All functions are plain C: pointers and sizes, no C++ or torch types. Every pointer is
+ * owned by the caller. Functions never abort or trap: failures set a thread-local error
+ * readable through imbart_last_error() / imbart_last_error_string().
+ */
+#ifndef IMBART_H
+#define IMBART_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------ */
+/* Types of the reference boundary (byte layouts shared with include/traversal_*.h)      */
+/* ------------------------------------------------------------------------------------ */
+
+/* Vec4/Vec2 as used for triangles and texture coordinates (ray_queue.h:47-50). */
+typedef struct { float x, y, z, w; } imbart_vec4;
+typedef struct { float x, y; } imbart_vec2;
+
+/* Ray: origin with tmin in org.w, direction with tmax in dir.w (camera.h:61-64, pt.cpp:37-41). 32 B. */
+typedef struct { imbart_vec4 org; imbart_vec4 dir; } imbart_ray;
+
+/* Hit: tri_id is the global triangle id (-1 = miss, ray_queue.h:168), inst_id the instance
+ * index, tmax the hit distance and u the barycentric weight of the triangle's second vertex
+ * (integrator.h:72-94, common.h:52-54). 16 B. */
+typedef struct { int tri_id; int inst_id; float tmax; float u; } imbart_hit;
+
+/* Two-wide BVH node written by the reference GPU adapter (gpu_adapter.cpp:84-101).
+ * left/right >= 0: node index; < 0: ~(index of the first Vec4 of a triangle run in `tris`)
+ * for bottom-level nodes, ~(index of the first instance node of a run) for top-level nodes.
+ * A root that is a single leaf is wrapped in a parent whose right child is 0x76543210
+ * (gpu_adapter.cpp:14-31). 64 B. */
+typedef struct { float lo_x, hi_x, lo_y, hi_y, lo_z, hi_z; } imbart_bbox;
+typedef struct { imbart_bbox left_bb; imbart_bbox right_bb; int left; int right; int pad[2]; } imbart_node2;
+
+/* Four-wide SoA BVH node written by the reference CPU adapter (cpu_adapter.cpp:79-101).
+ * children[j] > 0: node index; 0: empty slot; < 0: ~(index of the first Vec4 of a run of
+ * 13-Vec4 triangle packets, closed by an all-0x80000000 sentinel Vec4). 112 B. */
+typedef struct {
+    float min_x[4], max_x[4], min_y[4], max_y[4], min_z[4], max_z[4];
+    int children[4];
+} imbart_node4;
+
+/* Instance node (cpu_adapter.cpp:346-365, gpu_adapter.cpp:255-276): the instance's
+ * inverse transform as a row-major 3x4 matrix, the instance id, the node index of the
+ * instanced mesh's BVH root, and pad[0] == -1 on the last node of a leaf run. 64 B. */
+typedef struct { float transf[12]; int id; int next; int pad[2]; } imbart_instance_node;
+
+/* Transparency mask descriptor (mask.h:9-20): a width x height byte image at `offset` in
+ * the mask buffer, selected by the material id stored in indices[4*tri+3]. */
+typedef struct { int width; int height; int offset; } imbart_mask_desc;
+
+/* ------------------------------------------------------------------------------------ */
+/* 1. Drop-in traversal entry points                                                      */
+/* ------------------------------------------------------------------------------------ */
+/*
+ * Closest hit over the two-level instanced BVH for `count` rays (replaces
+ * traversal_gpu::intersect_gpu_masked_instanced, called at ray_queue.h:279-290).
+ * Every pointer is a DEVICE pointer allocated by the caller. `count` is the queue size
+ * rounded up to a multiple of 64 (ray_queue.h:60,273); padding rays (zeroed, ray_queue.h:74)
+ * produce misses. The reference layout is converted to the compressed 8-wide layout on the
+ * first call for a given `nodes` buffer and cached; imbart_invalidate_scenes() drops the
+ * cache after the caller rewrites the buffers. Returns after the hits are written
+ * (the caller copies them back right away, ray_queue.h:292).
+ * Triangles hit at the same t are resolved to the smallest (inst_id, tri_id).
+ */
+void intersect_gpu_masked_instanced(int root, imbart_node2* nodes, imbart_instance_node* instances,
+                                    imbart_vec4* tris, imbart_ray* rays, imbart_hit* hits,
+                                    int* indices, imbart_vec2* texcoords, imbart_mask_desc* masks,
+                                    char* mask_buffer, int count);
+
+/* Any hit within [tmin, tmax] (replaces traversal_gpu::occluded_gpu_masked_instanced,
+ * ray_queue.h:329-340). hits[i].tri_id >= 0 when ray i is occluded, -1 otherwise
+ * (consumer: integrator.h:57). Same pointer conventions as above. */
+void occluded_gpu_masked_instanced(int root, imbart_node2* nodes, imbart_instance_node* instances,
+                                   imbart_vec4* tris, imbart_ray* rays, imbart_hit* hits,
+                                   int* indices, imbart_vec2* texcoords, imbart_mask_desc* masks,
+                                   char* mask_buffer, int count);
+
+/* Host-buffer forms with the reference CPU layout (replace traversal_cpu::intersect_cpu_masked_instanced
+ * and occluded_cpu_masked_instanced, ray_queue.h:254-265 and 304-315). All pointers are HOST
+ * pointers; the scene is converted once and kept resident on the GPU, rays are copied to the
+ * device and hits back inside the call. The B200 does the traversal: there is no CPU path. */
+void intersect_cpu_masked_instanced(int root, imbart_node4* nodes, imbart_instance_node* instances,
+                                    imbart_vec4* tris, imbart_ray* rays, imbart_hit* hits,
+                                    int* indices, imbart_vec2* texcoords, imbart_mask_desc* masks,
+                                    char* mask_buffer, int count);
+void occluded_cpu_masked_instanced(int root, imbart_node4* nodes, imbart_instance_node* instances,
+                                   imbart_vec4* tris, imbart_ray* rays, imbart_hit* hits,
+                                   int* indices, imbart_vec2* texcoords, imbart_mask_desc* masks,
+                                   char* mask_buffer, int count);
+
+/* Drops every scene the drop-in entry points converted and cached. Call after rewriting
+ * node, triangle or instance buffers in place (Scene::upload_top_level_accel, scene.cpp:167-188). */
+void imbart_invalidate_scenes(void);
+
+/* ------------------------------------------------------------------------------------ */
+/* 2. Extended API                                                                         */
+/* ------------------------------------------------------------------------------------ */
+
+/* Error codes. */
+enum {
+    IMBART_OK = 0,
+    IMBART_ERR_INVALID_ARGUMENT = 1,
+    IMBART_ERR_CUDA = 2,
+    IMBART_ERR_OUT_OF_MEMORY = 3,
+    IMBART_ERR_BAD_SCENE = 4,
+    IMBART_ERR_STACK_OVERFLOW = 5,
+    IMBART_ERR_LIMIT = 6,
+    IMBART_ERR_TIMEOUT = 7
+};
+
+/* Last error of the calling thread (0 = none) and its message; imbart_clear_error resets it. */
+int imbart_last_error(void);
+const char* imbart_last_error_string(void);
+void imbart_clear_error(void);
+/* Library version string. */
+const char* imbart_version(void);
+
+/* An opaque prepared scene: the compressed 8-wide BVH resident on one GPU. */
+typedef struct imbart_scene imbart_scene;
+
+/* Flags for scene preparation. */
+enum { IMBART_SCENE_MASKED = 1 };
+
+/* Prepares a scene from HOST arrays in the reference GPU (two-wide) layout.
+ * n_nodes/n_tri_vec4/n_instances bound the arrays (for validation; the tree is walked from
+ * `root`). indices/texcoords/masks/mask_buffer are only read when masks other than the
+ * default opaque one are present (any mask with width*height > 1 or a zero texel).
+ * Returns NULL on error. */
+imbart_scene* imbart_scene_from_node2(int root, const imbart_node2* nodes, int n_nodes,
+                                      const imbart_instance_node* instances, int n_instances,
+                                      const imbart_vec4* tris, int n_tri_vec4,
+                                      const int* indices, int n_indices,
+                                      const imbart_vec2* texcoords, int n_texcoords,
+                                      const imbart_mask_desc* masks, int n_masks,
+                                      const char* mask_buffer, int mask_buffer_size,
+                                      int device);
+
+/* Same from HOST arrays in the reference CPU (four-wide, 13-Vec4 packet) layout. Vertices are
+ * rebuilt as v1 = v0 - e1 and v2 = v0 + e2 from the packet's edges (cpu_adapter.cpp:129-201). */
+imbart_scene* imbart_scene_from_node4(int root, const imbart_node4* nodes, int n_nodes,
+                                      const imbart_instance_node* instances, int n_instances,
+                                      const imbart_vec4* tris, int n_tri_vec4,
+                                      const int* indices, int n_indices,
+                                      const imbart_vec2* texcoords, int n_texcoords,
+                                      const imbart_mask_desc* masks, int n_masks,
+                                      const char* mask_buffer, int mask_buffer_size,
+                                      int device);
+
+void imbart_scene_destroy(imbart_scene* scene);
+
+/* Host-only conversion of the two-wide layout into the 8-wide layout, without a GPU (for
+ * inspection, byte accounting and tests). Writes up to the given capacities and returns the
+ * required sizes in counts[0..3] = {wide nodes, triangles, instances, root}. Call with zero
+ * capacities to query the sizes. Returns 0 or an error code. */
+int imbart_wide_from_node2(int root, const imbart_node2* nodes, int n_nodes,
+                           const imbart_instance_node* instances, int n_instances,
+                           const imbart_vec4* tris, int n_tri_vec4,
+                           void* nodes_out, int nodes_cap, void* tris_out, int tris_cap,
+                           void* insts_out, int insts_cap, int* counts);
+
+/* Sizes of a prepared scene. */
+typedef struct {
+    int64_t wide_nodes;        /* 80 B compressed 8-wide nodes (top and bottom level) */
+    int64_t top_nodes;         /* of which top level */
+    int64_t triangles;         /* 48 B triangle records (SBVH duplicates counted) */
+    int64_t instances;         /* 64 B instance records */
+    int64_t device_bytes;      /* total device memory held */
+    int32_t root;              /* wide index of the top-level root */
+    int32_t masked;            /* 1 when the alpha-mask test is active */
+} imbart_scene_info;
+int imbart_scene_get_info(const imbart_scene* scene, imbart_scene_info* out);
+
+/* Device pointers of the prepared scene's arrays (for measurement and tests):
+ * nodes (80 B records), tris (3 float4 per triangle), instances (4 float4 per instance). */
+int imbart_scene_get_device_arrays(const imbart_scene* scene, const void** nodes,
+                                   const void** tris, const void** instances);
+
+/* Trace flags. */
+enum { IMBART_TRACE_CLOSEST = 0, IMBART_TRACE_ANY = 1 };
+
+/* Traces `count` rays from DEVICE buffers, stream-ordered on `stream` (a cudaStream_t,
+ * NULL = legacy default stream). Returns 0 or an error code; does not synchronize. */
+int imbart_trace(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits,
+                 int count, int flags, void* stream);
+
+/* Like imbart_trace, and also writes the barycentric weight of the third vertex per ray
+ * to `v_out` (device, may be NULL) — the reference recomputes it (integrator.h:89-94). */
+int imbart_trace_uv(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits,
+                    float* v_out, int count, int flags, void* stream);
+
+/* Traces from HOST buffers (pinned or pageable): copies rays in, traces, copies hits out,
+ * and synchronizes `stream`. */
+int imbart_trace_host(const imbart_scene* scene, const imbart_ray* rays_host, imbart_hit* hits_host,
+                      int count, int flags, void* stream);
+
+/* Statistics variant of imbart_trace: same hits, and adds the numbers of 8-wide nodes
+ * fetched, triangles tested and instances entered to stats[0..2] (DEVICE, 3 x uint64).
+ * Used to compute the algorithmic bytes of a launch. */
+int imbart_trace_stats(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count,
+                       int flags, unsigned long long* stats, void* stream);
+
+/* Number of rays that ran out of traversal stack (reported as misses) since the scene was
+ * prepared; -1 on error. Synchronous. */
+int imbart_scene_error_count(const imbart_scene* scene);
+
+/* Number of kernel launches issued by this process so far (for launch accounting). */
+int64_t imbart_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------------------ */
+/* BVH construction (the builder side of the boundary)                                     */
+/* ------------------------------------------------------------------------------------ */
+
+/* Builds one mesh's bottom-level BVH with a binned SAH (32 bins, leaf threshold
+ * `leaf_size`) and APPENDS it in the reference GPU two-wide layout: nodes to
+ * `nodes_out` (capacity `nodes_cap`), triangle Vec4 triples (global id = tri_offset + local
+ * id in v1.w, sentinel 0x80000000 in the last v2.w of each leaf) to `tris_out` (capacity
+ * `tris_cap` Vec4s). `*n_nodes` / `*n_tri_vec4` are in/out fill counts. `vertices` are
+ * xyz floats with stride `vertex_stride` floats, `indices` 4 ints per triangle
+ * {i0, i1, i2, material} (mesh.h:103-114). Node indices written are absolute in nodes_out.
+ * Returns 0 or an error code (IMBART_ERR_LIMIT when a capacity is too small). */
+int imbart_build_mesh_node2(const float* vertices, int n_vertices, int vertex_stride,
+                            const int* indices, int n_tris, int tri_offset, int leaf_size,
+                            imbart_node2* nodes_out, int nodes_cap, int* n_nodes,
+                            imbart_vec4* tris_out, int tris_cap, int* n_tri_vec4);
+
+/* Builds the top-level BVH over instance boxes (binned SAH, one instance per leaf) and
+ * APPENDS it in the reference two-wide layout at node index `*n_nodes` (the root is that
+ * index), writing instance nodes to `inst_out` (`n_instances` of them). inv_mats are the
+ * 3x4 row-major inverse transforms, mesh_roots[i] the BVH root node of instance i's mesh,
+ * boxes the world-space instance boxes (6 floats: lo xyz, hi xyz). */
+int imbart_build_top_node2(const float* boxes, const float* inv_mats, const int* mesh_roots,
+                           int n_instances, imbart_node2* nodes_out, int nodes_cap, int* n_nodes,
+                           imbart_instance_node* inst_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMBART_H */

@@ -1,0 +1,140 @@
+"""CPU tests of the traversal boundary: the oracle against brute force, the restated 8-wide
+walk against the oracle (which checks libimbart's layout conversion on the host), the
+library's exported symbols, and the builder's reference-layout output."""
+import re
+import os
+
+import numpy as np
+import pytest
+
+from imbatracer_b200 import native as N
+from oracle import oracle as O
+from tests import helpers as H
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if not f.endswith(".h"):
+            continue
+        text = open(os.path.join(inc, f)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([a-z_][a-z0-9_]*)\s*\(", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof", "defined"):
+                names.add(name)
+    return sorted(names)
+
+
+def test_library_loads_and_exports_every_header_symbol():
+    lib = N.load()
+    declared = [n for n in header_functions() if n.startswith(("imbart_", "intersect_", "occluded_"))]
+    assert "intersect_gpu_masked_instanced" in declared
+    missing = [n for n in declared if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+    unbound = [n for n in declared if n not in N.exported_symbols()]
+    assert not unbound, f"declared but not bound in native.py: {unbound}"
+    assert lib.imbart_version().startswith(b"imbart")
+
+
+def test_error_reporting_without_gpu():
+    lib = N.load()
+    lib.imbart_clear_error()
+    rc = lib.imbart_trace(None, None, None, 10, 0, None)
+    assert rc == 1
+    code, msg = N.last_error()
+    assert code == 1 and "imbart_trace" in msg
+    lib.imbart_clear_error()
+    assert N.last_error()[0] == 0
+
+
+@pytest.mark.parametrize("name", ["tiny", "config1", "config2"])
+def test_oracle_bvh_walk_matches_brute_force(name):
+    d = H.scene_desc(name)
+    td = H.traversal_data(name)
+    n = 3000 if name != "config2" else 600
+    rays = H.ray_set(name, n, seed=1)
+    for any_hit in (False, True):
+        hb, vb = O.trace_brute(d.meshes, d.instances, td.tri_layout, rays, any_hit=any_hit, with_v=True)
+        h2, v2 = O.trace_node2(td, rays, any_hit=any_hit, with_v=True)
+        if any_hit:
+            # Any hit: occlusion must agree; the reported triangle may differ.
+            assert np.array_equal(hb["tri_id"] >= 0, h2["tri_id"] >= 0)
+        else:
+            assert H.hits_equal(hb, h2).all()
+            assert np.array_equal(vb.view(np.int32), v2.view(np.int32))
+
+
+@pytest.mark.parametrize("name", ["tiny", "config1", "config2"])
+def test_wide_layout_walk_matches_oracle(name):
+    """The restated GPU walk over libimbart's converted 8-wide layout finds bit-identical
+    closest hits: the conversion (collapse + conservative 8-bit quantization) loses nothing."""
+    td = H.traversal_data(name)
+    wn, wt, wi, root = H.wide_arrays(td)
+    rays = H.ray_set(name, 20000, seed=2)
+    h2 = O.trace_node2(td, rays)
+    hw, nbytes, counts = O.wide_walk(wn, wt, wi, root, rays)
+    assert H.hits_equal(h2, hw).all()
+    h2a = O.trace_node2(td, rays, any_hit=True)
+    hwa, _, _ = O.wide_walk(wn, wt, wi, root, rays, any_hit=True)
+    assert np.array_equal(h2a["tri_id"] >= 0, hwa["tri_id"] >= 0)
+    assert (nbytes >= 48).all()
+    assert counts[0] > 0 and counts[1] > 0
+
+
+def test_wide_layout_invariants():
+    td = H.traversal_data("config2")
+    wn, wt, wi, root = H.wide_arrays(td)
+    # every internal child index is in range, leaf ranges stay in the triangle/instance arrays
+    for n in wn[:2000]:
+        k = bin(int(n["imask"])).count("1")
+        assert n["child_base"] + k <= len(wn)
+        for s in range(8):
+            meta = int(n["meta"][s])
+            if not (int(n["imask"]) >> s) & 1 and meta:
+                assert (meta >> 5) <= 3
+    assert set(np.unique(wt["id"])) <= set(range(sum(m.triangle_count for m in H.scene_desc("config2").meshes)))
+    assert len(wi) == len(H.scene_desc("config2").instances)
+    assert 0 <= root < len(wn)
+
+
+def test_builder_writes_reference_layout():
+    """Leaves end with the 0x80000000 sentinel in the last v2.w, ids sit in v1.w
+    (gpu_adapter.cpp:129-141), every triangle appears, node links are in range."""
+    d = H.scene_desc("config1")
+    td = H.traversal_data("config1")
+    tris = td.tris
+    ids = tris[1::3, 3].view(np.int32)
+    assert sorted(ids.tolist()) == list(range(d.meshes[0].triangle_count))
+    sent = tris[2::3, 3].view(np.int32)
+    assert (sent == np.int32(-2 ** 31)).sum() > 0
+    nodes = td.nodes
+    for k in ("left", "right"):
+        c = nodes[k]
+        inner = c[(c >= 0) & (c != 0x76543210)]
+        assert (inner < len(nodes)).all()
+        leaf = ~c[c < 0]
+        assert (leaf < len(tris)).all() and (leaf % 3 == 0).all()
+    assert td.root == td.layout[-1] + 0 or td.root >= td.layout[-1]
+
+
+def test_single_triangle_mesh_root_wrapper():
+    td = H.traversal_data("tiny")
+    mesh1_root = td.layout[1]
+    assert td.nodes[mesh1_root]["right"] == 0x76543210
+
+
+def test_node_layout_guards():
+    """Malformed input is rejected with an error, not a crash."""
+    lib = N.load()
+    td = H.traversal_data("tiny")
+    cnt = np.zeros(4, np.int32)
+    bad = td.nodes.copy()
+    bad["left"][0] = 10 ** 6
+    rc = lib.imbart_wide_from_node2(td.root, N.ptr(bad), len(bad), N.ptr(td.instances), len(td.instances),
+                                    N.ptr(td.tris), len(td.tris), None, 0, None, 0, None, 0, N.ptr(cnt))
+    assert rc == 4
+    assert "out of bounds" in N.last_error()[1]

@@ -1,0 +1,176 @@
+"""GPU parity of the traversal kernels against the oracle, through the C ABI.
+
+Closest hits must match the oracle bit for bit (triangle id, instance id, t, u, and v through
+imbart_trace_uv): the kernel evaluates the same watertight test with the same rounding, and
+equal-t hits resolve to the smallest (inst_id, tri_id). Any-hit queries must agree on
+occlusion. The statistics variant must report exactly the work the restated walk counts.
+"""
+import numpy as np
+import pytest
+
+from imbatracer_b200 import native as N
+from imbatracer_b200 import scene as S
+from oracle import oracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(arr, torch, dev):
+    return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8)).to(dev)
+
+
+def run_gpu(ds, rays, any_hit=False, stats=False):
+    import torch
+    dev = torch.device("cuda:0")
+    d_rays = to_dev(rays, torch, dev)
+    d_hits = torch.zeros(len(rays) * 16, dtype=torch.uint8, device=dev)
+    d_v = torch.zeros(len(rays), dtype=torch.float32, device=dev)
+    lib = N.load()
+    flags = N.TRACE_ANY if any_hit else N.TRACE_CLOSEST
+    st = None
+    if stats:
+        st = torch.zeros(3, dtype=torch.int64, device=dev)
+        N.check(lib.imbart_trace_stats(ds.handle, N.ptr(d_rays), N.ptr(d_hits), len(rays), flags, N.ptr(st), None),
+                "trace_stats")
+    else:
+        N.check(lib.imbart_trace_uv(ds.handle, N.ptr(d_rays), N.ptr(d_hits), N.ptr(d_v), len(rays), flags, None),
+                "trace")
+    torch.cuda.synchronize()
+    hits = d_hits.cpu().numpy().view(N.HIT_DTYPE)
+    return hits, d_v.cpu().numpy(), (st.cpu().numpy() if st is not None else None)
+
+
+@pytest.mark.parametrize("name,n", [("tiny", 4000), ("config1", 200000), ("config2", 200000)])
+def test_closest_hit_bit_exact(cuda, name, n):
+    td = H.traversal_data(name)
+    ds = S.DeviceScene(td)
+    rays = H.ray_set(name, n, seed=3)
+    ref, ref_v = O.trace_node2(td, rays, with_v=True)
+    hits, v, _ = run_gpu(ds, rays)
+    eq = H.hits_equal(ref, hits)
+    bad = np.nonzero(~eq)[0]
+    assert eq.all(), f"{len(bad)} of {len(rays)} differ, e.g. {ref[bad[:3]]} vs {hits[bad[:3]]}"
+    assert np.array_equal(ref_v.view(np.int32), v.view(np.int32))
+    assert (ref["tri_id"] >= 0).mean() > 0.1
+    assert N.load().imbart_scene_error_count(ds.handle) == 0
+
+
+@pytest.mark.parametrize("name", ["tiny", "config1", "config2"])
+def test_any_hit_occlusion(cuda, name):
+    td = H.traversal_data(name)
+    ds = S.DeviceScene(td)
+    rays = H.ray_set(name, 100000, seed=4)
+    # shadow-style rays: bounded segments
+    rays["dir"][: len(rays) // 2, 3] = np.float32(5.0)
+    ref = O.trace_node2(td, rays, any_hit=True)
+    hits, _, _ = run_gpu(ds, rays, any_hit=True)
+    assert np.array_equal(ref["tri_id"] >= 0, hits["tri_id"] >= 0)
+    occ = hits["tri_id"] >= 0
+    # a reported occluder lies within the segment
+    t = hits["tmax"][occ]
+    assert (t >= rays["org"][occ, 3]).all() and (t <= rays["dir"][occ, 3]).all()
+
+
+@pytest.mark.parametrize("name", ["config1", "config2"])
+def test_stats_match_restated_walk(cuda, name):
+    """The kernel's node/triangle/instance counts equal the restated walk's, ray for ray in
+    aggregate: the bytes used for the roofline are the bytes the kernel fetches."""
+    td = H.traversal_data(name)
+    ds = S.DeviceScene(td)
+    wn, wt, wi, root = H.wide_arrays(td)
+    rays = H.ray_set(name, 50000, seed=5)
+    for any_hit in (False, True):
+        hits, _, st = run_gpu(ds, rays, any_hit=any_hit, stats=True)
+        hw, nbytes, counts = O.wide_walk(wn, wt, wi, root, rays, any_hit=any_hit)
+        assert np.array_equal(st, counts), (st, counts)
+        if not any_hit:
+            assert H.hits_equal(hw, hits).all()
+
+
+def test_dropin_device_entry_points(cuda):
+    """intersect_/occluded_gpu_masked_instanced with device buffers in the reference layout."""
+    import torch
+    td = H.traversal_data("config1")
+    dev = torch.device("cuda:0")
+    lib = N.load()
+    lib.imbart_invalidate_scenes()
+    d_nodes = to_dev(td.nodes, torch, dev)
+    d_insts = to_dev(td.instances, torch, dev)
+    d_tris = to_dev(td.tris, torch, dev)
+    d_idx = to_dev(td.indices, torch, dev)
+    d_tc = to_dev(td.texcoords, torch, dev)
+    d_masks = to_dev(td.masks, torch, dev)
+    d_mb = to_dev(td.mask_buffer, torch, dev)
+    rays = H.ray_set("config1", 65536, seed=6)
+    count = (len(rays) + 63) // 64 * 64
+    padded = np.zeros(count, N.RAY_DTYPE)
+    padded[: len(rays)] = rays
+    d_rays = to_dev(padded, torch, dev)
+    d_hits = torch.zeros(count * 16, dtype=torch.uint8, device=dev)
+    args = (td.root, N.ptr(d_nodes), N.ptr(d_insts), N.ptr(d_tris), N.ptr(d_rays), N.ptr(d_hits), N.ptr(d_idx),
+            N.ptr(d_tc), N.ptr(d_masks), N.ptr(d_mb), count)
+    lib.imbart_clear_error()
+    lib.intersect_gpu_masked_instanced(*args)
+    assert N.last_error()[0] == 0, N.last_error()
+    hits = d_hits.cpu().numpy().view(N.HIT_DTYPE)
+    ref = O.trace_node2(td, padded)
+    assert H.hits_equal(ref, hits).all()
+    assert (hits["tri_id"][len(rays):] == -1).all()     # zeroed padding rays miss
+    lib.occluded_gpu_masked_instanced(*args)
+    assert N.last_error()[0] == 0
+    occ = d_hits.cpu().numpy().view(N.HIT_DTYPE)
+    refa = O.trace_node2(td, padded, any_hit=True)
+    assert np.array_equal(refa["tri_id"] >= 0, occ["tri_id"] >= 0)
+    lib.imbart_invalidate_scenes()
+
+
+def test_host_buffer_trace(cuda):
+    td = H.traversal_data("config2")
+    ds = S.DeviceScene(td)
+    rays = H.ray_set("config2", 30000, seed=7)
+    hits = np.zeros(len(rays), N.HIT_DTYPE)
+    ds.trace_host(rays, hits)
+    assert H.hits_equal(O.trace_node2(td, rays), hits).all()
+
+
+def test_alpha_masks(cuda):
+    """Checkerboard opacity masks on config1's sphere materials: transparent texels let rays
+    through; GPU and oracle agree bit for bit."""
+    d = H.scene_desc("config1")
+    mesh = d.meshes[0]
+    rng = np.random.default_rng(8)
+    tc = rng.uniform(-1.5, 1.5, size=(len(mesh.vertices), 2)).astype(np.float32)
+    m2 = S.Mesh(mesh.vertices, mesh.indices, mesh.normals, tc, mesh.geom_normals)
+    n_mats = int(mesh.indices[:, 3].max()) + 1
+    masks = np.zeros(n_mats, N.MASK_DTYPE)
+    masks["width"] = 1
+    masks["height"] = 1
+    buf = [1, 1, 1, 1]
+    checker = (np.indices((8, 8)).sum(0) % 2).astype(np.uint8).reshape(-1)
+    for m in range(0, n_mats - 3, 2):       # every other sphere material gets the checkerboard
+        masks[m] = (8, 8, len(buf))
+        buf += checker.tolist()
+    masks[n_mats - 3] = (1, 1, len(buf))    # the ground: a single transparent texel
+    buf.append(0)
+    td = S.build_traversal_data([m2], d.instances, masks=masks, mask_buffer=np.array(buf, np.uint8))
+    ds = S.DeviceScene(td)
+    assert ds.info.masked == 1
+    rays = H.ray_set("config1", 100000, seed=9)
+    ref = O.trace_node2(td, rays)
+    hits, _, _ = run_gpu(ds, rays)
+    assert H.hits_equal(ref, hits).all()
+    unmasked = O.trace_node2(H.traversal_data("config1"), rays)
+    assert (unmasked["tri_id"] != ref["tri_id"]).sum() > 100   # the masks matter
+    refa = O.trace_node2(td, rays, any_hit=True)
+    occ, _, _ = run_gpu(ds, rays, any_hit=True)
+    assert np.array_equal(refa["tri_id"] >= 0, occ["tri_id"] >= 0)
+
+
+def test_empty_and_zero_count(cuda):
+    import torch
+    ds = S.DeviceScene(H.traversal_data("tiny"))
+    lib = N.load()
+    d = torch.zeros(64, dtype=torch.uint8, device="cuda")
+    assert lib.imbart_trace(ds.handle, N.ptr(d), N.ptr(d), 0, 0, None) == 0
+    assert lib.imbart_trace(ds.handle, N.ptr(d), N.ptr(d), -1, 0, None) == 1
