@@ -50,12 +50,21 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except FileNotFoundError:
             self.proc = None
+            return
+        # Wait for the first sample so that the timed region is covered.
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+
+    def mark(self):
+        """Starts counting samples from here (the timed region)."""
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -71,7 +80,10 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # Samples from the timed region; keep the one before it when the region is shorter
+        # than the sampling interval.
+        lines = self.lines[max(getattr(self, "first", 0) - 1, 0):]
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -227,14 +239,15 @@ def run_ours(args):
             if events is not None:
                 events[i][1].record(stream)
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     launches_before = lib.imbart_kernel_launch_count()
     per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                    for _ in sets] for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks.mark()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -415,8 +428,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -10,9 +10,10 @@ lights, camera and environment.
            vertices displaced radially by U[-5%,+5%]; a 2-triangle ground quad at y=-10;
            one 2-triangle area light; Lambertian albedo U[0.2,0.8]. One mesh, one instance.
   config2  8 meshes (displaced icospheres and extruded random polygons, 2k-50k triangles)
-           instanced 200 times (random rotation, uniform scale U[0.5,3]): ~1.14M instanced
-           triangles; materials split over Lambertian, Phong, Cook-Torrance, glass, mirror;
-           16 triangular area lights plus a constant environment light.
+           instanced 200 times (random rotation, uniform scale U[0.5,3], positions
+           U[-10,10]^3): ~1.30M instanced triangles; materials split over Lambertian, Phong,
+           Cook-Torrance, glass, mirror; 16 triangular area lights plus a constant environment
+           light; a ground quad at y=-13 closes the view (~80% of camera rays hit geometry).
   config3  the config1 generator scaled to ~2M triangles (400 spheres).
 """
 from __future__ import annotations
@@ -231,22 +232,26 @@ def config2(seed: int = 1, width: int = 1920, height: int = 1080) -> SceneDesc:
             m = np.eye(4)
             s = rng.uniform(0.5, 3.0)
             m[:3, :3] = rotation(rng) * s
-            m[:3, 3] = rng.uniform(-40, 40, 3)
+            m[:3, 3] = rng.uniform(-10, 10, 3)
             instances.append(Instance(mesh_id, m.astype(np.float32)))
     # 16 triangular area lights in one mesh above the field.
     lparts = []
     lights = []
     for i in range(16):
-        c = np.array([rng.uniform(-40, 40), 60.0, rng.uniform(-40, 40)])
+        c = np.array([rng.uniform(-15, 15), 25.0, rng.uniform(-15, 15)])
         p0, p1, p2 = c + [-3, 0, -3], c + [3, 0, -3], c + [0, 0, 3]
         tri = np.array([p0, p2, p1], np.float32)   # facing down
         intensity = np.array(rng.uniform(20, 60, 3), np.float32)
         materials.append(Material(EMISSIVE, color=(0.0, 0.0, 0.0), emission=tuple(intensity)))
         lparts.append((tri, np.array([[0, 1, 2]], np.int32), len(materials) - 1))
         lights.append((tri[0], tri[1], tri[2], intensity))
+    # A Lambertian ground quad below the field closes the view (as in config1).
+    materials.append(Material(LAMBERT, color=tuple(rng.uniform(0.2, 0.8, 3))))
+    lparts.append((*quad([-200, -13, -200], [-200, -13, 200], [200, -13, 200], [200, -13, -200]),
+                   len(materials) - 1))
     meshes.append(_merge(lparts))
     instances.append(Instance(len(meshes) - 1))
-    cam = Camera(pos=(0.0, 20.0, -120.0), dir=(0.0, -0.15, 1.0), up=(0.0, 1.0, 0.0), fov=50.0,
+    cam = Camera(pos=(0.0, 4.0, -30.0), dir=(0.0, -0.12, 1.0), up=(0.0, 1.0, 0.0), fov=50.0,
                  width=width, height=height)
     return SceneDesc(meshes, instances, materials, lights, cam, (0.3, 0.35, 0.4), "config2")
 
