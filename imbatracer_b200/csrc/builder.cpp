@@ -56,7 +56,8 @@ void write_bb(imbart_bbox& bb, const Box& b) {
 // Finds the best binned-SAH split of refs[begin, end). Returns false to make a leaf.
 // On success refs are partitioned and *mid is the first ref of the right side.
 bool split(std::vector<int>& refs, const std::vector<Prim>& prims, int begin, int end,
-           int leaf_size, int depth, float traversal_cost, int* mid, Box* lbox, Box* rbox) {
+           int leaf_size, int max_sah_leaf, int depth, float traversal_cost, int* mid, Box* lbox,
+           Box* rbox) {
     const int count = end - begin;
     if (count <= leaf_size) return false;
     Box cb; cb.reset();
@@ -96,7 +97,7 @@ bool split(std::vector<int>& refs, const std::vector<Prim>& prims, int begin, in
 
     const float leaf_cost = count * nb.half_area();
     const float split_cost = traversal_cost * nb.half_area() + best_cost;
-    if (best_axis >= 0 && !(split_cost < leaf_cost) && count <= 4) return false;
+    if (best_axis >= 0 && !(split_cost < leaf_cost) && count <= max_sah_leaf) return false;
 
     int m;
     if (best_axis >= 0) {
@@ -129,7 +130,7 @@ bool split(std::vector<int>& refs, const std::vector<Prim>& prims, int begin, in
 // Generic preorder build. `emit_leaf(begin, end)` writes the leaf payload and returns the
 // negative child code (~index). Nodes are appended to nodes_out from *n_nodes on.
 template <typename EmitLeaf>
-int build_generic(std::vector<Prim>& prims, int leaf_size, float traversal_cost,
+int build_generic(std::vector<Prim>& prims, int leaf_size, int max_sah_leaf, float traversal_cost,
                   imbart_node2* nodes_out, int nodes_cap, int* n_nodes, EmitLeaf emit_leaf) {
     const int n = (int)prims.size();
     std::vector<int> refs(n);
@@ -144,7 +145,8 @@ int build_generic(std::vector<Prim>& prims, int leaf_size, float traversal_cost,
     while (!stack.empty()) {
         Task t = stack.back(); stack.pop_back();
         int mid; Box lb, rb;
-        const bool inner = split(refs, prims, t.begin, t.end, leaf_size, t.depth, traversal_cost, &mid, &lb, &rb);
+        const bool inner = split(refs, prims, t.begin, t.end, leaf_size, max_sah_leaf, t.depth, traversal_cost, &mid,
+                                 &lb, &rb);
         if (!inner) {
             leaf_refs.assign(refs.begin() + t.begin, refs.begin() + t.end);
             int code;
@@ -228,7 +230,7 @@ extern "C" int imbart_build_mesh_node2(const float* vertices, int n_vertices, in
         return 0;
     };
     // Traversal-cost factor 1.0 as the reference GPU mesh adapter (gpu_adapter.cpp:49-56).
-    const int err = build_generic(prims, leaf_size, 1.0f, nodes_out, nodes_cap, n_nodes, emit_leaf);
+    const int err = build_generic(prims, leaf_size, 4, 1.0f, nodes_out, nodes_cap, n_nodes, emit_leaf);
     if (err) set_error(err, "imbart_build_mesh_node2: output capacity too small");
     return err;
 }
@@ -265,7 +267,7 @@ extern "C" int imbart_build_top_node2(const float* boxes, const float* inv_mats,
     };
     // One instance per leaf and traversal-cost factor 0.5 as the reference top-level adapter
     // (gpu_adapter.cpp:188-197, leaf threshold 1 at :183).
-    const int err = build_generic(prims, 1, 0.5f, nodes_out, nodes_cap, n_nodes, emit_leaf);
+    const int err = build_generic(prims, 1, 1, 0.5f, nodes_out, nodes_cap, n_nodes, emit_leaf);
     if (err) set_error(err, "imbart_build_top_node2: output capacity too small");
     return err;
 }

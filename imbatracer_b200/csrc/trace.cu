@@ -119,6 +119,121 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
     return upload_scene(h, device);
 }
 
+// ---------------------------------------------------------------------------------------
+// Kernel variants. Variant 0 is the one-ray-per-thread kernel; variants 1..5 are the
+// persistent-warp kernel at different block sizes / register budgets / shared stack depths.
+// The configuration is process-wide (imbart_set_trace_config, or IMBART_TRACE_VARIANT,
+// IMBART_TRACE_REFILL and IMBART_TRACE_POSTPONE in the environment).
+// ---------------------------------------------------------------------------------------
+struct TraceConfig {
+    int variant, refill, postpone;
+};
+
+std::mutex g_cfg_mutex;
+bool g_cfg_init = false;
+TraceConfig g_cfg{1, 16, 0};
+
+int env_int(const char* name, int dflt) {
+    const char* v = getenv(name);
+    return v && *v ? atoi(v) : dflt;
+}
+
+TraceConfig current_config() {
+    std::lock_guard<std::mutex> lk(g_cfg_mutex);
+    if (!g_cfg_init) {
+        g_cfg.variant = env_int("IMBART_TRACE_VARIANT", g_cfg.variant);
+        g_cfg.refill = env_int("IMBART_TRACE_REFILL", g_cfg.refill);
+        g_cfg.postpone = env_int("IMBART_TRACE_POSTPONE", g_cfg.postpone);
+        g_cfg_init = true;
+    }
+    return g_cfg;
+}
+
+// Work counters of the persistent kernel: a ring of self-resetting (next, done) pairs per
+// device. A launch takes the next slot; the kernel's last warp zeroes it on exit, so slots
+// are reusable in stream order and concurrent launches on different streams use different
+// slots (a collision would need 4096 launches in flight).
+constexpr int kWorkSlots = 4096;
+std::mutex g_work_mutex;
+std::map<int, int*> g_work_pool;
+std::atomic<uint32_t> g_work_next{0};
+
+int* work_slot(int device) {
+    int* pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_work_mutex);
+        auto it = g_work_pool.find(device);
+        if (it == g_work_pool.end()) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(device);
+            const bool ok = cuda_ok(cudaMalloc((void**)&pool, sizeof(int) * 2 * kWorkSlots), "cudaMalloc") &&
+                            cuda_ok(cudaMemset(pool, 0, sizeof(int) * 2 * kWorkSlots), "cudaMemset");
+            cudaSetDevice(prev);
+            if (!ok) return nullptr;
+            g_work_pool[device] = pool;
+        } else {
+            pool = it->second;
+        }
+    }
+    const uint32_t slot = g_work_next.fetch_add(1, std::memory_order_relaxed) % kWorkSlots;
+    return pool + 2 * slot;
+}
+
+template <bool kStats>
+bool dispatch_simple(bool any, bool masked, int grid, int block, cudaStream_t stream, const TraceParams& p) {
+    if (any && masked) trace_kernel<true, true, kStats><<<grid, block, 0, stream>>>(p);
+    else if (any) trace_kernel<true, false, kStats><<<grid, block, 0, stream>>>(p);
+    else if (masked) trace_kernel<false, true, kStats><<<grid, block, 0, stream>>>(p);
+    else trace_kernel<false, false, kStats><<<grid, block, 0, stream>>>(p);
+    return true;
+}
+
+template <typename Kernel>
+int max_grid(Kernel k, int block, int device) {
+    static std::mutex m;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> lk(m);
+    const auto key = std::make_pair((const void*)k, device);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int g = std::max(1, per_sm) * std::max(1, sms);
+    cache[key] = g;
+    return g;
+}
+
+template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
+void launch_persistent(int count, int device, cudaStream_t stream, TraceParams p) {
+    auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh>;
+    const int grid = std::min(max_grid(k, kBlock, device), (count + kBlock - 1) / kBlock);
+    p.total_warps = grid * (kBlock / 32);
+    k<<<grid, kBlock, 0, stream>>>(p);
+}
+
+template <bool kAny, bool kMasked, bool kStats>
+bool dispatch_variant(int variant, int count, int device, cudaStream_t stream, const TraceParams& p) {
+    switch (variant) {
+        case 1: launch_persistent<kAny, kMasked, kStats, 128, 4, 16>(count, device, stream, p); return true;
+        case 2: launch_persistent<kAny, kMasked, kStats, 128, 6, 12>(count, device, stream, p); return true;
+        case 3: launch_persistent<kAny, kMasked, kStats, 256, 2, 16>(count, device, stream, p); return true;
+        case 4: launch_persistent<kAny, kMasked, kStats, 256, 3, 12>(count, device, stream, p); return true;
+        case 5: launch_persistent<kAny, kMasked, kStats, 64, 8, 16>(count, device, stream, p); return true;
+        default: return false;
+    }
+}
+
+template <bool kStats>
+bool dispatch_persistent(int variant, bool any, bool masked, int count, int device, cudaStream_t stream,
+                         const TraceParams& p) {
+    if (any && masked) return dispatch_variant<true, true, kStats>(variant, count, device, stream, p);
+    if (any) return dispatch_variant<true, false, kStats>(variant, count, device, stream, p);
+    if (masked) return dispatch_variant<false, true, kStats>(variant, count, device, stream, p);
+    return dispatch_variant<false, false, kStats>(variant, count, device, stream, p);
+}
+
 int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out,
                  int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr) {
     if (!s || (!rays && count > 0) || (!hits && count > 0) || count < 0) {
@@ -136,20 +251,27 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
     p.count = count;
     p.error_flags = s->error_flags;
     p.stats = stats;
-    const int block = 128;
-    const int grid = (count + block - 1) / block;
     const bool any = (flags & IMBART_TRACE_ANY) != 0;
     const bool masked = s->info.masked != 0;
-    if (stats) {
-        if (any && masked) trace_kernel<true, true, true><<<grid, block, 0, stream>>>(p);
-        else if (any) trace_kernel<true, false, true><<<grid, block, 0, stream>>>(p);
-        else if (masked) trace_kernel<false, true, true><<<grid, block, 0, stream>>>(p);
-        else trace_kernel<false, false, true><<<grid, block, 0, stream>>>(p);
+    const TraceConfig cfg = current_config();
+    bool launched;
+    if (cfg.variant == 0) {
+        const int block = 128;
+        const int grid = (count + block - 1) / block;
+        if (stats) launched = dispatch_simple<true>(any, masked, grid, block, stream, p);
+        else launched = dispatch_simple<false>(any, masked, grid, block, stream, p);
     } else {
-        if (any && masked) trace_kernel<true, true, false><<<grid, block, 0, stream>>>(p);
-        else if (any) trace_kernel<true, false, false><<<grid, block, 0, stream>>>(p);
-        else if (masked) trace_kernel<false, true, false><<<grid, block, 0, stream>>>(p);
-        else trace_kernel<false, false, false><<<grid, block, 0, stream>>>(p);
+        int* work = work_slot(s->device);
+        if (!work) return IMBART_ERR_CUDA;
+        p.work = work;
+        p.refill_lanes = std::min(std::max(cfg.refill, 1), 32);
+        p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
+        if (stats) launched = dispatch_persistent<true>(cfg.variant, any, masked, count, s->device, stream, p);
+        else launched = dispatch_persistent<false>(cfg.variant, any, masked, count, s->device, stream, p);
+    }
+    if (!launched) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");
+        return IMBART_ERR_INVALID_ARGUMENT;
     }
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (!cuda_ok(cudaGetLastError(), "trace kernel launch")) return IMBART_ERR_CUDA;
@@ -410,6 +532,26 @@ int imbart_scene_error_count(const imbart_scene* scene) {
 }
 
 int64_t imbart_kernel_launch_count(void) { return g_launches.load(); }
+
+int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
+    if (variant < 0 || variant > 5 || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||
+        postpone_lanes > 32) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_config: out of range");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    current_config();
+    std::lock_guard<std::mutex> lk(g_cfg_mutex);
+    g_cfg = TraceConfig{variant, refill_lanes, postpone_lanes};
+    return 0;
+}
+
+int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes) {
+    const TraceConfig c = current_config();
+    if (variant) *variant = c.variant;
+    if (refill_lanes) *refill_lanes = c.refill;
+    if (postpone_lanes) *postpone_lanes = c.postpone;
+    return 0;
+}
 
 void imbart_invalidate_scenes(void) { clear_cache(); }
 

@@ -46,7 +46,14 @@ struct TraceParams {
     int count;
     int* __restrict__ error_flags;          // [0]: stack overflow count
     unsigned long long* __restrict__ stats; // statistics variant: nodes, triangles, instances
+    // persistent variant
+    int* __restrict__ work;                 // [0]: next ray index, [1]: finished warps (self-resetting)
+    int total_warps;                        // warps in the launch
+    int refill_lanes;                       // refill a warp's idle lanes once this many are idle
+    int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
 };
+
+constexpr uint32_t kEntryTri = 3u;      // triangle group (postponed): x = prim base, y = prim mask
 
 // Work counters of one ray, accumulated only by the statistics variant of the kernel.
 struct RayStats {
@@ -94,9 +101,11 @@ __device__ __forceinline__ void setup_space(SpaceRay& r) {
     const float dkz = comp3(r.dx, r.dy, r.dz, kz);
     if (dkz < 0.0f) { const int t = kx; kx = ky; ky = t; }
     r.kx = kx; r.ky = ky; r.kz = kz;
-    r.Sx = __fdiv_rn(comp3(r.dx, r.dy, r.dz, kx), dkz);
-    r.Sy = __fdiv_rn(comp3(r.dx, r.dy, r.dz, ky), dkz);
-    r.Sz = __fdiv_rn(1.0f, dkz);
+    // Shear constants from the (correctly rounded) reciprocal of the dominant component:
+    // Sz = 1/d[kz], Sx = d[kx] * Sz, Sy = d[ky] * Sz (the oracle uses the same definition).
+    r.Sz = comp3(r.ix, r.iy, r.iz, kz);
+    r.Sx = __fmul_rn(comp3(r.dx, r.dy, r.dz, kx), r.Sz);
+    r.Sy = __fmul_rn(comp3(r.dx, r.dy, r.dz, ky), r.Sz);
 }
 
 // Watertight ray/triangle test. Returns true and writes t/u/v when the ray's line hits the
@@ -144,8 +153,10 @@ __device__ __forceinline__ float xform_row(const float4 m, float x, float y, flo
     return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
 }
 
+// Byte k of w as an exact float: the byte is placed in the mantissa of 2^23 with one byte
+// permute, then 2^23 is subtracted (both full-rate ALU operations, no conversion unit).
 __device__ __forceinline__ float byte_to_float(uint32_t w, int k) {
-    return __uint2float_rn((w >> (8 * k)) & 0xffu);
+    return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (uint32_t)k)) - 8388608.0f;
 }
 
 // Intersects the 8 child boxes of a node. Returns internal-child hits in octant order
@@ -349,6 +360,218 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
     h.w = __float_as_int(best_tri >= 0 ? best_u : 0.0f);
     p.hits[ray_index] = h;
     if (p.v_out) p.v_out[ray_index] = best_tri >= 0 ? best_v : 0.0f;
+}
+
+// ---------------------------------------------------------------------------------------
+// Persistent-warp traversal.
+//
+// Each warp keeps 32 rays in flight and pulls new ray indices from a global counter with one
+// warp-aggregated atomic whenever `refill_lanes` of its lanes have finished, so lanes do not
+// idle until the slowest ray of a static batch ends. The loop follows the node-group /
+// triangle-group scheme of Ylitie, Karras and Laine (HPG 2017): a node step pops the next hit
+// child of the current group and intersects its 8 boxes, producing a group of hit internal
+// children and a group of hit leaf primitives; triangle tests are postponed (the triangle
+// group goes onto the stack) while fewer than postpone_lanes/32 of the live lanes would test
+// triangles together. The stack lives in shared memory (kSh entries per thread, laid out so
+// that neighbouring threads touch neighbouring words) and spills to local memory.
+// Results are identical to the per-thread kernel: same tests, same tie rule.
+// ---------------------------------------------------------------------------------------
+template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TraceParams p) {
+    __shared__ uint2 sstack[kSh][kBlock];
+    uint2 lstack[kStackSize - kSh];
+    const int tid = threadIdx.x;
+    const unsigned lane = tid & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    int ray = -1;                       // -1: idle (wants a ray), >= count: queue exhausted
+    SpaceRay r;                         // current space (world or instance)
+    float wox = 0, woy = 0, woz = 0, wdx = 0, wdy = 0, wdz = 0, wix = 0, wiy = 0, wiz = 0, wpad = 0;
+    uint32_t woct = 0;
+    float tmin = 0.0f, best_t = 0.0f, best_u = 0.0f, best_v = 0.0f, tlimit = 0.0f;
+    int best_tri = -1, best_inst = -1, cur_inst = -1;
+    bool bottom = false;
+    uint32_t g_base = 0, g_imask = 0, g_hits = 0, t_base = 0, t_mask = 0;
+    int sp = 0;
+    RayStats st;
+    r.kx = r.ky = r.kz = 0;
+
+    auto push = [&](uint32_t x, uint32_t y) -> bool {
+        if (sp >= kStackSize) return false;
+        if (sp < kSh) sstack[sp][tid] = make_uint2(x, y);
+        else lstack[sp - kSh] = make_uint2(x, y);
+        ++sp;
+        return true;
+    };
+    auto finish = [&]() {
+        int4 h;
+        h.x = best_tri;
+        h.y = best_tri >= 0 ? best_inst : -1;
+        h.z = __float_as_int(best_t);
+        h.w = __float_as_int(best_tri >= 0 ? best_u : 0.0f);
+        p.hits[ray] = h;
+        if (p.v_out) p.v_out[ray] = best_tri >= 0 ? best_v : 0.0f;
+        ray = -1;
+    };
+
+    for (;;) {
+        // Refill idle lanes in warp-wide batches.
+        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
+        unsigned live = __ballot_sync(0xffffffffu, ray >= 0 && ray < p.count);
+        if (idle != 0u && (live == 0u || __popc(idle) >= p.refill_lanes)) {
+            const int leader = __ffs(idle) - 1;
+            int base = 0;
+            if ((int)lane == leader) base = atomicAdd(p.work, __popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (ray < 0) {
+                const int idx = base + __popc(idle & lt_mask);
+                if (idx >= p.count) {
+                    ray = p.count;
+                } else {
+                    ray = idx;
+                    const float4 ro = __ldg(p.rays + 2 * ray + 0);
+                    const float4 rd = __ldg(p.rays + 2 * ray + 1);
+                    tmin = ro.w; best_t = rd.w; best_u = 0.0f; best_v = 0.0f;
+                    best_tri = -1; best_inst = -1; cur_inst = -1; bottom = false; sp = 0;
+                    if (!((tmin <= best_t) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f))) {
+                        finish();
+                    } else {
+                        r.ox = ro.x; r.oy = ro.y; r.oz = ro.z;
+                        r.dx = rd.x; r.dy = rd.y; r.dz = rd.z;
+                        setup_space(r);
+                        wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
+                        wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
+                        tlimit = best_t * IMBART_SLACK;
+                        g_base = (uint32_t)p.root; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                        t_mask = 0;
+                    }
+                }
+            }
+            live = __ballot_sync(0xffffffffu, ray >= 0 && ray < p.count);
+        }
+        if (live == 0u) {
+            if (__ballot_sync(0xffffffffu, ray < 0) == 0u) break;   // every lane exhausted
+            continue;
+        }
+        const bool active = ray >= 0 && ray < p.count;
+        if (!active) continue;
+        const int n_live = __popc(live);
+
+        // Node step.
+        if (t_mask == 0 && g_hits != 0) {
+            const uint32_t bitpos = __ffs(g_hits) - 1;
+            g_hits &= g_hits - 1;
+            const uint32_t slot = bitpos ^ r.oct;
+            const uint32_t idx = g_base + __popc(g_imask & ((1u << slot) - 1u));
+            if (g_hits != 0 && !push(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask)) {
+                atomicAdd(p.error_flags, 1);
+                finish();
+                continue;
+            }
+            intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+            if (kStats) st.nodes++;
+        }
+
+        // Primitive step.
+        if (t_mask != 0) {
+            if (bottom) {
+                bool stop = false;
+                while (t_mask != 0) {
+                    // Postpone only while node work remains, so that a ray with nothing
+                    // but triangles left always makes progress.
+                    if (g_hits != 0 && __popc(__activemask()) * 32 < n_live * p.postpone_lanes) {
+                        if (!push(t_base | (kEntryTri << kTypeShift), t_mask)) {
+                            atomicAdd(p.error_flags, 1);
+                            stop = true;
+                        }
+                        t_mask = 0;
+                        break;
+                    }
+                    const uint32_t i = __ffs(t_mask) - 1;
+                    t_mask &= t_mask - 1;
+                    const float4* tp = reinterpret_cast<const float4*>(p.tris + t_base + i);
+                    const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    if (kStats) st.tris++;
+                    float t, u, v;
+                    if (!tri_test(r, a, b, c, t, u, v)) continue;
+                    if (!(t >= tmin)) continue;
+                    const int tri = __float_as_int(a.w);
+                    const bool closer = (t < best_t) ||
+                        (t == best_t && (best_tri < 0 || cur_inst < best_inst ||
+                                         (cur_inst == best_inst && tri < best_tri)));
+                    if (!closer) continue;
+                    if (kMasked && !mask_opaque(p, tri, u, v)) continue;
+                    best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
+                    tlimit = best_t * IMBART_SLACK;
+                    if (kAnyHit) { stop = true; break; }
+                }
+                if (stop) { finish(); continue; }
+            } else {
+                // Enter the next instance of the group.
+                const uint32_t i = __ffs(t_mask) - 1;
+                t_mask &= t_mask - 1;
+                bool ok = true;
+                if (g_hits != 0) ok = push(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask);
+                if (ok && t_mask != 0) ok = push(t_base | (kEntryInst << kTypeShift), t_mask);
+                if (ok) ok = push(kEntryMarker << kTypeShift, 0u);
+                if (!ok) { atomicAdd(p.error_flags, 1); finish(); continue; }
+                t_mask = 0;
+                const float4* ip = reinterpret_cast<const float4*>(p.insts + t_base + i);
+                const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+                const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
+                if (kStats) st.insts++;
+                r.ox = xform_row(m0, wox, woy, woz, 1.0f);
+                r.oy = xform_row(m1, wox, woy, woz, 1.0f);
+                r.oz = xform_row(m2, wox, woy, woz, 1.0f);
+                r.dx = xform_row(m0, wdx, wdy, wdz, 0.0f);
+                r.dy = xform_row(m1, wdx, wdy, wdz, 0.0f);
+                r.dz = xform_row(m2, wdx, wdy, wdz, 0.0f);
+                setup_space(r);
+                cur_inst = meta.x;
+                bottom = true;
+                g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                continue;
+            }
+        }
+
+        // Pop the next group when the current ones are exhausted.
+        if (g_hits == 0 && t_mask == 0) {
+            for (;;) {
+                if (sp == 0) { finish(); break; }
+                --sp;
+                const uint2 e = sp < kSh ? sstack[sp][tid] : lstack[sp - kSh];
+                const uint32_t type = e.x >> kTypeShift;
+                if (type == kEntryMarker) {
+                    r.ox = wox; r.oy = woy; r.oz = woz; r.dx = wdx; r.dy = wdy; r.dz = wdz;
+                    r.ix = wix; r.iy = wiy; r.iz = wiz; r.pad = wpad; r.oct = woct;
+                    bottom = false; cur_inst = -1;
+                    continue;
+                }
+                if (type == kEntryNode) { g_base = e.x & kIndexMask; g_imask = e.y & 0xffu; g_hits = e.y >> 8; }
+                else { t_base = e.x & kIndexMask; t_mask = e.y; }
+                break;
+            }
+        }
+    }
+
+    if (kStats) {
+        const unsigned n = __reduce_add_sync(0xffffffffu, st.nodes);
+        const unsigned t = __reduce_add_sync(0xffffffffu, st.tris);
+        const unsigned k = __reduce_add_sync(0xffffffffu, st.insts);
+        if (lane == 0) {
+            atomicAdd(p.stats + 0, (unsigned long long)n);
+            atomicAdd(p.stats + 1, (unsigned long long)t);
+            atomicAdd(p.stats + 2, (unsigned long long)k);
+        }
+    }
+    // The last warp to finish resets the work counter for the next launch on this slot.
+    if (lane == 0) {
+        __threadfence();
+        if (atomicAdd(p.work + 1, 1) == p.total_warps - 1) {
+            atomicExch(p.work + 0, 0);
+            atomicExch(p.work + 1, 0);
+        }
+    }
 }
 
 template <bool kAnyHit, bool kMasked, bool kStats>

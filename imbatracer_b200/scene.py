@@ -114,19 +114,20 @@ def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_siz
         N.check(rc, "imbart_build_mesh_node2")
         tri_off += m.triangle_count
     node_count = n_nodes.value
-    # Instance world boxes: transformed mesh box centre +- |M| * half extent (gpu_adapter.cpp:171-179).
+    # Instance world boxes. The reference transforms the mesh box (centre +- |M| * half extent,
+    # gpu_adapter.cpp:171-179), which for rotated instances is up to sqrt(3) times wider per
+    # axis than the instance itself; here the box is the bound of the transformed vertices
+    # (of their convex hull for large meshes, which has the same bound), rounded outward.
     boxes = np.zeros((len(instances), 6), np.float32)
     inv = np.zeros((len(instances), 12), np.float32)
     roots = np.zeros(len(instances), np.int32)
-    mesh_boxes = [m.bounding_box() for m in meshes]
+    hull = [m.vertices.astype(np.float64) for m in meshes]
     for i, inst in enumerate(instances):
-        lo, hi = mesh_boxes[inst.mesh_id]
-        c = (hi + lo) * np.float32(0.5)
-        e = (hi - lo) * np.float32(0.5)
-        wc = inst.mat[:3, :3] @ c + inst.mat[:3, 3]
-        we = np.abs(inst.mat[:3, :3]) @ e
-        boxes[i, :3] = wc - we
-        boxes[i, 3:] = wc + we
+        w = hull[inst.mesh_id] @ inst.mat[:3, :3].astype(np.float64).T + inst.mat[:3, 3].astype(np.float64)
+        lo, hi = w.min(0), w.max(0)
+        pad = 1e-6 * (np.abs(lo).max() + np.abs(hi).max() + (hi - lo).max())
+        boxes[i, :3] = np.nextafter((lo - pad).astype(np.float32), np.float32(-np.inf))
+        boxes[i, 3:] = np.nextafter((hi + pad).astype(np.float32), np.float32(np.inf))
         inv[i] = inst.inv_mat.reshape(-1)
         roots[i] = layout[inst.mesh_id]
     insts = np.zeros(len(instances), N.INST_DTYPE)

@@ -225,6 +225,16 @@ int imbart_scene_error_count(const imbart_scene* scene);
 /* Number of kernel launches issued by this process so far (for launch accounting). */
 int64_t imbart_kernel_launch_count(void);
 
+/* Process-wide traversal kernel configuration (the tuning knobs of the autotuner):
+ * variant 0 = one ray per thread; 1..5 = persistent warps (1: 128 threads x 4 blocks/SM,
+ * 16-entry shared stack; 2: 128 x 6, 12; 3: 256 x 2, 16; 4: 256 x 3, 12; 5: 64 x 8, 16);
+ * refill_lanes (1..32): a warp fetches new rays once this many lanes are idle;
+ * postpone_lanes (0..32): triangle tests are postponed while fewer than
+ * postpone_lanes/32 of the live lanes would test together (0 = never).
+ * The defaults can also be set with IMBART_TRACE_VARIANT / _REFILL / _POSTPONE. */
+int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes);
+int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes);
+
 /* ------------------------------------------------------------------------------------ */
 /* BVH construction (the builder side of the boundary)                                     */
 /* ------------------------------------------------------------------------------------ */

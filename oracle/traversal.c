@@ -44,15 +44,25 @@ typedef struct {
 
 static int max_dim3(float x, float y, float z) { return (x > y) ? ((x > z) ? 0 : 2) : ((y > z) ? 1 : 2); }
 
+/* Reciprocal with zero components replaced by +-1e-30 (keeps slab tests finite). */
+static float safe_rcp(float d) {
+    const float tiny = 1e-30f;
+    const float dd = fabsf(d) < tiny ? copysignf(tiny, d) : d;
+    return 1.0f / dd;
+}
+
+/* Shear constants of the watertight test: Sz = 1/d[kz] (rounded once), Sx = d[kx] * Sz,
+ * Sy = d[ky] * Sz. The paper writes the divisions d[kx]/d[kz]; any fixed definition keeps
+ * the test watertight, and this one is shared with the GPU kernel. */
 static void setup_shear(space_t* s) {
     const int kz = max_dim3(fabsf(s->d[0]), fabsf(s->d[1]), fabsf(s->d[2]));
     int kx = kz + 1; if (kx == 3) kx = 0;
     int ky = kx + 1; if (ky == 3) ky = 0;
     if (s->d[kz] < 0.0f) { const int t = kx; kx = ky; ky = t; }
     s->kx = kx; s->ky = ky; s->kz = kz;
-    s->Sx = s->d[kx] / s->d[kz];
-    s->Sy = s->d[ky] / s->d[kz];
-    s->Sz = 1.0f / s->d[kz];
+    s->Sz = safe_rcp(s->d[kz]);
+    s->Sx = s->d[kx] * s->Sz;
+    s->Sy = s->d[ky] * s->Sz;
 }
 
 /* Watertight test; identical operation order to the GPU kernel (trace_kernel.cuh). */
@@ -332,12 +342,6 @@ typedef struct {
     unsigned oct;
     space_t sh;
 } wspace_t;
-
-static float safe_rcp(float d) {
-    const float tiny = 1e-30f;
-    const float dd = fabsf(d) < tiny ? copysignf(tiny, d) : d;
-    return 1.0f / dd;
-}
 
 static void wsetup(wspace_t* r) {
     r->pad = fmaxf(fmaxf(fabsf(r->o[0]), fabsf(r->o[1])), fabsf(r->o[2])) * 9.5367431640625e-07f;
