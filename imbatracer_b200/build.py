@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES_CU = ["trace.cu"]
+SOURCES_CU = ["trace.cu", "hashgrid.cu"]
 SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp"]
 
 

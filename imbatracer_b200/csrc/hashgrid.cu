@@ -1,0 +1,408 @@
+// Photon hash grid on the GPU: build (bounding box, hashed counting sort) and batched
+// k-capped radius queries, with the semantics of the reference's HashGrid
+// (src/imbatracer/rangesearch/rangesearch.h):
+//   build  :25-75   r^2, cell size (2r in the reference, a parameter here), bbox of the
+//                   photon positions inflated by 0.1 % of its extent per side, counting sort
+//                   into `table_size` buckets (2 * photon count in the reference)
+//   hash   :137-148 ((x*73856093) ^ (y*19349663) ^ (z*83492791)) mod table_size on unsigned
+//                   coordinates, coordinates = floor((p - bbox.min) / cell size)
+//   query  :77-129  outside the bbox -> nothing; home cell plus the nearer neighbour per
+//                   axis (8 buckets in the reference's order, a bucket hit twice is scanned
+//                   twice), squared distance <= r^2, k nearest kept by insertion sort
+// Every float operation is explicitly rounded (no contraction) so that cell indices and
+// distances equal the reference's bit for bit. Within a bucket photons are placed by an
+// atomic cursor, as in the reference's parallel scatter (rangesearch.h:68-74); the query
+// returns its k photons ordered by (distance, photon index).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <string>
+
+#include "imbart_internal.h"
+
+struct imbart_hashgrid {
+    int device = 0;
+    int n = 0;              // photons in the current build
+    int table = 0;          // buckets in the current build
+    int sorted_cap = 0, cell_of_cap = 0, ends_cap = 0, cursor_cap = 0;
+    float4* sorted = nullptr;   // position xyz + original index (int bits) in bucket order
+    int* cell_ends = nullptr;   // inclusive end of each bucket
+    int* cell_of = nullptr;     // bucket of each photon (scratch)
+    int* cursor = nullptr;      // scatter cursor per bucket (scratch)
+    int* block_sums = nullptr;  // scan scratch
+    int block_sums_cap = 0;
+    float* params = nullptr;    // device: lo[3], hi[3], radius, r^2, cell, inv_cell
+    float host_params[10] = {};
+};
+
+namespace imbart {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kScanItems = 8;                 // items per thread in the scan kernels
+constexpr int kScanTile = kBlock * kScanItems;
+constexpr int kMaxK = 64;
+
+bool ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? IMBART_ERR_OUT_OF_MEMORY : IMBART_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+// Order-preserving float <-> int mapping for atomicMin/atomicMax on floats.
+__device__ __forceinline__ int float_to_ordered(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ordered_to_float(int i) {
+    return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+}
+
+__global__ void bbox_init_kernel(int* box) {
+    if (threadIdx.x < 3) box[threadIdx.x] = float_to_ordered(FLT_MAX);
+    else if (threadIdx.x < 6) box[threadIdx.x] = float_to_ordered(-FLT_MAX);
+}
+
+// Exact min/max of the positions (order-independent, so bit-identical to a serial pass).
+__global__ void bbox_kernel(const float* __restrict__ pos, int stride, int n, int* __restrict__ box) {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* p = pos + (size_t)i * stride;
+        for (int a = 0; a < 3; ++a) {
+            const float v = p[a];
+            lo[a] = lo[a] < v ? lo[a] : v;
+            hi[a] = hi[a] > v ? hi[a] : v;
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int off = 16; off > 0; off >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(box + a, float_to_ordered(lo[a]));
+            atomicMax(box + 3 + a, float_to_ordered(hi[a]));
+        }
+    }
+}
+
+// Inflates the box (rangesearch.h:44-46) and derives the cell parameters (:27-30).
+__global__ void params_kernel(const int* __restrict__ box, float radius, float cell_factor, float* __restrict__ prm) {
+    if (threadIdx.x != 0) return;
+    float lo[3], hi[3], ext[3];
+    for (int a = 0; a < 3; ++a) { lo[a] = ordered_to_float(box[a]); hi[a] = ordered_to_float(box[3 + a]); }
+    for (int a = 0; a < 3; ++a) ext[a] = __fsub_rn(hi[a], lo[a]);
+    for (int a = 0; a < 3; ++a) hi[a] = __fadd_rn(hi[a], __fmul_rn(ext[a], 0.001f));
+    for (int a = 0; a < 3; ++a) lo[a] = __fsub_rn(lo[a], __fmul_rn(ext[a], 0.001f));
+    const float cell = __fmul_rn(radius, cell_factor);
+    for (int a = 0; a < 3; ++a) { prm[a] = lo[a]; prm[3 + a] = hi[a]; }
+    prm[6] = radius;
+    prm[7] = __fmul_rn(radius, radius);
+    prm[8] = cell;
+    prm[9] = __fdiv_rn(1.0f, cell);
+}
+
+__device__ __forceinline__ int hash_cell(uint32_t x, uint32_t y, uint32_t z, uint32_t table) {
+    return (int)(((x * 73856093u) ^ (y * 19349663u) ^ (z * 83492791u)) % table);
+}
+
+__device__ __forceinline__ int cell_of_point(const float* prm, float px, float py, float pz, uint32_t table) {
+    const float inv = prm[9];
+    const int cx = (int)floorf(__fmul_rn(inv, __fsub_rn(px, prm[0])));
+    const int cy = (int)floorf(__fmul_rn(inv, __fsub_rn(py, prm[1])));
+    const int cz = (int)floorf(__fmul_rn(inv, __fsub_rn(pz, prm[2])));
+    return hash_cell((uint32_t)cx, (uint32_t)cy, (uint32_t)cz, table);
+}
+
+__global__ void count_kernel(const float* __restrict__ pos, int stride, int n, const float* __restrict__ prm,
+                             uint32_t table, int* __restrict__ counts, int* __restrict__ cell_of) {
+    __shared__ float sp[10];
+    if (threadIdx.x < 10) sp[threadIdx.x] = prm[threadIdx.x];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* p = pos + (size_t)i * stride;
+        const int c = cell_of_point(sp, p[0], p[1], p[2], table);
+        cell_of[i] = c;
+        atomicAdd(counts + c, 1);
+    }
+}
+
+// Three-phase exclusive scan: per-tile sums, scan of the tile sums, tile-local scan + offset.
+__global__ void scan_tiles_kernel(const int* __restrict__ in, int n, int* __restrict__ tile_sums) {
+    __shared__ int warp_sums[kBlock / 32];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int s = 0;
+    for (int k = 0; k < kScanItems; ++k) s += (base + k < n) ? in[base + k] : 0;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kBlock / 32; ++w) t += warp_sums[w];
+        tile_sums[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the tile sums by one block (tiles <= kBlock * kScanItems * ... looped).
+__global__ void scan_sums_kernel(int* __restrict__ sums, int n_tiles) {
+    __shared__ int buf[kBlock];
+    int carry = 0;
+    for (int base = 0; base < n_tiles; base += kBlock) {
+        const int i = base + threadIdx.x;
+        const int v = i < n_tiles ? sums[i] : 0;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < kBlock; off <<= 1) {
+            const int t = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < n_tiles) sums[i] = carry + buf[threadIdx.x] - v;
+        __syncthreads();
+        carry += buf[kBlock - 1];
+        __syncthreads();
+    }
+}
+
+// Writes inclusive ends (cell_ends) and exclusive starts (cursor) of every bucket. `starts`
+// may alias `counts_in`: every thread reads its items before writing them.
+__global__ void scan_apply_kernel(const int* counts_in, int n, const int* __restrict__ tile_off,
+                                  int* __restrict__ ends, int* starts) {
+    __shared__ int warp_sums[kBlock / 32];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
+    for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < n) ? counts_in[base + k] : 0; s += v[k]; }
+    // exclusive scan of per-thread sums within the block
+    int incl = s;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, off);
+        if ((int)(threadIdx.x & 31) >= off) incl += t;
+    }
+    if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = incl;
+    __syncthreads();
+    int warp_off = 0;
+    for (int w = 0; w < (int)(threadIdx.x >> 5); ++w) warp_off += warp_sums[w];
+    int run = tile_off[blockIdx.x] + warp_off + incl - s;
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) {
+            starts[base + k] = run;
+            run += v[k];
+            ends[base + k] = run;
+        }
+    }
+}
+
+__global__ void scatter_kernel(const float* __restrict__ pos, int stride, int n, const int* __restrict__ cell_of,
+                               int* __restrict__ cursor, float4* __restrict__ sorted) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* p = pos + (size_t)i * stride;
+        const int slot = atomicAdd(cursor + cell_of[i], 1);
+        sorted[slot] = make_float4(p[0], p[1], p[2], __int_as_float(i));
+    }
+}
+
+// One query per thread. The k best photons are kept sorted by squared distance with the
+// reference's insertion rule; the result is then ordered by (distance, index).
+__global__ void query_kernel(const float4* __restrict__ sorted, const int* __restrict__ ends,
+                             const float* __restrict__ prm, uint32_t table, const float* __restrict__ queries,
+                             int nq, int k, int* __restrict__ out_ids, int* __restrict__ out_count,
+                             float* __restrict__ out_d2) {
+    __shared__ float sp[10];
+    if (threadIdx.x < 10) sp[threadIdx.x] = prm[threadIdx.x];
+    __syncthreads();
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const float qx = queries[3 * (size_t)q + 0], qy = queries[3 * (size_t)q + 1], qz = queries[3 * (size_t)q + 2];
+    float dist[kMaxK];
+    int ids[kMaxK];
+    int count = 0;
+    const bool inside = qx >= sp[0] && qy >= sp[1] && qz >= sp[2] && qx <= sp[3] && qy <= sp[4] && qz <= sp[5];
+    if (inside) {
+        const float inv = sp[9], r2 = sp[7];
+        const float cx = __fmul_rn(inv, __fsub_rn(qx, sp[0]));
+        const float cy = __fmul_rn(inv, __fsub_rn(qy, sp[1]));
+        const float cz = __fmul_rn(inv, __fsub_rn(qz, sp[2]));
+        const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+        const int px = (int)fx, py = (int)fy, pz = (int)fz;
+        const int pxo = px + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
+        const int pyo = py + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
+        const int pzo = pz + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
+        for (int j = 0; j < 8; ++j) {
+            const int x = (j & 4) ? pxo : px;
+            const int y = (j & 2) ? pyo : py;
+            const int z = (j & 1) ? pzo : pz;
+            const int c = hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, table);
+            const int b = c == 0 ? 0 : __ldg(ends + c - 1);
+            const int e = __ldg(ends + c);
+            for (int s = b; s < e; ++s) {
+                const float4 ph = __ldg(sorted + s);
+                const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
+                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                if (!(d2 <= r2)) continue;
+                if (count == k) {
+                    if (dist[count - 1] < d2) continue;
+                } else {
+                    count++;
+                }
+                dist[count - 1] = d2;
+                ids[count - 1] = __float_as_int(ph.w);
+                for (int l = count - 2; l >= 0; --l) {
+                    if (dist[l] > d2) {
+                        const float td = dist[l]; dist[l] = dist[l + 1]; dist[l + 1] = td;
+                        const int ti = ids[l]; ids[l] = ids[l + 1]; ids[l + 1] = ti;
+                    } else {
+                        break;
+                    }
+                }
+            }
+        }
+        // Deterministic order among equal distances: by photon index.
+        for (int i = 1; i < count; ++i) {
+            const float d = dist[i];
+            const int id = ids[i];
+            int l = i - 1;
+            while (l >= 0 && dist[l] == d && ids[l] > id) { dist[l + 1] = dist[l]; ids[l + 1] = ids[l]; --l; }
+            dist[l + 1] = d;
+            ids[l + 1] = id;
+        }
+    }
+    out_count[q] = count;
+    int* o = out_ids + (size_t)q * k;
+    for (int i = 0; i < k; ++i) o[i] = i < count ? ids[i] : -1;
+    if (out_d2) {
+        float* od = out_d2 + (size_t)q * k;
+        for (int i = 0; i < k; ++i) od[i] = i < count ? dist[i] : 0.0f;
+    }
+}
+
+int grid_for(int n) {
+    static int sms = 0;
+    if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    return std::max(1, std::min((n + kBlock - 1) / kBlock, sms * 8));
+}
+
+template <typename T>
+bool grow(T** p, int* cap, int need) {
+    if (*cap >= need) return true;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (!ok(cudaMalloc((void**)p, sizeof(T) * (size_t)std::max(need, 1)), "cudaMalloc")) return false;
+    *cap = need;
+    return true;
+}
+
+}  // namespace
+}  // namespace imbart
+
+using namespace imbart;
+
+extern "C" {
+
+imbart_hashgrid* imbart_hashgrid_create(int device) {
+    imbart_hashgrid* g = new imbart_hashgrid;
+    g->device = device;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    const bool good = ok(cudaMalloc((void**)&g->params, sizeof(float) * 16), "cudaMalloc");
+    cudaSetDevice(prev);
+    if (!good) { delete g; return nullptr; }
+    return g;
+}
+
+void imbart_hashgrid_destroy(imbart_hashgrid* g) {
+    if (!g) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    cudaFree(g->sorted); cudaFree(g->cell_ends); cudaFree(g->cell_of); cudaFree(g->cursor);
+    cudaFree(g->block_sums); cudaFree(g->params);
+    cudaSetDevice(prev);
+    delete g;
+}
+
+int imbart_hashgrid_build(imbart_hashgrid* g, const float* positions, int stride, int n, float radius,
+                          float cell_factor, int table_size, void* stream) {
+    if (!g || n < 0 || (n > 0 && !positions) || stride < 3 || !(radius > 0.0f) || !(cell_factor > 0.0f)) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_build: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (table_size <= 0) table_size = std::max(2 * n, 1);   // reference: 2 * photons (rangesearch.h:26)
+    cudaStream_t st = (cudaStream_t)stream;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    int rc = 0;
+    const int n_tiles = (table_size + kScanTile - 1) / kScanTile;
+    int* box = nullptr;
+    if (!grow(&g->sorted, &g->sorted_cap, n) || !grow(&g->cell_of, &g->cell_of_cap, n) ||
+        !grow(&g->cell_ends, &g->ends_cap, table_size) || !grow(&g->cursor, &g->cursor_cap, table_size) ||
+        !grow(&g->block_sums, &g->block_sums_cap, n_tiles + 8))
+        rc = IMBART_ERR_OUT_OF_MEMORY;
+    if (!rc) {
+        box = g->block_sums + n_tiles;   // 6 ints after the tile sums
+        const int grid = grid_for(std::max(n, 1));
+        bbox_init_kernel<<<1, 32, 0, st>>>(box);
+        if (n > 0) bbox_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, box);
+        params_kernel<<<1, 32, 0, st>>>(box, radius, cell_factor, g->params);
+        ok(cudaMemsetAsync(g->cursor, 0, sizeof(int) * (size_t)table_size, st), "cudaMemsetAsync");
+        if (n > 0) count_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, g->params, (uint32_t)table_size,
+                                                         g->cursor, g->cell_of);
+        scan_tiles_kernel<<<n_tiles, kBlock, 0, st>>>(g->cursor, table_size, g->block_sums);
+        scan_sums_kernel<<<1, kBlock, 0, st>>>(g->block_sums, n_tiles);
+        scan_apply_kernel<<<n_tiles, kBlock, 0, st>>>(g->cursor, table_size, g->block_sums, g->cell_ends, g->cursor);
+        if (n > 0) scatter_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, g->cell_of, g->cursor, g->sorted);
+        if (!ok(cudaGetLastError(), "hash grid build")) rc = IMBART_ERR_CUDA;
+        g->n = n;
+        g->table = table_size;
+    }
+    cudaSetDevice(prev);
+    return rc;
+}
+
+int imbart_hashgrid_query(const imbart_hashgrid* g, const float* queries, int nq, int k, int* out_ids,
+                          int* out_counts, float* out_d2, void* stream) {
+    if (!g || nq < 0 || k < 1 || k > kMaxK || (nq > 0 && (!queries || !out_ids || !out_counts)) || g->table == 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_query: invalid argument (k must be 1..64, grid built)");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (nq == 0) return 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    const int grid = (nq + 127) / 128;
+    query_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(g->sorted, g->cell_ends, g->params, (uint32_t)g->table,
+                                                         queries, nq, k, out_ids, out_counts, out_d2);
+    const bool good = ok(cudaGetLastError(), "hash grid query");
+    cudaSetDevice(prev);
+    return good ? 0 : IMBART_ERR_CUDA;
+}
+
+int imbart_hashgrid_get_params(const imbart_hashgrid* g, float* params10, int* n, int* table_size) {
+    if (!g) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_get_params"); return IMBART_ERR_INVALID_ARGUMENT; }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    bool good = true;
+    if (params10) good = ok(cudaMemcpy(params10, g->params, sizeof(float) * 10, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    cudaSetDevice(prev);
+    if (n) *n = g->n;
+    if (table_size) *table_size = g->table;
+    return good ? 0 : IMBART_ERR_CUDA;
+}
+
+int imbart_hashgrid_get_arrays(const imbart_hashgrid* g, const void** sorted, const int** cell_ends) {
+    if (!g) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_get_arrays"); return IMBART_ERR_INVALID_ARGUMENT; }
+    if (sorted) *sorted = g->sorted;
+    if (cell_ends) *cell_ends = g->cell_ends;
+    return 0;
+}
+
+}  // extern "C"

@@ -65,6 +65,12 @@ _SIGNATURES = {
     "imbart_trace_stats": (I, [P, P, P, I, I, P, P]),
     "imbart_scene_error_count": (I, [P]),
     "imbart_kernel_launch_count": (C.c_int64, []),
+    "imbart_hashgrid_create": (P, [I]),
+    "imbart_hashgrid_destroy": (None, [P]),
+    "imbart_hashgrid_build": (I, [P, P, I, I, C.c_float, C.c_float, I, P]),
+    "imbart_hashgrid_query": (I, [P, P, I, I, P, P, P, P]),
+    "imbart_hashgrid_get_params": (I, [P, P, P, P]),
+    "imbart_hashgrid_get_arrays": (I, [P, C.POINTER(P), C.POINTER(P)]),
     "imbart_set_trace_config": (I, [I, I, I]),
     "imbart_get_trace_config": (I, [C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),

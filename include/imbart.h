@@ -236,6 +236,40 @@ int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes);
 int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes);
 
 /* ------------------------------------------------------------------------------------ */
+/* Photon hash grid (replaces HashGrid::build / HashGrid::query, rangesearch.h:25-129,     */
+/* used by LightVertices::build / get_merge, light_vertices.h:70-100)                      */
+/* ------------------------------------------------------------------------------------ */
+
+typedef struct imbart_hashgrid imbart_hashgrid;
+
+/* Creates an empty grid whose buffers live on `device`. NULL on error. */
+imbart_hashgrid* imbart_hashgrid_create(int device);
+void imbart_hashgrid_destroy(imbart_hashgrid* grid);
+
+/* Builds the grid over n photon positions (DEVICE pointer; photon i's xyz at
+ * positions + i * stride floats, stride >= 3). cell size = radius * cell_factor (the reference
+ * uses 2, rangesearch.h:29); table_size buckets (<= 0: 2 * n, the reference's choice,
+ * rangesearch.h:26). Stream-ordered; device buffers grow as needed and are kept. */
+int imbart_hashgrid_build(imbart_hashgrid* grid, const float* positions, int stride, int n, float radius,
+                          float cell_factor, int table_size, void* stream);
+
+/* k-capped radius queries for nq positions (DEVICE, 3 packed floats each), 1 <= k <= 64.
+ * out_ids (nq*k) receives the indices (build order) of the photons within the radius, at most
+ * the k nearest, ordered by (squared distance, index) and padded with -1; out_counts (nq) the
+ * count; out_d2 (nq*k, may be NULL) the squared distances. A bucket reached twice through the
+ * 8 neighbour cells is scanned twice, as in the reference (rangesearch.h:94-104). */
+int imbart_hashgrid_query(const imbart_hashgrid* grid, const float* queries, int nq, int k, int* out_ids,
+                          int* out_counts, float* out_d2, void* stream);
+
+/* Grid parameters after a build (synchronous): params10 = {lo xyz, hi xyz, radius, radius^2,
+ * cell size, 1 / cell size}, photon count and table size. */
+int imbart_hashgrid_get_params(const imbart_hashgrid* grid, float* params10, int* n, int* table_size);
+
+/* Device arrays of the built grid: photons in bucket order (float4: xyz + index bits) and
+ * the inclusive bucket ends (table_size ints). */
+int imbart_hashgrid_get_arrays(const imbart_hashgrid* grid, const void** sorted, const int** cell_ends);
+
+/* ------------------------------------------------------------------------------------ */
 /* BVH construction (the builder side of the boundary)                                     */
 /* ------------------------------------------------------------------------------------ */
 

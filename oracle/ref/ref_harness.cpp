@@ -1,0 +1,333 @@
+// Harness around the reference's own C++ (compiled in place from the reference tree into
+// oracle/_ref/libref.so by oracle/ref/build_ref.py). TEST INFRASTRUCTURE ONLY: it runs the
+// reference's RNG, camera, ray generation, HashGrid, BVH builders/adapters, Scene and
+// integrators on the CPU to pin the oracle and to produce golden outputs. The traversal
+// behind the reference's traversal_gpu entry points is the oracle's CPU restatement
+// (oracle/traversal.c), since the reference's AnyDSL traversal library is not in its tree.
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "imbatracer/render/scene.h"
+#include "imbatracer/core/adapter.h"
+#include "imbatracer/loaders/loaders.h"
+#include "imbatracer/rangesearch/rangesearch.h"
+#include "imbatracer/render/integrators/pt.h"
+#include "imbatracer/render/ray_gen/camera.h"
+#include "imbatracer/render/ray_gen/ray_gen.h"
+#include "imbatracer/render/ray_gen/tile_gen.h"
+#include "imbatracer/render/random.h"
+#include "imbatracer/render/scheduling/tile_scheduler.h"
+
+uint64_t imbart_ref_seed_value = 0;
+uint64_t imbart_ref_seed_step = 0;
+int imbart_ref_tbb_threads = 1;
+
+// The oracle's two-wide traversal (oracle/traversal.c).
+extern "C" void oracle_trace_node2(int root, const void* nodes, const void* insts, const void* tris,
+                                   const int* indices, const void* texcoords, const void* masks, int n_masks,
+                                   const uint8_t* mask_buffer, const void* rays, void* hits, float* v_out,
+                                   int count, int any, int threads);
+
+namespace {
+int g_masks_active = 0;
+int g_n_masks = 0;
+int g_trace_threads = 1;
+}
+
+// The reference's GPU entry points, served on the CPU by the oracle.
+extern "C" void intersect_gpu_masked_instanced(int root, traversal_gpu::Node* nodes, traversal_gpu::InstanceNode* insts,
+                                               traversal_gpu::Vec4* tris, traversal_gpu::Ray* rays,
+                                               traversal_gpu::Hit* hits, int* indices, traversal_gpu::Vec2* texcoords,
+                                               traversal_gpu::TransparencyMask* masks, char* mask_buffer, int count) {
+    oracle_trace_node2(root, nodes, insts, tris, g_masks_active ? indices : nullptr, texcoords,
+                       g_masks_active ? masks : nullptr, g_n_masks, (const uint8_t*)mask_buffer, rays, hits, nullptr,
+                       count, 0, g_trace_threads);
+}
+extern "C" void occluded_gpu_masked_instanced(int root, traversal_gpu::Node* nodes, traversal_gpu::InstanceNode* insts,
+                                              traversal_gpu::Vec4* tris, traversal_gpu::Ray* rays,
+                                              traversal_gpu::Hit* hits, int* indices, traversal_gpu::Vec2* texcoords,
+                                              traversal_gpu::TransparencyMask* masks, char* mask_buffer, int count) {
+    oracle_trace_node2(root, nodes, insts, tris, g_masks_active ? indices : nullptr, texcoords,
+                       g_masks_active ? masks : nullptr, g_n_masks, (const uint8_t*)mask_buffer, rays, hits, nullptr,
+                       count, 1, g_trace_threads);
+}
+// The CPU-layout entry points are referenced by the reference's scheduler templates but
+// never reached: the harness always selects the GPU traversal path.
+extern "C" void intersect_cpu_masked_instanced(int, traversal_cpu::Node*, traversal_cpu::InstanceNode*,
+                                               traversal_cpu::Vec4*, traversal_cpu::Ray*, traversal_cpu::Hit* hits,
+                                               int*, traversal_cpu::Vec2*, traversal_cpu::TransparencyMask*, char*,
+                                               int count) {
+    for (int i = 0; i < count; ++i) hits[i].tri_id = -1;
+}
+extern "C" void occluded_cpu_masked_instanced(int, traversal_cpu::Node*, traversal_cpu::InstanceNode*,
+                                              traversal_cpu::Vec4*, traversal_cpu::Ray*, traversal_cpu::Hit* hits,
+                                              int*, traversal_cpu::Vec2*, traversal_cpu::TransparencyMask*, char*,
+                                              int count) {
+    for (int i = 0; i < count; ++i) hits[i].tri_id = -1;
+}
+
+// Loaders the reference's Scene links against; the harness never uses accel cache files.
+namespace imba {
+bool load_png(const Path&, Image&) { return false; }
+bool load_tga(const Path&, Image&) { return false; }
+bool load_hdr(const Path&, Image&) { return false; }
+}  // namespace imba
+
+using namespace imba;
+
+namespace {
+
+// Phong material for workloads that ask for one: a 50/50 mix of the reference's Phong and
+// Lambertian BxDFs (brdfs.h:8-91), built like GlossyMaterial (materials.h:151-189).
+class PhongMaterialRef : public Material {
+public:
+    PhongMaterialRef(float exponent, const rgb& spec, const rgb& diff) : exponent_(exponent), spec_(spec), diff_(diff) {}
+    Material* duplicate() const override { return new PhongMaterialRef(exponent_, spec_, diff_); }
+    BSDF* get_bsdf(const Intersection& isect, MemoryArena& arena, bool) const override {
+        auto a = arena.alloc<Phong>(spec_, exponent_);
+        auto b = arena.alloc<Lambertian>(diff_);
+        auto brdf = arena.alloc<CombineBxDF>(a, b);
+        return arena.alloc<BSDF>(isect, brdf, nullptr);
+    }
+
+private:
+    float exponent_;
+    rgb spec_, diff_;
+};
+
+struct RefScene {
+    Scene scene{false, true};
+    MaskBuffer masks;
+};
+
+float3 f3(const float* p) { return float3(p[0], p[1], p[2]); }
+
+}  // namespace
+
+extern "C" {
+
+void imbart_ref_set_seed(uint64_t value, uint64_t step) {
+    imbart_ref_seed_value = value;
+    imbart_ref_seed_step = step;
+}
+
+void imbart_ref_set_threads(int tbb_threads, int trace_threads) {
+    imbart_ref_tbb_threads = tbb_threads < 1 ? 1 : tbb_threads;
+    g_trace_threads = trace_threads < 1 ? 1 : trace_threads;
+}
+
+// MWC64X draws (random.h:15-47).
+void ref_rng_floats(uint64_t seed, int n, float* out) {
+    RNG rng(seed);
+    for (int i = 0; i < n; ++i) out[i] = rng.random_float();
+}
+
+void ref_rng_ints(uint64_t seed, int n, int lo, int hi, int* out) {
+    RNG rng(seed);
+    for (int i = 0; i < n; ++i) out[i] = rng.random_int(lo, hi);
+}
+
+// Camera samples of one frame through PixelRayGen::fill_queue (ray_gen.h:36-80) with the
+// path tracer's pixel sampling (pt.cpp:168-177) and PerspectiveCamera (camera.h:27-65).
+// Writes rays (8 floats), pixel ids, sample ids and the RNG state after sampling.
+int ref_camera_rays(int w, int h, int spp, const float* pos, const float* dir, const float* up, float fov,
+                    uint64_t seed_base, float* rays_out, int* pixel_ids, int* sample_ids, uint64_t* rng_states) {
+    PerspectiveCamera cam((float)w, (float)h, fov);
+    cam.move(f3(pos), f3(dir), f3(up));
+    const int n = w * h * spp;
+    RayQueue<PTState> q(n, false);
+    PixelRayGen<PTState> gen(w, h, spp);
+    gen.start_frame();
+    imbart_ref_set_seed(seed_base, 0);
+    gen.fill_queue(q, [&](int x, int y, ::Ray& ray_out, PTState& st) {
+        const float sx = static_cast<float>(x) + st.rng.random_float();
+        const float sy = static_cast<float>(y) + st.rng.random_float();
+        ray_out = cam.generate_ray(sx, sy);
+        st.throughput = rgb(1.0f);
+        st.bounces = 0;
+        st.last_specular = false;
+    });
+    if (q.size() != n) return -1;
+    std::memcpy(rays_out, q.rays(), sizeof(float) * 8 * n);
+    for (int i = 0; i < n; ++i) {
+        pixel_ids[i] = q.states()[i].pixel_id;
+        sample_ids[i] = q.states()[i].sample_id;
+        std::memcpy(rng_states + i, &q.states()[i].rng, sizeof(uint64_t));
+    }
+    return n;
+}
+
+// HashGrid::build + query (rangesearch.h:25-129) over n photons; output ids are the photons'
+// indices in the input, in the order the reference's query returns them.
+struct RefPhotonIn {
+    float3 p;
+    int id;
+    float3& position() { return p; }
+    const float3& position() const { return p; }
+};
+struct RefPhoton {
+    float3 position;
+    int id;
+    RefPhoton() {}
+    RefPhoton(const RefPhotonIn& in) : position(in.p), id(in.id) {}
+};
+
+int ref_hashgrid_query(const float* pos, int n, float radius, const float* queries, int nq, int k, int* out_ids,
+                       int* out_counts) {
+    std::vector<RefPhotonIn> ph(n);
+    for (int i = 0; i < n; ++i) { ph[i].p = float3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]); ph[i].id = i; }
+    HashGrid<std::vector<RefPhotonIn>::iterator, RefPhoton> grid;
+    grid.build(ph.begin(), ph.end(), radius);
+    std::vector<const RefPhoton*> out(k);
+    for (int q = 0; q < nq; ++q) {
+        const float3 qp(queries[3 * q], queries[3 * q + 1], queries[3 * q + 2]);
+        const int c = grid.query(qp, out, k);
+        out_counts[q] = c;
+        for (int j = 0; j < k; ++j) out_ids[(size_t)q * k + j] = j < c ? out[j]->id : -1;
+    }
+    return 0;
+}
+
+// Scene from arrays. Materials: kind per material (0 Lambert, 1 mirror, 2 glass, 3 glossy,
+// 4 phong, 5 emissive) and 16 parameters each: color[3], specular[3], exponent, eta, kappa,
+// emission[3]. Lights: 12 floats each (p0, p1, p2, intensity), world space. env: 3 floats or
+// NULL (a constant environment as a 1x1 EnvMap, listed before the triangle lights as the
+// reference's scene parser adds it).
+void* ref_scene_create(int n_meshes, const int* mesh_nverts, const int* mesh_ntris, const float* verts,
+                       const int* indices, const float* normals, const float* texcoords, const float* geom_normals,
+                       int n_inst, const int* inst_mesh, const float* inst_mats, int n_mats, const int* mat_kind,
+                       const float* mat_params, int n_lights, const float* lights, const float* env) {
+    RefScene* rs = new RefScene;
+    Scene& scene = rs->scene;
+    size_t vo = 0, io = 0;
+    for (int m = 0; m < n_meshes; ++m) {
+        scene.meshes().emplace_back();
+        Mesh& mesh = scene.meshes().back();
+        mesh.add_attribute(Mesh::AttributeType::FLOAT2);
+        mesh.add_attribute(Mesh::AttributeType::FLOAT3);
+        mesh.add_attribute(Mesh::AttributeType::FLOAT3, Mesh::AttributeBinding::PER_FACE);
+        mesh.set_index_count(4 * (size_t)mesh_ntris[m]);
+        mesh.set_vertex_count(mesh_nverts[m]);
+        for (int i = 0; i < 4 * mesh_ntris[m]; ++i) mesh.indices()[i] = (uint32_t)indices[io + i];
+        auto tc = mesh.attribute<float2>(MeshAttributes::TEXCOORDS);
+        auto nr = mesh.attribute<float3>(MeshAttributes::NORMALS);
+        auto gn = mesh.attribute<float3>(MeshAttributes::GEOM_NORMALS);
+        for (int v = 0; v < mesh_nverts[m]; ++v) {
+            const size_t g = vo + v;
+            mesh.vertices()[v] = float4(verts[3 * g], verts[3 * g + 1], verts[3 * g + 2], 1.0f);
+            tc[v] = float2(texcoords[2 * g], texcoords[2 * g + 1]);
+            nr[v] = float3(normals[3 * g], normals[3 * g + 1], normals[3 * g + 2]);
+        }
+        for (int t = 0; t < mesh_ntris[m]; ++t) {
+            const size_t g = io / 4 + t;
+            gn[t] = float3(geom_normals[3 * g], geom_normals[3 * g + 1], geom_normals[3 * g + 2]);
+        }
+        vo += mesh_nverts[m];
+        io += 4 * (size_t)mesh_ntris[m];
+        mesh.compute_bounding_box();
+    }
+    for (int i = 0; i < n_inst; ++i) {
+        const float* a = inst_mats + 16 * i;
+        float4x4 mat(float4(a[0], a[1], a[2], a[3]), float4(a[4], a[5], a[6], a[7]), float4(a[8], a[9], a[10], a[11]),
+                     float4(a[12], a[13], a[14], a[15]));
+        scene.instances().emplace_back(inst_mesh[i], mat);
+    }
+    if (env) {
+        Image img(1, 1);
+        img(0, 0) = float4(env[0], env[1], env[2], 1.0f);
+        scene.set_env_map(new EnvMap(img, 1.0f, scene.bounding_sphere()));
+        scene.lights().emplace_back(new EnvLight(scene.env_map(), scene.bounding_sphere()));
+    }
+    for (int m = 0; m < n_mats; ++m) {
+        const float* p = mat_params + 16 * m;
+        const rgb color(p[0], p[1], p[2]), spec(p[3], p[4], p[5]), emit(p[9], p[10], p[11]);
+        Material* mat = nullptr;
+        switch (mat_kind[m]) {
+            case 1: mat = new MirrorMaterial(p[7], p[8], color); break;
+            case 2: mat = new GlassMaterial(p[7], color, spec); break;
+            case 3: mat = new GlossyMaterial(p[6], spec, color); break;
+            case 4: mat = new PhongMaterialRef(p[6], spec, color); break;
+            default: mat = new DiffuseMaterial(color); break;
+        }
+        scene.materials().emplace_back(mat);
+        rs->masks.add_desc();
+    }
+    for (int l = 0; l < n_lights; ++l) {
+        const float* p = lights + 12 * l;
+        scene.lights().emplace_back(new TriangleLight(rgb(p[9], p[10], p[11]), f3(p), f3(p + 3), f3(p + 6)));
+    }
+    // Emitters of emissive materials: the area of the face in object space (build_scene.cpp:233).
+    io = 0;
+    for (int m = 0; m < n_meshes; ++m) {
+        const Mesh& mesh = scene.meshes()[m];
+        for (int t = 0; t < mesh_ntris[m]; ++t) {
+            const int mat = indices[io + 4 * t + 3];
+            if (mat_kind[mat] != 5) continue;
+            const float* p = mat_params + 16 * mat;
+            const Tri tri = mesh.triangle(t);
+            scene.material(mat)->set_emitter(new AreaEmitter(rgb(p[9], p[10], p[11]), tri.area()));
+        }
+        io += 4 * (size_t)mesh_ntris[m];
+    }
+    std::vector<std::string> names(n_meshes, "");
+    scene.build_mesh_accels(names);
+    scene.build_top_level_accel();
+    scene.compute_bounding_sphere();
+    scene.upload_mesh_accels();
+    scene.upload_top_level_accel();
+    scene.upload_mask_buffer(rs->masks);
+    return rs;
+}
+
+void ref_scene_destroy(void* h) { delete static_cast<RefScene*>(h); }
+
+// The reference-layout arrays the reference's adapters wrote (GPU two-wide layout).
+int ref_scene_gpu_layout(void* h, int* root, const void** nodes, const void** insts, const void** tris,
+                         int64_t* sizes) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    const auto& td = rs->scene.traversal_data_gpu();
+    *root = td.root;
+    *nodes = td.nodes.data();
+    *insts = td.instances.data();
+    *tris = td.tris.data();
+    sizes[0] = td.nodes.size();
+    sizes[1] = td.instances.size();
+    sizes[2] = td.tris.size();
+    return 0;
+}
+
+void ref_scene_bsphere(void* h, float* out4) {
+    const BSphere& s = static_cast<RefScene*>(h)->scene.bounding_sphere();
+    out4[0] = s.center.x; out4[1] = s.center.y; out4[2] = s.center.z; out4[3] = s.radius;
+}
+
+// One frame of the reference path tracer (pt.cpp) with the TileScheduler: one tile covering
+// the image (tile-local sample indices are then global, ray_gen.h:51-56), `threads` tile
+// threads, `spp` samples per pixel, seed_base for the frame's queue fill. image_out: w*h*3.
+int ref_render_pt(void* h, int w, int ht, const float* pos, const float* dir, const float* up, float fov, int spp,
+                  int max_path_len, uint64_t seed_base, float* image_out) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    PerspectiveCamera cam((float)w, (float)ht, fov);
+    cam.move(f3(pos), f3(dir), f3(up));
+    const int tile = w > ht ? w : ht;
+    DefaultTileGen<PTState> gen(w, ht, spp, tile);
+    TileScheduler<PTState, ShadowState, false> sched(gen, rs->scene, 1, 1, tile * tile * spp, true);
+    PathTracer pt(rs->scene, cam, sched, max_path_len);
+    AtomicImage img(w, ht);
+    img.clear();
+    imbart_ref_set_seed(seed_base, 0);
+    pt.render(img);
+    for (int i = 0; i < w * ht; ++i) {
+        image_out[3 * i + 0] = img.pixels()[i][0];
+        image_out[3 * i + 1] = img.pixels()[i][1];
+        image_out[3 * i + 2] = img.pixels()[i][2];
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+"""Python access to oracle/_ref/libref.so — the reference's own C++ built in place from its
+sources (oracle/ref/build_ref.py). TEST INFRASTRUCTURE ONLY: used to pin the oracle and to
+produce golden outputs; the product never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        lib = C.CDLL(LIB)
+        P, I, U64, F = C.c_void_p, C.c_int, C.c_uint64, C.c_float
+        sig = {
+            "imbart_ref_set_seed": (None, [U64, U64]),
+            "imbart_ref_set_threads": (None, [I, I]),
+            "ref_rng_floats": (None, [U64, I, P]),
+            "ref_rng_ints": (None, [U64, I, I, I, P]),
+            "ref_camera_rays": (I, [I, I, I, P, P, P, F, U64, P, P, P, P]),
+            "ref_hashgrid_query": (I, [P, I, F, P, I, I, P, P]),
+            "ref_scene_create": (P, [I, P, P, P, P, P, P, P, I, P, P, I, P, P, I, P, P]),
+            "ref_scene_destroy": (None, [P]),
+            "ref_scene_gpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
+            "ref_scene_bsphere": (None, [P, P]),
+            "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def rng_floats(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    load().ref_rng_floats(seed & (2 ** 64 - 1), n, _p(out))
+    return out
+
+
+def rng_ints(seed: int, n: int, lo: int, hi: int) -> np.ndarray:
+    out = np.zeros(n, np.int32)
+    load().ref_rng_ints(seed & (2 ** 64 - 1), n, lo, hi, _p(out))
+    return out
+
+
+def camera_rays(w, h, spp, pos, dir, up, fov, seed_base):
+    n = w * h * spp
+    rays = np.zeros((n, 8), np.float32)
+    pid = np.zeros(n, np.int32)
+    sid = np.zeros(n, np.int32)
+    st = np.zeros(n, np.uint64)
+    f = lambda v: np.ascontiguousarray(np.asarray(v, np.float32))
+    rc = load().ref_camera_rays(w, h, spp, _p(f(pos)), _p(f(dir)), _p(f(up)), fov, seed_base, _p(rays), _p(pid),
+                                _p(sid), _p(st))
+    assert rc == n
+    return rays, pid, sid, st
+
+
+def hashgrid_query(pos, radius, queries, k):
+    pos = np.ascontiguousarray(pos, np.float32)
+    q = np.ascontiguousarray(queries, np.float32)
+    ids = np.zeros((len(q), k), np.int32)
+    cnt = np.zeros(len(q), np.int32)
+    load().ref_hashgrid_query(_p(pos), len(pos), radius, _p(q), len(q), k, _p(ids), _p(cnt))
+    return ids, cnt
+
+
+def material_arrays(materials):
+    kinds = np.array([m.kind for m in materials], np.int32)
+    prm = np.zeros((len(materials), 16), np.float32)
+    for i, m in enumerate(materials):
+        prm[i, 0:3] = m.color
+        prm[i, 3:6] = m.specular
+        prm[i, 6] = m.exponent
+        prm[i, 7] = m.eta
+        prm[i, 8] = m.kappa
+        prm[i, 9:12] = m.emission
+    return kinds, prm
+
+
+class RefScene:
+    """The reference's Scene built from a SceneDesc with the reference's adapters (SBVH
+    bottom level, binned top level) into its GPU two-wide layout."""
+
+    def __init__(self, desc):
+        self.desc = desc
+        meshes = desc.meshes
+        nv = np.array([len(m.vertices) for m in meshes], np.int32)
+        nt = np.array([m.triangle_count for m in meshes], np.int32)
+        verts = np.ascontiguousarray(np.concatenate([m.vertices for m in meshes]).astype(np.float32))
+        idx = np.ascontiguousarray(np.concatenate([m.indices.reshape(-1) for m in meshes]).astype(np.int32))
+        nrm = np.ascontiguousarray(np.concatenate([m.normals for m in meshes]).astype(np.float32))
+        tc = np.ascontiguousarray(np.concatenate([m.texcoords for m in meshes]).astype(np.float32))
+        gn = np.ascontiguousarray(np.concatenate([m.geom_normals for m in meshes]).astype(np.float32))
+        im = np.array([i.mesh_id for i in desc.instances], np.int32)
+        mats = np.ascontiguousarray(np.stack([i.mat.reshape(-1) for i in desc.instances]).astype(np.float32))
+        kinds, prm = material_arrays(desc.materials)
+        lights = np.zeros((max(len(desc.lights), 1), 12), np.float32)
+        for i, (p0, p1, p2, e) in enumerate(desc.lights):
+            lights[i] = np.concatenate([p0, p1, p2, e])
+        env = None if desc.env_intensity is None else np.array(desc.env_intensity, np.float32)
+        self._keep = (nv, nt, verts, idx, nrm, tc, gn, im, mats, kinds, prm, lights, env)
+        self.handle = load().ref_scene_create(len(meshes), _p(nv), _p(nt), _p(verts), _p(idx), _p(nrm), _p(tc),
+                                              _p(gn), len(im), _p(im), _p(mats), len(kinds), _p(kinds), _p(prm),
+                                              len(desc.lights), _p(lights), _p(env))
+        assert self.handle
+
+    def gpu_layout(self):
+        """(root, nodes, instances, tris) copies of the reference adapters' output."""
+        from imbatracer_b200.native import INST_DTYPE, NODE2_DTYPE
+        root = C.c_int(0)
+        pn, pi, pt = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        sizes = np.zeros(3, np.int64)
+        load().ref_scene_gpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt), _p(sizes))
+
+        def grab(ptr, n, dtype):
+            buf = (C.c_char * (int(n) * dtype.itemsize)).from_address(ptr)
+            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+
+        # The reference over-allocates the node array (scene.cpp:14): keep the reachable range.
+        nodes = grab(pn.value, sizes[0], NODE2_DTYPE)
+        insts = grab(pi.value, sizes[1], INST_DTYPE)
+        tris = grab(pt.value, sizes[2], np.dtype((np.float32, 4)))
+        return root.value, nodes, insts, tris
+
+    def render_pt(self, w, h, spp, max_path_len, seed_base, cam=None):
+        cam = cam or self.desc.camera
+        img = np.zeros((h, w, 3), np.float32)
+        f = lambda v: np.ascontiguousarray(np.asarray(v, np.float32))
+        rc = load().ref_render_pt(self.handle, w, h, _p(f(cam.pos)), _p(f(cam.dir)), _p(f(cam.up)), cam.fov, spp,
+                                  max_path_len, seed_base, _p(img))
+        assert rc == 0
+        return img
+
+    def close(self):
+        if self.handle:
+            load().ref_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

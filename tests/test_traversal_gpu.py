@@ -125,6 +125,34 @@ def test_dropin_device_entry_points(cuda):
     lib.imbart_invalidate_scenes()
 
 
+@pytest.mark.skipif(not __import__("oracle.refwrap", fromlist=["x"]).available(), reason="oracle/_ref not built")
+def test_dropin_with_reference_sbvh_layout(cuda):
+    """The reference's own SBVH/binned adapters' output, uploaded to device buffers the way
+    Scene::upload_* does, traced through intersect_gpu_masked_instanced."""
+    import torch
+    from tests.test_reference_pins import ref_traversal_data
+    td = ref_traversal_data(H.scene_desc("config1"))
+    lib = N.load()
+    lib.imbart_invalidate_scenes()
+    dev = torch.device("cuda:0")
+    bufs = [to_dev(a, torch, dev) for a in (td.nodes, td.instances, td.tris, td.indices, td.texcoords, td.masks,
+                                            td.mask_buffer)]
+    rays = H.ray_set("config1", 30000, seed=12)
+    count = (len(rays) + 63) // 64 * 64
+    padded = np.zeros(count, N.RAY_DTYPE)
+    padded[: len(rays)] = rays
+    d_rays = to_dev(padded, torch, dev)
+    d_hits = torch.zeros(count * 16, dtype=torch.uint8, device=dev)
+    lib.imbart_clear_error()
+    lib.intersect_gpu_masked_instanced(td.root, N.ptr(bufs[0]), N.ptr(bufs[1]), N.ptr(bufs[2]), N.ptr(d_rays),
+                                       N.ptr(d_hits), N.ptr(bufs[3]), N.ptr(bufs[4]), N.ptr(bufs[5]), N.ptr(bufs[6]),
+                                       count)
+    assert N.last_error()[0] == 0, N.last_error()
+    hits = d_hits.cpu().numpy().view(N.HIT_DTYPE)
+    assert H.hits_equal(O.trace_node2(td, padded), hits).all()
+    lib.imbart_invalidate_scenes()
+
+
 def test_host_buffer_trace(cuda):
     td = H.traversal_data("config2")
     ds = S.DeviceScene(td)
