@@ -18,8 +18,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES_CU = ["trace.cu", "hashgrid.cu"]
-SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp"]
+SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu"]
+SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp"]
+# Shading and sample generation mirror the reference's separately rounded single-precision
+# arithmetic: no fused multiply-add in device code, no contraction in the host camera set-up.
+# (The traversal kernels spell out their rounding with intrinsics and keep FMA elsewhere.)
+EXTRA_FLAGS = {"wavefront.cu": ["-fmad=false"], "camera.cpp": ["-Xcompiler", "-ffp-contract=off"]}
 
 
 def nvcc() -> str:
@@ -51,12 +55,13 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     inc = ["-I", CSRC, "-I", os.path.join(HERE, "..", "include")]
     for src in SOURCES_CU:
         obj = os.path.join(objdir, src + ".o")
-        extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+        extra = (["-Xptxas", "-v"] if ptxas_verbose else []) + EXTRA_FLAGS.get(src, [])
         _run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj], verbose)
         objs.append(obj)
     for src in SOURCES_CPP:
         obj = os.path.join(objdir, src + ".o")
-        _run([nvcc(), *NVCC_FLAGS, *inc, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+        _run([nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src, []), *inc, "-x", "c++", "-c", os.path.join(CSRC, src), "-o",
+              obj], verbose)
         objs.append(obj)
     out = lib_path()
     tmp = out + ".tmp"

@@ -89,6 +89,11 @@ void attach_masks(HostWideScene& out, const int* indices, int n_indices,
 // Thread-local error reporting (error.cpp).
 void set_error(int code, const std::string& msg);
 
+// Stream-ordered traversal launch used by the wavefront integrators (trace.cu). `stream` is
+// a cudaStream_t; rays are imbart_ray records, hits imbart_hit records.
+int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
+                          int flags, void* stream, unsigned long long* stats);
+
 inline int float_bits(float f) { union { float f; int i; } u; u.f = f; return u.i; }
 inline float bits_float(int i) { union { float f; int i; } u; u.i = i; return u.f; }
 

@@ -1,0 +1,476 @@
+// Device restatement of the reference's shading math, used by the wavefront integrators.
+// Compiled with -fmad=false: every + - * / rounds separately, as in the reference's x86-64
+// SSE build. Where the reference passes two rng.random_float() calls as arguments of one
+// call, the reference build (g++) evaluated the RIGHT argument first; the draws below are
+// taken in that order (checked against the reference itself).
+//
+//   vectors, dot, cross, normalize           core/float3.h, core/float4.h, core/common.h
+//   local_coordinates, samplers, RR          render/random.h:57-188
+//   calculate_intersection                   render/integrators/integrator.h:71-123
+//   BSDF frame, lobe choice, eval/pdf         render/materials/bsdf.h:125-238
+//   Lambertian, SpecularReflection, Phong,   render/materials/brdfs.h:8-227
+//   CookTorrance
+//   SpecularTransmission                      render/materials/btdfs.h:6-65
+//   Fresnel                                   render/materials/fresnel.h:7-75
+//   materials (Diffuse, Mirror, Glass, Glossy) render/materials/materials.h:62-189
+//   AreaEmitter, TriangleLight, EnvMap/Light  render/light.h:14-190, 361-544
+#pragma once
+
+#include <cfloat>
+#include <stdint.h>
+
+#include "rng.cuh"
+
+namespace imbart {
+namespace sh {
+
+constexpr float kPi = 3.14159265359f;
+
+struct V3 {
+    float x, y, z;
+    __device__ V3() {}
+    __device__ V3(float a, float b, float c) : x(a), y(b), z(c) {}
+    __device__ explicit V3(float a) : x(a), y(a), z(a) {}
+    __device__ float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 operator-(V3 a) { return V3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ V3 operator*(V3 a, V3 b) { return V3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ V3 operator*(float a, V3 b) { return V3(a * b.x, a * b.y, a * b.z); }
+__device__ __forceinline__ V3 operator*(V3 a, float b) { return V3(a.x * b, a.y * b, a.z * b); }
+__device__ __forceinline__ V3 operator/(V3 a, float b) { return V3(a.x / b, a.y / b, a.z / b); }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return V3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float length(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 normalize(V3 a) { return a * (1.0f / length(a)); }
+__device__ __forceinline__ float sqr(float x) { return x * x; }
+__device__ __forceinline__ float smin(float a, float b) { return (b < a) ? b : a; }   // std::min
+__device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a; }   // std::max
+__device__ __forceinline__ float clampf(float a, float lo, float hi) { return (a < lo) ? lo : ((a > hi) ? hi : a); }
+__device__ __forceinline__ bool is_black(V3 c) { return c.x <= 0.0f && c.y <= 0.0f && c.z <= 0.0f; }
+__device__ __forceinline__ float luminance(V3 c) { return dot(c, V3(0.2126f, 0.7152f, 0.0722f)); }
+
+// random.h:57-72
+__device__ __forceinline__ void local_coordinates(V3 n, V3& tangent, V3& binormal) {
+    const bool xy = fabsf(n.x) > fabsf(n.y);
+    const int id0 = xy ? 0 : 1;
+    const float sig = xy ? -1.0f : 1.0f;
+    const float n0 = id0 == 0 ? n.x : n.y;
+    const float inv_len = 1.0f / sqrtf(sqr(n0) + sqr(n.z));
+    float t[3];
+    t[id0] = n.z * sig * inv_len;
+    t[1 - id0] = 0.0f;
+    t[2] = n0 * -1.0f * sig * inv_len;
+    tangent = V3(t[0], t[1], t[2]);
+    binormal = cross(n, tangent);
+    tangent = normalize(tangent);
+    binormal = normalize(binormal);
+}
+
+__device__ __forceinline__ V3 spherical_dir(float sin_t, float cos_t, float phi) {
+    return V3(sin_t * cosf(phi), sin_t * sinf(phi), cos_t);
+}
+
+// sample_cos_hemisphere(u1, u2) (random.h:81-84); returns pdf in *pdf.
+__device__ __forceinline__ V3 sample_cos_hemisphere(float u1, float u2, float* pdf) {
+    const V3 d = spherical_dir(sqrtf(1 - u2), sqrtf(u2), 2.f * kPi * u1);
+    *pdf = d.z / kPi;
+    return d;
+}
+__device__ __forceinline__ float cos_hemisphere_pdf(float c) { return fabsf(c) / kPi; }
+
+__device__ __forceinline__ V3 sample_power_cos_hemisphere(float power, float u1, float u2, float* pdf) {
+    const float phi = kPi * 2.0f * u1;
+    const float cos_t = powf(u2, 1.0f / (power + 1.0f));
+    const float sin_t = sqrtf(1.0f - sqr(cos_t));
+    const V3 d = spherical_dir(sin_t, cos_t, phi);
+    *pdf = (power + 1.0f) * powf(cos_t, power) * 1.0f / (2.0f * kPi);
+    return d;
+}
+__device__ __forceinline__ float power_cos_hemisphere_pdf(float power, float c) {
+    return c > 0.0f ? ((power + 1.0f) * powf(c, power) * 1.0f / (2.0f * kPi)) : 0.0f;
+}
+
+// Two draws passed as (u1, u2) in the reference: the second argument is drawn first.
+__device__ __forceinline__ void draw2(Rng& rng, float& u1, float& u2) {
+    u2 = rng.next_float();
+    u1 = rng.next_float();
+}
+
+// ---------------------------------------------------------------------------------------
+// Scene data for shading
+// ---------------------------------------------------------------------------------------
+enum MaterialKind { kLambert = 0, kMirror = 1, kGlass = 2, kGlossy = 3, kPhong = 4, kEmissive = 5 };
+
+struct Material {
+    int kind;
+    float color[3];     // diffuse colour / mirror scale / glass transmittance
+    float spec[3];      // glossy & phong specular colour / glass reflectance
+    float exponent;
+    float eta, kappa;
+    float emission[3];  // area emitter intensity
+    float area;         // area of the emissive face (object space)
+};
+
+struct TriLight {
+    float v[3][3];
+    float normal[3], tangent[3], binormal[3];
+    float area;
+    float intensity[3];
+};
+
+struct ShadingScene {
+    const float* vertices;      // 3 floats per global vertex
+    const float* normals;       // 3 floats per global vertex
+    const float* texcoords;     // 2 floats per global vertex
+    const int4* tris;           // global vertex indices + material, per global triangle
+    const float* geom_normals;  // 3 floats per global triangle
+    const float* inst_inv;      // 12 floats (3x4 row-major world-to-object) per instance
+    const Material* materials;
+    const TriLight* lights;     // triangle lights, in light-list order after the environment
+    int n_tri_lights;
+    int light_count;            // environment (if any) + triangle lights
+    int has_env;
+    float env_color[3];         // intensity * constant environment colour
+    float bsphere[5];           // centre xyz, radius, 1/radius^2
+};
+
+// ---------------------------------------------------------------------------------------
+// Intersection (integrator.h:71-123)
+// ---------------------------------------------------------------------------------------
+struct Isect {
+    V3 pos, out_dir, normal, geom_normal, u_tangent, v_tangent;
+    float uv[2];
+    int mat;
+};
+
+__device__ __forceinline__ V3 load3(const float* p, int i) { return V3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+__device__ __forceinline__ Isect calculate_intersection(const ShadingScene& s, int tri_id, int inst_id, float tmax,
+                                                         float hit_u, V3 org, V3 out_dir) {
+    const int4 t = s.tris[tri_id];
+    const float* m = s.inst_inv + 12 * inst_id;
+    Isect r;
+    r.mat = t.w;
+    const V3 pos = org + tmax * out_dir;
+    // local_pos = inv_mat * float4(pos, 1) (float3x4.h:36-40)
+    const V3 lp(m[0] * pos.x + m[1] * pos.y + m[2] * pos.z + m[3] * 1.0f,
+                m[4] * pos.x + m[5] * pos.y + m[6] * pos.z + m[7] * 1.0f,
+                m[8] * pos.x + m[9] * pos.y + m[10] * pos.z + m[11] * 1.0f);
+    const float u = hit_u;
+    const V3 v0 = load3(s.vertices, t.x);
+    const V3 e1 = load3(s.vertices, t.y) - v0;
+    const V3 e2 = load3(s.vertices, t.z) - v0;
+    const float v = dot(lp - v0 - u * e1, e2) / dot(e2, e2);
+    const float w0 = 1 - u - v;
+    r.uv[0] = s.texcoords[2 * t.x] * w0 + s.texcoords[2 * t.y] * u + s.texcoords[2 * t.z] * v;
+    r.uv[1] = s.texcoords[2 * t.x + 1] * w0 + s.texcoords[2 * t.y + 1] * u + s.texcoords[2 * t.z + 1] * v;
+    const V3 ln = load3(s.normals, t.x) * w0 + load3(s.normals, t.y) * u + load3(s.normals, t.z) * v;
+    // float3 * float3x4 (float3x4.h:43-48): the transposed product, used for normals.
+    auto tmul = [&](V3 a) {
+        return V3(m[0] * a.x + m[4] * a.y + m[8] * a.z, m[1] * a.x + m[5] * a.y + m[9] * a.z,
+                  m[2] * a.x + m[6] * a.y + m[10] * a.z);
+    };
+    r.normal = normalize(tmul(ln));
+    r.geom_normal = normalize(tmul(load3(s.geom_normals, tri_id)));
+    r.out_dir = -normalize(out_dir);
+    r.pos = pos;
+    local_coordinates(r.normal, r.u_tangent, r.v_tangent);
+    if (dot(r.geom_normal, r.normal) < 0.0f) r.normal = -r.normal;
+    return r;
+}
+
+// ---------------------------------------------------------------------------------------
+// BxDFs in shading space (normal = z)
+// ---------------------------------------------------------------------------------------
+enum Flags { kNone = 0, kRefl = 1, kTrans = 2, kDiffuse = 4, kGlossyF = 8, kSpecular = 16 };
+
+__device__ __forceinline__ bool same_hemisphere(V3 a, V3 b) { return a.z * b.z > 0.0f; }
+
+__device__ __forceinline__ float fresnel_conductor(float cosi, float eta, float kappa) {
+    const float ekc = (eta * eta + kappa * kappa) * cosi * cosi;
+    const float par = (ekc - (2.f * eta * cosi) + 1) / (ekc + (2.f * eta * cosi) + 1);
+    const float ek = eta * eta + kappa * kappa;
+    const float perp = (ek - (2.f * eta * cosi) + cosi * cosi) / (ek + (2.f * eta * cosi) + cosi * cosi);
+    return (par + perp) / 2.f;
+}
+
+__device__ __forceinline__ float fresnel_dielectric_eval(float cosi, float eta_outside, float eta_inside) {
+    float eta_in = eta_outside, eta_trans = eta_inside;
+    if (cosi <= 0.0f) { const float t = eta_in; eta_in = eta_trans; eta_trans = t; }
+    const float sin_trans = eta_in / eta_trans * sqrtf(smax(0.0f, 1.0f - sqr(cosi)));
+    if (sin_trans >= 1.0f) return 1.0f;
+    const float cos_trans = sqrtf(smax(0.0f, 1.0f - sqr(sin_trans)));
+    const float ci = fabsf(cosi);
+    const float par = (eta_trans * ci - eta_in * cos_trans) / (eta_trans * ci + eta_in * cos_trans);
+    const float perp = (eta_in * ci - eta_trans * cos_trans) / (eta_in * ci + eta_trans * cos_trans);
+    return (par * par + perp * perp) / 2.f;
+}
+
+// Lambertian (brdfs.h:8-21)
+__device__ __forceinline__ V3 lambert_eval(const float* c, V3 o, V3 i) {
+    return same_hemisphere(o, i) ? V3(c[0], c[1], c[2]) * (1.0f / kPi) : V3(0.0f);
+}
+__device__ __forceinline__ float default_pdf(V3 o, V3 i) { return same_hemisphere(o, i) ? cos_hemisphere_pdf(i.z) : 0.0f; }
+// BxDF::sample default (bsdf.h:54-64)
+__device__ __forceinline__ V3 lambert_sample(const float* c, V3 o, V3& in, Rng& rng, float* pdf) {
+    float u1, u2;
+    draw2(rng, u1, u2);
+    in = sample_cos_hemisphere(u1, u2, pdf);
+    if (o.z < 0.0f) in.z = -in.z;
+    return lambert_eval(c, o, in);
+}
+
+// Phong (brdfs.h:48-91)
+__device__ __forceinline__ V3 phong_eval(const float* c, float e, V3 o, V3 i) {
+    const V3 ri(-i.x, -i.y, i.z);
+    float cos_r_o = smax(0.0f, dot(ri, o));
+    cos_r_o = smin(cos_r_o, 1.0f);
+    return same_hemisphere(o, i) ? (e + 2.0f) / (2.0f * kPi) * V3(c[0], c[1], c[2]) * powf(cos_r_o, e) : V3(0.0f);
+}
+__device__ __forceinline__ V3 phong_sample(const float* c, float e, V3 o, V3& in, Rng& rng, float* pdf) {
+    float u1, u2;
+    draw2(rng, u1, u2);
+    float p;
+    const V3 d = sample_power_cos_hemisphere(e, u1, u2, &p);
+    const V3 ri(-o.x, -o.y, o.z);
+    V3 rt, rb;
+    local_coordinates(ri, rt, rb);
+    in = V3(rb.x * d.x + rt.x * d.y + ri.x * d.z, rb.y * d.x + rt.y * d.y + ri.y * d.z,
+            rb.z * d.x + rt.z * d.y + ri.z * d.z);
+    *pdf = p;
+    return same_hemisphere(o, in) ? phong_eval(c, e, o, in) : V3(0.0f);
+}
+__device__ __forceinline__ float phong_pdf(float e, V3 o, V3 i) { return power_cos_hemisphere_pdf(e, i.z); }
+
+// CookTorrance with Blinn distribution (brdfs.h:147-227); Fresnel = conductor(1, exponent)
+// as GlossyMaterial builds it (materials.h:179).
+__device__ __forceinline__ float abs_cos(V3 d) { return fabsf(d.z); }
+__device__ __forceinline__ V3 ct_eval(const float* c, float e, V3 o, V3 i) {
+    if (abs_cos(o) == 0.0f || abs_cos(i) == 0.0f) return V3(0.0f);
+    const V3 h = normalize(i + o);
+    const float cos_half = dot(i, h);
+    const float fr = fresnel_conductor(cos_half, 1.0f, e);
+    if (!same_hemisphere(o, i)) return V3(0.0f);
+    const float D = (e + 2.0f) / (2.0f * kPi) * powf(abs_cos(h), e);
+    const float out_dot_half = dot(o, h);
+    const float G = smin(1.0f, smin(2.0f * abs_cos(h) * abs_cos(o) / out_dot_half,
+                                    2.0f * abs_cos(h) * abs_cos(i) / out_dot_half));
+    return (V3(c[0], c[1], c[2]) * D * G * fr) / (4.0f * abs_cos(i) * abs_cos(o));
+}
+__device__ __forceinline__ V3 ct_sample(const float* c, float e, V3 o, V3& in, Rng& rng, float* pdf) {
+    float r1, r2;
+    draw2(rng, r1, r2);
+    const float c_theta = powf(r1, 1.0f / (e + 1.0f));
+    const float s_theta = sqrtf(smax(0.0f, 1.0f - sqr(c_theta)));
+    const float phi = r2 * 2.0f * kPi;
+    V3 h = spherical_dir(s_theta, c_theta, phi);
+    if (!same_hemisphere(o, h)) h = -h;
+    in = -o + 2.0f * dot(o, h) * h;
+    if (dot(o, h) <= 0.0f) *pdf = 1.0f;
+    else *pdf = (e + 1.0f) * powf(c_theta, e) / (2.0f * kPi * 4.0f * dot(o, h));
+    return same_hemisphere(o, in) ? ct_eval(c, e, o, in) : V3(0.0f);
+}
+__device__ __forceinline__ float ct_pdf(float e, V3 o, V3 i) {
+    if (!same_hemisphere(o, i)) return 0.0f;
+    const V3 h = normalize(i + o);
+    if (dot(o, h) <= 0.0f) return 0.0f;
+    return (e + 1.0f) * powf(abs_cos(h), e) / (2.0f * kPi * 4.0f * dot(o, h));
+}
+
+// ---------------------------------------------------------------------------------------
+// BSDF (bsdf.h:125-238) for the material kinds
+// ---------------------------------------------------------------------------------------
+struct Bsdf {
+    const Material* m;
+    V3 n, ut, vt, gn;
+    __device__ V3 to_local(V3 d) const { return V3(dot(vt, d), dot(ut, d), dot(n, d)); }
+    __device__ V3 to_world(V3 d) const {
+        return V3(vt.x * d.x + ut.x * d.y + n.x * d.z, vt.y * d.x + ut.y * d.y + n.y * d.z,
+                  vt.z * d.x + ut.z * d.y + n.z * d.z);
+    }
+    __device__ bool has_btdf() const { return m->kind == kGlass; }
+    __device__ int brdf_flags() const {
+        switch (m->kind) {
+            case kMirror: case kGlass: return kSpecular | kRefl;
+            case kGlossy: case kPhong: return kGlossyF | kRefl | kDiffuse;
+            default: return kDiffuse | kRefl;
+        }
+    }
+    __device__ V3 brdf_eval(V3 o, V3 i) const {
+        switch (m->kind) {
+            case kMirror: case kGlass: return V3(0.0f);
+            case kGlossy: return 0.5f * (ct_eval(m->spec, m->exponent, o, i) + lambert_eval(m->color, o, i));
+            case kPhong: return 0.5f * (phong_eval(m->spec, m->exponent, o, i) + lambert_eval(m->color, o, i));
+            default: return lambert_eval(m->color, o, i);
+        }
+    }
+    __device__ float brdf_pdf(V3 o, V3 i) const {
+        switch (m->kind) {
+            case kMirror: case kGlass: return 0.0f;
+            case kGlossy: return (ct_pdf(m->exponent, o, i) + default_pdf(o, i)) * 0.5f;
+            case kPhong: return (phong_pdf(m->exponent, o, i) + default_pdf(o, i)) * 0.5f;
+            default: return default_pdf(o, i);
+        }
+    }
+    __device__ V3 eval(V3 out_dir, V3 in_dir) const {
+        const V3 lo = to_local(out_dir), li = to_local(in_dir);
+        if (dot(in_dir, gn) * dot(out_dir, gn) <= 0.0f) return V3(0.0f);   // BTDFs are all specular: eval 0
+        return brdf_eval(lo, li);
+    }
+    __device__ float pdf(V3 out_dir, V3 in_dir) const {
+        const V3 lo = to_local(out_dir), li = to_local(in_dir);
+        if (dot(in_dir, gn) * dot(out_dir, gn) <= 0.0f) return 0.0f;
+        return brdf_pdf(lo, li);
+    }
+    // Samples a direction; returns the BSDF value, sets in_dir, pdf and sampled flags.
+    __device__ V3 sample(V3 out_dir, V3& in_dir, Rng& rng, int& flags, float& pdf) const {
+        const V3 lo = to_local(out_dir);
+        float btdf_prob = 0.0f;
+        if (has_btdf()) btdf_prob = 1.0f - fresnel_dielectric_eval(lo.z, 1.0f, m->eta);   // importance()
+        const float rnd = rng.next_float();
+        const bool use_btdf = rnd < btdf_prob;
+        const float component_pdf = use_btdf ? btdf_prob : 1.0f - btdf_prob;
+        V3 li, value;
+        int f;
+        if (use_btdf) {
+            // SpecularTransmission<false>(eta_inside = eta, eta_outside = 1) (btdfs.h:19-48)
+            f = kTrans | kSpecular;
+            pdf = 1.0f;
+            float eta_in = 1.0f, eta_trans = m->eta;
+            const bool entering = lo.z > 0.0f;
+            if (!entering) { const float t = eta_in; eta_in = eta_trans; eta_trans = t; }
+            const float sin_in_sqr = smax(0.0f, 1.0f - sqr(lo.z));
+            const float eta_frac = eta_in / eta_trans;
+            const float sin_trans_sqr = sqr(eta_frac) * sin_in_sqr;
+            if (sin_trans_sqr >= 1.0f) {
+                li = V3(-lo.x, -lo.y, lo.z);
+                value = V3(0.0f);
+            } else {
+                float cos_trans = sqrtf(smax(0.0f, 1.0f - sin_trans_sqr));
+                if (entering) cos_trans = -cos_trans;
+                li = V3(eta_frac * -lo.x, eta_frac * -lo.y, cos_trans);
+                const float fr = fresnel_dielectric_eval(lo.z, 1.0f, m->eta);
+                const float factor = sqr(eta_in / eta_trans);
+                value = factor * (1.0f - fr) * V3(m->color[0], m->color[1], m->color[2]) / fabsf(li.z);
+            }
+        } else {
+            f = brdf_flags();
+            switch (m->kind) {
+                case kMirror: case kGlass: {
+                    // SpecularReflection (brdfs.h:23-46)
+                    li = V3(-lo.x, -lo.y, lo.z);
+                    pdf = 1.0f;
+                    const float fr = m->kind == kMirror ? fresnel_conductor(lo.z, m->eta, m->kappa)
+                                                        : fresnel_dielectric_eval(lo.z, 1.0f, m->eta);
+                    const float* sc = m->kind == kMirror ? m->color : m->spec;
+                    value = fr * V3(sc[0], sc[1], sc[2]) / fabsf(li.z);
+                    break;
+                }
+                case kGlossy: case kPhong: {
+                    // CombineBxDF::sample (bsdf.h:84-86): one draw picks the lobe; the sampled
+                    // flags stay the union of both lobes' (bsdf.h:76, 185).
+                    const bool first = rng.next_float() < 0.5f;
+                    if (first) {
+                        value = m->kind == kGlossy ? ct_sample(m->spec, m->exponent, lo, li, rng, &pdf)
+                                                   : phong_sample(m->spec, m->exponent, lo, li, rng, &pdf);
+                    } else {
+                        value = lambert_sample(m->color, lo, li, rng, &pdf);
+                    }
+                    break;
+                }
+                default:
+                    value = lambert_sample(m->color, lo, li, rng, &pdf);
+                    break;
+            }
+        }
+        if (pdf == 0.0f) { flags = kNone; return V3(0.0f); }
+        flags = f;
+        in_dir = to_world(li);
+        pdf *= component_pdf;
+        const float side = dot(in_dir, gn) * dot(out_dir, gn);
+        if ((!use_btdf && side <= 0.0f) || (use_btdf && side >= 0.0f)) { flags = kNone; return V3(0.0f); }
+        return value;
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Lights
+// ---------------------------------------------------------------------------------------
+struct DirectSample {
+    V3 dir;
+    float distance;
+    V3 radiance;
+    float pdf_direct_w;
+    bool delta;
+};
+
+// TriangleLight::sample_direct (light.h:142-175)
+__device__ __forceinline__ DirectSample tri_light_sample(const TriLight& L, V3 from, Rng& rng) {
+    DirectSample s;
+    float r1, r2;
+    draw2(rng, r1, r2);
+    const float sr = sqrtf(r1);
+    const float u = 1.0f - sr, v = r2 * sr;
+    const V3 p0(L.v[0][0], L.v[0][1], L.v[0][2]), p1(L.v[1][0], L.v[1][1], L.v[1][2]), p2(L.v[2][0], L.v[2][1], L.v[2][2]);
+    const V3 pos = u * p0 + v * p1 + (1.0f - u - v) * p2;
+    V3 d = pos - from;
+    const float distsq = dot(d, d);
+    s.distance = sqrtf(distsq);
+    s.dir = d * (1.0f / s.distance);
+    const V3 n(L.normal[0], L.normal[1], L.normal[2]);
+    const float cos_out = dot(n, -1.0f * s.dir);
+    if (cos_out > 0.0f && cos_out < 1.0f) {
+        s.radiance = V3(L.intensity[0], L.intensity[1], L.intensity[2]) * cos_out * (L.area / distsq);
+        s.pdf_direct_w = 1.0f / L.area * distsq / cos_out;
+    } else {
+        s.radiance = V3(0.0f);
+        s.pdf_direct_w = 1.0f;
+    }
+    s.delta = false;
+    return s;
+}
+
+// EnvLight::sample_direct with a constant 1x1 map (light.h:446-485, 525-539).
+__device__ __forceinline__ DirectSample env_light_sample(const ShadingScene& sc, Rng& rng) {
+    DirectSample s;
+    float pdf = 1.0f / float(1 * 1);
+    const float ux = rng.next_float();
+    const float uy = rng.next_float();
+    pdf *= float(1 * 1);
+    const V3 color(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    const float theta = kPi * uy;
+    const float sin_theta = sinf(theta);
+    const float phi = 2.0f * kPi * ux;
+    s.dir = V3(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+    if (sin_theta != 0.0f) pdf /= 2.0f * kPi * kPi * sin_theta;
+    else pdf = 0.0f;
+    s.distance = FLT_MAX;
+    s.radiance = color / pdf;
+    s.pdf_direct_w = pdf;
+    s.delta = false;
+    return s;
+}
+
+// EnvMap::radiance with a constant map (light.h:413-424): pdf_direct_w = 1 / (2 pi^2 sin t).
+__device__ __forceinline__ V3 env_radiance(const ShadingScene& sc, V3 out_dir, float* pdf_direct_w) {
+    float phi = atan2f(out_dir.x, out_dir.z);
+    phi = (phi < 0.0f) ? (phi + 2.0f * kPi) : phi;
+    const float t = acosf(out_dir.y) / kPi;
+    *pdf_direct_w = 1.0f / (2.0f * kPi * kPi * sinf(t));
+    (void)phi;
+    return V3(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+}
+
+// Russian roulette (random.h:183-188)
+__device__ __forceinline__ bool russian_roulette(V3 thr, float rnd, float& pdf) {
+    const float kill_prob = luminance(thr) * 2.0f;
+    pdf = smin(1.0f, kill_prob);
+    return rnd < pdf;
+}
+
+}  // namespace sh
+}  // namespace imbart

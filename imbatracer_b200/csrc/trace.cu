@@ -131,7 +131,7 @@ struct TraceConfig {
 
 std::mutex g_cfg_mutex;
 bool g_cfg_init = false;
-TraceConfig g_cfg{1, 16, 0};
+TraceConfig g_cfg{4, 20, 0};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -420,6 +420,13 @@ void dropin_host(bool any, int root, imbart_node4* nodes, imbart_instance_node* 
 }
 
 }  // namespace
+
+int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
+                          int flags, void* stream, unsigned long long* stats) {
+    return launch_trace(scene, reinterpret_cast<const imbart_ray*>(rays), reinterpret_cast<imbart_hit*>(hits), v_out,
+                        count, flags, (cudaStream_t)stream, stats);
+}
+
 }  // namespace imbart
 
 using namespace imbart;

@@ -71,6 +71,13 @@ _SIGNATURES = {
     "imbart_hashgrid_query": (I, [P, P, I, I, P, P, P, P]),
     "imbart_hashgrid_get_params": (I, [P, P, P, P]),
     "imbart_hashgrid_get_arrays": (I, [P, C.POINTER(P), C.POINTER(P)]),
+    "imbart_camera_setup": (I, [P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, P, P, P]),
+    "imbart_camera_rays": (I, [P, P, I, I, I, C.c_uint64, C.c_longlong, I, P, P, P, P, P]),
+    "imbart_shading_create": (P, [I, P, I, P, P, P, P, I, P, I, P, P, I, P, I, P, P]),
+    "imbart_shading_destroy": (None, [P]),
+    "imbart_pt_create": (P, [I]),
+    "imbart_pt_destroy": (None, [P]),
+    "imbart_pt_render": (I, [P, P, P, P, P, I, I, I, I, I, C.c_uint64, P, C.c_longlong, P, P]),
     "imbart_set_trace_config": (I, [I, I, I]),
     "imbart_get_trace_config": (I, [C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),

@@ -270,6 +270,58 @@ int imbart_hashgrid_get_params(const imbart_hashgrid* grid, float* params10, int
 int imbart_hashgrid_get_arrays(const imbart_hashgrid* grid, const void** sorted, const int** cell_ends);
 
 /* ------------------------------------------------------------------------------------ */
+/* Sample generation and wavefront path tracing                                            */
+/* ------------------------------------------------------------------------------------ */
+
+/* Camera matrices of PerspectiveCamera::move (camera.h:27-56) for a camera at `pos` looking
+ * along `dir` with `up`, horizontal field of view `fov` degrees, a width x height raster and
+ * `aspect` (1 in the reference): raster_to_world and world_to_raster (16 floats row-major,
+ * either output may be NULL except raster_to_world) and the image-plane distance. Host only. */
+int imbart_camera_setup(const float* pos, const float* dir, const float* up, float fov, float width,
+                        float height, float aspect, float* raster_to_world, float* world_to_raster,
+                        float* img_plane_dist);
+
+/* Camera samples first..first+count-1 of a width x height frame with `spp` samples per
+ * pixel: the reference's PixelRayGen seeding (ray_gen.h:49-72, sample index = global index
+ * into the frame) and the path tracer's pixel jitter (pt.cpp:168-177). DEVICE outputs: rays,
+ * pixel ids, sample ids (may be NULL) and the 64-bit RNG state after the jitter draws. */
+int imbart_camera_rays(const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
+                       unsigned long long seed_base, long long first, int count, imbart_ray* rays,
+                       int* pixel_ids, int* sample_ids, unsigned long long* rng_states, void* stream);
+
+/* Shading data of a scene, resident on one GPU: global vertex arrays (positions, normals,
+ * texture coordinates), per global triangle {v0, v1, v2, material} and geometric normal,
+ * per instance the 3x4 world-to-object matrix, materials (kind: 0 Lambertian, 1 mirror,
+ * 2 glass, 3 glossy Cook-Torrance+Lambert, 4 Phong+Lambert, 5 emissive; 16 parameters:
+ * colour[3], specular[3], exponent, eta, kappa, emission[3], unused[4]), triangle lights
+ * (12 floats: p0, p1, p2, intensity; world space) and an optional constant environment
+ * colour (light 0 when present). bsphere = scene bounding sphere {centre, radius, 1/r^2}. */
+typedef struct imbart_shading imbart_shading;
+imbart_shading* imbart_shading_create(int device, const float* vertices, int n_vertices, const float* normals,
+                                      const float* texcoords, const int* tris, const float* geom_normals,
+                                      int n_tris, const float* inst_inv, int n_inst, const int* mat_kind,
+                                      const float* mat_params, int n_mats, const float* tri_lights,
+                                      int n_tri_lights, const float* env_color, const float* bsphere);
+void imbart_shading_destroy(imbart_shading* shading);
+
+/* Wavefront path-tracing context (device queues, grown on demand). */
+typedef struct imbart_pt_context imbart_pt_context;
+imbart_pt_context* imbart_pt_create(int device);
+void imbart_pt_destroy(imbart_pt_context* ctx);
+
+/* Renders one frame of the path tracer (PathTracer, pt.cpp) into `image` (DEVICE,
+ * width*height*3 floats, accumulated: contributions are added). max_path_len as in the
+ * reference (path vertices incl. camera and light; a path continues while bounces + 1 <
+ * max_path_len); Russian roulette from bounce `rr_start` on (0 = the reference). At most
+ * max_paths_in_flight paths (<= 0: 16M) are in flight; larger frames run in consecutive
+ * sample ranges with unchanged seeding. stats (host, may be NULL): closest-hit rays, shadow
+ * rays, wavefronts. Synchronizes `stream` once per wavefront. */
+int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* shading,
+                     const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
+                     int max_path_len, int rr_start, unsigned long long seed_base, float* image,
+                     long long max_paths_in_flight, long long* stats, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
 /* BVH construction (the builder side of the boundary)                                     */
 /* ------------------------------------------------------------------------------------ */
 

@@ -286,6 +286,48 @@ void* ref_scene_create(int n_meshes, const int* mesh_nverts, const int* mesh_ntr
 
 void ref_scene_destroy(void* h) { delete static_cast<RefScene*>(h); }
 
+// Samplers of the reference evaluated with a fresh RNG(seed). Several of them take two
+// rng.random_float() calls as arguments of one call, whose evaluation order C++ leaves to
+// the compiler; the values here show which draw went to which argument in this build.
+void ref_probe_samplers(uint64_t seed, float* out) {
+    {
+        RNG rng(seed);
+        Lambertian l(rgb(1.0f));
+        float3 in;
+        float pdf;
+        l.sample(float3(0.0f, 0.0f, 1.0f), in, rng, pdf);   // sample_cos_hemisphere (bsdf.h:54-64)
+        out[0] = in.x; out[1] = in.y; out[2] = in.z;
+    }
+    {
+        RNG rng(seed);
+        TriangleLight t(rgb(1.0f), float3(0, 0, 0), float3(1, 0, 0), float3(0, 1, 0));
+        auto s = t.sample_direct(float3(0.2f, 0.2f, 1.0f), rng);   // sample_uniform_triangle (light.h:146)
+        out[3] = s.dir.x; out[4] = s.dir.y; out[5] = s.dir.z;
+    }
+    {
+        RNG rng(seed);
+        FresnelConductor f(1.0f, 20.0f);
+        CookTorrance ct(rgb(1.0f), &f, 20.0f);
+        float3 in;
+        float pdf;
+        ct.sample(float3(0.3f, 0.1f, 0.9f), in, rng, pdf);   // sample_blinn_distribution (brdfs.h:177)
+        out[6] = in.x; out[7] = in.y; out[8] = in.z;
+    }
+    {
+        RNG rng(seed);
+        Phong ph(rgb(1.0f), 20.0f);
+        float3 in;
+        float pdf;
+        ph.sample(float3(0.3f, 0.1f, 0.9f), in, rng, pdf);   // sample_power_cos_hemisphere (brdfs.h:69)
+        out[9] = in.x; out[10] = in.y; out[11] = in.z;
+    }
+    {
+        RNG rng(seed);
+        float2 d = sample_concentric_disc(rng.random_float(), rng.random_float());
+        out[12] = d.x; out[13] = d.y;
+    }
+}
+
 // The reference-layout arrays the reference's adapters wrote (GPU two-wide layout).
 int ref_scene_gpu_layout(void* h, int* root, const void** nodes, const void** insts, const void** tris,
                          int64_t* sizes) {

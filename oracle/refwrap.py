@@ -69,9 +69,10 @@ def camera_rays(w, h, spp, pos, dir, up, fov, seed_base):
     pid = np.zeros(n, np.int32)
     sid = np.zeros(n, np.int32)
     st = np.zeros(n, np.uint64)
-    f = lambda v: np.ascontiguousarray(np.asarray(v, np.float32))
-    rc = load().ref_camera_rays(w, h, spp, _p(f(pos)), _p(f(dir)), _p(f(up)), fov, seed_base, _p(rays), _p(pid),
-                                _p(sid), _p(st))
+    # Keep the input arrays alive across the call.
+    p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (pos, dir, up))
+    rc = load().ref_camera_rays(w, h, spp, _p(p3), _p(d3), _p(u3), fov, seed_base, _p(rays), _p(pid), _p(sid),
+                                _p(st))
     assert rc == n
     return rays, pid, sid, st
 
@@ -146,9 +147,9 @@ class RefScene:
     def render_pt(self, w, h, spp, max_path_len, seed_base, cam=None):
         cam = cam or self.desc.camera
         img = np.zeros((h, w, 3), np.float32)
-        f = lambda v: np.ascontiguousarray(np.asarray(v, np.float32))
-        rc = load().ref_render_pt(self.handle, w, h, _p(f(cam.pos)), _p(f(cam.dir)), _p(f(cam.up)), cam.fov, spp,
-                                  max_path_len, seed_base, _p(img))
+        p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
+        rc = load().ref_render_pt(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, seed_base,
+                                  _p(img))
         assert rc == 0
         return img
 

@@ -1,0 +1,116 @@
+"""Sample generation and the wavefront path tracer against the reference itself.
+
+Camera rays and RNG states must equal the reference's PixelRayGen + PerspectiveCamera bit
+for bit. Images from identical per-pixel seeding must be within relative RMSE 1e-3 of the
+reference's PathTracer (the reference's own pt.cpp, built in oracle/_ref, tracing through
+the oracle traversal) at the same spp: paths are deterministic per sample, so the only
+differences are float rounding in transcendental functions and atomic accumulation order,
+which can flip a rare Russian-roulette or lobe decision.
+"""
+import numpy as np
+import pytest
+
+from imbatracer_b200 import native as N
+from imbatracer_b200 import scenegen as G
+from oracle import refwrap as R
+from tests import helpers as H
+
+needs_ref = pytest.mark.skipif(not R.available(), reason="oracle/_ref not built (reference tree absent)")
+
+RMSE_TOL = 1e-3
+
+
+def rel_rmse(a, b):
+    return float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / np.sqrt(np.mean(b.astype(np.float64) ** 2)))
+
+
+def small_mixed_scene():
+    """Every material kind, a constant environment and triangle lights, instanced meshes."""
+    rng = np.random.default_rng(5)
+    meshes, materials, instances = [], [], []
+    kinds = [G.LAMBERT, G.PHONG, G.GLOSSY, G.MIRROR, G.GLASS]
+    for k, kind in enumerate(kinds):
+        v, f = G.displaced_sphere(rng, 2, (0, 0, 0), 1.0)
+        if kind == G.LAMBERT:
+            mat = G.Material(G.LAMBERT, color=(0.7, 0.5, 0.3))
+        elif kind == G.PHONG:
+            mat = G.Material(G.PHONG, color=(0.3, 0.6, 0.3), specular=(0.5, 0.5, 0.5), exponent=40.0)
+        elif kind == G.GLOSSY:
+            mat = G.Material(G.GLOSSY, color=(0.2, 0.2, 0.6), specular=(0.6, 0.6, 0.6), exponent=30.0)
+        elif kind == G.MIRROR:
+            mat = G.Material(G.MIRROR, color=(0.9, 0.9, 0.9), eta=0.2, kappa=3.0)
+        else:
+            mat = G.Material(G.GLASS, color=(0.95, 0.95, 0.95), specular=(1.0, 1.0, 1.0), eta=1.5)
+        materials.append(mat)
+        meshes.append(G.Mesh(v, np.concatenate([f, np.full((len(f), 1), k, np.int32)], 1)))
+        m = np.eye(4, dtype=np.float32)
+        m[:3, :3] = G.rotation(rng) * rng.uniform(0.8, 1.4)
+        m[:3, 3] = [(k - 2) * 2.6, 0.0, rng.uniform(-1, 1)]
+        instances.append(G.Instance(k, m))
+    # ground + two triangle lights in one mesh
+    parts = []
+    materials.append(G.Material(G.LAMBERT, color=(0.5, 0.5, 0.5)))
+    parts.append((*G.quad([-20, -1.6, -20], [-20, -1.6, 20], [20, -1.6, 20], [20, -1.6, -20]), len(materials) - 1))
+    lights = []
+    for tri, e in (([[-3, 6, -2], [3, 6, 2], [3, 6, -2]], (30.0, 28.0, 24.0)),
+                   ([[-3, 6, -2], [-3, 6, 2], [3, 6, 2]], (24.0, 28.0, 30.0))):
+        materials.append(G.Material(G.EMISSIVE, color=(0, 0, 0), emission=e))
+        parts.append((np.array(tri, np.float32), np.array([[0, 1, 2]], np.int32), len(materials) - 1))
+        lights.append((np.array(tri[0], np.float32), np.array(tri[1], np.float32), np.array(tri[2], np.float32),
+                       np.array(e, np.float32)))
+    meshes.append(G._merge(parts))
+    instances.append(G.Instance(len(meshes) - 1))
+    cam = G.Camera(pos=(0.0, 1.5, -9.0), dir=(0.0, -0.1, 1.0), up=(0.0, 1.0, 0.0), fov=60.0, width=96, height=64)
+    return G.SceneDesc(meshes, instances, materials, lights, cam, (0.4, 0.45, 0.5), "mixed")
+
+
+@needs_ref
+def test_reference_path_tracer_is_deterministic():
+    d = small_mixed_scene()
+    rs = R.RefScene(d)
+    a = rs.render_pt(48, 32, 2, 5, 1234)
+    b = rs.render_pt(48, 32, 2, 5, 1234)
+    assert np.array_equal(a, b) and a.sum() > 0
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("w,h,spp,seed", [(64, 48, 2, 987654321), (33, 17, 3, 5)])
+def test_camera_rays_bit_exact(cuda, w, h, spp, seed):
+    import torch
+    from imbatracer_b200.integrators import camera_matrix
+    cam = G.Camera(pos=(1.0, 2.0, -7.0), dir=(-0.1, -0.2, 1.0), up=(0.0, 1.0, 0.0), fov=55.0, width=w, height=h)
+    ref_rays, ref_pid, ref_sid, ref_st = R.camera_rays(w, h, spp, cam.pos, cam.dir, cam.up, cam.fov, seed)
+    n = w * h * spp
+    r2w = camera_matrix(cam)
+    pos = np.array(cam.pos, np.float32)
+    rays = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+    pid = torch.zeros(n, dtype=torch.int32, device="cuda")
+    sid = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(n, dtype=torch.int64, device="cuda")
+    N.check(N.load().imbart_camera_rays(N.ptr(r2w), N.ptr(pos), w, h, spp, seed, 0, n, N.ptr(rays), N.ptr(pid),
+                                        N.ptr(sid), N.ptr(st), None), "camera_rays")
+    torch.cuda.synchronize()
+    assert np.array_equal(pid.cpu().numpy(), ref_pid) and np.array_equal(sid.cpu().numpy(), ref_sid)
+    assert np.array_equal(st.cpu().numpy().view(np.uint64), ref_st)
+    got = rays.cpu().numpy()
+    assert np.array_equal(got.view(np.int32), ref_rays.view(np.int32))
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("name,w,h,spp,max_len", [
+    ("config1", 64, 64, 4, 5),      # Lambertian spheres, 2-triangle area light, 4 bounces
+    ("mixed", 96, 64, 8, 6),        # every material kind + constant environment
+])
+def test_path_tracer_image_matches_reference(cuda, name, w, h, spp, max_len):
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    d = small_mixed_scene() if name == "mixed" else H.scene_desc(name)
+    seed = 20240611
+    ref = R.RefScene(d).render_pt(w, h, spp, max_len, seed)
+    gs = GpuScene(d)
+    pt = PathTracer(gs, max_path_len=max_len)
+    img = pt.render(spp, seed, w, h).cpu().numpy()
+    err = rel_rmse(img, ref)
+    assert err <= RMSE_TOL, f"relative RMSE {err:.2e}"
+    assert pt.last_stats[0] >= w * h * spp and pt.last_stats[1] > 0
