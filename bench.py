@@ -1,17 +1,20 @@
-"""Benchmark of the wavefront hot path (Mrays/s, closest + shadow rays).
+"""Benchmark of the wavefront hot path: Mrays/s of closest-hit + shadow rays.
 
-Workload: the 1920x1080 instanced scene (200 instances of 8 seeded meshes, ~1.14M instanced
-triangles, 16 area lights + environment). One step traces one wavefront of that frame's rays
-through libimbart: the primary camera rays (closest hit), one bounce of incoherent secondary
-rays from the primary hits (closest hit) and one shadow ray per primary hit towards a random
-point on a random area light (any hit). Inputs are resident in HBM when timing starts; the
-rays and hits of one step (~300 MB) exceed the 126 MB L2.
+Default workload (`--mode pt`): the wavefront path tracer on the 1920x1080 instanced scene
+(200 instances of 8 seeded meshes, ~1.30M instanced triangles, materials Lambertian / Phong /
+Cook-Torrance / glass / mirror, 16 triangle area lights + constant environment), 16 samples
+per pixel, up to 8 bounces (max_path_len 9), Russian roulette from bounce 3. One step = one
+frame rendered entirely on the GPU (sample generation, traversal, shading, shadow rays).
+Scene data is resident in HBM; the path and shadow queues (~2.5 GB per 16M paths) exceed the
+126 MB L2. `value` counts every closest-hit and shadow ray the frame traced.
 
-`value` is device-timed Mrays/s over all ranks; `e2e` is the same metric through the host
-buffer C-ABI entry (pinned host rays copied in, hits copied out inside the timed region).
-`--impl reference` times the CPU traversal (the oracle restatement of the reference's
-traversal boundary; the reference's own traversal library is not in its tree) on all host
-cores on a bounded sample of the same rays.
+`e2e`: the same frames through the public API with the image copied back to pinned host
+memory every frame (the camera set-up goes host -> device per frame).
+`--impl reference`: the reference's own PathTracer / TileScheduler / Scene / materials (its
+C++ built in place as oracle/_ref) on all host cores, on a bounded image of the same scene,
+with the oracle's CPU traversal behind its traversal entry points (the reference's AnyDSL
+traversal library is not part of its tree). Its ray counts are the reference scheduler's own.
+`--mode trace`: traversal kernels alone on fixed ray sets of the same frame (kernel tuning).
 """
 from __future__ import annotations
 
@@ -28,8 +31,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "wavefront_1080p_instanced_200x8"
+WORKLOAD = "pt_1080p_16spp_8bounce_instanced_200x8"
 METRIC = "Mrays/s closest+shadow"
+SPP = 16
+MAX_PATH_LEN = 9        # 8 continuation bounces (path vertices incl. camera and light)
+RR_START = 3
+CPU_SAMPLE = (240, 135)  # bounded CPU sample: 1/64 of the pixels, same spp and bounces
 
 
 def log(*a):
@@ -46,6 +53,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines: list[str] = []
+        self.first = 0
 
     def start(self):
         try:
@@ -57,13 +65,11 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
             return
-        # Wait for the first sample so that the timed region is covered.
         t0 = time.time()
         while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
             time.sleep(0.02)
 
     def mark(self):
-        """Starts counting samples from here (the timed region)."""
         self.first = len(self.lines)
 
     def _read(self):
@@ -78,38 +84,267 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        # Samples from the timed region; keep the one before it when the region is shorter
-        # than the sampling interval.
-        lines = self.lines[max(getattr(self, "first", 0) - 1, 0):]
-        for ln in lines:
+        for ln in self.lines[max(self.first - 1, 0):]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
             try:
                 sm.append(float(parts[1]))
                 smax = float(parts[2])
+                power.append(float(parts[3]))
             except ValueError:
                 continue
             for name, val in zip(names, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
-def make_scene():
+def peak_hbm():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+def trace_bytes(rays: int, work) -> int:
+    """Algorithmic bytes of traversal launches: 32 B ray + 16 B hit per ray, 80 B per 8-wide
+    node fetched, 48 B per triangle tested, 64 B per instance entered."""
+    return 48 * rays + 80 * int(work[0]) + 48 * int(work[1]) + 64 * int(work[2])
+
+
+def reference_cpu(desc, steps, threads, w, h, seed=7):
+    """The reference's own CPU path tracer on a bounded image; returns (Mrays/s, rays/step, s/step)."""
+    from oracle import refwrap as R
+    rs = R.RefScene(desc)
+    tot_rays, tot_s = 0, 0.0
+    for k in range(steps):
+        t0 = time.perf_counter()
+        _, a, b = rs.render_pt_threads(w, h, SPP, MAX_PATH_LEN, seed + k, threads)
+        tot_s += time.perf_counter() - t0
+        tot_rays += a + b
+    rs.close()
+    return tot_rays / tot_s / 1e6, tot_rays // max(steps, 1), tot_s / max(steps, 1)
+
+
+def run_pt(args):
+    import torch
+    import torch.distributed as dist
+    from imbatracer_b200 import native as N
     from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = N.load()
+
+    desc = G.config2()
+    gs = GpuScene(desc, device=local)
+    pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
+    W, H = desc.camera.width, desc.camera.height
+    stream = torch.cuda.current_stream(dev)
+    image = torch.zeros((H, W, 3), dtype=torch.float32, device=dev)
+    base_seed = 1000 * (rank + 1)
+
+    def frame(k):
+        pt.render(SPP, base_seed + k, image=image, stream=stream)
+        return int(pt.last_stats[0] + pt.last_stats[1])
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(args.warmup):
+        frame(k)
+    torch.cuda.synchronize()
+    clocks.mark()
+    launches0 = lib.imbart_kernel_launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rays = 0
+    for k in range(args.steps):
+        rays += frame(args.warmup + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = lib.imbart_kernel_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms, float(rays)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms_max, all_rays = float(tmax[0]), float(t[1])
+    else:
+        ms_max, all_rays = ms, float(rays)
+
+    # e2e through the public API: render + image copied to pinned host memory per frame.
+    host_img = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
+    for k in range(max(1, args.warmup // 2)):
+        frame(10_000 + k)
+        host_img.copy_(image, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    e2e_rays = 0
+    for k in range(args.steps):
+        e2e_rays += frame(20_000 + k)
+        host_img.copy_(image, non_blocking=True)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = q0.elapsed_time(q1)
+    te = torch.tensor([e2e_ms, float(e2e_rays)], dtype=torch.float64, device=dev)
+    if world > 1:
+        temax = te.clone()
+        dist.all_reduce(temax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(te, op=dist.ReduceOp.SUM)
+        e2e_ms, e2e_all = float(temax[0]), float(te[1])
+    else:
+        e2e_all = float(e2e_rays)
+
+    # Roofline of the dominant kernel (closest-hit traversal): one frame with every traversal
+    # launch timed by CUDA events on the launching stream, one frame with the statistics
+    # variant (identical hits) for the node / triangle / instance counts.
+    prof = N.PtProfile()
+    prof.events = 1
+    lib.imbart_pt_set_profile(pt.ctx, C_ref(prof))
+    frame(30_000)
+    lib.imbart_pt_set_profile(pt.ctx, None)
+    work = N.PtProfile()
+    work.work = 1
+    lib.imbart_pt_set_profile(pt.ctx, C_ref(work))
+    frame(30_000)
+    lib.imbart_pt_set_profile(pt.ctx, None)
+    torch.cuda.synchronize()
+    closest_bytes = trace_bytes(work.closest_rays, work.closest_work)
+    shadow_bytes = trace_bytes(work.shadow_rays, work.shadow_work)
+    per_launch_bytes = closest_bytes / max(prof.closest_launches, 1)
+    per_launch_ms = prof.closest_ms / max(prof.closest_launches, 1)
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_src = peak_hbm()
+
+    if rank == 0:
+        value = all_rays / (ms_max * 1e-3) / 1e6
+        e2e_value = e2e_all / (e2e_ms * 1e-3) / 1e6
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            from oracle import refwrap as R
+            if R.available():
+                threads = os.cpu_count() or 1
+                mr, rps, sps = reference_cpu(desc, 2, threads, *CPU_SAMPLE)
+                cpu = {"value": round(mr, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                       "sample": f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} at {SPP} spp, max_path_len {MAX_PATH_LEN} "
+                                 f"(1/64 of the frame's pixels), 2 frames, {rps} rays/frame: the reference's "
+                                 f"PathTracer+TileScheduler ({threads} tile threads) with the oracle CPU traversal"}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generator, per-pixel MWC64X seeding)",
+            "config": {"workload": WORKLOAD, "resolution": f"{W}x{H}", "spp": SPP, "max_path_len": MAX_PATH_LEN,
+                       "rr_start_bounce": RR_START, "instances": len(desc.instances), "meshes": len(desc.meshes),
+                       "instanced_triangles": desc.instanced_triangles, "lights": len(desc.lights) + 1,
+                       "rays_per_step": int(all_rays / world / args.steps),
+                       "l2": "inputs larger than L2 (path + shadow queues ~2.5 GB per 16M paths in flight)",
+                       "parallelism": f"replicas x{world} (independent frames per GPU, different seeds)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": "trace_persistent (closest hit) inside the frame", "peak_source": peak_src,
+                         "bytes_per_launch": int(per_launch_bytes), "launch_ms": round(per_launch_ms, 4),
+                         "launches": int(prof.closest_launches),
+                         "bytes_per_ray": round(closest_bytes / max(work.closest_rays, 1), 1),
+                         "shadow": {"ms": round(prof.shadow_ms, 3), "launches": int(prof.shadow_launches),
+                                    "achieved_gbs": round(shadow_bytes / max(prof.shadow_ms, 1e-9) / 1e6, 1),
+                                    "bytes_per_ray": round(shadow_bytes / max(work.shadow_rays, 1), 1)},
+                         "trace_share_of_frame": round((prof.closest_ms + prof.shadow_ms) / (ms_max / args.steps), 3),
+                         "closest_mrays_s": round(work.closest_rays / max(prof.closest_ms, 1e-9) / 1e3, 1),
+                         "shadow_mrays_s": round(work.shadow_rays / max(prof.shadow_ms, 1e-9) / 1e3, 1)},
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 16 * 4 + 12,
+                    "d2h_bytes_per_step": W * H * 12},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    pt.close()
+    gs.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def C_ref(s):
+    import ctypes
+    return ctypes.byref(s)
+
+
+def run_reference(args):
+    """The reference's own CPU path tracer (oracle/_ref) on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import refwrap as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so was not built (the reference "
+                                                              "tree was absent when build() ran)"}))
+        return
+    from imbatracer_b200 import scenegen as G
+    desc = G.config2()
+    threads = os.cpu_count() or 1
+    rs = R.RefScene(desc)
+    for k in range(args.warmup):
+        rs.render_pt_threads(60, 34, SPP, MAX_PATH_LEN, 99 + k, threads)
+    tot, el = 0, 0.0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        _, a, b = rs.render_pt_threads(*CPU_SAMPLE, SPP, MAX_PATH_LEN, 7 + k, threads)
+        el += time.perf_counter() - t0
+        tot += a + b
+    value = tot / el / 1e6
+    sample = (f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} at {SPP} spp per step (1/64 of the 1080p frame), "
+              f"{tot // max(args.steps, 1)} rays/step counted by the reference scheduler")
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "impl": "reference",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(el / args.steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": WORKLOAD, "sample": sample,
+                       "reference": "PathTracer/TileScheduler/Scene/materials of the reference built in place "
+                                    "(oracle/_ref); traversal = the oracle's CPU restatement"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# --mode trace: traversal kernels alone on fixed ray sets of the frame (kernel tuning)
+# ---------------------------------------------------------------------------------------
+def make_scene():
     from imbatracer_b200 import scene as S
+    from imbatracer_b200 import scenegen as G
     desc = G.config2()
     td = S.build_traversal_data(desc.meshes, desc.instances)
     return desc, td
 
 
 def make_wavefront(desc, ds, torch, dev, seed: int):
-    """Builds the step's three ray sets on the device (untimed setup)."""
-    from imbatracer_b200 import native as N
+    """Primary camera rays, one bounce of incoherent secondary rays from their hits, and one
+    shadow ray per hit towards a random light point (untimed set-up on the device)."""
     cam = desc.camera
     w, h = cam.width, cam.height
     g = torch.Generator(device=dev)
@@ -123,10 +358,8 @@ def make_wavefront(desc, ds, torch, dev, seed: int):
     upv = torch.linalg.cross(right, fwd)
     scale = float(np.tan(np.radians(cam.fov) / 2)) * 2.0 / h
     ys, xs = torch.meshgrid(torch.arange(h, device=dev), torch.arange(w, device=dev), indexing="ij")
-    jx = torch.rand((h, w), generator=g, device=dev)
-    jy = torch.rand((h, w), generator=g, device=dev)
-    px = (xs.float() + jx - w / 2) * scale
-    py = (h / 2 - ys.float() - jy) * scale
+    px = (xs.float() + torch.rand((h, w), generator=g, device=dev) - w / 2) * scale
+    py = (h / 2 - ys.float() - torch.rand((h, w), generator=g, device=dev)) * scale
     d = fwd + px[..., None] * right + py[..., None] * upv
     d = (d / d.norm(dim=-1, keepdim=True)).reshape(-1, 3)
     n = d.shape[0]
@@ -142,7 +375,6 @@ def make_wavefront(desc, ds, torch, dev, seed: int):
     p = prim[:, :3] + t[:, None] * prim[:, 4:7]
     hp, hd, ht = p[hit], prim[hit, 4:7], t[hit]
     m = hp.shape[0]
-    # Secondary rays: uniform directions on the hemisphere facing back along the ray.
     sd = torch.randn((m, 3), generator=g, device=dev)
     sd = sd / sd.norm(dim=-1, keepdim=True)
     flip = (sd * hd).sum(-1) > 0
@@ -152,7 +384,6 @@ def make_wavefront(desc, ds, torch, dev, seed: int):
     sec[:, 3] = 1e-3 * ht
     sec[:, 4:7] = sd
     sec[:, 7] = 3.0e38
-    # Shadow rays towards a random point on a random light (offset as pt.cpp:37-41).
     lights = torch.tensor(np.stack([np.stack(l[:3]) for l in desc.lights]), dtype=torch.float32, device=dev)
     li = torch.randint(0, lights.shape[0], (m,), generator=g, device=dev)
     r1 = torch.rand(m, generator=g, device=dev).sqrt()
@@ -171,275 +402,50 @@ def make_wavefront(desc, ds, torch, dev, seed: int):
     return [(prim.contiguous(), False), (sec.contiguous(), False), (sh.contiguous(), True)]
 
 
-def algorithmic_bytes(ds, sets, torch, dev):
-    """Bytes per launch from the statistics variant: 32 B ray + 16 B hit per ray, 80 B per
-    8-wide node, 48 B per triangle, 64 B per instance entered."""
-    from imbatracer_b200 import native as N
-    lib = N.load()
-    out = []
-    for rays, any_hit in sets:
-        st = torch.zeros(3, dtype=torch.int64, device=dev)
-        hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
-        N.check(lib.imbart_trace_stats(ds.handle, N.ptr(rays), N.ptr(hits), rays.shape[0],
-                                       N.TRACE_ANY if any_hit else N.TRACE_CLOSEST, N.ptr(st), None), "stats")
-        torch.cuda.synchronize()
-        nodes, tris, insts = (int(x) for x in st.cpu())
-        out.append({"rays": int(rays.shape[0]), "nodes": nodes, "tris": tris, "insts": insts,
-                    "bytes": 48 * int(rays.shape[0]) + 80 * nodes + 48 * tris + 64 * insts})
-    return out
-
-
-def cpu_baseline(td, sets, torch, sample: int, threads: int, seconds: float = 12.0):
-    """Times the oracle's traversal on the host cores on a bounded sample of every ray set."""
-    from oracle import oracle as O
-    from imbatracer_b200 import native as N
-    samples = []
-    for rays, any_hit in sets:
-        r = rays[:sample].cpu().numpy().copy().view(N.RAY_DTYPE).reshape(-1)
-        samples.append((np.ascontiguousarray(r), any_hit))
-    O.trace_node2(td, samples[0][0][:1000], nthreads=threads)  # warm up
-    total, elapsed, reps = 0, 0.0, 0
-    while elapsed < seconds or reps == 0:
-        t0 = time.perf_counter()
-        for r, any_hit in samples:
-            O.trace_node2(td, r, any_hit=any_hit, nthreads=threads)
-            total += len(r)
-        elapsed += time.perf_counter() - t0
-        reps += 1
-    return total / elapsed / 1e6, total, reps
-
-
-def run_ours(args):
+def run_trace(args):
     import torch
-    import torch.distributed as dist
     from imbatracer_b200 import native as N
     from imbatracer_b200 import scene as S
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    lib = N.load()
-
+    dev = torch.device("cuda", 0)
     desc, td = make_scene()
-    ds = S.DeviceScene(td, device=local)
-    sets = make_wavefront(desc, ds, torch, dev, seed=1234 + rank)
-    n_rays = sum(r.shape[0] for r, _ in sets)
+    ds = S.DeviceScene(td)
+    sets = make_wavefront(desc, ds, torch, dev, 1234)
     hits = [torch.zeros((r.shape[0], 4), dtype=torch.int32, device=dev) for r, _ in sets]
-    stream = torch.cuda.current_stream(dev)
-
-    def step(events=None):
-        for i, ((rays, any_hit), h) in enumerate(zip(sets, hits)):
-            if events is not None:
-                events[i][0].record(stream)
-            ds.trace(rays, h, any_hit=any_hit, stream=stream)
-            if events is not None:
-                events[i][1].record(stream)
-
-    clocks = ClockSampler(local)
-    clocks.start()
     for _ in range(args.warmup):
-        step()
+        for (r, a), h in zip(sets, hits):
+            ds.trace(r, h, any_hit=a)
     torch.cuda.synchronize()
-    launches_before = lib.imbart_kernel_launch_count()
-    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                   for _ in sets] for _ in range(args.steps)]
-    clocks.mark()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for k in range(args.steps):
-        step(per_launch[k])
-    end.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    launches = lib.imbart_kernel_launch_count() - launches_before
-    ms = start.elapsed_time(end)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    launch_ms = np.array([[a.elapsed_time(b) for a, b in row] for row in per_launch]).mean(0)
-
-    # e2e: same metric through the host-buffer entry, pinned host memory, copies inside.
-    host_sets = [(r.cpu().pin_memory(), a) for r, a in sets]
-    host_hits = [torch.zeros((r.shape[0], 4), dtype=torch.int32).pin_memory() for r, _ in host_sets]
-
-    def e2e_step():
-        for (r, a), h in zip(host_sets, host_hits):
-            N.check(lib.imbart_trace_host(ds.handle, N.ptr(r), N.ptr(h), r.shape[0],
-                                          N.TRACE_ANY if a else N.TRACE_CLOSEST, stream.cuda_stream), "e2e")
-
-    for _ in range(args.warmup):
-        e2e_step()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e_start = torch.cuda.Event(enable_timing=True)
-    e_end = torch.cuda.Event(enable_timing=True)
-    e_start.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e_end.record(stream)
-    torch.cuda.synchronize()
-    e_ms = e_start.elapsed_time(e_end)
-    te = torch.tensor([e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e_ms_max = float(te.item())
-
-    stats = algorithmic_bytes(ds, sets, torch, dev)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    dom = int(np.argmax(launch_ms))
-    achieved = stats[dom]["bytes"] / (launch_ms[dom] * 1e-3) / 1e9
-
-    if rank == 0:
-        total_rays = n_rays * world * args.steps
-        value = total_rays / (ms_max * 1e-3) / 1e6
-        e2e_value = total_rays / (e_ms_max * 1e-3) / 1e6
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            sample = 65536
-            mr, tot, reps = cpu_baseline(td, sets, torch, sample, threads)
-            cpu = {"value": round(mr, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
-                   "sample": f"first {sample} rays of each of the 3 ray sets ({tot} rays over {reps} passes), "
-                             f"oracle traversal of the reference layout, {threads} threads"}
-        names = ["primary_closest", "secondary_closest", "shadow_any"]
-        line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene generator; seeded ray sets)",
-            "config": {"workload": WORKLOAD, "resolution": "1920x1080", "instances": len(desc.instances),
-                       "meshes": len(desc.meshes) - 1, "instanced_triangles": desc.instanced_triangles,
-                       "rays_per_step": n_rays, "ray_sets": {nm: s["rays"] for nm, s in zip(names, stats)},
-                       "l2": "inputs larger than L2 (rays+hits per step ~%d MB)" % (n_rays * 48 // 2 ** 20),
-                       "parallelism": f"replicas x{world} (independent ray wavefronts per GPU)"},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak_gbs, "unit": "GB/s",
-                         "frac": round(achieved / peak_gbs, 4), "traffic": None,
-                         "kernel": f"trace_kernel ({names[dom]})", "peak_source": peak_src,
-                         "bytes_per_launch": stats[dom]["bytes"], "launch_ms": round(float(launch_ms[dom]), 4),
-                         "bytes_per_ray": round(stats[dom]["bytes"] / stats[dom]["rays"], 1)},
-            "launch_ms": {nm: round(float(x), 4) for nm, x in zip(names, launch_ms)},
-            "work": {nm: {k: s[k] for k in ("nodes", "tris", "insts")} for nm, s in zip(names, stats)},
-            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
-                    "h2d_bytes_per_step": 32 * n_rays, "d2h_bytes_per_step": 16 * n_rays},
-            "gpu_launches": int(launches),
-            "clocks": clk,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-
-
-def run_reference(args):
-    """CPU arm: the traversal restatement on all host cores, bounded sample per step."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    import torch
-    from imbatracer_b200 import native as N
-    from oracle import oracle as O
-    desc, td = make_scene()
-    # The same three ray sets, built on the CPU from the same generator as the GPU arm would
-    # need a GPU; here a bounded sample with the same composition: camera rays, secondary
-    # rays and shadow rays traced by the CPU traversal.
-    rng = np.random.default_rng(1234)
-    cam = desc.camera
-    n = 65536
-    fwd = np.array(cam.dir, np.float64); fwd /= np.linalg.norm(fwd)
-    right = np.cross(fwd, cam.up); right /= np.linalg.norm(right)
-    upv = np.cross(right, fwd)
-    scale = np.tan(np.radians(cam.fov) / 2) * 2.0 / cam.height
-    pix = rng.integers(0, cam.width * cam.height, n)
-    px = (pix % cam.width + rng.random(n) - cam.width / 2) * scale
-    py = (cam.height / 2 - pix // cam.width - rng.random(n)) * scale
-    d = fwd + px[:, None] * right + py[:, None] * upv
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    prim = np.zeros(n, N.RAY_DTYPE)
-    prim["org"][:, :3] = cam.pos
-    prim["dir"][:, :3] = d
-    prim["dir"][:, 3] = 3e38
-    threads = os.cpu_count() or 1
-    h = O.trace_node2(td, prim, nthreads=threads)
-    hit = h["tri_id"] >= 0
-    hp = (prim["org"][hit, :3] + h["tmax"][hit, None] * prim["dir"][hit, :3]).astype(np.float32)
-    m = len(hp)
-    sd = rng.normal(size=(m, 3)); sd /= np.linalg.norm(sd, axis=1, keepdims=True)
-    flip = (sd * prim["dir"][hit, :3]).sum(1) > 0
-    sd[flip] *= -1
-    sec = np.zeros(m, N.RAY_DTYPE)
-    sec["org"][:, :3] = hp
-    sec["org"][:, 3] = 1e-3 * h["tmax"][hit]
-    sec["dir"][:, :3] = sd
-    sec["dir"][:, 3] = 3e38
-    lights = np.stack([np.stack(l[:3]) for l in desc.lights])
-    li = rng.integers(0, len(lights), m)
-    r1 = np.sqrt(rng.random(m)); r2 = rng.random(m)
-    bu, bv = 1 - r1, r2 * r1
-    lp = bu[:, None] * lights[li, 0] + bv[:, None] * lights[li, 1] + (1 - bu - bv)[:, None] * lights[li, 2]
-    dv = lp - hp
-    dist = np.linalg.norm(dv, axis=1)
-    sh = np.zeros(m, N.RAY_DTYPE)
-    sh["org"][:, :3] = hp
-    sh["org"][:, 3] = 1e-3 * dist
-    sh["dir"][:, :3] = dv / dist[:, None]
-    sh["dir"][:, 3] = dist - 1e-3 * dist
-    sets = [(prim, False), (sec, False), (sh, True)]
-    for _ in range(args.warmup):
-        for r, a in sets:
-            O.trace_node2(td, r[:4096], any_hit=a, nthreads=threads)
-    total, t0 = 0, time.perf_counter()
-    for _ in range(args.steps):
-        for r, a in sets:
-            O.trace_node2(td, r, any_hit=a, nthreads=threads)
-            total += len(r)
-    el = time.perf_counter() - t0
-    value = total / el / 1e6
-    line = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "impl": "reference",
-            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator; seeded ray sets)",
-            "config": {"workload": WORKLOAD, "rays_per_step": total // args.steps,
-                       "sample": "65536 camera rays + their secondary and shadow rays per step"},
-            "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
-                             "sample": f"{total // args.steps} rays per step (65536 camera rays + secondary + shadow)"},
-            "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    out = {}
+    for name, (r, a), h in zip(["primary", "secondary", "shadow"], sets, hits):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            ds.trace(r, h, any_hit=a)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = round(r.shape[0] * args.steps / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)
+    print(json.dumps({"mode": "trace", "Mrays_s": out, "rays": [r.shape[0] for r, _ in sets]}), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="pt", choices=["pt", "trace"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
-        log("warmup raised to 3 (timing rule)")
-        args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.warmup < 3:
+        log("warmup raised to 3 (timing rule)")
+        args.warmup = 3
+    if args.mode == "trace":
+        run_trace(args)
     else:
-        run_ours(args)
+        run_pt(args)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
 // Thread-local error state of the C ABI. The reference entry points return void and the
 // reference reports failures through assert (ray_queue.h:248,270-271); here nothing aborts,
 // the failing call records an error that the caller reads with imbart_last_error().
+#include <atomic>
 #include <string>
 
 #include "imbart_internal.h"
@@ -15,6 +16,11 @@ void set_error(int code, const std::string& msg) {
     g_code = code;
     g_msg = msg;
 }
+
+// Process-wide count of kernel launches issued by libimbart.
+static std::atomic<long long> g_launches{0};
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_total() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace imbart
 
 extern "C" int imbart_last_error(void) { return g_code; }

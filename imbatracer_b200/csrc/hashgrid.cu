@@ -359,6 +359,7 @@ int imbart_hashgrid_build(imbart_hashgrid* g, const float* positions, int stride
         scan_sums_kernel<<<1, kBlock, 0, st>>>(g->block_sums, n_tiles);
         scan_apply_kernel<<<n_tiles, kBlock, 0, st>>>(g->cursor, table_size, g->block_sums, g->cell_ends, g->cursor);
         if (n > 0) scatter_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, g->cell_of, g->cursor, g->sorted);
+        note_launches(n > 0 ? 8 : 5);
         if (!ok(cudaGetLastError(), "hash grid build")) rc = IMBART_ERR_CUDA;
         g->n = n;
         g->table = table_size;
@@ -380,6 +381,7 @@ int imbart_hashgrid_query(const imbart_hashgrid* g, const float* queries, int nq
     const int grid = (nq + 127) / 128;
     query_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(g->sorted, g->cell_ends, g->params, (uint32_t)g->table,
                                                          queries, nq, k, out_ids, out_counts, out_d2);
+    note_launches(1);
     const bool good = ok(cudaGetLastError(), "hash grid query");
     cudaSetDevice(prev);
     return good ? 0 : IMBART_ERR_CUDA;

@@ -89,6 +89,10 @@ void attach_masks(HostWideScene& out, const int* indices, int n_indices,
 // Thread-local error reporting (error.cpp).
 void set_error(int code, const std::string& msg);
 
+// Kernel launch accounting (error.cpp): every launch site adds its launches.
+void note_launches(int n);
+long long launches_total();
+
 // Stream-ordered traversal launch used by the wavefront integrators (trace.cu). `stream` is
 // a cudaStream_t; rays are imbart_ray records, hits imbart_hit records.
 int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,

@@ -34,7 +34,6 @@ struct imbart_scene {
 namespace imbart {
 namespace {
 
-std::atomic<int64_t> g_launches{0};
 
 bool cuda_ok(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return true;
@@ -273,7 +272,7 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    note_launches(1);
     if (!cuda_ok(cudaGetLastError(), "trace kernel launch")) return IMBART_ERR_CUDA;
     return 0;
 }
@@ -538,7 +537,7 @@ int imbart_scene_error_count(const imbart_scene* scene) {
     return ok ? v : -1;
 }
 
-int64_t imbart_kernel_launch_count(void) { return g_launches.load(); }
+int64_t imbart_kernel_launch_count(void) { return launches_total(); }
 
 int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
     if (variant < 0 || variant > 5 || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||

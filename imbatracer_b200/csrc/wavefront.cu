@@ -50,6 +50,9 @@ struct imbart_pt_context {
     float4* scontrib = nullptr;
     int* counts = nullptr;                   // [0] next path queue size, [1] shadow queue size
     int* host_counts = nullptr;              // pinned
+    imbart_pt_profile* profile = nullptr;    // measurement of the traversal launches
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    unsigned long long* work = nullptr;      // device: closest nodes/tris/insts, shadow nodes/tris/insts
 };
 
 namespace imbart {
@@ -424,6 +427,8 @@ void imbart_pt_destroy(imbart_pt_context* c) {
     free_ctx_buffers(c);
     cudaFree(c->counts);
     cudaFreeHost(c->host_counts);
+    cudaFree(c->work);
+    if (c->ev[0]) { cudaEventDestroy(c->ev[0]); cudaEventDestroy(c->ev[1]); }
     cudaSetDevice(prev);
     delete c;
 }
@@ -445,6 +450,7 @@ int imbart_camera_rays(const float* raster_to_world, const float* cam_pos, int w
     c.seed_base = seed_base;
     camera_kernel<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
         c, first, count, reinterpret_cast<float4*>(rays), pixel_ids, rng_states, nullptr, nullptr, sample_ids);
+    note_launches(1);
     return ok(cudaGetLastError(), "camera kernel") ? 0 : IMBART_ERR_CUDA;
 }
 
@@ -474,13 +480,42 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     c.seed_base = seed_base;
     long long n_closest = 0, n_shadow = 0, n_waves = 0;
     int rc = 0;
+    imbart_pt_profile* prof = ctx->profile;
+    if (prof) {
+        if (!ctx->ev[0]) { cudaEventCreate(&ctx->ev[0]); cudaEventCreate(&ctx->ev[1]); }
+        if (prof->work && !ctx->work && !ok(cudaMalloc((void**)&ctx->work, sizeof(unsigned long long) * 6), "cudaMalloc")) {
+            cudaSetDevice(prev);
+            return IMBART_ERR_OUT_OF_MEMORY;
+        }
+        if (prof->work) cudaMemsetAsync(ctx->work, 0, sizeof(unsigned long long) * 6, st);
+    }
+    // One traversal launch, timed / counted when profiling.
+    auto trace = [&](const void* rays, void* hits, int count, int flags) -> int {
+        const bool any = flags == IMBART_TRACE_ANY;
+        unsigned long long* work = (prof && prof->work) ? ctx->work + (any ? 3 : 0) : nullptr;
+        if (prof && prof->events) cudaEventRecord(ctx->ev[0], st);
+        const int r = launch_trace_internal(scene, rays, hits, nullptr, count, flags, st, work);
+        if (prof && prof->events) {
+            cudaEventRecord(ctx->ev[1], st);
+            cudaEventSynchronize(ctx->ev[1]);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+            (any ? prof->shadow_ms : prof->closest_ms) += ms;
+        }
+        if (prof) {
+            (any ? prof->shadow_launches : prof->closest_launches) += 1;
+            (any ? prof->shadow_rays : prof->closest_rays) += count;
+        }
+        return r;
+    };
     for (long long first = 0; first < total && !rc; first += chunk) {
         int n = (int)std::min(chunk, total - first);
         int cur = 0;
         camera_kernel<<<(n + 127) / 128, 128, 0, st>>>(c, first, n, ctx->rays[cur], ctx->pixel[cur], ctx->rng[cur],
                                                        ctx->thr[cur], ctx->bounces[cur], nullptr);
+        note_launches(1);
         while (n > 0) {
-            rc = launch_trace_internal(scene, ctx->rays[cur], ctx->hits, nullptr, n, IMBART_TRACE_CLOSEST, st, nullptr);
+            rc = trace(ctx->rays[cur], ctx->hits, n, IMBART_TRACE_CLOSEST);
             if (rc) break;
             n_closest += n;
             ++n_waves;
@@ -499,6 +534,7 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
             p.counts = ctx->counts;
             p.image = image;
             pt_shade_kernel<<<(n + 127) / 128, 128, 0, st>>>(p);
+            note_launches(1);
             if (!ok(cudaGetLastError(), "shade kernel") ||
                 !ok(cudaMemcpyAsync(ctx->host_counts, ctx->counts, sizeof(int) * 2, cudaMemcpyDeviceToHost, st),
                     "cudaMemcpyAsync") ||
@@ -509,11 +545,12 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
             const int n_next = ctx->host_counts[0];
             const int n_sh = ctx->host_counts[1];
             if (n_sh > 0) {
-                rc = launch_trace_internal(scene, ctx->srays, ctx->shits, nullptr, n_sh, IMBART_TRACE_ANY, st, nullptr);
+                rc = trace(ctx->srays, ctx->shits, n_sh, IMBART_TRACE_ANY);
                 if (rc) break;
                 n_shadow += n_sh;
                 shadow_accumulate_kernel<<<(n_sh + 127) / 128, 128, 0, st>>>(n_sh, ctx->shits, ctx->spixel,
                                                                              ctx->scontrib, image);
+                note_launches(1);
                 if (!ok(cudaGetLastError(), "shadow kernel")) { rc = IMBART_ERR_CUDA; break; }
             }
             n = n_next;
@@ -521,8 +558,23 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
         }
     }
     if (stats) { stats[0] = n_closest; stats[1] = n_shadow; stats[2] = n_waves; }
+    if (!rc && prof && prof->work) {
+        unsigned long long w[6];
+        if (ok(cudaMemcpyAsync(w, ctx->work, sizeof(w), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync") &&
+            ok(cudaStreamSynchronize(st), "cudaStreamSynchronize")) {
+            for (int k = 0; k < 3; ++k) { prof->closest_work[k] += w[k]; prof->shadow_work[k] += w[3 + k]; }
+        } else {
+            rc = IMBART_ERR_CUDA;
+        }
+    }
     cudaSetDevice(prev);
     return rc;
+}
+
+int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile) {
+    if (!ctx) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_pt_set_profile"); return IMBART_ERR_INVALID_ARGUMENT; }
+    ctx->profile = profile;
+    return 0;
 }
 
 }  // extern "C"

@@ -37,6 +37,13 @@ class SceneInfo(C.Structure):
                 ("masked", C.c_int32)]
 
 
+class PtProfile(C.Structure):
+    _fields_ = [("events", C.c_int), ("work", C.c_int), ("closest_ms", C.c_double), ("shadow_ms", C.c_double),
+                ("closest_launches", C.c_longlong), ("shadow_launches", C.c_longlong),
+                ("closest_rays", C.c_longlong), ("shadow_rays", C.c_longlong),
+                ("closest_work", C.c_ulonglong * 3), ("shadow_work", C.c_ulonglong * 3)]
+
+
 class ImbartError(RuntimeError):
     pass
 
@@ -78,6 +85,7 @@ _SIGNATURES = {
     "imbart_pt_create": (P, [I]),
     "imbart_pt_destroy": (None, [P]),
     "imbart_pt_render": (I, [P, P, P, P, P, I, I, I, I, I, C.c_uint64, P, C.c_longlong, P, P]),
+    "imbart_pt_set_profile": (I, [P, P]),
     "imbart_set_trace_config": (I, [I, I, I]),
     "imbart_get_trace_config": (I, [C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),

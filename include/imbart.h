@@ -321,6 +321,23 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
                      int max_path_len, int rr_start, unsigned long long seed_base, float* image,
                      long long max_paths_in_flight, long long* stats, void* stream);
 
+/* Measurement of the traversal launches inside imbart_pt_render (for roofline reporting). */
+typedef struct {
+    int events;                 /* in: time every traversal launch with CUDA events on the stream */
+    int work;                   /* in: run the statistics variant (counts nodes/triangles/instances) */
+    double closest_ms;          /* out: summed closest-hit launch time */
+    double shadow_ms;           /* out: summed any-hit launch time */
+    long long closest_launches; /* out */
+    long long shadow_launches;  /* out */
+    long long closest_rays;     /* out */
+    long long shadow_rays;      /* out */
+    unsigned long long closest_work[3]; /* out: nodes, triangles, instances (work != 0) */
+    unsigned long long shadow_work[3];
+} imbart_pt_profile;
+
+/* Makes the following imbart_pt_render calls of `ctx` fill `profile` (NULL: stop). */
+int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile);
+
 /* ------------------------------------------------------------------------------------ */
 /* BVH construction (the builder side of the boundary)                                     */
 /* ------------------------------------------------------------------------------------ */

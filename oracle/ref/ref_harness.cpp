@@ -4,8 +4,12 @@
 // integrators on the CPU to pin the oracle and to produce golden outputs. The traversal
 // behind the reference's traversal_gpu entry points is the oracle's CPU restatement
 // (oracle/traversal.c), since the reference's AnyDSL traversal library is not in its tree.
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -370,6 +374,52 @@ int ref_render_pt(void* h, int w, int ht, const float* pos, const float* dir, co
         image_out[3 * i + 2] = img.pixels()[i][2];
     }
     return 0;
+}
+
+// The reference path tracer as its CPU baseline runs it: `threads` TileScheduler threads on
+// tiles of `tile` pixels, traversal by the oracle on the calling thread of each tile. Ray
+// counts are the reference TileScheduler's own statistics (tile_scheduler.h:117-127), which
+// it prints when destroyed (:59-60); the harness reads that line from stdout.
+int ref_render_pt_threads(void* h, int w, int ht, const float* pos, const float* dir, const float* up, float fov,
+                          int spp, int max_path_len, uint64_t seed_base, int tile, int threads, float* image_out,
+                          long long* counts) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    PerspectiveCamera cam((float)w, (float)ht, fov);
+    cam.move(f3(pos), f3(dir), f3(up));
+    DefaultTileGen<PTState> gen(w, ht, spp, tile);
+    auto* sched = new TileScheduler<PTState, ShadowState, true>(gen, rs->scene, 1, threads, tile * tile * spp, true);
+    AtomicImage img(w, ht);
+    img.clear();
+    {
+        PathTracer pt(rs->scene, cam, *sched, max_path_len);
+        imbart_ref_set_seed(seed_base, 0);
+        pt.render(img);
+    }
+    // Capture the statistics line printed by the scheduler's destructor.
+    fflush(stdout);
+    std::cout.flush();
+    char path[] = "/tmp/imbart_ref_statsXXXXXX";
+    const int fd = mkstemp(path);
+    const int saved = dup(1);
+    dup2(fd, 1);
+    delete sched;
+    std::cout.flush();
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+    lseek(fd, 0, SEEK_SET);
+    char buf[256] = {0};
+    const ssize_t got = read(fd, buf, sizeof(buf) - 1);
+    close(fd);
+    unlink(path);
+    long long prim = -1, shadow = -1;
+    if (got > 0) sscanf(buf, "%lld primary ray(s), %lld shadow ray(s)", &prim, &shadow);
+    counts[0] = prim;
+    counts[1] = shadow;
+    if (image_out)
+        for (int i = 0; i < w * ht; ++i)
+            for (int k = 0; k < 3; ++k) image_out[3 * i + k] = img.pixels()[i][k];
+    return prim >= 0 ? 0 : -1;
 }
 
 }  // extern "C"

@@ -36,6 +36,7 @@ def load() -> C.CDLL:
             "ref_scene_gpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
             "ref_scene_bsphere": (None, [P, P]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
+            "ref_render_pt_threads": (I, [P, I, I, P, P, P, F, I, I, U64, I, I, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -152,6 +153,19 @@ class RefScene:
                                   _p(img))
         assert rc == 0
         return img
+
+    def render_pt_threads(self, w, h, spp, max_path_len, seed_base, threads, tile=32, cam=None):
+        """The reference PT with `threads` tile threads; returns (image, closest rays, shadow
+        rays) with the ray counts of the reference's own TileScheduler statistics."""
+        cam = cam or self.desc.camera
+        img = np.zeros((h, w, 3), np.float32)
+        counts = np.zeros(2, np.int64)
+        p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
+        load().imbart_ref_set_threads(1, 1)
+        rc = load().ref_render_pt_threads(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len,
+                                          seed_base, tile, threads, _p(img), _p(counts))
+        assert rc == 0
+        return img, int(counts[0]), int(counts[1])
 
     def close(self):
         if self.handle:
