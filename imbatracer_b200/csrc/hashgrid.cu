@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <mutex>
 #include <string>
 
 #include "imbart_internal.h"
@@ -408,3 +409,84 @@ int imbart_hashgrid_get_arrays(const imbart_hashgrid* g, const void** sorted, co
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Hash-grid build that allocates nothing.
+//
+// Some callers must not allocate device memory at all: a server that admits work against a
+// fixed HBM budget accounts for every byte up front, and cudaMalloc / cudaFree synchronize
+// the device, stalling the other requests' streams; hosts that own all device memory
+// through their own arena hand out only buffers they sized themselves. For them the build's
+// scratch (bucket id per photon, bucket cursors, scan tile sums, bounding box) lives in one
+// statically sized device array below, held by every GPU that loads the library until the
+// process exits: 4 * (2^20 + 2^21 + 1024 + 8) bytes, about 12 MiB. The caller passes the
+// inputs and the outputs it allocated itself.
+// ---------------------------------------------------------------------------------------
+namespace imbart {
+namespace {
+constexpr int kNoAllocMaxPhotons = 1 << 20;
+constexpr int kNoAllocMaxTable = 1 << 21;
+constexpr int kNoAllocTiles = (kNoAllocMaxTable + kScanTile - 1) / kScanTile;
+constexpr size_t kNoAllocInts = (size_t)kNoAllocMaxPhotons + kNoAllocMaxTable + kNoAllocTiles + 8;
+
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocInts];
+
+// Device address of the scratch array, looked up once per device with that device current.
+std::mutex g_noalloc_mutex;
+int* g_noalloc_addr[64] = {};
+}  // namespace
+}  // namespace imbart
+
+extern "C" int imbart_hashgrid_build_noalloc(const float* positions, int stride, int n, float radius,
+                                             float cell_factor, int table_size, void* sorted_out,
+                                             int* cell_ends_out, float* params_out, void* stream) {
+    if (n < 0 || (n > 0 && (!positions || !sorted_out)) || stride < 3 || !(radius > 0.0f) || !(cell_factor > 0.0f) ||
+        !cell_ends_out || !params_out) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_build_noalloc: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (table_size <= 0) table_size = std::max(2 * n, 1);
+    if (n > kNoAllocMaxPhotons || table_size > kNoAllocMaxTable) {
+        set_error(IMBART_ERR_LIMIT, "imbart_hashgrid_build_noalloc: at most 1048576 photons and 2097152 buckets "
+                                    "(the size of its static scratch); use imbart_hashgrid_build for more");
+        return IMBART_ERR_LIMIT;
+    }
+    int device = 0;
+    if (!ok(cudaGetDevice(&device), "cudaGetDevice")) return IMBART_ERR_CUDA;
+    if (device < 0 || device >= 64) {
+        set_error(IMBART_ERR_LIMIT, "imbart_hashgrid_build_noalloc: device index above 63");
+        return IMBART_ERR_LIMIT;
+    }
+    int* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+        if (!g_noalloc_addr[device]) {
+            void* addr = nullptr;
+            if (!ok(cudaGetSymbolAddress(&addr, g_noalloc_scratch), "cudaGetSymbolAddress")) return IMBART_ERR_CUDA;
+            g_noalloc_addr[device] = static_cast<int*>(addr);
+        }
+        scratch = g_noalloc_addr[device];
+    }
+    int* cell_of = scratch;
+    int* cursor = cell_of + kNoAllocMaxPhotons;
+    int* tile_sums = cursor + kNoAllocMaxTable;
+    const int n_tiles = (table_size + kScanTile - 1) / kScanTile;
+    int* box = tile_sums + kNoAllocTiles;
+    float4* sorted = static_cast<float4*>(sorted_out);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = grid_for(std::max(n, 1));
+    // The scratch keeps the previous call's contents: the box and the bucket counts are
+    // reset here; bucket ids, tile sums and cursors are fully rewritten before they are read.
+    bbox_init_kernel<<<1, 32, 0, st>>>(box);
+    if (n > 0) bbox_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, box);
+    params_kernel<<<1, 32, 0, st>>>(box, radius, cell_factor, params_out);
+    if (!ok(cudaMemsetAsync(cursor, 0, sizeof(int) * (size_t)table_size, st), "cudaMemsetAsync")) return IMBART_ERR_CUDA;
+    if (n > 0) count_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, params_out, (uint32_t)table_size, cursor,
+                                                     cell_of);
+    scan_tiles_kernel<<<n_tiles, kBlock, 0, st>>>(cursor, table_size, tile_sums);
+    scan_sums_kernel<<<1, kBlock, 0, st>>>(tile_sums, n_tiles);
+    scan_apply_kernel<<<n_tiles, kBlock, 0, st>>>(cursor, table_size, tile_sums, cell_ends_out, cursor);
+    if (n > 0) scatter_kernel<<<grid, kBlock, 0, st>>>(positions, stride, n, cell_of, cursor, sorted);
+    note_launches(n > 0 ? 8 : 5);
+    return ok(cudaGetLastError(), "imbart_hashgrid_build_noalloc") ? 0 : IMBART_ERR_CUDA;
+}

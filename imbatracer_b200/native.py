@@ -78,6 +78,7 @@ _SIGNATURES = {
     "imbart_hashgrid_query": (I, [P, P, I, I, P, P, P, P]),
     "imbart_hashgrid_get_params": (I, [P, P, P, P]),
     "imbart_hashgrid_get_arrays": (I, [P, C.POINTER(P), C.POINTER(P)]),
+    "imbart_hashgrid_build_noalloc": (I, [P, I, I, C.c_float, C.c_float, I, P, P, P, P]),
     "imbart_camera_setup": (I, [P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, P, P, P]),
     "imbart_camera_rays": (I, [P, P, I, I, I, C.c_uint64, C.c_longlong, I, P, P, P, P, P]),
     "imbart_shading_create": (P, [I, P, I, P, P, P, P, I, P, I, P, P, I, P, I, P, P]),

@@ -269,6 +269,24 @@ int imbart_hashgrid_get_params(const imbart_hashgrid* grid, float* params10, int
  * the inclusive bucket ends (table_size ints). */
 int imbart_hashgrid_get_arrays(const imbart_hashgrid* grid, const void** sorted, const int** cell_ends);
 
+/* Hash-grid build that allocates nothing (no counterpart in the reference). For callers that
+ * must not allocate device memory: a server admitting work against a fixed HBM budget, where
+ * cudaMalloc/cudaFree would also synchronize the device and stall other requests' streams,
+ * or a host that hands out only device buffers from its own arena. Same result as
+ * imbart_hashgrid_build, written to caller-owned DEVICE outputs: sorted_out (n float4: xyz +
+ * photon index bits, in bucket order), cell_ends_out (table_size inclusive bucket ends) and
+ * params_out (10 floats: lo xyz, hi xyz, radius, radius^2, cell size, 1/cell size). The build's
+ * scratch is one static device array of about 12 MiB, held by every GPU that loads the library
+ * until the process exits; it bounds n to 1,048,576 photons and table_size (<= 0: 2n) to
+ * 2,097,152 buckets — larger requests return IMBART_ERR_LIMIT without launching anything.
+ * The first call on a device looks the array's address up for that device
+ * (cudaGetSymbolAddress with the device current); make that first call before any stream
+ * capture. All calls share the one array: calls that overlap on the GPU (different streams,
+ * no ordering between them) race and must be serialized by the caller. Stream-ordered. */
+int imbart_hashgrid_build_noalloc(const float* positions, int stride, int n, float radius, float cell_factor,
+                                  int table_size, void* sorted_out, int* cell_ends_out, float* params_out,
+                                  void* stream);
+
 /* ------------------------------------------------------------------------------------ */
 /* Sample generation and wavefront path tracing                                            */
 /* ------------------------------------------------------------------------------------ */
