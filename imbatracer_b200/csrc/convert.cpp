@@ -177,9 +177,13 @@ struct WideBuilder {
         }
     }
 
-    // Quantizes one axis of up to 8 child boxes. Child boxes are first enlarged by a small
-    // absolute pad so that every decoded plane lies strictly outside the true one, which
-    // absorbs the rounding of the slab computation on the GPU.
+    // Quantizes one axis of up to 8 child boxes for the decoder used by the kernel:
+    //     plane = P + (32768 + q) * 2^e,
+    // where the GPU forms 32768 + q as a float with one byte permute (the byte in the mantissa
+    // of 2^15) and evaluates the slab distance with a single FMA. The stored origin P lies
+    // 32768 quanta below the node, so the slab terms carry an extra rounding of up to about
+    // 2^-9 quanta; every child box is therefore enlarged by 1/128 of a quantum in addition to
+    // the absolute pad (2^-20 of the node's magnitude). All checks here are exact (double).
     static void quantize_axis(const float* lo, const float* hi, const bool* valid, int nkids, float pad,
                               float* p_out, uint8_t* bexp_out, uint8_t* qlo, uint8_t* qhi) {
         double nlo = DBL_MAX, nhi = -DBL_MAX;
@@ -188,34 +192,37 @@ struct WideBuilder {
             nlo = std::min(nlo, (double)lo[i] - pad);
             nhi = std::max(nhi, (double)hi[i] + pad);
         }
-        // p must not exceed any padded lower bound: round down to float.
-        float p = (float)nlo;
-        if ((double)p > nlo) p = std::nextafter(p, -FLT_MAX);
-        const double ext = nhi - (double)p;
+        if (nlo > nhi) { nlo = 0.0; nhi = 0.0; }
+        const double ext = nhi - nlo;
         int e = -126;
         if (ext > 0.0) {
             int ex;
-            std::frexp(ext / 255.0, &ex);   // ext / 255 < 2^ex
+            std::frexp(ext / 252.0, &ex);   // ext / 252 < 2^ex; 3 quanta of slack for margins and P's rounding
             e = std::max(ex - 1, -126);
-            while (e < 127 && std::ldexp(255.0, e) < ext) ++e;
+            while (e < 127 && std::ldexp(252.0, e) < ext) ++e;
         }
+        float P = 0.0f;
         for (;;) {
             const double s = std::ldexp(1.0, e);
+            const double margin = s / 128.0;
+            const double origin = nlo - margin - 32768.0 * s;
+            P = (float)origin;
+            if ((double)P > origin) P = std::nextafter(P, -FLT_MAX);
             bool ok = true;
             for (int i = 0; i < nkids; ++i) {
                 if (!valid[i]) { qlo[i] = 1; qhi[i] = 0; continue; }
-                double ql = std::floor(((double)lo[i] - pad - (double)p) / s);
-                double qh = std::ceil(((double)hi[i] + pad - (double)p) / s);
-                if (ql < 0) ql = 0;
-                while (ql > 0 && (double)p + ql * s > (double)lo[i] - pad) ql -= 1;
-                while ((double)p + qh * s < (double)hi[i] + pad) qh += 1;
-                if (qh > 255) { ok = false; break; }
+                const double L = (double)lo[i] - pad - margin, H = (double)hi[i] + pad + margin;
+                double ql = std::floor((L - (double)P) / s) - 32768.0;
+                double qh = std::ceil((H - (double)P) / s) - 32768.0;
+                while ((double)P + (32768.0 + ql) * s > L) ql -= 1;
+                while ((double)P + (32768.0 + qh) * s < H) qh += 1;
+                if (ql < 0 || qh > 255) { ok = false; break; }
                 qlo[i] = (uint8_t)ql; qhi[i] = (uint8_t)qh;
             }
             if (ok || e >= 127) break;
             ++e;
         }
-        *p_out = p;
+        *p_out = P;
         *bexp_out = (uint8_t)(e + 127);
     }
 

@@ -119,18 +119,21 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 }
 
 // ---------------------------------------------------------------------------------------
-// Kernel variants. Variant 0 is the one-ray-per-thread kernel; variants 1..5 are the
+// Kernel variants. Variant 0 is the one-ray-per-thread kernel; variants 1..7 are the
 // persistent-warp kernel at different block sizes / register budgets / shared stack depths.
-// The configuration is process-wide (imbart_set_trace_config, or IMBART_TRACE_VARIANT,
+// Closest-hit and any-hit queries pick their variants separately (measured on the B200:
+// persistent warps win on incoherent closest-hit rays, the one-ray-per-thread kernel on
+// short any-hit traversals). The configuration is process-wide (imbart_set_trace_config /
+// imbart_set_trace_variant_any, or IMBART_TRACE_VARIANT, IMBART_TRACE_VARIANT_ANY,
 // IMBART_TRACE_REFILL and IMBART_TRACE_POSTPONE in the environment).
 // ---------------------------------------------------------------------------------------
 struct TraceConfig {
-    int variant, refill, postpone;
+    int variant, refill, postpone, variant_any;
 };
 
 std::mutex g_cfg_mutex;
 bool g_cfg_init = false;
-TraceConfig g_cfg{4, 20, 0};
+TraceConfig g_cfg{4, 24, 0, 0};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -141,6 +144,7 @@ TraceConfig current_config() {
     std::lock_guard<std::mutex> lk(g_cfg_mutex);
     if (!g_cfg_init) {
         g_cfg.variant = env_int("IMBART_TRACE_VARIANT", g_cfg.variant);
+        g_cfg.variant_any = env_int("IMBART_TRACE_VARIANT_ANY", g_cfg.variant_any);
         g_cfg.refill = env_int("IMBART_TRACE_REFILL", g_cfg.refill);
         g_cfg.postpone = env_int("IMBART_TRACE_POSTPONE", g_cfg.postpone);
         g_cfg_init = true;
@@ -220,6 +224,8 @@ bool dispatch_variant(int variant, int count, int device, cudaStream_t stream, c
         case 3: launch_persistent<kAny, kMasked, kStats, 256, 2, 16>(count, device, stream, p); return true;
         case 4: launch_persistent<kAny, kMasked, kStats, 256, 3, 12>(count, device, stream, p); return true;
         case 5: launch_persistent<kAny, kMasked, kStats, 64, 8, 16>(count, device, stream, p); return true;
+        case 6: launch_persistent<kAny, kMasked, kStats, 256, 4, 8>(count, device, stream, p); return true;
+        case 7: launch_persistent<kAny, kMasked, kStats, 128, 7, 10>(count, device, stream, p); return true;
         default: return false;
     }
 }
@@ -253,8 +259,9 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
     const bool any = (flags & IMBART_TRACE_ANY) != 0;
     const bool masked = s->info.masked != 0;
     const TraceConfig cfg = current_config();
+    const int variant = any ? cfg.variant_any : cfg.variant;
     bool launched;
-    if (cfg.variant == 0) {
+    if (variant == 0) {
         const int block = 128;
         const int grid = (count + block - 1) / block;
         if (stats) launched = dispatch_simple<true>(any, masked, grid, block, stream, p);
@@ -265,8 +272,8 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
         p.work = work;
         p.refill_lanes = std::min(std::max(cfg.refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
-        if (stats) launched = dispatch_persistent<true>(cfg.variant, any, masked, count, s->device, stream, p);
-        else launched = dispatch_persistent<false>(cfg.variant, any, masked, count, s->device, stream, p);
+        if (stats) launched = dispatch_persistent<true>(variant, any, masked, count, s->device, stream, p);
+        else launched = dispatch_persistent<false>(variant, any, masked, count, s->device, stream, p);
     }
     if (!launched) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");
@@ -540,14 +547,25 @@ int imbart_scene_error_count(const imbart_scene* scene) {
 int64_t imbart_kernel_launch_count(void) { return launches_total(); }
 
 int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
-    if (variant < 0 || variant > 5 || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||
+    if (variant < 0 || variant > 7 || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||
         postpone_lanes > 32) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_config: out of range");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
     current_config();
     std::lock_guard<std::mutex> lk(g_cfg_mutex);
-    g_cfg = TraceConfig{variant, refill_lanes, postpone_lanes};
+    g_cfg = TraceConfig{variant, refill_lanes, postpone_lanes, variant};
+    return 0;
+}
+
+int imbart_set_trace_variant_any(int variant) {
+    if (variant < 0 || variant > 7) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_variant_any: out of range");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    current_config();
+    std::lock_guard<std::mutex> lk(g_cfg_mutex);
+    g_cfg.variant_any = variant;
     return 0;
 }
 
@@ -558,6 +576,8 @@ int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes
     if (postpone_lanes) *postpone_lanes = c.postpone;
     return 0;
 }
+
+int imbart_get_trace_variant_any(void) { return current_config().variant_any; }
 
 void imbart_invalidate_scenes(void) { clear_cache(); }
 

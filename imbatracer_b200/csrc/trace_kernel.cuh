@@ -86,7 +86,7 @@ struct SpaceRay {
 __device__ __forceinline__ float safe_rcp(float d) {
     // Zero components get a huge finite inverse of the right sign so that slab tests stay
     // free of 0 * inf; the triangle test uses the true direction.
-    const float tiny = 1e-30f;
+    const float tiny = 1e-20f;
     const float dd = fabsf(d) < tiny ? copysignf(tiny, d) : d;
     return __frcp_rn(dd);
 }
@@ -153,10 +153,11 @@ __device__ __forceinline__ float xform_row(const float4 m, float x, float y, flo
     return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
 }
 
-// Byte k of w as an exact float: the byte is placed in the mantissa of 2^23 with one byte
-// permute, then 2^23 is subtracted (both full-rate ALU operations, no conversion unit).
-__device__ __forceinline__ float byte_to_float(uint32_t w, int k) {
-    return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (uint32_t)k)) - 8388608.0f;
+// 32768 + (byte k of w) as an exact float, with one byte permute: the byte lands in bits
+// 8..15 of the float 2^15 (0x47000000), whose mantissa step there is 1. The node's origin
+// is stored 32768 quanta low, so this value feeds the slab FMA directly.
+__device__ __forceinline__ float byte_plane(uint32_t w, int k) {
+    return __int_as_float(__byte_perm(w, 0x47000000u, 0x7604u | ((uint32_t)k << 4)));
 }
 
 // Intersects the 8 child boxes of a node. Returns internal-child hits in octant order
@@ -191,33 +192,37 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
     if (r.ix < 0.0f) { uint32_t t0 = qx.x, t1 = qx.y; qx.x = qx.z; qx.y = qx.w; qx.z = t0; qx.w = t1; }
     if (r.iy < 0.0f) { uint32_t t0 = qy.x, t1 = qy.y; qy.x = qy.z; qy.y = qy.w; qy.z = t0; qy.w = t1; }
     if (r.iz < 0.0f) { uint32_t t0 = qz.x, t1 = qz.y; qz.x = qz.z; qz.y = qz.w; qz.z = t0; qz.w = t1; }
-    hits8 = 0;
-    prim_mask = 0;
+    uint32_t hitbits = 0;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const uint32_t wn_x = s < 4 ? qx.x : qx.y, wf_x = s < 4 ? qx.z : qx.w;
         const uint32_t wn_y = s < 4 ? qy.x : qy.y, wf_y = s < 4 ? qy.z : qy.w;
         const uint32_t wn_z = s < 4 ? qz.x : qz.y, wf_z = s < 4 ? qz.z : qz.w;
         const int k = s & 3;
-        const float tnx = fmaf(byte_to_float(wn_x, k), ax, bnx);
-        const float tfx = fmaf(byte_to_float(wf_x, k), ax, bfx);
-        const float tny = fmaf(byte_to_float(wn_y, k), ay, bny);
-        const float tfy = fmaf(byte_to_float(wf_y, k), ay, bfy);
-        const float tnz = fmaf(byte_to_float(wn_z, k), az, bnz);
-        const float tfz = fmaf(byte_to_float(wf_z, k), az, bfz);
+        const float tnx = fmaf(byte_plane(wn_x, k), ax, bnx);
+        const float tfx = fmaf(byte_plane(wf_x, k), ax, bfx);
+        const float tny = fmaf(byte_plane(wn_y, k), ay, bny);
+        const float tfy = fmaf(byte_plane(wf_y, k), ay, bfy);
+        const float tnz = fmaf(byte_plane(wn_z, k), az, bnz);
+        const float tfz = fmaf(byte_plane(wf_z, k), az, bfz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
         const float tf = fminf(fminf(tfx, tfy), tfz) * IMBART_SLACK;
-        const bool hit = tn <= fminf(tf, tlimit);
-        if (hit) {
-            if ((imask >> s) & 1u) {
-                hits8 |= 1u << (s ^ r.oct);
-            } else {
-                const uint32_t meta = ((s < 4 ? q1.z : q1.w) >> (8 * k)) & 0xffu;
-                const uint32_t cnt = meta >> 5;
-                const uint32_t off = meta & 31u;
-                prim_mask |= ((1u << cnt) - 1u) << off;
-            }
-        }
+        hitbits |= (tn <= fminf(tf, tlimit) ? 1u : 0u) << s;
+    }
+    // Internal children, with bit s moved to s ^ oct (three conditional bit-group swaps).
+    uint32_t ib = hitbits & imask;
+    if (r.oct & 1u) ib = ((ib & 0x55u) << 1) | ((ib & 0xAAu) >> 1);
+    if (r.oct & 2u) ib = ((ib & 0x33u) << 2) | ((ib & 0xCCu) >> 2);
+    if (r.oct & 4u) ib = ((ib & 0x0Fu) << 4) | ((ib & 0xF0u) >> 4);
+    hits8 = ib;
+    // Leaf children: their primitive runs (count << 5 | offset in the meta byte).
+    uint32_t lb = hitbits & ~imask;
+    prim_mask = 0;
+    while (lb != 0u) {
+        const uint32_t s = __ffs(lb) - 1;
+        lb &= lb - 1;
+        const uint32_t meta = __byte_perm(s < 4 ? q1.z : q1.w, 0u, s & 3u) & 0xffu;
+        prim_mask |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
     }
 }
 

@@ -89,6 +89,8 @@ _SIGNATURES = {
     "imbart_pt_set_profile": (I, [P, P]),
     "imbart_set_trace_config": (I, [I, I, I]),
     "imbart_get_trace_config": (I, [C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+    "imbart_set_trace_variant_any": (I, [I]),
+    "imbart_get_trace_variant_any": (I, []),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
     "intersect_gpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),

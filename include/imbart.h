@@ -226,14 +226,18 @@ int imbart_scene_error_count(const imbart_scene* scene);
 int64_t imbart_kernel_launch_count(void);
 
 /* Process-wide traversal kernel configuration (the tuning knobs of the autotuner):
- * variant 0 = one ray per thread; 1..5 = persistent warps (1: 128 threads x 4 blocks/SM,
- * 16-entry shared stack; 2: 128 x 6, 12; 3: 256 x 2, 16; 4: 256 x 3, 12; 5: 64 x 8, 16);
- * refill_lanes (1..32): a warp fetches new rays once this many lanes are idle;
- * postpone_lanes (0..32): triangle tests are postponed while fewer than
+ * variant 0 = one ray per thread; 1..7 = persistent warps (1: 128 threads x 4 blocks/SM,
+ * 16-entry shared stack; 2: 128 x 6, 12; 3: 256 x 2, 16; 4: 256 x 3, 12; 5: 64 x 8, 16;
+ * 6: 256 x 4, 8; 7: 128 x 7, 10); refill_lanes (1..32): a warp fetches new rays once this
+ * many lanes are idle; postpone_lanes (0..32): triangle tests are postponed while fewer than
  * postpone_lanes/32 of the live lanes would test together (0 = never).
- * The defaults can also be set with IMBART_TRACE_VARIANT / _REFILL / _POSTPONE. */
+ * imbart_set_trace_config sets the variant of both query types; imbart_set_trace_variant_any
+ * then overrides the any-hit one. Defaults: closest 4, any-hit 0, refill 24, postpone 0
+ * (environment: IMBART_TRACE_VARIANT, _VARIANT_ANY, _REFILL, _POSTPONE). */
 int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes);
+int imbart_set_trace_variant_any(int variant);
 int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes);
+int imbart_get_trace_variant_any(void);
 
 /* ------------------------------------------------------------------------------------ */
 /* Photon hash grid (replaces HashGrid::build / HashGrid::query, rangesearch.h:25-129,     */

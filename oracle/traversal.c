@@ -44,9 +44,10 @@ typedef struct {
 
 static int max_dim3(float x, float y, float z) { return (x > y) ? ((x > z) ? 0 : 2) : ((y > z) ? 1 : 2); }
 
-/* Reciprocal with zero components replaced by +-1e-30 (keeps slab tests finite). */
+/* Reciprocal with components below 1e-20 in magnitude replaced by +-1e-20 (keeps slab tests
+ * finite, also when the kernel scales slab terms by 32768 + q). */
 static float safe_rcp(float d) {
-    const float tiny = 1e-30f;
+    const float tiny = 1e-20f;
     const float dd = fabsf(d) < tiny ? copysignf(tiny, d) : d;
     return 1.0f / dd;
 }
@@ -373,8 +374,8 @@ static void wnode_hit(const o_wnode* n, const wspace_t* r, float tmin, float tli
         for (int a = 0; a < 3; ++a) {
             const uint8_t qn = r->i[a] < 0.0f ? hi[a][sl] : lo[a][sl];
             const uint8_t qf = r->i[a] < 0.0f ? lo[a][sl] : hi[a][sl];
-            tn[a] = fmaf((float)qn, ax[a], bn[a]);
-            tf[a] = fmaf((float)qf, ax[a], bf[a]);
+            tn[a] = fmaf(32768.0f + (float)qn, ax[a], bn[a]);
+            tf[a] = fmaf(32768.0f + (float)qf, ax[a], bf[a]);
         }
         const float tnear = fmaxf(fmaxf(tn[0], tn[1]), fmaxf(tn[2], tmin));
         const float tfar = fminf(fminf(tf[0], tf[1]), tf[2]) * W_SLACK;
