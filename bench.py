@@ -117,17 +117,35 @@ def trace_bytes(rays: int, work) -> int:
     return 48 * rays + 80 * int(work[0]) + 48 * int(work[1]) + 64 * int(work[2])
 
 
+class _StdoutToStderr:
+    """Sends file descriptor 1 to stderr while the reference's C++ code prints its progress, so
+    that the bench's stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def reference_cpu(desc, steps, threads, w, h, seed=7):
     """The reference's own CPU path tracer on a bounded image; returns (Mrays/s, rays/step, s/step)."""
     from oracle import refwrap as R
-    rs = R.RefScene(desc)
-    tot_rays, tot_s = 0, 0.0
-    for k in range(steps):
-        t0 = time.perf_counter()
-        _, a, b = rs.render_pt_threads(w, h, SPP, MAX_PATH_LEN, seed + k, threads)
-        tot_s += time.perf_counter() - t0
-        tot_rays += a + b
-    rs.close()
+    with _StdoutToStderr():
+        rs = R.RefScene(desc)
+        tot_rays, tot_s = 0, 0.0
+        for k in range(steps):
+            t0 = time.perf_counter()
+            _, a, b = rs.render_pt_threads(w, h, SPP, MAX_PATH_LEN, seed + k, threads)
+            tot_s += time.perf_counter() - t0
+            tot_rays += a + b
+        rs.close()
     return tot_rays / tot_s / 1e6, tot_rays // max(steps, 1), tot_s / max(steps, 1)
 
 

@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -18,12 +19,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu"]
+SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu", "server.cu"]
 SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp"]
 # Shading and sample generation mirror the reference's separately rounded single-precision
 # arithmetic: no fused multiply-add in device code, no contraction in the host camera set-up.
 # (The traversal kernels spell out their rounding with intrinsics and keep FMA elsewhere.)
-EXTRA_FLAGS = {"wavefront.cu": ["-fmad=false"], "camera.cpp": ["-Xcompiler", "-ffp-contract=off"]}
+EXTRA_FLAGS = {"wavefront.cu": ["-fmad=false"], "server.cu": ["-fmad=false"],
+               "camera.cpp": ["-Xcompiler", "-ffp-contract=off"]}
 
 
 def nvcc() -> str:
@@ -51,18 +53,20 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     inc = ["-I", CSRC, "-I", os.path.join(HERE, "..", "include")]
     for src in SOURCES_CU:
         obj = os.path.join(objdir, src + ".o")
         extra = (["-Xptxas", "-v"] if ptxas_verbose else []) + EXTRA_FLAGS.get(src, [])
-        _run([nvcc(), *ARCH, *NVCC_FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+        cmds.append([nvcc(), *ARCH, *NVCC_FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     for src in SOURCES_CPP:
         obj = os.path.join(objdir, src + ".o")
-        _run([nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src, []), *inc, "-x", "c++", "-c", os.path.join(CSRC, src), "-o",
-              obj], verbose)
+        cmds.append([nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src, []), *inc, "-x", "c++", "-c", os.path.join(CSRC, src),
+                     "-o", obj])
         objs.append(obj)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(lambda c: _run(c, verbose), cmds))
     out = lib_path()
     tmp = out + ".tmp"
     _run([nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lpthread"], verbose)

@@ -95,8 +95,19 @@ long long launches_total();
 
 // Stream-ordered traversal launch used by the wavefront integrators (trace.cu). `stream` is
 // a cudaStream_t; rays are imbart_ray records, hits imbart_hit records.
+// `roots` (optional): per-ray root node for batches over several scenes of one pool;
+// `count_ptr` (optional): device-resident ray count, `count` being its upper bound.
 int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
-                          int flags, void* stream, unsigned long long* stats);
+                          int flags, void* stream, unsigned long long* stats, const int* roots = nullptr,
+                          const int* count_ptr = nullptr);
+
+// Uploads a converted scene into arrays of its own (the path of imbart_scene_from_node2).
+imbart_scene* upload_wide_scene(const HostWideScene& h, int device);
+
+// A scene whose node, triangle and instance arrays are all `pool`, indexed in units of their
+// own record sizes (WideNode, WideTri, WideInst); the pool stays owned by the caller.
+imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes);
+void scene_pool_view_destroy(imbart_scene* s);
 
 inline int float_bits(float f) { union { float f; int i; } u; u.f = f; return u.i; }
 inline float bits_float(int i) { union { float f; int i; } u; u.i = i; return u.f; }

@@ -29,6 +29,7 @@ struct imbart_scene {
     int n_masks = 0;
     int* error_flags = nullptr;
     imbart_scene_info info{};
+    bool owns_arrays = true;   // false for views into a node pool shared by several scenes
 };
 
 namespace imbart {
@@ -56,8 +57,10 @@ void free_scene(imbart_scene* s) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
-    cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->insts);
-    cudaFree(s->indices); cudaFree(s->texcoords); cudaFree(s->masks); cudaFree(s->mask_buffer);
+    if (s->owns_arrays) {
+        cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->insts);
+        cudaFree(s->indices); cudaFree(s->texcoords); cudaFree(s->masks); cudaFree(s->mask_buffer);
+    }
     cudaFree(s->error_flags);
     cudaSetDevice(prev);
     delete s;
@@ -133,7 +136,7 @@ struct TraceConfig {
 
 std::mutex g_cfg_mutex;
 bool g_cfg_init = false;
-TraceConfig g_cfg{4, 24, 0, 0};
+TraceConfig g_cfg{4, 24, 0, 6};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -240,8 +243,9 @@ bool dispatch_persistent(int variant, bool any, bool masked, int count, int devi
 }
 
 int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out,
-                 int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr) {
-    if (!s || (!rays && count > 0) || (!hits && count > 0) || count < 0) {
+                 int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr,
+                 const int* roots = nullptr, const int* count_ptr = nullptr) {
+    if (!s || (!rays && count > 0) || (!hits && count > 0) || count < 0 || (roots && s->info.masked)) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: invalid argument");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
@@ -254,6 +258,8 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
     p.hits = reinterpret_cast<int4*>(hits);
     p.v_out = v_out;
     p.count = count;
+    p.roots = roots;
+    p.count_ptr = count_ptr;
     p.error_flags = s->error_flags;
     p.stats = stats;
     const bool any = (flags & IMBART_TRACE_ANY) != 0;
@@ -428,10 +434,33 @@ void dropin_host(bool any, int root, imbart_node4* nodes, imbart_instance_node* 
 }  // namespace
 
 int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
-                          int flags, void* stream, unsigned long long* stats) {
+                          int flags, void* stream, unsigned long long* stats, const int* roots,
+                          const int* count_ptr) {
     return launch_trace(scene, reinterpret_cast<const imbart_ray*>(rays), reinterpret_cast<imbart_hit*>(hits), v_out,
-                        count, flags, (cudaStream_t)stream, stats);
+                        count, flags, (cudaStream_t)stream, stats, roots, count_ptr);
 }
+
+imbart_scene* upload_wide_scene(const HostWideScene& h, int device) { return upload_scene(h, device); }
+
+imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return nullptr;
+    imbart_scene* s = new imbart_scene;
+    s->device = device;
+    s->owns_arrays = false;
+    s->nodes = (WideNode*)pool;
+    s->tris = (WideTri*)pool;
+    s->insts = (WideInst*)pool;
+    s->info.device_bytes = (int64_t)pool_bytes;
+    const bool ok = cuda_ok(cudaMalloc((void**)&s->error_flags, 4 * sizeof(int)), "cudaMalloc") &&
+                    cuda_ok(cudaMemset(s->error_flags, 0, 4 * sizeof(int)), "cudaMemset");
+    cudaSetDevice(prev);
+    if (!ok) { free_scene(s); return nullptr; }
+    return s;
+}
+
+void scene_pool_view_destroy(imbart_scene* s) { free_scene(s); }
 
 }  // namespace imbart
 

@@ -44,6 +44,11 @@ struct TraceParams {
     int4* __restrict__ hits;                // 1 int4 per hit (tri, inst, t bits, u bits)
     float* __restrict__ v_out;              // optional
     int count;
+    // Batches over several scenes of one node pool: ray i starts at node roots[i] instead of
+    // `root`. With count_ptr set, the ray count is read from device memory at kernel start
+    // (`count` is then an upper bound the launch was sized for).
+    const int* __restrict__ roots;
+    const int* __restrict__ count_ptr;
     int* __restrict__ error_flags;          // [0]: stack overflow count
     unsigned long long* __restrict__ stats; // statistics variant: nodes, triangles, instances
     // persistent variant
@@ -271,7 +276,8 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
         uint2 stack[kStackSize];
         int sp = 0;
         // Root group: one internal child in slot 0.
-        uint32_t g_base = (uint32_t)p.root, g_imask = 1u, g_hits = 1u << (0u ^ r.oct);
+        uint32_t g_base = (uint32_t)(p.roots ? __ldg(p.roots + ray_index) : p.root), g_imask = 1u,
+                 g_hits = 1u << (0u ^ r.oct);
         uint32_t t_base = 0, t_mask = 0;
         bool done = false;
 
@@ -400,6 +406,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     int sp = 0;
     RayStats st;
     r.kx = r.ky = r.kz = 0;
+    const int count = p.count_ptr ? min(__ldg(p.count_ptr), p.count) : p.count;
 
     auto push = [&](uint32_t x, uint32_t y) -> bool {
         if (sp >= kStackSize) return false;
@@ -422,7 +429,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     for (;;) {
         // Refill idle lanes in warp-wide batches.
         const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
-        unsigned live = __ballot_sync(0xffffffffu, ray >= 0 && ray < p.count);
+        unsigned live = __ballot_sync(0xffffffffu, ray >= 0 && ray < count);
         if (idle != 0u && (live == 0u || __popc(idle) >= p.refill_lanes)) {
             const int leader = __ffs(idle) - 1;
             int base = 0;
@@ -430,8 +437,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
             base = __shfl_sync(0xffffffffu, base, leader);
             if (ray < 0) {
                 const int idx = base + __popc(idle & lt_mask);
-                if (idx >= p.count) {
-                    ray = p.count;
+                if (idx >= count) {
+                    ray = count;
                 } else {
                     ray = idx;
                     const float4 ro = __ldg(p.rays + 2 * ray + 0);
@@ -447,18 +454,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                         wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
                         wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
                         tlimit = best_t * IMBART_SLACK;
-                        g_base = (uint32_t)p.root; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                        g_base = (uint32_t)(p.roots ? __ldg(p.roots + ray) : p.root); g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
                         t_mask = 0;
                     }
                 }
             }
-            live = __ballot_sync(0xffffffffu, ray >= 0 && ray < p.count);
+            live = __ballot_sync(0xffffffffu, ray >= 0 && ray < count);
         }
         if (live == 0u) {
             if (__ballot_sync(0xffffffffu, ray < 0) == 0u) break;   // every lane exhausted
             continue;
         }
-        const bool active = ray >= 0 && ray < p.count;
+        const bool active = ray >= 0 && ray < count;
         if (!active) continue;
         const int n_live = __popc(live);
 
@@ -583,7 +590,8 @@ template <bool kAnyHit, bool kMasked, bool kStats>
 __global__ void __launch_bounds__(128) trace_kernel(TraceParams p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     RayStats st;
-    if (i < p.count) trace_one<kAnyHit, kMasked, kStats>(p, i, st);
+    const int count = p.count_ptr ? min(__ldg(p.count_ptr), p.count) : p.count;
+    if (i < count) trace_one<kAnyHit, kMasked, kStats>(p, i, st);
     if (kStats) {
         // Warp-aggregated accumulation of the per-ray counters.
         const unsigned m = __activemask();

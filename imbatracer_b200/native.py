@@ -44,6 +44,37 @@ class PtProfile(C.Structure):
                 ("closest_work", C.c_ulonglong * 3), ("shadow_work", C.c_ulonglong * 3)]
 
 
+class SceneSource(C.Structure):
+    _fields_ = [("root", C.c_int), ("nodes", C.c_void_p), ("n_nodes", C.c_int),
+                ("instances", C.c_void_p), ("n_instances", C.c_int), ("tris", C.c_void_p), ("n_tri_vec4", C.c_int),
+                ("vertices", C.c_void_p), ("n_vertices", C.c_int), ("normals", C.c_void_p), ("texcoords", C.c_void_p),
+                ("mesh_tris", C.c_void_p), ("geom_normals", C.c_void_p), ("n_mesh_tris", C.c_int),
+                ("inst_inv", C.c_void_p), ("n_inst_inv", C.c_int), ("mat_kind", C.c_void_p),
+                ("mat_params", C.c_void_p), ("n_mats", C.c_int), ("tri_lights", C.c_void_p), ("n_tri_lights", C.c_int),
+                ("env_color", C.c_void_p), ("bsphere", C.c_void_p)]
+
+
+class RenderRequest(C.Structure):
+    _fields_ = [("scene", C.c_int), ("raster_to_world", C.c_float * 16), ("cam_pos", C.c_float * 3),
+                ("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("max_path_len", C.c_int),
+                ("rr_start", C.c_int), ("seed_base", C.c_ulonglong), ("image_host", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("kind", C.c_int), ("submit_ms", C.c_double), ("start_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in ("submitted", "completed", "failed", "waves", "closest_rays", "shadow_rays",
+                                            "batch_rays", "scene_uploads", "scene_evictions", "pool_bytes",
+                                            "pool_used_bytes", "kernel_launches")]
+
+
+SERVE_BATCHED = 0
+SERVE_PLAIN = 1
+
+
 class ImbartError(RuntimeError):
     pass
 
@@ -93,6 +124,14 @@ _SIGNATURES = {
     "imbart_get_trace_variant_any": (I, []),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
+    "imbart_server_create": (P, [I, I, C.c_longlong, C.c_longlong]),
+    "imbart_server_destroy": (None, [P]),
+    "imbart_server_add_scene": (I, [P, C.POINTER(SceneSource)]),
+    "imbart_server_submit_render": (C.c_longlong, [P, C.POINTER(RenderRequest)]),
+    "imbart_server_submit_rays": (C.c_longlong, [P, I, P, P, I, I]),
+    "imbart_server_wait": (I, [P, C.c_longlong, C.POINTER(RequestResult)]),
+    "imbart_server_drain": (I, [P]),
+    "imbart_server_get_stats": (I, [P, C.POINTER(ServerStats)]),
     "intersect_gpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
     "occluded_gpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),
     "intersect_cpu_masked_instanced": (None, [I, P, P, P, P, P, P, P, P, P, I]),

@@ -1,0 +1,116 @@
+"""Request server over libimbart's imbart_server_* entry points (include/imbart.h).
+
+    srv = Server(mode="batched", hbm_budget=8 << 30)
+    sid = srv.add_scene(desc)                              # SceneDesc from scenegen
+    t, img = srv.submit_render(sid, desc.camera, 256, 256, spp=4, max_path_len=5, seed_base=1)
+    res = srv.wait(t)                                      # img (host numpy) is now filled
+
+"batched" merges the wavefronts of all admitted requests over all resident scenes (one pool
+of `hbm_budget` bytes with LRU eviction); "plain" serves the same requests one at a time
+through imbart_pt_render / imbart_trace. Both run on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+
+from . import native as N
+from . import scene as S
+from . import scenegen as G
+from .integrators import ShadingData, camera_matrix
+
+MODES = {"batched": N.SERVE_BATCHED, "plain": N.SERVE_PLAIN}
+
+
+class Server:
+    def __init__(self, device: int = 0, mode: str = "batched", hbm_budget: int = 4 << 30, max_paths: int = 4 << 20):
+        self.lib = N.load()
+        self.mode = mode
+        self.h = self.lib.imbart_server_create(device, MODES[mode], int(hbm_budget), int(max_paths))
+        if not self.h:
+            raise N.ImbartError("imbart_server_create: " + N.last_error()[1])
+        self._keep = {}            # ticket -> buffers the server still reads or writes
+        self._scenes = []          # host arrays of registered scenes (the server copies them; kept for reuse)
+        self._lock = threading.Lock()
+
+    def add_scene(self, desc: G.SceneDesc, td: S.TraversalData | None = None) -> int:
+        td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances)
+        sd = ShadingData(desc)
+        src = N.SceneSource()
+        src.root = td.root
+        src.nodes, src.n_nodes = N.ptr(td.nodes), len(td.nodes)
+        src.instances, src.n_instances = N.ptr(td.instances), len(td.instances)
+        src.tris, src.n_tri_vec4 = N.ptr(td.tris), len(td.tris)
+        src.vertices, src.n_vertices = N.ptr(sd.vertices), len(sd.vertices)
+        src.normals, src.texcoords = N.ptr(sd.normals), N.ptr(sd.texcoords)
+        src.mesh_tris, src.geom_normals, src.n_mesh_tris = N.ptr(sd.tris), N.ptr(sd.geom_normals), len(sd.tris)
+        src.inst_inv, src.n_inst_inv = N.ptr(sd.inst_inv), len(sd.inst_inv)
+        src.mat_kind, src.mat_params, src.n_mats = N.ptr(sd.mat_kind), N.ptr(sd.mat_params), len(sd.mat_kind)
+        src.tri_lights, src.n_tri_lights = N.ptr(sd.lights), sd.n_lights
+        src.env_color, src.bsphere = N.ptr(sd.env), N.ptr(sd.bsphere)
+        sid = self.lib.imbart_server_add_scene(self.h, C.byref(src))
+        if sid < 0:
+            raise N.ImbartError("imbart_server_add_scene: " + N.last_error()[1])
+        return sid
+
+    def submit_render(self, scene: int, cam: G.Camera, width: int, height: int, spp: int, max_path_len: int,
+                      seed_base: int, rr_start: int = 0, image: np.ndarray | None = None):
+        """Returns (ticket, image): `image` (height, width, 3) float32 host array, filled when
+        the request completes."""
+        if image is None:
+            image = np.zeros((height, width, 3), np.float32)
+        assert image.dtype == np.float32 and image.flags.c_contiguous and image.size == width * height * 3
+        q = N.RenderRequest()
+        q.scene = scene
+        q.raster_to_world[:] = [float(v) for v in camera_matrix(cam, width, height)]
+        q.cam_pos[:] = [float(v) for v in cam.pos]
+        q.width, q.height, q.spp, q.max_path_len, q.rr_start = width, height, spp, max_path_len, rr_start
+        q.seed_base = seed_base & (2 ** 64 - 1)
+        q.image_host = N.ptr(image)
+        t = self.lib.imbart_server_submit_render(self.h, C.byref(q))
+        if t < 0:
+            raise N.ImbartError("imbart_server_submit_render: " + N.last_error()[1])
+        with self._lock:
+            self._keep[t] = image
+        return t, image
+
+    def submit_rays(self, scene: int, rays, hits, flags: int = N.TRACE_CLOSEST) -> int:
+        """rays / hits: numpy arrays (RAY_DTYPE / HIT_DTYPE, pageable or pinned) or CUDA
+        tensors of the same byte layout."""
+        n = len(rays)
+        t = self.lib.imbart_server_submit_rays(self.h, scene, N.ptr(rays), N.ptr(hits), n, flags)
+        if t < 0:
+            raise N.ImbartError("imbart_server_submit_rays: " + N.last_error()[1])
+        with self._lock:
+            self._keep[t] = (rays, hits)
+        return t
+
+    def wait(self, ticket: int) -> dict:
+        r = N.RequestResult()
+        self.lib.imbart_server_wait(self.h, ticket, C.byref(r))
+        with self._lock:
+            self._keep.pop(ticket, None)
+        return {"status": r.status, "kind": r.kind, "submit_ms": r.submit_ms, "start_ms": r.start_ms,
+                "done_ms": r.done_ms}
+
+    def drain(self) -> None:
+        N.check(self.lib.imbart_server_drain(self.h), "imbart_server_drain")
+
+    def stats(self) -> dict:
+        s = N.ServerStats()
+        N.check(self.lib.imbart_server_get_stats(self.h, C.byref(s)), "imbart_server_get_stats")
+        return {k: getattr(s, k) for k, _ in N.ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.imbart_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -232,7 +232,7 @@ int64_t imbart_kernel_launch_count(void);
  * many lanes are idle; postpone_lanes (0..32): triangle tests are postponed while fewer than
  * postpone_lanes/32 of the live lanes would test together (0 = never).
  * imbart_set_trace_config sets the variant of both query types; imbart_set_trace_variant_any
- * then overrides the any-hit one. Defaults: closest 4, any-hit 0, refill 24, postpone 0
+ * then overrides the any-hit one. Defaults: closest 4, any-hit 6, refill 24, postpone 0
  * (environment: IMBART_TRACE_VARIANT, _VARIANT_ANY, _REFILL, _POSTPONE). */
 int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes);
 int imbart_set_trace_variant_any(int variant);
@@ -359,6 +359,102 @@ typedef struct {
 
 /* Makes the following imbart_pt_render calls of `ctx` fill `profile` (NULL: stop). */
 int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile);
+
+/* ------------------------------------------------------------------------------------ */
+/* Request serving (no counterpart in the reference, which renders one frame per process)  */
+/* ------------------------------------------------------------------------------------ */
+
+/* A server owns one GPU and a worker thread. Render requests (path-traced frames) and ray
+ * batches (closest-hit / any-hit queries) are submitted from any host thread and complete
+ * asynchronously.
+ *
+ * IMBART_SERVE_BATCHED: continuous batching. All resident scenes live in one device pool of
+ * `hbm_budget_bytes` (scene data and render accumulation images); a scene is uploaded when a
+ * request needs it, and when the pool is full the least recently used scene without
+ * outstanding requests is evicted. Every wavefront merges the paths of all admitted render
+ * requests (new camera samples are admitted between wavefronts, max-min fair across requests,
+ * up to `max_paths_in_flight` paths) and the rays of all admitted ray batches, and runs one
+ * closest-hit launch, one shading launch and one any-hit launch over all of them, whatever
+ * their scenes.
+ * IMBART_SERVE_PLAIN: the same requests one at a time in arrival order through the
+ * single-request entry points (imbart_pt_render, imbart_trace) on scenes uploaded once each
+ * (the budget is not applied). This is the baseline the batched mode is measured against.
+ *
+ * A request renders the same image in both modes and alone or in any mix (up to the order
+ * of float additions into its image); a ray batch returns the same hits as imbart_trace. */
+#define IMBART_SERVE_BATCHED 0
+#define IMBART_SERVE_PLAIN 1
+
+typedef struct imbart_server imbart_server;
+
+/* Scene registration data: traversal arrays in the reference GPU layout (as
+ * imbart_scene_from_node2, unmasked) and shading arrays (as imbart_shading_create). All
+ * HOST pointers; the server keeps its own copies. */
+typedef struct {
+    int root;
+    const imbart_node2* nodes; int n_nodes;
+    const imbart_instance_node* instances; int n_instances;
+    const imbart_vec4* tris; int n_tri_vec4;
+    const float* vertices; int n_vertices;
+    const float* normals; const float* texcoords;
+    const int* mesh_tris; const float* geom_normals; int n_mesh_tris;
+    const float* inst_inv; int n_inst_inv;
+    const int* mat_kind; const float* mat_params; int n_mats;
+    const float* tri_lights; int n_tri_lights;
+    const float* env_color;    /* NULL: no environment light */
+    const float* bsphere;      /* NULL: zero */
+} imbart_scene_source;
+
+/* One path-traced frame (as imbart_pt_render with a fresh zeroed image). image_host: HOST
+ * width*height*3 floats, written before the request completes. */
+typedef struct {
+    int scene;
+    float raster_to_world[16];
+    float cam_pos[3];
+    int width, height, spp, max_path_len, rr_start;
+    unsigned long long seed_base;
+    float* image_host;
+} imbart_render_request;
+
+/* Completion record. Times are milliseconds of the host steady clock since the server was
+ * created: submission, admission (scene resident, memory granted) and completion (result in
+ * the caller's buffer). */
+typedef struct {
+    int status;          /* 0 or an IMBART_ERR_* code */
+    int kind;            /* 0 render, 1 ray batch */
+    double submit_ms, start_ms, done_ms;
+} imbart_request_result;
+
+typedef struct {
+    long long submitted, completed, failed;
+    long long waves;             /* merged wavefronts (batched) or per-request wavefronts (plain) */
+    long long closest_rays, shadow_rays, batch_rays;
+    long long scene_uploads, scene_evictions;
+    long long pool_bytes, pool_used_bytes;
+    long long kernel_launches;
+} imbart_server_stats;
+
+/* hbm_budget_bytes: device pool for scenes and images (batched mode; <= 0: 4 GiB);
+ * max_paths_in_flight: paths per merged wavefront (<= 0: 4M); also the limit of ray-batch
+ * rays per wavefront. NULL on error (imbart_last_error). */
+imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_bytes, long long max_paths_in_flight);
+/* Waits for every submitted request, then stops the worker and frees the device memory. */
+void imbart_server_destroy(imbart_server* server);
+/* Registers a scene; returns its id (>= 0) or -(error code). Scenes are not uploaded until
+ * a request needs them. */
+int imbart_server_add_scene(imbart_server* server, const imbart_scene_source* source);
+/* Submits a request; returns a ticket (> 0) or -(error code). */
+long long imbart_server_submit_render(imbart_server* server, const imbart_render_request* request);
+/* rays / hits: HOST (pageable or pinned) or DEVICE pointers of `count` records; flags
+ * IMBART_TRACE_CLOSEST or IMBART_TRACE_ANY. */
+long long imbart_server_submit_rays(imbart_server* server, int scene, const imbart_ray* rays, imbart_hit* hits,
+                                    int count, int flags);
+/* Blocks until the request completed; fills `result` (may be NULL) and forgets the ticket.
+ * Returns the request's status (IMBART_ERR_INVALID_ARGUMENT for an unknown ticket). */
+int imbart_server_wait(imbart_server* server, long long ticket, imbart_request_result* result);
+/* Blocks until every request submitted so far completed. */
+int imbart_server_drain(imbart_server* server);
+int imbart_server_get_stats(imbart_server* server, imbart_server_stats* stats);
 
 /* ------------------------------------------------------------------------------------ */
 /* BVH construction (the builder side of the boundary)                                     */

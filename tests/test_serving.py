@@ -1,0 +1,182 @@
+"""The request server (imbart_server_*): merged wavefronts over several resident scenes.
+
+A render served in a mix of other requests must give the image the single-request path
+(imbart_pt_render) gives alone: paths are seeded per sample and shaded by the same code, so
+only the order of the float additions into the image differs (tolerance: relative RMSE
+1e-5). Ray batches must return exactly the hits of imbart_trace. Eviction under a small
+pool must not change results.
+"""
+import numpy as np
+import pytest
+
+from imbatracer_b200 import native as N
+from imbatracer_b200 import scenegen as G
+from tests import helpers as H
+from tests.test_pt import small_mixed_scene
+
+MIX_TOL = 1e-5
+
+
+def rel_rmse(a, b):
+    return float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / max(np.sqrt(np.mean(b.astype(np.float64) ** 2)),
+                                                                          1e-30))
+
+
+def sphere_scene(seed, n, level):
+    return G._sphere_field(seed, n, level, 64, 64, f"spheres{seed}")
+
+
+@pytest.fixture(scope="module")
+def scenes():
+    from imbatracer_b200 import scene as S
+    out = []
+    for d in (small_mixed_scene(), sphere_scene(3, 6, 2), sphere_scene(4, 10, 3)):
+        out.append((d, S.build_traversal_data(d.meshes, d.instances)))
+    return out
+
+
+def plain_image(d, td, w, h, spp, max_len, seed, rr_start=0):
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    gs = GpuScene(d, td=td)
+    pt = PathTracer(gs, max_path_len=max_len, rr_start=rr_start)
+    img = pt.render(spp, seed, w, h).cpu().numpy()
+    pt.close()
+    gs.close()
+    return img
+
+
+REQS = [  # (scene index, width, height, spp, max_path_len, seed, rr_start)
+    (0, 48, 32, 4, 6, 11, 0),
+    (1, 40, 40, 2, 5, 12, 2),
+    (2, 64, 48, 3, 5, 13, 0),
+    (0, 17, 9, 5, 4, 14, 1),
+    (1, 1, 1, 7, 3, 15, 0),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_renders_in_a_mix_match_single_request_path(cuda, scenes, mode):
+    from imbatracer_b200.serving import Server
+    srv = Server(mode=mode, hbm_budget=256 << 20, max_paths=20000)
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    tickets = []
+    for si, w, h, spp, ml, seed, rr in REQS:
+        d = scenes[si][0]
+        tickets.append(srv.submit_render(ids[si], d.camera, w, h, spp, ml, seed, rr_start=rr))
+    for (t, img), (si, w, h, spp, ml, seed, rr) in zip(tickets, REQS):
+        res = srv.wait(t)
+        assert res["status"] == 0 and res["done_ms"] >= res["start_ms"] >= res["submit_ms"]
+        d, td = scenes[si]
+        ref = plain_image(d, td, w, h, spp, ml, seed, rr)
+        assert rel_rmse(img, ref) <= MIX_TOL, (si, w, h, rel_rmse(img, ref))
+    st = srv.stats()
+    assert st["completed"] == len(REQS) and st["failed"] == 0
+    if mode == "batched":
+        # Several requests shared wavefronts: far fewer waves than the requests' own sum.
+        assert st["waves"] < sum(r[4] for r in REQS) * 2
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_render_alone_equals_render_in_mix(cuda, scenes):
+    from imbatracer_b200.serving import Server
+    d, td = scenes[2]
+    alone = Server(hbm_budget=256 << 20, max_paths=8192)
+    sid = alone.add_scene(d, td)
+    t, img_alone = alone.submit_render(sid, d.camera, 64, 48, 4, 5, 99)
+    assert alone.wait(t)["status"] == 0
+    alone.close()
+    mix = Server(hbm_budget=256 << 20, max_paths=8192)
+    ids = [mix.add_scene(dd, tt) for dd, tt in scenes]
+    others = [mix.submit_render(ids[k % 3], scenes[k % 3][0].camera, 32, 32, 2, 5, 500 + k) for k in range(6)]
+    t, img_mix = mix.submit_render(ids[2], d.camera, 64, 48, 4, 5, 99)
+    rays = G.random_rays(np.random.default_rng(1), 5000, -12, 12)
+    hits = np.zeros(len(rays), N.HIT_DTYPE)
+    tr = mix.submit_rays(ids[0], rays, hits)
+    assert mix.wait(t)["status"] == 0
+    for tt, _ in others:
+        assert mix.wait(tt)["status"] == 0
+    assert mix.wait(tr)["status"] == 0
+    mix.close()
+    assert rel_rmse(img_mix, img_alone) <= MIX_TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("where", ["pageable", "pinned", "device"])
+def test_ray_batches_bit_exact(cuda, scenes, where):
+    import torch
+    from imbatracer_b200 import scene as S
+    from imbatracer_b200.serving import Server
+    srv = Server(hbm_budget=256 << 20, max_paths=30000)   # batches larger than a wavefront are split
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    rng = np.random.default_rng(7)
+    jobs = []
+    for k, (d, td) in enumerate(scenes):
+        for flags in (N.TRACE_CLOSEST, N.TRACE_ANY):
+            n = int(rng.integers(1, 70000))
+            rays = G.random_rays(rng, n, -12, 12)
+            if flags == N.TRACE_ANY:
+                rays["dir"][:, 3] = rng.uniform(0.1, 30.0, n).astype(np.float32)
+            ds = S.DeviceScene(td)
+            want = np.zeros(n, N.HIT_DTYPE)
+            ds.trace_host(rays, want, any_hit=flags == N.TRACE_ANY)
+            ds.close()
+            if where == "pageable":
+                r_in, h_out = rays, np.zeros(n, N.HIT_DTYPE)
+            elif where == "pinned":
+                r_in = torch.from_numpy(rays.view(np.float32).reshape(n, 8)).pin_memory()
+                h_out = torch.zeros((n, 4), dtype=torch.int32).pin_memory()
+            else:
+                r_in = torch.from_numpy(rays.view(np.float32).reshape(n, 8)).cuda()
+                h_out = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+            jobs.append((srv.submit_rays(ids[k], r_in, h_out, flags), h_out, want, flags))
+    for t, h_out, want, flags in jobs:
+        assert srv.wait(t)["status"] == 0
+        got = h_out if isinstance(h_out, np.ndarray) else h_out.cpu().numpy().view(N.HIT_DTYPE).reshape(-1)
+        if flags == N.TRACE_CLOSEST:
+            assert H.hits_equal(got, want).all()
+        else:
+            assert np.array_equal(got["tri_id"] >= 0, want["tri_id"] >= 0)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_lru_eviction_keeps_results(cuda, scenes):
+    from imbatracer_b200.serving import Server
+    probe = Server(hbm_budget=256 << 20, max_paths=4096)
+    ids = [probe.add_scene(d, td) for d, td in scenes]
+    sizes = []
+    for k in range(3):
+        before = probe.stats()["pool_used_bytes"]
+        t, _ = probe.submit_render(ids[k], scenes[k][0].camera, 1, 1, 1, 2, 1)
+        probe.wait(t)
+        sizes.append(probe.stats()["pool_used_bytes"] - before)
+    probe.close()
+    # Room for the largest scene plus an image, not for two scenes at once.
+    assert min(sizes) >= 32 << 10
+    budget = max(sizes) + min(sizes) // 2
+    srv = Server(hbm_budget=budget, max_paths=4096)
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    order = [0, 1, 2, 0, 2, 1]
+    imgs = []
+    for k in order:          # one at a time, so every switch of scene evicts
+        t, img = srv.submit_render(ids[k], scenes[k][0].camera, 24, 16, 2, 4, 70 + k)
+        assert srv.wait(t)["status"] == 0
+        imgs.append(img)
+    st = srv.stats()
+    assert st["scene_evictions"] >= len(order) - 1 and st["scene_uploads"] >= len(order)
+    for k, img in zip(order, imgs):
+        d, td = scenes[k]
+        assert rel_rmse(img, plain_image(d, td, 24, 16, 2, 4, 70 + k)) <= MIX_TOL
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_scene_larger_than_pool_is_refused(cuda, scenes):
+    from imbatracer_b200.serving import Server
+    srv = Server(hbm_budget=64 << 10, max_paths=1024)
+    d, td = scenes[2]
+    with pytest.raises(N.ImbartError):
+        srv.add_scene(d, td)
+    srv.close()
