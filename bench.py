@@ -15,6 +15,12 @@ C++ built in place as oracle/_ref) on all host cores, on a bounded image of the 
 with the oracle's CPU traversal behind its traversal entry points (the reference's AnyDSL
 traversal library is not part of its tree). Its ray counts are the reference scheduler's own.
 `--mode trace`: traversal kernels alone on fixed ray sets of the same frame (kernel tuning).
+
+`serving` (single GPU; `--mode serve` alone): the request server against the same requests
+served one at a time through the single-request path, on the same GPU with the same resident
+scenes (12 sphere fields of 10k-2M triangles). Config 4: 256 renders submitted at once
+(requests/s = 256 / makespan; latency = submission to image in host memory). Config 5:
+Poisson arrivals of 1080p 1-spp frames and 64k-4M-ray batches (p50 / p99 latency).
 """
 from __future__ import annotations
 
@@ -298,6 +304,8 @@ def run_pt(args):
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        if world == 1 and not args.no_serving:
+            line["serving"] = run_serving()
         print(json.dumps(line), flush=True)
     pt.close()
     gs.close()
@@ -324,7 +332,8 @@ def run_reference(args):
     from imbatracer_b200 import scenegen as G
     desc = G.config2()
     threads = os.cpu_count() or 1
-    rs = R.RefScene(desc)
+    with _StdoutToStderr():
+        rs = R.RefScene(desc)
     for k in range(args.warmup):
         rs.render_pt_threads(60, 34, SPP, MAX_PATH_LEN, 99 + k, threads)
     tot, el = 0, 0.0
@@ -347,6 +356,116 @@ def run_reference(args):
                              "sample": sample},
             "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# Serving: the request server (batched) against the same requests one at a time (plain)
+# ---------------------------------------------------------------------------------------
+SERVE_MAX_PATH_LEN = 5        # 4 bounces, as the sphere-field renders
+SERVE_PATHS = 4 << 20         # paths per merged wavefront (and per single-request wavefront)
+SERVE_BUDGET = 16 << 30       # device pool of the batched server
+
+
+def serve_scenes():
+    from imbatracer_b200 import scene as S
+    from imbatracer_b200 import scenegen as G
+    descs = G.config4_scenes()
+    return [(d, S.build_traversal_data(d.meshes, d.instances)) for d in descs]
+
+
+def _percentile(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
+
+
+def serve_arm(mode, scenes, jobs, open_loop, ray_buf=None, hit_buf=None):
+    """Runs `jobs` through a server of `mode`; returns latency / throughput figures."""
+    import ctypes
+    from imbatracer_b200 import native as N
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.serving import Server
+    srv = Server(mode=mode, hbm_budget=SERVE_BUDGET, max_paths=SERVE_PATHS)
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    # Warm-up: every scene once (uploads it), so that both arms start with resident scenes.
+    warm = [srv.submit_render(ids[k], scenes[k][0].camera, 64, 64, 1, SERVE_MAX_PATH_LEN, 1) for k in range(len(ids))]
+    for t, _ in warm:
+        srv.wait(t)
+    s0 = srv.stats()
+    images = {}
+    for j in jobs:
+        if isinstance(j, G.RenderJob) and (j.width, j.height) not in images:
+            images[(j.width, j.height)] = np.zeros((j.height, j.width, 3), np.float32)
+    tickets = []
+    t_start = time.perf_counter()
+    for j in jobs:
+        if open_loop:
+            delay = t_start + j.arrival_s - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+        if isinstance(j, G.RenderJob):
+            cam = scenes[j.scene][0].camera
+            t, _ = srv.submit_render(ids[j.scene], cam, j.width, j.height, j.spp, SERVE_MAX_PATH_LEN, j.seed,
+                                     image=images[(j.width, j.height)])
+        else:
+            off = j.seed % (len(ray_buf) - j.count + 1)
+            t = srv.lib.imbart_server_submit_rays(srv.h, ids[j.scene], N.ptr(ray_buf) + 32 * off,
+                                                  N.ptr(hit_buf) + 16 * off, j.count, j.flags)
+            assert t > 0
+        tickets.append((t, j))
+    res = [(srv.wait(t), j) for t, j in tickets]
+    s1 = srv.stats()
+    srv.close()
+    assert all(r["status"] == 0 for r, _ in res)
+    lat = [r["done_ms"] - r["submit_ms"] for r, _ in res]
+    first = min(r["submit_ms"] for r, _ in res)
+    last = max(r["done_ms"] for r, _ in res)
+    renders = [r["done_ms"] - r["submit_ms"] for r, j in res if isinstance(j, G.RenderJob)]
+    batches = [r["done_ms"] - r["submit_ms"] for r, j in res if not isinstance(j, G.RenderJob)]
+    rays = (s1["closest_rays"] - s0["closest_rays"]) + (s1["shadow_rays"] - s0["shadow_rays"]) + \
+           (s1["batch_rays"] - s0["batch_rays"])
+    span_s = (last - first) * 1e-3
+    out = {"requests_per_s": round(len(res) / span_s, 2), "makespan_s": round(span_s, 3),
+           "p50_ms": round(_percentile(lat, 50), 2), "p99_ms": round(_percentile(lat, 99), 2),
+           "mrays_s": round(rays / span_s / 1e6, 1), "waves": s1["waves"] - s0["waves"]}
+    if renders and batches:
+        out["render_p99_ms"] = round(_percentile(renders, 99), 2)
+        out["batch_p99_ms"] = round(_percentile(batches, 99), 2)
+    return out
+
+
+def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0):
+    """Config 4 (closed batch of 256 renders) and config 5 (Poisson arrivals) in both arms."""
+    import torch
+    from imbatracer_b200 import scenegen as G
+    scenes = scenes or serve_scenes()
+    out = {"scenes": len(scenes), "scene_triangles": [d.instanced_triangles for d, _ in scenes],
+           "max_path_len": SERVE_MAX_PATH_LEN, "paths_per_wavefront": SERVE_PATHS,
+           "pool_bytes": SERVE_BUDGET}
+    jobs4 = G.config4_requests()
+    c4 = {"workload": f"{len(jobs4)} renders at once, square, 64^2-1024^2 px log-uniform, spp in {{1,4,16,64}}, "
+                      f"path tracer (the 20% BPT / 10% VCM share of the mix is rendered with PT)"}
+    for mode in ("plain", "batched"):
+        c4[mode] = serve_arm(mode, scenes, jobs4, open_loop=False)
+    c4["requests_per_s_ratio"] = round(c4["batched"]["requests_per_s"] / c4["plain"]["requests_per_s"], 3)
+    c4["p99_ratio"] = round(c4["plain"]["p99_ms"] / c4["batched"]["p99_ms"], 3)
+    out["config4"] = c4
+    if config5_rates:
+        n_rays = 4 << 20
+        ray_buf = torch.empty((n_rays, 8), dtype=torch.float32).pin_memory().numpy()
+        r = G.random_rays(np.random.default_rng(5), n_rays, -12.0, 12.0)
+        ray_buf[:] = r.view(np.float32).reshape(n_rays, 8)
+        hit_buf = torch.empty((n_rays, 4), dtype=torch.int32).pin_memory().numpy()   # shared by all batches
+        out["config5"] = []
+        for rate in config5_rates:
+            jobs5 = G.config5_requests(rate=rate, duration_s=config5_s)
+            c5 = {"rate_per_s": rate,
+                  "workload": f"Poisson arrivals at {rate:g} req/s for {config5_s:g} s ({len(jobs5)} requests): "
+                              f"1920x1080 1-spp increments and ray batches of 64k-4M rays (half each; pinned host "
+                              f"buffers)"}
+            for mode in ("plain", "batched"):
+                c5[mode] = serve_arm(mode, scenes, jobs5, open_loop=True, ray_buf=ray_buf, hit_buf=hit_buf)
+            c5["p99_ratio"] = round(c5["plain"]["p99_ms"] / c5["batched"]["p99_ms"], 3)
+            out["config5"].append(c5)
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -451,8 +570,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="pt", choices=["pt", "trace"])
+    ap.add_argument("--mode", default="pt", choices=["pt", "trace", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
+    ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
+                    help="serve mode: config 5 arrival rates (req/s)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -462,6 +584,9 @@ def main():
         args.warmup = 3
     if args.mode == "trace":
         run_trace(args)
+    elif args.mode == "serve":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"mode": "serve", "serving": run_serving(config5_rates=tuple(args.rate))}), flush=True)
     else:
         run_pt(args)
 

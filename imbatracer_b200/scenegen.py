@@ -15,6 +15,12 @@ lights, camera and environment.
            Cook-Torrance, glass, mirror; 16 triangular area lights plus a constant environment
            light; a ground quad at y=-13 closes the view (~80% of camera rays hit geometry).
   config3  the config1 generator scaled to ~2M triangles (400 spheres).
+  config4  serving: 12 resident scenes of the config1 generator with 10k-2M triangles
+           (log-uniform), 256 render requests (scene uniform, pixel count log-uniform in
+           [64^2, 1024^2], square, spp in {1, 4, 16, 64}).
+  config5  serving under load: Poisson arrivals of progressive 1080p 1-spp increments and
+           ray batches of 64k-4M rays (log-uniform; origins uniform in the scene box,
+           directions uniform on the sphere) over the config4 scenes.
 """
 from __future__ import annotations
 
@@ -268,3 +274,85 @@ def random_rays(rng: np.random.Generator, n: int, lo, hi, tmin: float = 0.0, tma
     rays["dir"][:, :3] = d.astype(np.float32)
     rays["dir"][:, 3] = tmax
     return rays
+
+
+# ---------------------------------------------------------------------------------------
+# Serving workloads
+# ---------------------------------------------------------------------------------------
+def config4_scene_sizes(n_scenes: int = 12, lo: int = 10_000, hi: int = 2_000_000) -> list[int]:
+    """Triangle counts of the resident scenes: log-uniformly spaced from lo to hi."""
+    return [int(round(lo * (hi / lo) ** (k / max(n_scenes - 1, 1)))) for k in range(n_scenes)]
+
+
+def config4_scenes(seed: int = 1, n_scenes: int = 12, lo: int = 10_000, hi: int = 2_000_000) -> list[SceneDesc]:
+    """Sphere fields (the config1 generator) with about the requested triangle counts."""
+    out = []
+    for k, tris in enumerate(config4_scene_sizes(n_scenes, lo, hi)):
+        n_spheres = max(1, int(round(tris / 5120)))
+        out.append(_sphere_field(seed + 100 * k, n_spheres, 4, 512, 512, f"serve{k}"))
+    return out
+
+
+@dataclass
+class RenderJob:
+    scene: int
+    width: int
+    height: int
+    spp: int
+    seed: int
+    arrival_s: float = 0.0
+
+
+@dataclass
+class RayJob:
+    scene: int
+    count: int
+    flags: int
+    seed: int
+    arrival_s: float = 0.0
+
+
+def config4_requests(seed: int = 1, n: int = 256, n_scenes: int = 12, min_side: int = 64,
+                     max_side: int = 1024) -> list[RenderJob]:
+    """All requests arrive at once (a closed batch)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n):
+        side = int(round(np.exp(rng.uniform(np.log(min_side), np.log(max_side)))))
+        jobs.append(RenderJob(int(rng.integers(n_scenes)), side, side, int(rng.choice([1, 4, 16, 64])),
+                              int(rng.integers(1, 2 ** 31))))
+    return jobs
+
+
+def config5_requests(seed: int = 1, rate: float = 100.0, duration_s: float = 4.0, n_scenes: int = 12,
+                     ray_share: float = 0.5, min_rays: int = 65536, max_rays: int = 4 << 20,
+                     width: int = 1920, height: int = 1080) -> list:
+    """Poisson arrivals at `rate` requests/s for `duration_s`: 1-spp frames of width x height
+    (a progressive increment: its own seed) or ray batches (closest-hit and any-hit alike)."""
+    rng = np.random.default_rng(seed)
+    t, jobs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration_s:
+            break
+        scene = int(rng.integers(n_scenes))
+        if rng.uniform() < ray_share:
+            count = int(round(np.exp(rng.uniform(np.log(min_rays), np.log(max_rays)))))
+            jobs.append(RayJob(scene, count, int(rng.integers(2)), int(rng.integers(1, 2 ** 31)), t))
+        else:
+            jobs.append(RenderJob(scene, width, height, 1, int(rng.integers(1, 2 ** 31)), t))
+    return jobs
+
+
+def scene_box(desc: SceneDesc) -> tuple[np.ndarray, np.ndarray]:
+    """World-space box of a scene's instanced meshes."""
+    lo = np.full(3, np.inf, np.float32)
+    hi = np.full(3, -np.inf, np.float32)
+    for inst in desc.instances:
+        mlo, mhi = desc.meshes[inst.mesh_id].bounding_box()
+        m = inst.mat[:3, :]
+        c = m[:, :3] @ ((mhi + mlo) * np.float32(0.5)) + m[:, 3]
+        e = np.abs(m[:, :3]) @ ((mhi - mlo) * np.float32(0.5))
+        lo = np.minimum(lo, c - e)
+        hi = np.maximum(hi, c + e)
+    return lo, hi
