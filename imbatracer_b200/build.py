@@ -19,12 +19,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu", "server.cu"]
+SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu", "server.cu", "vcm.cu"]
 SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp"]
 # Shading and sample generation mirror the reference's separately rounded single-precision
 # arithmetic: no fused multiply-add in device code, no contraction in the host camera set-up.
 # (The traversal kernels spell out their rounding with intrinsics and keep FMA elsewhere.)
-EXTRA_FLAGS = {"wavefront.cu": ["-fmad=false"], "server.cu": ["-fmad=false"],
+EXTRA_FLAGS = {"wavefront.cu": ["-fmad=false"], "server.cu": ["-fmad=false"], "vcm.cu": ["-fmad=false"],
                "camera.cpp": ["-Xcompiler", "-ffp-contract=off"]}
 
 

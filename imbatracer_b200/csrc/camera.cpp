@@ -155,3 +155,21 @@ extern "C" int imbart_camera_setup(const float* pos, const float* dir, const flo
     }
     return 0;
 }
+
+extern "C" int imbart_camera_make(const float* pos, const float* dir, const float* up, float fov, int width,
+                                  int height, imbart_camera* out) {
+    if (!out || !pos || !dir || !up || width <= 0 || height <= 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_camera_make: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    const int rc = imbart_camera_setup(pos, dir, up, fov, (float)width, (float)height, 1.0f, out->raster_to_world,
+                                       out->world_to_raster, &out->img_plane_dist);
+    if (rc) return rc;
+    // forward_ = normalize(dir) (camera.h:29-34)
+    const V3 d = normalize(V3{dir[0], dir[1], dir[2]});
+    out->dir[0] = d.x; out->dir[1] = d.y; out->dir[2] = d.z;
+    out->pos[0] = pos[0]; out->pos[1] = pos[1]; out->pos[2] = pos[2];
+    out->width = width;
+    out->height = height;
+    return 0;
+}

@@ -20,6 +20,7 @@
 #include <mutex>
 #include <string>
 
+#include "hashgrid_query.cuh"
 #include "imbart_internal.h"
 
 struct imbart_hashgrid {
@@ -43,7 +44,7 @@ namespace {
 constexpr int kBlock = 256;
 constexpr int kScanItems = 8;                 // items per thread in the scan kernels
 constexpr int kScanTile = kBlock * kScanItems;
-constexpr int kMaxK = 64;
+constexpr int kMaxK = kGridMaxK;
 
 bool ok(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return true;
@@ -107,9 +108,6 @@ __global__ void params_kernel(const int* __restrict__ box, float radius, float c
     prm[9] = __fdiv_rn(1.0f, cell);
 }
 
-__device__ __forceinline__ int hash_cell(uint32_t x, uint32_t y, uint32_t z, uint32_t table) {
-    return (int)(((x * 73856093u) ^ (y * 19349663u) ^ (z * 83492791u)) % table);
-}
 
 __device__ __forceinline__ int cell_of_point(const float* prm, float px, float py, float pz, uint32_t table) {
     const float inv = prm[9];
@@ -208,8 +206,7 @@ __global__ void scatter_kernel(const float* __restrict__ pos, int stride, int n,
     }
 }
 
-// One query per thread. The k best photons are kept sorted by squared distance with the
-// reference's insertion rule; the result is then ordered by (distance, index).
+// One query per thread (the search itself is grid_query_knn, hashgrid_query.cuh).
 __global__ void query_kernel(const float4* __restrict__ sorted, const int* __restrict__ ends,
                              const float* __restrict__ prm, uint32_t table, const float* __restrict__ queries,
                              int nq, int k, int* __restrict__ out_ids, int* __restrict__ out_count,
@@ -222,57 +219,7 @@ __global__ void query_kernel(const float4* __restrict__ sorted, const int* __res
     const float qx = queries[3 * (size_t)q + 0], qy = queries[3 * (size_t)q + 1], qz = queries[3 * (size_t)q + 2];
     float dist[kMaxK];
     int ids[kMaxK];
-    int count = 0;
-    const bool inside = qx >= sp[0] && qy >= sp[1] && qz >= sp[2] && qx <= sp[3] && qy <= sp[4] && qz <= sp[5];
-    if (inside) {
-        const float inv = sp[9], r2 = sp[7];
-        const float cx = __fmul_rn(inv, __fsub_rn(qx, sp[0]));
-        const float cy = __fmul_rn(inv, __fsub_rn(qy, sp[1]));
-        const float cz = __fmul_rn(inv, __fsub_rn(qz, sp[2]));
-        const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
-        const int px = (int)fx, py = (int)fy, pz = (int)fz;
-        const int pxo = px + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
-        const int pyo = py + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
-        const int pzo = pz + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
-        for (int j = 0; j < 8; ++j) {
-            const int x = (j & 4) ? pxo : px;
-            const int y = (j & 2) ? pyo : py;
-            const int z = (j & 1) ? pzo : pz;
-            const int c = hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, table);
-            const int b = c == 0 ? 0 : __ldg(ends + c - 1);
-            const int e = __ldg(ends + c);
-            for (int s = b; s < e; ++s) {
-                const float4 ph = __ldg(sorted + s);
-                const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
-                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                if (!(d2 <= r2)) continue;
-                if (count == k) {
-                    if (dist[count - 1] < d2) continue;
-                } else {
-                    count++;
-                }
-                dist[count - 1] = d2;
-                ids[count - 1] = __float_as_int(ph.w);
-                for (int l = count - 2; l >= 0; --l) {
-                    if (dist[l] > d2) {
-                        const float td = dist[l]; dist[l] = dist[l + 1]; dist[l + 1] = td;
-                        const int ti = ids[l]; ids[l] = ids[l + 1]; ids[l + 1] = ti;
-                    } else {
-                        break;
-                    }
-                }
-            }
-        }
-        // Deterministic order among equal distances: by photon index.
-        for (int i = 1; i < count; ++i) {
-            const float d = dist[i];
-            const int id = ids[i];
-            int l = i - 1;
-            while (l >= 0 && dist[l] == d && ids[l] > id) { dist[l + 1] = dist[l]; ids[l + 1] = ids[l]; --l; }
-            dist[l + 1] = d;
-            ids[l + 1] = id;
-        }
-    }
+    const int count = grid_query_knn(sorted, ends, sp, table, qx, qy, qz, k, dist, ids);
     out_count[q] = count;
     int* o = out_ids + (size_t)q * k;
     for (int i = 0; i < k; ++i) o[i] = i < count ? ids[i] : -1;
@@ -300,6 +247,18 @@ bool grow(T** p, int* cap, int need) {
 }
 
 }  // namespace
+
+bool hashgrid_device_view(const imbart_hashgrid* g, const void** sorted, const int** cell_ends, const float** params,
+                          int* table, int* n) {
+    if (!g || g->table == 0) return false;
+    *sorted = g->sorted;
+    *cell_ends = g->cell_ends;
+    *params = g->params;
+    *table = g->table;
+    *n = g->n;
+    return true;
+}
+
 }  // namespace imbart
 
 using namespace imbart;

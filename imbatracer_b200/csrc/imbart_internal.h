@@ -101,6 +101,11 @@ int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hit
                           int flags, void* stream, unsigned long long* stats, const int* roots = nullptr,
                           const int* count_ptr = nullptr);
 
+// Device arrays of a built photon grid (hashgrid.cu): photons in bucket order (float4 xyz +
+// index bits), inclusive bucket ends, the 10 grid parameters; false before the first build.
+bool hashgrid_device_view(const imbart_hashgrid* g, const void** sorted, const int** cell_ends, const float** params,
+                          int* table, int* n);
+
 // Uploads a converted scene into arrays of its own (the path of imbart_scene_from_node2).
 imbart_scene* upload_wide_scene(const HostWideScene& h, int device);
 

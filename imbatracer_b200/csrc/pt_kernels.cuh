@@ -21,6 +21,13 @@
 #include "rng.cuh"
 #include "shade.cuh"
 
+// Shading data of one scene on one GPU (imbart_shading_create).
+struct imbart_shading {
+    int device = 0;
+    imbart::sh::ShadingScene s{};
+    std::vector<void*> allocations;
+};
+
 namespace imbart {
 namespace pt {
 namespace {   // every including translation unit gets its own copy of the kernels

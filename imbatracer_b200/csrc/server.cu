@@ -431,6 +431,7 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
     ss.geom_normals = reinterpret_cast<const float*>(b + s.o_gn);
     ss.inst_inv = reinterpret_cast<const float*>(b + s.o_inv);
     ss.materials = mats;
+    ss.n_materials = (int)s.mats.size();
     ss.lights = lights;
     ss.n_tri_lights = s.n_tri_lights;
     ss.has_env = s.has_env ? 1 : 0;

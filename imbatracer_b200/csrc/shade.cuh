@@ -100,6 +100,34 @@ __device__ __forceinline__ void draw2(Rng& rng, float& u1, float& u2) {
     u1 = rng.next_float();
 }
 
+// sample_concentric_disc (random.h:126-155, Shirley-Chiu as in SmallVCM).
+__device__ __forceinline__ void sample_concentric_disc(float u1, float u2, float& dx, float& dy) {
+    float phi, r;
+    const float a = 2 * u1 - 1;
+    const float b = 2 * u2 - 1;
+    if (a > -b) {
+        if (a > b) {
+            r = a;
+            phi = (kPi * 0.25f) * (b / a);
+        } else {
+            r = b;
+            phi = (kPi * 0.25f) * (2.f - (a / b));
+        }
+    } else {
+        if (a < b) {
+            r = -a;
+            phi = (kPi * 0.25f) * (4.f + (b / a));
+        } else {
+            r = -b;
+            if (b != 0) phi = (kPi * 0.25f) * (6.f - (a / b));
+            else phi = 0;
+        }
+    }
+    dx = r * cosf(phi);
+    dy = r * sinf(phi);
+}
+__device__ __forceinline__ float concentric_disc_pdf() { return 1.0f / kPi; }
+
 // ---------------------------------------------------------------------------------------
 // Scene data for shading
 // ---------------------------------------------------------------------------------------
@@ -131,6 +159,7 @@ struct ShadingScene {
     const float* inst_inv;      // 12 floats (3x4 row-major world-to-object) per instance
     const Material* materials;
     const TriLight* lights;     // triangle lights, in light-list order after the environment
+    int n_materials;
     int n_tri_lights;
     int light_count;            // environment (if any) + triangle lights
     int has_env;
@@ -284,9 +313,16 @@ __device__ __forceinline__ float ct_pdf(float e, V3 o, V3 i) {
 // ---------------------------------------------------------------------------------------
 // BSDF (bsdf.h:125-238) for the material kinds
 // ---------------------------------------------------------------------------------------
+enum { kAllFlags = kRefl | kTrans | kDiffuse | kGlossyF | kSpecular };
+
+__device__ __forceinline__ bool is_specular_material(const Material& m) {
+    return m.kind == kMirror || m.kind == kGlass;   // Material::is_specular (materials.h:92, 145)
+}
+
 struct Bsdf {
     const Material* m;
     V3 n, ut, vt, gn;
+    bool adjoint = false;   // light paths: the glass BTDF drops the (eta_in / eta_trans)^2 factor
     __device__ V3 to_local(V3 d) const { return V3(dot(vt, d), dot(ut, d), dot(n, d)); }
     __device__ V3 to_world(V3 d) const {
         return V3(vt.x * d.x + ut.x * d.y + n.x * d.z, vt.y * d.x + ut.y * d.y + n.y * d.z,
@@ -326,11 +362,18 @@ struct Bsdf {
         if (dot(in_dir, gn) * dot(out_dir, gn) <= 0.0f) return 0.0f;
         return brdf_pdf(lo, li);
     }
-    // Samples a direction; returns the BSDF value, sets in_dir, pdf and sampled flags.
-    __device__ V3 sample(V3 out_dir, V3& in_dir, Rng& rng, int& flags, float& pdf) const {
+    // Samples a direction among the lobes whose flags all lie in `allowed` (BSDF::sample,
+    // bsdf.h:147-199); returns the BSDF value, sets in_dir, pdf and the sampled flags.
+    __device__ V3 sample(V3 out_dir, V3& in_dir, Rng& rng, int& flags, float& pdf, int allowed = kAllFlags) const {
         const V3 lo = to_local(out_dir);
-        float btdf_prob = 0.0f;
-        if (has_btdf()) btdf_prob = 1.0f - fresnel_dielectric_eval(lo.z, 1.0f, m->eta);   // importance()
+        const int bf = brdf_flags();
+        const bool brdf_matches = (bf & allowed) == bf;
+        const bool btdf_matches = has_btdf() && ((kTrans | kSpecular) & allowed) == (kTrans | kSpecular);
+        float btdf_prob;
+        if (brdf_matches && btdf_matches) btdf_prob = 1.0f - fresnel_dielectric_eval(lo.z, 1.0f, m->eta);  // importance()
+        else if (brdf_matches) btdf_prob = 0.0f;
+        else if (btdf_matches) btdf_prob = 1.0f;
+        else { pdf = 0.0f; flags = kNone; return V3(0.0f); }
         const float rnd = rng.next_float();
         const bool use_btdf = rnd < btdf_prob;
         const float component_pdf = use_btdf ? btdf_prob : 1.0f - btdf_prob;
@@ -354,7 +397,7 @@ struct Bsdf {
                 if (entering) cos_trans = -cos_trans;
                 li = V3(eta_frac * -lo.x, eta_frac * -lo.y, cos_trans);
                 const float fr = fresnel_dielectric_eval(lo.z, 1.0f, m->eta);
-                const float factor = sqr(eta_in / eta_trans);
+                const float factor = adjoint ? 1.0f : sqr(eta_in / eta_trans);
                 value = factor * (1.0f - fr) * V3(m->color[0], m->color[1], m->color[2]) / fabsf(li.z);
             }
         } else {
@@ -405,7 +448,15 @@ struct DirectSample {
     float distance;
     V3 radiance;
     float pdf_direct_w;
+    float pdf_emit_w;
+    float cos_out;
     bool delta;
+};
+
+// Light::EmitSample (light.h:65-80)
+struct EmitSample {
+    V3 pos, dir, radiance;
+    float cos_out, pdf_emit_w, pdf_direct_a;
 };
 
 // TriangleLight::sample_direct (light.h:142-175)
@@ -425,9 +476,13 @@ __device__ __forceinline__ DirectSample tri_light_sample(const TriLight& L, V3 f
     const float cos_out = dot(n, -1.0f * s.dir);
     if (cos_out > 0.0f && cos_out < 1.0f) {
         s.radiance = V3(L.intensity[0], L.intensity[1], L.intensity[2]) * cos_out * (L.area / distsq);
+        s.cos_out = cos_out;
+        s.pdf_emit_w = cos_hemisphere_pdf(cos_out) / L.area;
         s.pdf_direct_w = 1.0f / L.area * distsq / cos_out;
     } else {
         s.radiance = V3(0.0f);
+        s.cos_out = 1.0f;
+        s.pdf_emit_w = 1.0f;
         s.pdf_direct_w = 1.0f;
     }
     s.delta = false;
@@ -451,8 +506,87 @@ __device__ __forceinline__ DirectSample env_light_sample(const ShadingScene& sc,
     s.distance = FLT_MAX;
     s.radiance = color / pdf;
     s.pdf_direct_w = pdf;
+    s.pdf_emit_w = concentric_disc_pdf() * sc.bsphere[4] * pdf;
+    s.cos_out = 1.0f;
     s.delta = false;
     return s;
+}
+
+// TriangleLight::sample_emit (light.h:109-140)
+__device__ __forceinline__ EmitSample tri_light_emit(const TriLight& L, Rng& rng) {
+    EmitSample s;
+    float r1, r2;
+    draw2(rng, r1, r2);
+    const float sr = sqrtf(r1);
+    const float u = 1.0f - sr, v = r2 * sr;
+    const V3 p0(L.v[0][0], L.v[0][1], L.v[0][2]), p1(L.v[1][0], L.v[1][1], L.v[1][2]), p2(L.v[2][0], L.v[2][1], L.v[2][2]);
+    s.pos = u * p0 + v * p1 + (1.0f - u - v) * p2;
+    float c1, c2, pdf;
+    draw2(rng, c1, c2);
+    const V3 d = sample_cos_hemisphere(c1, c2, &pdf);
+    const V3 n(L.normal[0], L.normal[1], L.normal[2]), t(L.tangent[0], L.tangent[1], L.tangent[2]),
+        b(L.binormal[0], L.binormal[1], L.binormal[2]);
+    s.dir = d.x * b + d.y * t + d.z * n;
+    if (pdf <= 0.0f) {
+        s.radiance = V3(0.0f);
+        s.cos_out = 0.0f;
+        s.pdf_emit_w = 1.0f;
+        s.pdf_direct_a = 1.0f;
+        return s;
+    }
+    s.radiance = V3(L.intensity[0], L.intensity[1], L.intensity[2]) * L.area * kPi;
+    s.cos_out = d.z;
+    s.pdf_emit_w = pdf / L.area;
+    s.pdf_direct_a = 1.0f / L.area;
+    return s;
+}
+
+// EnvLight::sample_emit with a constant map (light.h:494-523, 446-485): a direction from the
+// map, then a point on the disc of the scene's bounding sphere facing it.
+__device__ __forceinline__ EmitSample env_light_emit(const ShadingScene& sc, Rng& rng) {
+    EmitSample s;
+    float pdf = 1.0f / float(1 * 1);
+    const float ux = rng.next_float();
+    const float uy = rng.next_float();
+    pdf *= float(1 * 1);
+    const V3 color(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    const float theta = kPi * uy;
+    const float sin_theta = sinf(theta);
+    const float phi = 2.0f * kPi * ux;
+    V3 dir(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+    if (sin_theta != 0.0f) pdf /= 2.0f * kPi * kPi * sin_theta;
+    else pdf = 0.0f;
+    dir = dir * -1.0f;
+    float d1, d2, dx, dy;
+    draw2(rng, d1, d2);
+    sample_concentric_disc(d1, d2, dx, dy);
+    V3 tangent, binormal;
+    local_coordinates(dir, tangent, binormal);
+    const V3 c(sc.bsphere[0], sc.bsphere[1], sc.bsphere[2]);
+    s.pos = c + sc.bsphere[3] * (-dir + binormal * dx + tangent * dy);
+    s.dir = dir;
+    s.pdf_direct_a = pdf;
+    s.pdf_emit_w = concentric_disc_pdf() * sc.bsphere[4] * pdf;
+    s.cos_out = 1.0f;
+    s.radiance = color / s.pdf_emit_w;
+    return s;
+}
+
+// AreaEmitter::radiance (light.h:22-43) with both pdfs.
+__device__ __forceinline__ V3 area_emitter_radiance(const Material& m, V3 out_dir, V3 normal, float* pdf_direct_a,
+                                                    float* pdf_emit_w) {
+    const float cos_theta_o = dot(normal, out_dir);
+    if (cos_theta_o <= 0.0f) {
+        *pdf_direct_a = 1.0f;
+        *pdf_emit_w = 1.0f;
+        return V3(0.0f);
+    }
+    *pdf_direct_a = 1.0f / m.area;
+    V3 tangent, binormal;
+    local_coordinates(normal, tangent, binormal);
+    const float lz = dot(normal, out_dir);
+    *pdf_emit_w = 1.0f / m.area * cos_hemisphere_pdf(lz);
+    return V3(m.emission[0], m.emission[1], m.emission[2]);
 }
 
 // EnvMap::radiance with a constant map (light.h:413-424): pdf_direct_w = 1 / (2 pi^2 sin t).
@@ -463,6 +597,13 @@ __device__ __forceinline__ V3 env_radiance(const ShadingScene& sc, V3 out_dir, f
     *pdf_direct_w = 1.0f / (2.0f * kPi * kPi * sinf(t));
     (void)phi;
     return V3(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+}
+
+__device__ __forceinline__ V3 env_radiance_emit(const ShadingScene& sc, V3 out_dir, float* pdf_direct_w,
+                                                float* pdf_emit_w) {
+    const V3 r = env_radiance(sc, out_dir, pdf_direct_w);
+    *pdf_emit_w = concentric_disc_pdf() * sc.bsphere[4] * *pdf_direct_w;
+    return r;
 }
 
 // Russian roulette (random.h:183-188)

@@ -29,12 +29,6 @@ using imbart::Rng;
 using namespace imbart::sh;
 using namespace imbart::pt;
 
-struct imbart_shading {
-    int device = 0;
-    ShadingScene s{};
-    std::vector<void*> allocations;
-};
-
 struct imbart_pt_context {
     int device = 0;
     long long cap = 0;       // paths per queue
@@ -139,6 +133,7 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
     Material* dmats = (Material*)upl(mats.data(), sizeof(Material) * mats.size());
     TriLight* dlights = (TriLight*)upl(lights.data(), sizeof(TriLight) * lights.size());
     s.materials = dmats;
+    s.n_materials = n_mats;
     s.lights = dlights;
     s.n_tri_lights = n_tri_lights;
     s.has_env = env_color ? 1 : 0;

@@ -60,20 +60,30 @@ class ShadingData:
 
 
 def bounding_sphere(desc) -> np.ndarray:
-    """Scene::compute_bounding_sphere (scene.cpp:190-200): the box of the transformed mesh
-    boxes; radius = half its diagonal."""
-    lo = np.full(3, np.inf, np.float32)
-    hi = np.full(3, -np.inf, np.float32)
+    """Scene::compute_bounding_sphere (scene.cpp:189-200): the union of the instances' mesh
+    boxes transformed by transform(float3x4, BBox) (float3x4.h:52-56: centre and half extent
+    through the matrix and its absolute value); radius = half the diagonal. Evaluated in
+    single precision in the reference's operation order, so the sphere is the reference's.
+    Returns centre xyz, radius, 1 / radius^2."""
+    f = np.float32
+    lo = [f(np.inf)] * 3
+    hi = [f(-np.inf)] * 3
+    half = f(0.5)
     for inst in desc.instances:
         mlo, mhi = desc.meshes[inst.mesh_id].bounding_box()
-        m = inst.mat[:3, :]
-        c = m[:, :3] @ ((mhi + mlo) * np.float32(0.5)) + m[:, 3]
-        e = np.abs(m[:, :3]) @ ((mhi - mlo) * np.float32(0.5))
-        lo = np.minimum(lo, c - e)
-        hi = np.maximum(hi, c + e)
-    r = np.float32(np.linalg.norm(hi - lo) * 0.5)
-    c = (hi + lo) * np.float32(0.5)
-    return np.array([c[0], c[1], c[2], r, 1.0 / (r * r)], np.float32)
+        m = inst.mat.astype(np.float32)
+        c3 = [f(f(mhi[k] + mlo[k]) * half) for k in range(3)]
+        e3 = [f(f(mhi[k] - mlo[k]) * half) for k in range(3)]
+        for r in range(3):
+            c = f(f(f(f(m[r, 0] * c3[0]) + f(m[r, 1] * c3[1])) + f(m[r, 2] * c3[2])) + f(m[r, 3] * f(1.0)))
+            a = [f(abs(m[r, k])) for k in range(4)]
+            e = f(f(f(f(a[0] * e3[0]) + f(a[1] * e3[1])) + f(a[2] * e3[2])) + f(a[3] * f(0.0)))
+            lo[r] = min(lo[r], f(c - e))
+            hi[r] = max(hi[r], f(c + e))
+    d = [f(hi[k] - lo[k]) for k in range(3)]
+    r = f(f(np.sqrt(f(f(f(d[0] * d[0]) + f(d[1] * d[1])) + f(d[2] * d[2])))) * half)
+    c = [f(f(hi[k] + lo[k]) * half) for k in range(3)]
+    return np.array([c[0], c[1], c[2], r, f(f(1.0) / f(r * r))], np.float32)
 
 
 class GpuScene:
@@ -158,6 +168,133 @@ class PathTracer:
     def close(self):
         if getattr(self, "ctx", None):
             N.load().imbart_pt_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_camera(cam: G.Camera, width: int | None = None, height: int | None = None) -> N.Camera:
+    """PerspectiveCamera(width, height, fov).move(pos, dir, up) (camera.h:20-56)."""
+    c = N.Camera()
+    f = lambda v: np.ascontiguousarray(np.asarray(v, np.float32))
+    p, d, u = f(cam.pos), f(cam.dir), f(cam.up)
+    N.check(N.load().imbart_camera_make(N.ptr(p), N.ptr(d), N.ptr(u), float(cam.fov), int(width or cam.width),
+                                        int(height or cam.height), C.byref(c)), "imbart_camera_make")
+    return c
+
+
+def estimate_pixel_size(scene: GpuScene, cam: N.Camera) -> float:
+    """Integrator::estimate_pixel_size (integrator.cpp:14-70) on the GPU."""
+    out = np.zeros(1, np.float32)
+    N.check(N.load().imbart_estimate_pixel_size(scene.trace_scene.handle, C.byref(cam), N.ptr(out), None),
+            "imbart_estimate_pixel_size")
+    return float(out[0])
+
+
+class VcmIntegrator:
+    """VCMIntegrator<algo> (vcm.h:54-150) on the GPU: algorithm "vcm", "bpt", "ppm", "lt" or
+    "pt"; settings as the reference's UserSettings (cmd_line.h:40-58). render(iteration) =
+    light pass + camera pass (vcm.cpp:25-55); the photon radius shrinks with the iteration.
+    Images are (height, width, 3) float32 CUDA tensors, accumulated like the reference's
+    AtomicImage."""
+
+    def __init__(self, scene: GpuScene, algorithm: str = "vcm", width: int | None = None, height: int | None = None,
+                 spp: int = 1, max_path_len: int = 10, light_path_count: int | None = None,
+                 num_connections: int = 1, num_knn: int = 10, radius_factor: float = 2.0,
+                 base_radius: float | None = None, light_tile_size: int = 0, cam: G.Camera | None = None,
+                 max_paths_in_flight: int = 0):
+        self.scene = scene
+        cam = cam or scene.desc.camera
+        self.width = width or cam.width
+        self.height = height or cam.height
+        self.camera = make_camera(cam, self.width, self.height)
+        st = self.settings = N.VcmSettings()
+        st.algorithm = N.VCM_ALGORITHMS[algorithm]
+        st.spp = spp
+        st.max_path_len = max_path_len
+        st.light_path_count = light_path_count or (self.width * self.height // 2)
+        st.num_connections = num_connections
+        st.num_knn = num_knn
+        st.light_tile_size = light_tile_size
+        self.pixel_size = estimate_pixel_size(scene, self.camera)
+        st.base_radius = base_radius if base_radius is not None else self.pixel_size * radius_factor
+        self.max_paths = max_paths_in_flight
+        self.ctx = N.load().imbart_vcm_create(scene.device)
+        if not self.ctx:
+            raise N.ImbartError("imbart_vcm_create: " + N.last_error()[1])
+        self.last_stats = np.zeros(6, np.int64)
+
+    def _image(self, image):
+        import torch
+        if image is None:
+            image = torch.zeros((self.height, self.width, 3), dtype=torch.float32,
+                                device=torch.device("cuda", self.scene.device))
+        return image
+
+    def begin_iteration(self, iteration: int):
+        """Returns (photon radius, eta_vc, eta_vm) of the iteration."""
+        out = np.zeros(3, np.float32)
+        N.check(N.load().imbart_vcm_begin_iteration(self.ctx, C.byref(self.settings), iteration, N.ptr(out)),
+                "imbart_vcm_begin_iteration")
+        return float(out[0]), float(out[1]), float(out[2])
+
+    def light_pass(self, light_seed: int, light_seed_step: int = 0, image=None):
+        image = self._image(image)
+        self.settings.light_seed = light_seed & (2 ** 64 - 1)
+        self.settings.light_seed_step = light_seed_step & (2 ** 64 - 1)
+        stats = np.zeros(3, np.int64)
+        N.check(N.load().imbart_vcm_light_pass(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                               C.byref(self.camera), C.byref(self.settings), N.ptr(image),
+                                               N.ptr(stats), None), "imbart_vcm_light_pass")
+        self.last_stats[:3] = stats
+        return image
+
+    def camera_pass(self, camera_seed: int, image=None):
+        image = self._image(image)
+        self.settings.camera_seed = camera_seed & (2 ** 64 - 1)
+        stats = np.zeros(3, np.int64)
+        N.check(N.load().imbart_vcm_camera_pass(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                                C.byref(self.camera), C.byref(self.settings), N.ptr(image),
+                                                self.max_paths, N.ptr(stats), None), "imbart_vcm_camera_pass")
+        self.last_stats[3:] = stats
+        return image
+
+    def render(self, iteration: int, light_seed: int, camera_seed: int, light_seed_step: int = 0, image=None):
+        image = self._image(image)
+        self.settings.light_seed = light_seed & (2 ** 64 - 1)
+        self.settings.light_seed_step = light_seed_step & (2 ** 64 - 1)
+        self.settings.camera_seed = camera_seed & (2 ** 64 - 1)
+        stats = np.zeros(3, np.int64)
+        N.check(N.load().imbart_vcm_render(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                           C.byref(self.camera), C.byref(self.settings), iteration, N.ptr(image),
+                                           self.max_paths, N.ptr(stats), None), "imbart_vcm_render")
+        self.last_stats[:3] = stats
+        return image
+
+    def light_vertices(self) -> np.ndarray:
+        """The light-vertex cache as a (count, 28) float32 host array (layout: include/imbart.h)."""
+        lib = N.load()
+        n = lib.imbart_vcm_copy_light_vertices(self.ctx, None, 0)
+        if n < 0:
+            raise N.ImbartError("imbart_vcm_copy_light_vertices: " + N.last_error()[1])
+        out = np.zeros((n, 28), np.float32)
+        if n > 0 and lib.imbart_vcm_copy_light_vertices(self.ctx, N.ptr(out), n) != n:
+            raise N.ImbartError("imbart_vcm_copy_light_vertices: " + N.last_error()[1])
+        return out
+
+    def load_light_vertices(self, vertices: np.ndarray) -> None:
+        """Replaces the cache (e.g. with the reference's) and rebuilds the photon grid."""
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 28)
+        N.check(N.load().imbart_vcm_load_light_vertices(self.ctx, C.byref(self.settings), N.ptr(v), len(v), None),
+                "imbart_vcm_load_light_vertices")
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            N.load().imbart_vcm_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):

@@ -44,6 +44,22 @@ class PtProfile(C.Structure):
                 ("closest_work", C.c_ulonglong * 3), ("shadow_work", C.c_ulonglong * 3)]
 
 
+class Camera(C.Structure):
+    _fields_ = [("raster_to_world", C.c_float * 16), ("world_to_raster", C.c_float * 16), ("pos", C.c_float * 3),
+                ("dir", C.c_float * 3), ("img_plane_dist", C.c_float), ("width", C.c_int), ("height", C.c_int)]
+
+
+class VcmSettings(C.Structure):
+    _fields_ = [("algorithm", C.c_int), ("spp", C.c_int), ("max_path_len", C.c_int), ("light_path_count", C.c_int),
+                ("num_connections", C.c_int), ("num_knn", C.c_int), ("light_tile_size", C.c_int),
+                ("base_radius", C.c_float), ("light_seed", C.c_ulonglong), ("light_seed_step", C.c_ulonglong),
+                ("camera_seed", C.c_ulonglong)]
+
+
+VCM, BPT, PPM, LT, VCM_PT = 0, 1, 2, 3, 4
+VCM_ALGORITHMS = {"vcm": VCM, "bpt": BPT, "ppm": PPM, "lt": LT, "pt": VCM_PT}
+
+
 class SceneSource(C.Structure):
     _fields_ = [("root", C.c_int), ("nodes", C.c_void_p), ("n_nodes", C.c_int),
                 ("instances", C.c_void_p), ("n_instances", C.c_int), ("tris", C.c_void_p), ("n_tri_vec4", C.c_int),
@@ -124,6 +140,17 @@ _SIGNATURES = {
     "imbart_get_trace_variant_any": (I, []),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
+    "imbart_camera_make": (I, [P, P, P, C.c_float, I, I, C.POINTER(Camera)]),
+    "imbart_estimate_pixel_size": (I, [P, C.POINTER(Camera), P, P]),
+    "imbart_vcm_create": (P, [I]),
+    "imbart_vcm_destroy": (None, [P]),
+    "imbart_vcm_begin_iteration": (I, [P, C.POINTER(VcmSettings), I, P]),
+    "imbart_vcm_light_pass": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), P, P, P]),
+    "imbart_vcm_camera_pass": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), P, C.c_longlong, P, P]),
+    "imbart_vcm_render": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), I, P, C.c_longlong, P, P]),
+    "imbart_vcm_light_vertices": (I, [P, C.POINTER(P), C.POINTER(I)]),
+    "imbart_vcm_copy_light_vertices": (I, [P, P, I]),
+    "imbart_vcm_load_light_vertices": (I, [P, C.POINTER(VcmSettings), P, I, P]),
     "imbart_server_create": (P, [I, I, C.c_longlong, C.c_longlong]),
     "imbart_server_destroy": (None, [P]),
     "imbart_server_add_scene": (I, [P, C.POINTER(SceneSource)]),

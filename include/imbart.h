@@ -361,6 +361,93 @@ typedef struct {
 int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile);
 
 /* ------------------------------------------------------------------------------------ */
+/* VCM family: VCM, BPT, PPM, LT and the VCM path tracer (VCMIntegrator<algo>, vcm.cpp)    */
+/* ------------------------------------------------------------------------------------ */
+
+/* A PerspectiveCamera (camera.h:12-113): both raster matrices (row-major), position,
+ * normalized view direction, image-plane distance and the raster size. */
+typedef struct {
+    float raster_to_world[16];
+    float world_to_raster[16];
+    float pos[3];
+    float dir[3];
+    float img_plane_dist;
+    int width, height;
+} imbart_camera;
+
+/* PerspectiveCamera(width, height, fov).move(pos, dir, up) on the host. */
+int imbart_camera_make(const float* pos, const float* dir, const float* up, float fov, int width, int height,
+                       imbart_camera* out);
+
+/* Integrator::estimate_pixel_size (integrator.cpp:14-70): the mean distance between the hit
+ * points of rays through neighbouring raster corners of every 8th pixel (1 when nothing is
+ * hit). The photon radius of the VCM family is this times its radius factor. Synchronous. */
+int imbart_estimate_pixel_size(const imbart_scene* scene, const imbart_camera* camera, float* pixel_size,
+                               void* stream);
+
+#define IMBART_VCM 0      /* vertex connection and merging */
+#define IMBART_BPT 1      /* bidirectional path tracing (no merging) */
+#define IMBART_PPM 2      /* progressive photon mapping (camera paths sample only specular lobes) */
+#define IMBART_LT 3       /* light tracing (light paths connected to the camera only) */
+#define IMBART_VCM_PT 4   /* path tracing inside the VCM integrator (no light paths) */
+
+/* The reference's UserSettings that drive VCMIntegrator (cmd_line.h:40-58). */
+typedef struct {
+    int algorithm;            /* IMBART_VCM .. IMBART_VCM_PT */
+    int spp;                  /* camera samples per pixel per iteration (concurrent_spp) */
+    int max_path_len;         /* vertices per path (camera path + light path for connections) */
+    int light_path_count;     /* light paths per iteration */
+    int num_connections;      /* light vertices each camera vertex connects to */
+    int num_knn;              /* photons per merge (1..64) */
+    int light_tile_size;      /* paths per light tile (the reference: tile_size^2); 0: one tile per light */
+    float base_radius;        /* photon radius of iteration 1 (pixel size * radius factor) */
+    unsigned long long light_seed, light_seed_step;  /* light tile t is seeded from light_seed + t * step */
+    unsigned long long camera_seed;                  /* seed_base of the camera samples */
+} imbart_vcm_settings;
+
+/* Context with device buffers (light-path slots, light-vertex cache, photon grid, queues). */
+typedef struct imbart_vcm imbart_vcm;
+imbart_vcm* imbart_vcm_create(int device);
+void imbart_vcm_destroy(imbart_vcm* vcm);
+
+/* Iteration `iteration` (1-based): photon radius base / iteration^(0.5 * (1 - 0.75)) and the
+ * MIS constants (vcm.cpp:25-46); out3 (may be NULL) = radius, eta_vc, eta_vm. Clears the cache. */
+int imbart_vcm_begin_iteration(imbart_vcm* vcm, const imbart_vcm_settings* settings, int iteration, float* out3);
+
+/* Light pass (trace_light_paths, vcm.cpp:64-104): traces light_path_count light paths, stores
+ * their non-specular vertices in the cache (order: wavefront, then path), adds the camera
+ * connections to `image` (DEVICE, width*height*3 floats) and builds the photon grid (VCM, PPM).
+ * stats (host, may be NULL): closest rays, shadow rays, wavefronts. Synchronizes per wavefront. */
+int imbart_vcm_light_pass(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
+                          const imbart_camera* camera, const imbart_vcm_settings* settings, float* image,
+                          long long* stats, void* stream);
+
+/* Camera pass (trace_camera_paths, vcm.cpp:106-130, 322-611) against the current cache. */
+int imbart_vcm_camera_pass(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
+                           const imbart_camera* camera, const imbart_vcm_settings* settings, float* image,
+                           long long max_paths_in_flight, long long* stats, void* stream);
+
+/* begin_iteration + light pass + camera pass into `image` (accumulated). */
+int imbart_vcm_render(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
+                      const imbart_camera* camera, const imbart_vcm_settings* settings, int iteration, float* image,
+                      long long max_paths_in_flight, long long* stats, void* stream);
+
+/* The light-vertex cache: DEVICE pointer to `count` vertices of 28 floats (pos, material |
+ * out_dir, path_length | normal, dVC | geom_normal, dVCM | u_tangent, dVM | v_tangent, uv.x |
+ * throughput, uv.y; material and path_length as int32 bits). Valid until the next pass. */
+int imbart_vcm_light_vertices(imbart_vcm* vcm, const float** vertices, int* count);
+
+/* Copies up to `capacity` cache vertices to HOST memory (synchronous); returns the number
+ * copied, or the cache's vertex count when capacity is 0, or -(error code). */
+int imbart_vcm_copy_light_vertices(imbart_vcm* vcm, float* host_out, int capacity);
+
+/* Replaces the cache with `count` vertices in that format (HOST or DEVICE) and rebuilds the
+ * photon grid (VCM, PPM) for the current iteration's radius: camera passes can then run
+ * against a cache produced elsewhere (the reference's, a previous frame's). */
+int imbart_vcm_load_light_vertices(imbart_vcm* vcm, const imbart_vcm_settings* settings, const float* vertices,
+                                   int count, void* stream);
+
+/* ------------------------------------------------------------------------------------ */
 /* Request serving (no counterpart in the reference, which renders one frame per process)  */
 /* ------------------------------------------------------------------------------------ */
 

@@ -22,8 +22,10 @@ REF_SOURCES = [
     "src/imbatracer/loaders/load_bvh.cpp",
     "src/imbatracer/render/integrators/integrator.cpp",
     "src/imbatracer/render/integrators/pt.cpp",
+    "src/imbatracer/render/integrators/vcm.cpp",
+    "src/imbatracer/render/integrators/light_vertices.cpp",
 ]
-OWN_SOURCES = [os.path.join(HERE, "ref_harness.cpp")]
+OWN_SOURCES = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_vcm.cpp")]
 ORACLE_C = [os.path.join(ORACLE, "traversal.c")]
 
 FLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-w"]

@@ -113,6 +113,8 @@ float3 f3(const float* p) { return float3(p[0], p[1], p[2]); }
 
 }  // namespace
 
+imba::Scene* ref_scene_of(void* h) { return &static_cast<RefScene*>(h)->scene; }
+
 extern "C" {
 
 void imbart_ref_set_seed(uint64_t value, uint64_t step) {

@@ -37,6 +37,13 @@ def load() -> C.CDLL:
             "ref_scene_bsphere": (None, [P, P]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
             "ref_render_pt_threads": (I, [P, I, I, P, P, P, F, I, I, U64, I, I, P, P]),
+            "ref_vcm_create": (P, [P, I, I, I, P, P, P, F, I, I, I, I, I, F, I, U64]),
+            "ref_vcm_destroy": (None, [P]),
+            "ref_vcm_info": (None, [P, P]),
+            "ref_vcm_begin_iteration": (F, [P, I, P]),
+            "ref_vcm_light_pass": (None, [P, U64, U64, P]),
+            "ref_vcm_light_vertices": (I, [P, P, I]),
+            "ref_vcm_camera_pass": (None, [P, U64, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -170,6 +177,67 @@ class RefScene:
     def close(self):
         if self.handle:
             load().ref_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+VCM_ALGOS = {"vcm": 0, "bpt": 1, "ppm": 2, "lt": 3, "pt": 4}
+
+
+class RefVcm:
+    """The reference's VCMIntegrator<algo> (vcm.cpp) on a RefScene, driven pass by pass.
+
+    One camera tile covers the image (sample indices global); each light's paths form one
+    light tile when tile_size^2 is at least the paths per light. Light vertices are 28 floats:
+    pos, mat | out_dir, path_length | normal, dVC | geom_normal, dVCM | u_tangent, dVM |
+    v_tangent, uv.x | throughput, uv.y (mat and path_length as int32 bits)."""
+
+    def __init__(self, scene: RefScene, algo: str, w: int, h: int, spp: int = 1, max_path_len: int = 8,
+                 light_path_count: int = 1024, num_connections: int = 1, num_knn: int = 10,
+                 radius_factor: float = 2.0, tile_size: int | None = None, cam=None, preprocess_seed: int = 77):
+        cam = cam or scene.desc.camera
+        self.scene, self.w, self.h = scene, w, h
+        self.light_path_count = light_path_count
+        tile = tile_size or max(w, h, int(np.ceil(np.sqrt(light_path_count))) + 1)
+        self.tile_size = tile
+        p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
+        self.handle = load().ref_vcm_create(scene.handle, VCM_ALGOS[algo], w, h, _p(p3), _p(d3), _p(u3), cam.fov,
+                                            spp, max_path_len, light_path_count, num_connections, num_knn,
+                                            radius_factor, tile, preprocess_seed)
+        assert self.handle
+        info = np.zeros(3, np.float32)
+        load().ref_vcm_info(self.handle, _p(info))
+        self.pixel_size, self.base_radius, self.cache_capacity = float(info[0]), float(info[1]), int(info[2])
+
+    def begin_iteration(self, iteration: int):
+        eta = np.zeros(2, np.float32)
+        r = load().ref_vcm_begin_iteration(self.handle, iteration, _p(eta))
+        return float(r), float(eta[0]), float(eta[1])
+
+    def light_pass(self, seed: int, step: int = 0) -> np.ndarray:
+        img = np.zeros((self.h, self.w, 3), np.float32)
+        load().ref_vcm_light_pass(self.handle, seed & (2 ** 64 - 1), step & (2 ** 64 - 1), _p(img))
+        return img
+
+    def light_vertices(self) -> np.ndarray:
+        cap = max(self.cache_capacity, 1)
+        out = np.zeros((cap, 28), np.float32)
+        n = load().ref_vcm_light_vertices(self.handle, _p(out), cap)
+        return out[:n].copy()
+
+    def camera_pass(self, seed: int) -> np.ndarray:
+        img = np.zeros((self.h, self.w, 3), np.float32)
+        load().ref_vcm_camera_pass(self.handle, seed & (2 ** 64 - 1), _p(img))
+        return img
+
+    def close(self):
+        if self.handle:
+            load().ref_vcm_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,0 +1,157 @@
+"""The VCM family (VCM, BPT, PPM, LT, VCM-PT) on the GPU against the reference's own
+VCMIntegrator (vcm.cpp, built in oracle/_ref), pass by pass.
+
+Light pass: the same light paths are traced from the same seeds; the light-vertex caches are
+compared as sets (matched by path length and position; the two caches are ordered
+differently: the reference appends in queue order after a material sort, the GPU by
+wavefront and path) and the light-tracing image by relative RMSE. Camera pass: the GPU runs
+against the reference's own cache (imbart_vcm_load_light_vertices), so every connection and
+merge sees the same vertices as the reference's and the images must agree to rel. RMSE 1e-3,
+as for the path tracer. Pixel size, photon radius and MIS constants must agree exactly.
+"""
+import numpy as np
+import pytest
+
+from oracle import refwrap as R
+from tests import helpers as H
+from tests.test_pt import small_mixed_scene
+
+needs_ref = pytest.mark.skipif(not R.available(), reason="oracle/_ref not built (reference tree absent)")
+
+W, Hh = 48, 32
+LIGHT_PATHS = 3000
+MAX_LEN = 6
+IMAGE_TOL = 1e-3          # camera pass on the reference's cache
+LIGHT_IMAGE_TOL = 2e-2    # light tracing: sparse splats, a diverging path moves whole splats
+MATCH_MIN = 0.98          # fraction of the reference's light vertices found in the GPU cache
+
+
+def rel_rmse(a, b):
+    den = np.sqrt(np.mean(b.astype(np.float64) ** 2))
+    return float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / max(den, 1e-30))
+
+
+def scene(name):
+    return small_mixed_scene() if name == "mixed" else H.scene_desc(name)
+
+
+def gpu_integrator(gs, algo, rv):
+    from imbatracer_b200.integrators import VcmIntegrator
+    return VcmIntegrator(gs, algo, W, Hh, spp=1, max_path_len=MAX_LEN, light_path_count=LIGHT_PATHS,
+                         num_connections=1, num_knn=10, base_radius=rv.base_radius,
+                         light_tile_size=rv.tile_size * rv.tile_size)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["mixed", "config1"])
+def test_bounding_sphere_is_the_references(name):
+    from imbatracer_b200.integrators import bounding_sphere
+    d = scene(name)
+    rs = R.RefScene(d)
+    ref = np.zeros(4, np.float32)
+    R.load().ref_scene_bsphere(rs.handle, R._p(ref))
+    got = bounding_sphere(d)
+    assert np.array_equal(got[:4].view(np.int32), ref.view(np.int32))
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("name", ["mixed", "config1"])
+def test_pixel_size_radius_and_mis_constants(cuda, name):
+    from imbatracer_b200.integrators import GpuScene
+    d = scene(name)
+    rv = R.RefVcm(R.RefScene(d), "vcm", W, Hh, max_path_len=MAX_LEN, light_path_count=LIGHT_PATHS)
+    gs = GpuScene(d)
+    vi = gpu_integrator(gs, "vcm", rv)
+    assert np.float32(vi.pixel_size) == np.float32(rv.pixel_size)
+    for it in (1, 2, 7):
+        assert vi.begin_iteration(it) == rv.begin_iteration(it)
+
+
+def match_vertices(ref, got):
+    """Matches reference light vertices to GPU ones by path length and position."""
+    from scipy.spatial import cKDTree
+    tree = cKDTree(got[:, 0:3].astype(np.float64))
+    d, j = tree.query(ref[:, 0:3].astype(np.float64))
+    scale = np.maximum(np.abs(ref[:, 0:3]).max(1), 1.0)
+    ok = (d <= 1e-4 * scale) & (ref[:, 7].view(np.int32) == got[j, 7].view(np.int32))
+    return ok, j
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("name,algo", [("mixed", "vcm"), ("mixed", "bpt"), ("mixed", "ppm"), ("mixed", "lt"),
+                                       ("config1", "vcm")])
+def test_light_pass_matches_reference(cuda, name, algo):
+    from imbatracer_b200.integrators import GpuScene
+    d = scene(name)
+    rv = R.RefVcm(R.RefScene(d), algo, W, Hh, max_path_len=MAX_LEN, light_path_count=LIGHT_PATHS)
+    seed, step = 9876, 12345
+    rv.begin_iteration(1)
+    ref_img = rv.light_pass(seed, step)
+    ref_v = rv.light_vertices()
+    gs = GpuScene(d)
+    vi = gpu_integrator(gs, algo, rv)
+    vi.begin_iteration(1)
+    img = vi.light_pass(seed, step).cpu().numpy()
+    got_v = vi.light_vertices()
+    if algo == "lt":
+        assert len(ref_v) == 0 and len(got_v) == 0
+    else:
+        assert len(ref_v) > 100
+        assert abs(len(got_v) - len(ref_v)) <= max(2, 0.01 * len(ref_v))
+        ok, j = match_vertices(ref_v, got_v)
+        assert ok.mean() >= MATCH_MIN, ok.mean()
+        r, g = ref_v[ok], got_v[j[ok]]
+        assert np.array_equal(r[:, 3].view(np.int32), g[:, 3].view(np.int32))          # material
+        for cols in ([11], [15], [19], [24, 25, 26]):                                  # dVC, dVCM, dVM, thr
+            rel = np.abs(g[:, cols] - r[:, cols]) / np.maximum(np.abs(r[:, cols]), 1e-30)
+            assert np.median(rel) <= 1e-6 and np.mean(rel <= 1e-3) >= 0.99, cols
+    if algo != "ppm":
+        assert ref_img.sum() > 0
+        assert rel_rmse(img, ref_img) <= LIGHT_IMAGE_TOL
+    else:
+        assert img.sum() == 0 and ref_img.sum() == 0
+    assert vi.last_stats[0] >= LIGHT_PATHS
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("name,algo", [("mixed", "vcm"), ("mixed", "bpt"), ("mixed", "ppm"), ("mixed", "pt"),
+                                       ("config1", "vcm"), ("config1", "bpt")])
+def test_camera_pass_on_reference_cache_matches(cuda, name, algo):
+    from imbatracer_b200.integrators import GpuScene
+    d = scene(name)
+    rv = R.RefVcm(R.RefScene(d), algo, W, Hh, max_path_len=MAX_LEN, light_path_count=LIGHT_PATHS)
+    gs = GpuScene(d)
+    vi = gpu_integrator(gs, algo, rv)
+    for it, (ls, cs) in enumerate([(111, 222), (333, 444)], start=1):
+        rv.begin_iteration(it)
+        rv.light_pass(ls, 7)
+        ref_v = rv.light_vertices()
+        ref = rv.camera_pass(cs)
+        vi.begin_iteration(it)
+        vi.load_light_vertices(ref_v)
+        img = vi.camera_pass(cs).cpu().numpy()
+        assert ref.sum() > 0
+        err = rel_rmse(img, ref)
+        assert err <= IMAGE_TOL, (it, err)
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_gpu_vcm_is_deterministic(cuda):
+    from imbatracer_b200.integrators import GpuScene
+    d = small_mixed_scene()
+    rv = R.RefVcm(R.RefScene(d), "vcm", W, Hh, max_path_len=MAX_LEN, light_path_count=LIGHT_PATHS)
+    gs = GpuScene(d)
+    caches, images = [], []
+    for _ in range(2):
+        vi = gpu_integrator(gs, "vcm", rv)
+        img = vi.render(1, 5, 6, 3).cpu().numpy()
+        caches.append(vi.light_vertices())
+        images.append(img)
+        vi.close()
+    assert len(caches[0]) > 0
+    assert np.array_equal(caches[0].view(np.int32), caches[1].view(np.int32))
+    assert rel_rmse(images[0], images[1]) <= 1e-5
