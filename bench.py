@@ -306,6 +306,8 @@ def run_pt(args):
         }
         if world == 1 and not args.no_serving:
             line["serving"] = run_serving()
+        if world == 1 and not args.no_vcm:
+            line["vcm_family"] = run_vcm()
         print(json.dumps(line), flush=True)
     pt.close()
     gs.close()
@@ -430,6 +432,56 @@ def serve_arm(mode, scenes, jobs, open_loop, ray_buf=None, hit_buf=None):
         out["render_p99_ms"] = round(_percentile(renders, 99), 2)
         out["batch_p99_ms"] = round(_percentile(batches, 99), 2)
     return out
+
+
+# ---------------------------------------------------------------------------------------
+# VCM family: iterations of VCM / PPM / BPT on the 2M-triangle sphere field (config 3)
+# ---------------------------------------------------------------------------------------
+VCM_W, VCM_H = 1280, 720
+VCM_LIGHT_PATHS = 1 << 20
+VCM_MAX_PATH_LEN = 8
+
+
+def run_vcm(iterations=4, warmup=2, algos=("vcm", "ppm", "bpt")):
+    """Device time per iteration (light pass + camera pass, one camera sample per pixel)."""
+    import torch
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.integrators import GpuScene, VcmIntegrator
+    desc = G.config3(width=VCM_W, height=VCM_H)
+    gs = GpuScene(desc)
+    out = {"workload": f"config 3: {desc.instanced_triangles} triangles (400 displaced spheres), {VCM_W}x{VCM_H}, "
+                       f"{VCM_LIGHT_PATHS} light paths and 1 camera sample per pixel per iteration, max path "
+                       f"length {VCM_MAX_PATH_LEN}, 1 connection, 10 nearest photons, radius 2 pixel sizes "
+                       f"shrinking as iteration^-1/8",
+           "iterations": iterations, "warmup": warmup}
+    for algo in algos:
+        vi = VcmIntegrator(gs, algo, VCM_W, VCM_H, spp=1, max_path_len=VCM_MAX_PATH_LEN,
+                           light_path_count=VCM_LIGHT_PATHS, num_connections=1, num_knn=10, radius_factor=2.0)
+        image = torch.zeros((VCM_H, VCM_W, 3), dtype=torch.float32, device="cuda")
+        for k in range(warmup):
+            vi.render(k + 1, 11 + k, 101 + k, 0x9E3779B9, image=image)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rays, vertices = 0, 0
+        for k in range(iterations):
+            vi.render(warmup + k + 1, 1000 + k, 2000 + k, 0x9E3779B9, image=image)
+            rays += int(vi.last_stats[0] + vi.last_stats[1])
+            vertices += N_light_vertices(vi)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / iterations
+        out[algo] = {"ms_per_iteration": round(ms, 2), "mrays_s": round(rays / iterations / (ms * 1e-3) / 1e6, 1),
+                     "rays_per_iteration": rays // iterations, "light_vertices": vertices // iterations,
+                     "pixel_size": round(vi.pixel_size, 5)}
+        vi.close()
+    gs.close()
+    return out
+
+
+def N_light_vertices(vi):
+    from imbatracer_b200 import native as N
+    return max(int(N.load().imbart_vcm_copy_light_vertices(vi.ctx, None, 0)), 0)
 
 
 def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0):
@@ -570,7 +622,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="pt", choices=["pt", "trace", "serve"])
+    ap.add_argument("--mode", default="pt", choices=["pt", "trace", "serve", "vcm"])
+    ap.add_argument("--no-vcm", action="store_true", help="pt mode: skip the VCM-family iterations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
     ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
@@ -584,6 +637,9 @@ def main():
         args.warmup = 3
     if args.mode == "trace":
         run_trace(args)
+    elif args.mode == "vcm":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"mode": "vcm", "vcm_family": run_vcm(args.steps, args.warmup)}), flush=True)
     elif args.mode == "serve":
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({"mode": "serve", "serving": run_serving(config5_rates=tuple(args.rate))}), flush=True)

@@ -6,8 +6,9 @@ compared as sets (matched by path length and position; the two caches are ordere
 differently: the reference appends in queue order after a material sort, the GPU by
 wavefront and path) and the light-tracing image by relative RMSE. Camera pass: the GPU runs
 against the reference's own cache (imbart_vcm_load_light_vertices), so every connection and
-merge sees the same vertices as the reference's and the images must agree to rel. RMSE 1e-3,
-as for the path tracer. Pixel size, photon radius and MIS constants must agree exactly.
+merge sees the same vertices as the reference's and the images must agree to rel. RMSE 1e-4
+(float rounding of transcendental functions and of atomic accumulation order only). Pixel
+size, photon radius and MIS constants must agree exactly.
 """
 import numpy as np
 import pytest
@@ -21,8 +22,8 @@ needs_ref = pytest.mark.skipif(not R.available(), reason="oracle/_ref not built 
 W, Hh = 48, 32
 LIGHT_PATHS = 3000
 MAX_LEN = 6
-IMAGE_TOL = 1e-3          # camera pass on the reference's cache
-LIGHT_IMAGE_TOL = 2e-2    # light tracing: sparse splats, a diverging path moves whole splats
+IMAGE_TOL = 1e-4          # camera pass on the reference's cache (measured: <= 1.6e-6)
+LIGHT_IMAGE_TOL = 1e-3    # light tracing: a diverging light path moves whole splats (measured: <= 9e-6)
 MATCH_MIN = 0.98          # fraction of the reference's light vertices found in the GPU cache
 
 
