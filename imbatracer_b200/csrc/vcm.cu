@@ -70,7 +70,7 @@ struct VcmParams {
     unsigned int grid_table;
     int merging;
     float* image;
-    int* counts;          // [0] next camera queue, [1] shadow rays, [2] live light paths
+    int* counts;          // [0] next camera queue, [1] shadow rays, [2] live light paths, [3] merges
 };
 
 __device__ __forceinline__ V3 v3(float4 a) { return V3(a.x, a.y, a.z); }
@@ -466,7 +466,8 @@ __device__ __forceinline__ bool vcm_connect_one(const VcmParams& p, int cam_path
     return true;
 }
 
-// VCMIntegrator::vertex_merging (vcm.cpp:571-611): the k nearest photons of the grid.
+// VCMIntegrator::vertex_merging (vcm.cpp:571-611): the k nearest photons of the grid, one
+// thread per query (the path for k > 32; vcm_merge_warp_kernel serves k <= 32).
 __device__ __forceinline__ V3 vcm_merge(const VcmParams& p, V3 thr, float dVCM, float dVM, const Isect& is,
                                         const Bsdf& bsdf) {
     float dist[kGridMaxK];
@@ -503,13 +504,170 @@ __device__ __forceinline__ V3 vcm_merge(const VcmParams& p, V3 thr, float dVCM, 
     return thr * contrib;
 }
 
+// A camera vertex waiting for merging (7 float4): pos + pixel, out_dir + material, normal +
+// dVCM, geometric normal + dVM, u tangent, v tangent, throughput.
+constexpr int kMergeRec = 7;
+
+// Vertex merging for the camera vertices queued by the shading kernel (count on the device).
+__global__ void __launch_bounds__(128) vcm_merge_kernel(VcmParams p, const int* count, const float4* recs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *count) return;
+    const float4* r = recs + kMergeRec * (size_t)i;
+    const float4 m0 = r[0], m1 = r[1], m2 = r[2], m3 = r[3], m4 = r[4], m5 = r[5], m6 = r[6];
+    Isect is;
+    is.pos = v3(m0);
+    is.out_dir = v3(m1);
+    is.normal = v3(m2);
+    is.geom_normal = v3(m3);
+    is.u_tangent = v3(m4);
+    is.v_tangent = v3(m5);
+    is.mat = __float_as_int(m1.w);
+    const Bsdf bsdf = make_bsdf(&p.s.materials[is.mat], is.normal, is.u_tangent, is.v_tangent, is.geom_normal, false);
+    add_image(p.image, __float_as_int(m0.w), vcm_merge(p, v3(m6), m2.w, m3.w, is, bsdf));
+}
+
+// Vertex merging with one warp per queued camera vertex (k <= 32). The 32 lanes scan each of
+// the 8 buckets together, in the reference's order; photons inside the radius are inserted in
+// scan order into a k-nearest list held one entry per lane, with the reference's insertion
+// rule (after every kept photon at distance <= d2; when the list is full the last entry
+// leaves first). Equal distances are then ordered by photon index, the found photons are
+// evaluated one per lane, and their contributions are summed in list order, so the result
+// equals the per-thread query's.
+__global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const int* count_ptr, const float4* recs) {
+    const int lane = threadIdx.x & 31;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (q >= *count_ptr) return;   // uniform across the warp
+    const float4* r = recs + kMergeRec * (size_t)q;
+    const float4 m0 = r[0], m1 = r[1], m2 = r[2], m3 = r[3], m4 = r[4], m5 = r[5], m6 = r[6];
+    const float qx = m0.x, qy = m0.y, qz = m0.z;
+    float prm[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) prm[k] = __ldg(p.grid_params + k);
+    const int k = p.num_knn;
+    float my_d = 0.0f;      // list entry `lane`
+    int my_id = -1;
+    int count = 0;
+    const bool inside = qx >= prm[0] && qy >= prm[1] && qz >= prm[2] && qx <= prm[3] && qy <= prm[4] && qz <= prm[5];
+    if (inside) {
+        const float inv = prm[9], r2 = prm[7];
+        const float cx = __fmul_rn(inv, __fsub_rn(qx, prm[0]));
+        const float cy = __fmul_rn(inv, __fsub_rn(qy, prm[1]));
+        const float cz = __fmul_rn(inv, __fsub_rn(qz, prm[2]));
+        const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+        const int px = (int)fx, py = (int)fy, pz = (int)fz;
+        const int pxo = px + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
+        const int pyo = py + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
+        const int pzo = pz + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
+        for (int j = 0; j < 8; ++j) {
+            const int x = (j & 4) ? pxo : px;
+            const int y = (j & 2) ? pyo : py;
+            const int z = (j & 1) ? pzo : pz;
+            const int c = hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, p.grid_table);
+            const int b = c == 0 ? 0 : __ldg(p.grid_ends + c - 1);
+            const int e = __ldg(p.grid_ends + c);
+            for (int base = b; base < e; base += 32) {
+                const int s = base + lane;
+                float d2 = 0.0f;
+                int id = -1;
+                bool within = false;
+                if (s < e) {
+                    const float4 ph = __ldg(p.grid_sorted + s);
+                    const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
+                    d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                    id = __float_as_int(ph.w);
+                    within = d2 <= r2;
+                }
+                unsigned cand = __ballot_sync(0xffffffffu, within);
+                while (cand) {
+                    const int src = __ffs(cand) - 1;
+                    cand &= cand - 1;
+                    const float cd = __shfl_sync(0xffffffffu, d2, src);
+                    const int cid = __shfl_sync(0xffffffffu, id, src);
+                    int kept;
+                    if (count == k) {
+                        const float last = __shfl_sync(0xffffffffu, my_d, k - 1);
+                        if (last < cd) continue;
+                        kept = k - 1;
+                    } else {
+                        kept = count;
+                        count++;
+                    }
+                    const int pos = __popc(__ballot_sync(0xffffffffu, lane < kept && my_d <= cd));
+                    const float up_d = __shfl_up_sync(0xffffffffu, my_d, 1);
+                    const int up_id = __shfl_up_sync(0xffffffffu, my_id, 1);
+                    if (lane > pos && lane <= kept) { my_d = up_d; my_id = up_id; }
+                    if (lane == pos) { my_d = cd; my_id = cid; }
+                }
+            }
+        }
+        // Equal distances by photon index (odd-even transposition over adjacent equal pairs).
+        const float next_d = __shfl_down_sync(0xffffffffu, my_d, 1);
+        const unsigned ties = __ballot_sync(0xffffffffu, lane + 1 < count && my_d == next_d);
+        if (ties) {
+            for (int pass = 0; pass < count; ++pass) {
+                const float nd = __shfl_down_sync(0xffffffffu, my_d, 1);
+                const int nid = __shfl_down_sync(0xffffffffu, my_id, 1);
+                const float pd = __shfl_up_sync(0xffffffffu, my_d, 1);
+                const int pid = __shfl_up_sync(0xffffffffu, my_id, 1);
+                const bool left = ((lane & 1) == (pass & 1));   // this lane is the left of its pair
+                if (left) {
+                    if (lane + 1 < count && my_d == nd && my_id > nid) my_id = nid;
+                } else if (lane >= 1 && lane < count) {
+                    if (pd == my_d && pid > my_id) my_id = pid;
+                }
+            }
+        }
+    }
+    if (count == 0) return;
+    // Evaluate the found photons, one per lane.
+    const V3 pos(qx, qy, qz), out_dir = v3(m1), thr = v3(m6);
+    const float dVCM = m2.w, dVM = m3.w;
+    float radius_sqr = p.pm_radius * p.pm_radius;
+    V3 c(0.0f);
+    float4 lq0 = make_float4(0, 0, 0, 0);
+    if (lane < count) lq0 = __ldg(p.cache + 7 * (size_t)my_id);
+    if (count == k) {
+        const V3 d = V3(__shfl_sync(0xffffffffu, lq0.x, k - 1), __shfl_sync(0xffffffffu, lq0.y, k - 1),
+                        __shfl_sync(0xffffffffu, lq0.z, k - 1)) - pos;
+        radius_sqr = dot(d, d);
+    }
+    if (lane < count) {
+        const Material& mat = p.s.materials[__float_as_int(m1.w)];
+        const Bsdf bsdf = make_bsdf(&mat, v3(m2), v3(m4), v3(m5), v3(m3), false);
+        const float4* v = p.cache + 7 * (size_t)my_id;
+        const float4 q1 = __ldg(v + 1), q3 = __ldg(v + 3), q4 = __ldg(v + 4), q6 = __ldg(v + 6);
+        const V3 photon_in_dir = v3(q1);
+        const V3 bsdf_value = bsdf.eval(out_dir, photon_in_dir);
+        const float pdf_dir_w = bsdf.pdf(out_dir, photon_in_dir);
+        const float pdf_rev_w = bsdf.pdf(photon_in_dir, out_dir);
+        if (!(pdf_dir_w == 0.0f || pdf_rev_w == 0.0f || is_black(bsdf_value))) {
+            const float mis_weight_light = q3.w * p.eta_vc + q4.w * pdf_dir_w;
+            const float mis_weight_camera = dVCM * p.eta_vc + dVM * pdf_rev_w;
+            const float mis_weight = p.algo == kAlgoPpm ? 1.0f : (1.0f / (mis_weight_light + 1.0f + mis_weight_camera));
+            const V3 dp = v3(lq0) - pos;
+            const float d = dot(dp, dp);
+            const float kernel = 1.0f - d / radius_sqr;
+            c = mis_weight * bsdf_value * kernel * v3(q6);
+        }
+    }
+    // Sum in list order, as the reference accumulates.
+    V3 contrib(0.0f);
+    for (int l = 0; l < count; ++l)
+        contrib = contrib + V3(__shfl_sync(0xffffffffu, c.x, l), __shfl_sync(0xffffffffu, c.y, l),
+                               __shfl_sync(0xffffffffu, c.z, l));
+    if (lane == 0) {
+        contrib = contrib * (2.0f / (kPi * radius_sqr * (float)p.light_path_count));
+        add_image(p.image, __float_as_int(m0.w), thr * contrib);
+    }
+}
+
 // process_camera_rays (vcm.cpp:322-439) for one wavefront of camera paths. Shadow rays (next
 // event + connections, at most 1 + num_connections per path) go to the shadow queue, each kind
 // appended by the whole warp so that the warp stays converged.
 __global__ void __launch_bounds__(128) vcm_camera_shade_kernel(
     VcmParams p, int n, const float4* rays, const int4* hits, const int* pixels, const unsigned long long* rngs,
     const float4* thrs, const float4* ws, float4* o_rays, int* o_pixel, unsigned long long* o_rng, float4* o_thr,
-    float4* o_w, float4* s_rays, int* s_pixel, float4* s_contrib) {
+    float4* o_w, float4* s_rays, int* s_pixel, float4* s_contrib, float4* merge_recs) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool alive = false;
     float4 o_org = make_float4(0, 0, 0, 0), o_dir = o_org;
@@ -604,9 +762,20 @@ __global__ void __launch_bounds__(128) vcm_camera_shade_kernel(
             }
         }
     }
+    // Vertex merging runs in vcm_merge_kernel over the queued camera vertices.
+    const bool merge = surface && p.algo != kAlgoBpt && p.algo != kAlgoPt && nonspec && p.merging;
+    const int mslot = warp_append(p.counts + 3, merge);
+    if (merge) {
+        float4* r = merge_recs + kMergeRec * (size_t)mslot;
+        r[0] = f4(is.pos, __int_as_float(pixel));
+        r[1] = f4(is.out_dir, __int_as_float(is.mat));
+        r[2] = f4(is.normal, dVCM);
+        r[3] = f4(is.geom_normal, dVM);
+        r[4] = f4(is.u_tangent, 0.0f);
+        r[5] = f4(is.v_tangent, 0.0f);
+        r[6] = f4(thr, 0.0f);
+    }
     if (surface) {
-        if (p.algo != kAlgoBpt && p.algo != kAlgoPt && nonspec && p.merging)
-            add_image(p.image, pixel, vcm_merge(p, thr, dVCM, dVM, is, bsdf));
         const float offset = tmax * 1e-4f;
         alive = vcm_bounce(p, rng, thr, pl, dVC, dVCM, dVM, is, bsdf, false, offset, o_org, o_dir);
     }
@@ -712,6 +881,7 @@ struct imbart_vcm {
     float4* c_thr[2] = {nullptr, nullptr};
     float4* c_w[2] = {nullptr, nullptr};
     int4* c_hits = nullptr;
+    float4* c_merge = nullptr;      // queued camera vertices for merging (7 float4 each)
     // shadow queue
     long long s_cap = 0;
     float4* s_rays = nullptr;
@@ -730,7 +900,7 @@ namespace {
 
 void free_vcm(imbart_vcm* v) {
     void* ptrs[] = {v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage, v->vflags, v->bsums, v->d_tiles,
-                    v->cache, v->c_hits, v->s_rays, v->s_hits, v->s_pixel, v->s_contrib, v->counts};
+                    v->cache, v->c_hits, v->c_merge, v->s_rays, v->s_hits, v->s_pixel, v->s_contrib, v->counts};
     for (void* p : ptrs) cudaFree(p);
     for (int k = 0; k < 2; ++k) {
         void* q[] = {v->c_rays[k], v->c_pixel[k], v->c_rng[k], v->c_thr[k], v->c_w[k]};
@@ -1048,7 +1218,8 @@ int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbar
             good = realloc_exact(&v->c_rays[k], 2 * (size_t)chunk) && realloc_exact(&v->c_pixel[k], (size_t)chunk) &&
                    realloc_exact(&v->c_rng[k], (size_t)chunk) && realloc_exact(&v->c_thr[k], (size_t)chunk) &&
                    realloc_exact(&v->c_w[k], (size_t)chunk);
-        good = good && realloc_exact(&v->c_hits, (size_t)chunk);
+        good = good && realloc_exact(&v->c_hits, (size_t)chunk) &&
+               realloc_exact(&v->c_merge, (size_t)kMergeRec * chunk);
         v->c_cap = good ? chunk : 0;
     }
     good = good && ensure_shadow(v, chunk * per);
@@ -1072,8 +1243,16 @@ int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbar
             vcm_camera_shade_kernel<<<(n + 127) / 128, 128, 0, s>>>(
                 p, n, v->c_rays[cur], v->c_hits, v->c_pixel[cur], v->c_rng[cur], v->c_thr[cur], v->c_w[cur],
                 v->c_rays[nxt], v->c_pixel[nxt], v->c_rng[nxt], v->c_thr[nxt], v->c_w[nxt], v->s_rays, v->s_pixel,
-                v->s_contrib);
+                v->s_contrib, v->c_merge);
             note_launches(1);
+            if (p.merging && (st->algorithm == IMBART_VCM || st->algorithm == IMBART_PPM)) {
+                if (st->num_knn <= 32)   // one warp per queued vertex
+                    vcm_merge_warp_kernel<<<(int)(((long long)n * 32 + 127) / 128), 128, 0, s>>>(p, v->counts + 3,
+                                                                                               v->c_merge);
+                else
+                    vcm_merge_kernel<<<(n + 127) / 128, 128, 0, s>>>(p, v->counts + 3, v->c_merge);
+                note_launches(1);
+            }
             const int bound = n * per;
             rc = launch_trace_internal(scene, v->s_rays, v->s_hits, nullptr, bound, IMBART_TRACE_ANY, s, nullptr,
                                        nullptr, v->counts + 1);
