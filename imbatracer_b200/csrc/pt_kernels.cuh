@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -48,12 +49,21 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
     return pred ? base + __popc(m & ((1u << lane) - 1u)) : -1;
 }
 
-// Triangle-light frames and emitter areas, computed on the device with the reference's
-// formulas (TriangleLight ctor, light.h:99-108; Tri::area, tri.h:21).
-__global__ void setup_lights_kernel(TriLight* lights, int count) {
+// Light frames and emitter areas, computed on the device with the reference's formulas
+// (TriangleLight ctor, light.h:99-108: normal, area, frame; DirectionalLight and SpotLight
+// ctors, :195-199 and :294-302: frame of the direction; Tri::area, tri.h:21).
+__global__ void setup_lights_kernel(LightSrc* lights, int count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    TriLight& L = lights[i];
+    LightSrc& L = lights[i];
+    if (L.kind == kLightDirectional || L.kind == kLightSpot) {
+        V3 t, b;
+        local_coordinates(V3(L.normal[0], L.normal[1], L.normal[2]), t, b);
+        L.tangent[0] = t.x; L.tangent[1] = t.y; L.tangent[2] = t.z;
+        L.binormal[0] = b.x; L.binormal[1] = b.y; L.binormal[2] = b.z;
+        return;
+    }
+    if (L.kind != kLightTri) return;
     const V3 p0(L.v[0][0], L.v[0][1], L.v[0][2]), p1(L.v[1][0], L.v[1][1], L.v[1][2]), p2(L.v[2][0], L.v[2][1], L.v[2][2]);
     V3 n = cross(p1 - p0, p2 - p0);
     L.area = length(n) * 0.5f;
@@ -74,8 +84,9 @@ __global__ void emitter_area_kernel(const float* vertices, const int4* tris, int
     mats[t.w].area = length(cross(v1 - v0, v2 - v0)) / 2;
 }
 
-// Host-side decoding of the material / light arrays of imbart_shading_create.
-inline std::vector<Material> decode_materials(const int* kind, const float* params, int n) {
+// Host-side decoding of the material / light arrays of imbart_shading_create(_ex). With
+// textures, params[12] / params[13] are the diffuse-texture / bump-map indices (< 0: none).
+inline std::vector<Material> decode_materials(const int* kind, const float* params, int n, bool textured) {
     std::vector<Material> mats(n);
     for (int m = 0; m < n; ++m) {
         const float* q = params + 16 * m;
@@ -83,20 +94,42 @@ inline std::vector<Material> decode_materials(const int* kind, const float* para
         M.kind = kind[m];
         for (int k = 0; k < 3; ++k) { M.color[k] = q[k]; M.spec[k] = q[3 + k]; M.emission[k] = q[9 + k]; }
         M.exponent = q[6]; M.eta = q[7]; M.kappa = q[8]; M.area = 1.0f;
+        M.tex = textured && q[12] >= 0.0f ? (int)q[12] : -1;
+        M.bump = textured && q[13] >= 0.0f ? (int)q[13] : -1;
     }
     return mats;
 }
 
-inline std::vector<TriLight> decode_lights(const float* tri_lights, int n) {
-    std::vector<TriLight> lights(n > 1 ? n : 1);
+// Lights of 12 floats each; kinds (NULL: all triangles): triangle p0, p1, p2, intensity;
+// directional: direction (travel), 6 unused, intensity; point: position, 6 unused, intensity;
+// spot: position, axis, half-angle in radians, 2 unused, intensity.
+inline std::vector<LightSrc> decode_lights(const int* kinds, const float* params, int n) {
+    std::vector<LightSrc> lights(n > 1 ? n : 1);
     for (int l = 0; l < n; ++l) {
-        const float* q = tri_lights + 12 * l;
-        TriLight& L = lights[l];
+        const float* q = params + 12 * l;
+        LightSrc& L = lights[l];
         std::memset(&L, 0, sizeof(L));
-        for (int v = 0; v < 3; ++v) for (int a = 0; a < 3; ++a) L.v[v][a] = q[3 * v + a];
+        L.kind = kinds ? kinds[l] : kLightTri;
         for (int a = 0; a < 3; ++a) L.intensity[a] = q[9 + a];
+        if (L.kind == kLightTri) {
+            for (int v = 0; v < 3; ++v) for (int a = 0; a < 3; ++a) L.v[v][a] = q[3 * v + a];
+        } else if (L.kind == kLightDirectional) {
+            for (int a = 0; a < 3; ++a) L.normal[a] = q[a];
+        } else {
+            for (int a = 0; a < 3; ++a) L.v[0][a] = q[a];
+            if (L.kind == kLightSpot) {
+                for (int a = 0; a < 3; ++a) L.normal[a] = q[3 + a];
+                L.cos_angle = std::cos(q[6]);   // SpotLight ctor: cosf(angle) (light.h:298)
+            }
+        }
     }
     return lights;
+}
+
+inline bool valid_light_kinds(const int* kinds, int n) {
+    for (int l = 0; kinds && l < n; ++l)
+        if (kinds[l] < kLightTri || kinds[l] > kLightSpot) return false;
+    return true;
 }
 
 struct CameraParams {
@@ -268,12 +301,12 @@ __device__ __forceinline__ void shade_path(const ShadingScene& s, int max_path_l
         add_image(image, pixel, thr * li * mis);
         return;
     }
-    const Bsdf bsdf{&mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal};
+    const Bsdf bsdf = surface_bsdf(s, mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal, is.uv[0], is.uv[1],
+                                   false);
     // Next-event estimation (pt.cpp:17-44).
     const int l = rng.next_int(0, s.light_count);
     const float pdf_lightpick = 1.0f / (float)s.light_count;
-    const DirectSample ds = (s.has_env && l == 0) ? env_light_sample(s, rng)
-                                                  : tri_light_sample(s.lights[l - s.has_env], is.pos, rng);
+    const DirectSample ds = light_sample_direct(s, l, is.pos, rng);
     const V3 bsdf_value = bsdf.eval(is.out_dir, ds.dir);
     const float pdf_hit = bsdf.pdf(is.out_dir, ds.dir);
     const float pdf_di = pdf_lightpick * ds.pdf_direct_w;

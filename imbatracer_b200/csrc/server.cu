@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -163,17 +164,19 @@ double now_ms(std::chrono::steady_clock::time_point t0) {
 
 struct SceneRec {
     HostWideScene wide;
-    std::vector<float> vertices, normals, texcoords, geom_normals, inst_inv, mat_params, tri_lights;
-    std::vector<int> mesh_tris, mat_kind;
+    std::vector<float> vertices, normals, texcoords, geom_normals, inst_inv, mat_params, tri_lights, tex_pixels;
+    std::vector<int> mesh_tris, mat_kind, light_kinds, tex_dims;
     std::vector<Material> mats;
-    std::vector<TriLight> lights;
-    int n_tri_lights = 0;
+    std::vector<LightSrc> lights;
+    std::vector<int4> tex_info;
+    int n_tri_lights = 0;     // lights of every kind
+    int n_textures = 0;
     bool has_env = false;
     float env[3] = {0, 0, 0};
     float bsphere[5] = {0, 0, 0, 0, 0};
     // Block layout (byte offsets from the block start).
     size_t bytes = 0, o_nodes = 0, o_tris = 0, o_insts = 0, o_vert = 0, o_nrm = 0, o_tc = 0, o_mtris = 0,
-           o_gn = 0, o_inv = 0, o_mats = 0, o_lights = 0;
+           o_gn = 0, o_inv = 0, o_mats = 0, o_lights = 0, o_tex = 0, o_texinfo = 0;
     // Residency (batched mode).
     bool resident = false;
     size_t block = 0;
@@ -334,7 +337,9 @@ void layout_scene(SceneRec& s) {
     s.o_gn = o; o = align_up(o + s.geom_normals.size() * sizeof(float), kArrayAlign);
     s.o_inv = o; o = align_up(o + s.inst_inv.size() * sizeof(float), kArrayAlign);
     s.o_mats = o; o = align_up(o + s.mats.size() * sizeof(Material), kArrayAlign);
-    s.o_lights = o; o = align_up(o + s.lights.size() * sizeof(TriLight), kBlockAlign);
+    s.o_lights = o; o = align_up(o + s.lights.size() * sizeof(LightSrc), kArrayAlign);
+    s.o_tex = o; o = align_up(o + s.tex_pixels.size() * sizeof(float), kArrayAlign);
+    s.o_texinfo = o; o = align_up(o + s.tex_info.size() * sizeof(int4), kBlockAlign);
     s.bytes = o;
 }
 
@@ -395,7 +400,9 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
                 put(s.o_gn, s.geom_normals.data(), s.geom_normals.size() * sizeof(float)) &&
                 put(s.o_inv, s.inst_inv.data(), s.inst_inv.size() * sizeof(float)) &&
                 put(s.o_mats, s.mats.data(), s.mats.size() * sizeof(Material)) &&
-                put(s.o_lights, s.lights.data(), s.lights.size() * sizeof(TriLight));
+                put(s.o_lights, s.lights.data(), s.lights.size() * sizeof(LightSrc)) &&
+                put(s.o_tex, s.tex_pixels.data(), s.tex_pixels.size() * sizeof(float)) &&
+                put(s.o_texinfo, s.tex_info.data(), s.tex_info.size() * sizeof(int4));
     if (!good) {
         S->alloc.release(block, s.bytes);
         return IMBART_ERR_CUDA;
@@ -410,7 +417,7 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
     rebase_kernel<<<(n + 255) / 256, 256, 0, st>>>(nodes, n_nodes, s.wide.top_nodes, node_off, tri_off, inst_off,
                                                   insts, n_insts);
     Material* mats = reinterpret_cast<Material*>(b + s.o_mats);
-    TriLight* lights = reinterpret_cast<TriLight*>(b + s.o_lights);
+    LightSrc* lights = reinterpret_cast<LightSrc*>(b + s.o_lights);
     const int4* mtris = reinterpret_cast<const int4*>(b + s.o_mtris);
     const int n_mtris = (int)(s.mesh_tris.size() / 4);
     const float* verts = reinterpret_cast<const float*>(b + s.o_vert);
@@ -433,7 +440,10 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
     ss.materials = mats;
     ss.n_materials = (int)s.mats.size();
     ss.lights = lights;
-    ss.n_tri_lights = s.n_tri_lights;
+    ss.n_lights = s.n_tri_lights;
+    ss.tex_pixels = reinterpret_cast<const float4*>(b + s.o_tex);
+    ss.tex_info = reinterpret_cast<const int4*>(b + s.o_texinfo);
+    ss.n_textures = s.n_textures;
     ss.has_env = s.has_env ? 1 : 0;
     ss.light_count = s.n_tri_lights + ss.has_env;
     for (int k = 0; k < 3; ++k) ss.env_color[k] = s.env[k];
@@ -756,12 +766,13 @@ int plain_request(imbart_server* S, Request* r) {
     if (!s.plain_scene) {
         s.plain_scene = upload_wide_scene(s.wide, S->device);
         if (!s.plain_scene) return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
-        s.plain_shading = imbart_shading_create(
+        s.plain_shading = imbart_shading_create_ex(
             S->device, s.vertices.data(), (int)(s.vertices.size() / 3), s.normals.data(), s.texcoords.data(),
             s.mesh_tris.data(), s.geom_normals.data(), (int)(s.mesh_tris.size() / 4), s.inst_inv.data(),
             (int)(s.inst_inv.size() / 12), s.mat_kind.data(), s.mat_params.data(), (int)s.mat_kind.size(),
-            s.tri_lights.empty() ? nullptr : s.tri_lights.data(), s.n_tri_lights, s.has_env ? s.env : nullptr,
-            s.bsphere);
+            s.light_kinds.empty() ? nullptr : s.light_kinds.data(), s.tri_lights.empty() ? nullptr : s.tri_lights.data(),
+            s.n_tri_lights, s.has_env ? s.env : nullptr, s.bsphere, s.tex_dims.empty() ? nullptr : s.tex_dims.data(),
+            s.tex_pixels.empty() ? nullptr : s.tex_pixels.data(), s.n_textures);
         if (!s.plain_shading) return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
         S->stats.scene_uploads += 1;
     }
@@ -975,7 +986,9 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         src->n_tri_vec4 <= 0 || !src->vertices || src->n_vertices <= 0 || !src->normals || !src->texcoords ||
         !src->mesh_tris || !src->geom_normals || src->n_mesh_tris <= 0 || !src->inst_inv || src->n_inst_inv <= 0 ||
         !src->mat_kind || !src->mat_params || src->n_mats <= 0 || src->n_tri_lights < 0 ||
-        (src->n_tri_lights > 0 && !src->tri_lights) || (src->n_tri_lights == 0 && !src->env_color)) {
+        (src->n_tri_lights > 0 && !src->tri_lights) || (src->n_tri_lights == 0 && !src->env_color) ||
+        !valid_light_kinds(src->light_kinds, src->n_tri_lights) || src->n_textures < 0 ||
+        (src->n_textures > 0 && (!src->tex_dims || !src->tex_pixels))) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: invalid argument");
         return -IMBART_ERR_INVALID_ARGUMENT;
     }
@@ -996,8 +1009,30 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
     s->mat_kind = vec(src->mat_kind, (size_t)src->n_mats);
     s->mat_params = vec(src->mat_params, 16 * (size_t)src->n_mats);
     if (src->n_tri_lights > 0) s->tri_lights = vec(src->tri_lights, 12 * (size_t)src->n_tri_lights);
-    s->mats = decode_materials(src->mat_kind, src->mat_params, src->n_mats);
-    s->lights = decode_lights(src->tri_lights, src->n_tri_lights);
+    if (src->light_kinds && src->n_tri_lights > 0) s->light_kinds = vec(src->light_kinds, (size_t)src->n_tri_lights);
+    s->n_textures = src->n_textures;
+    long long texels = 0;
+    s->tex_info.assign(std::max(src->n_textures, 1), make_int4(0, 0, 0, 0));
+    for (int t = 0; t < src->n_textures; ++t) {
+        const int w = src->tex_dims[2 * t], h = src->tex_dims[2 * t + 1];
+        if (w <= 0 || h <= 0 || texels + (long long)w * h > INT_MAX) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: invalid texture size");
+            return -IMBART_ERR_INVALID_ARGUMENT;
+        }
+        s->tex_info[t] = make_int4((int)texels, w, h, 0);
+        texels += (long long)w * h;
+    }
+    if (src->n_textures > 0) {
+        s->tex_dims = vec(src->tex_dims, 2 * (size_t)src->n_textures);
+        s->tex_pixels = vec(src->tex_pixels, 4 * (size_t)texels);
+    }
+    s->mats = decode_materials(src->mat_kind, src->mat_params, src->n_mats, src->n_textures > 0);
+    for (const Material& m : s->mats)
+        if (m.tex >= src->n_textures || m.bump >= src->n_textures) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: texture index out of range");
+            return -IMBART_ERR_INVALID_ARGUMENT;
+        }
+    s->lights = decode_lights(src->light_kinds, src->tri_lights, src->n_tri_lights);
     s->n_tri_lights = src->n_tri_lights;
     s->has_env = src->env_color != nullptr;
     for (int k = 0; k < 3; ++k) s->env[k] = src->env_color ? src->env_color[k] : 0.0f;

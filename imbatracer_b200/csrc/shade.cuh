@@ -141,13 +141,22 @@ struct Material {
     float eta, kappa;
     float emission[3];  // area emitter intensity
     float area;         // area of the emissive face (object space)
+    int tex;            // diffuse texture (Lambertian, glossy, Phong): index or -1
+    int bump;           // bump map: texture index or -1
 };
 
-struct TriLight {
-    float v[3][3];
-    float normal[3], tangent[3], binormal[3];
-    float area;
+// Light kinds of light.h: triangle (TriangleLight :94-190), directional (:192-237), point
+// (:239-290), spot (:292-355). The constant environment is light 0 when present.
+enum LightKind { kLightTri = 0, kLightDirectional = 1, kLightPoint = 2, kLightSpot = 3 };
+
+struct LightSrc {
+    float v[3][3];      // triangle: vertices; point / spot: v[0] = position
+    float normal[3], tangent[3], binormal[3];   // triangle / spot: frame of the normal; directional:
+                                                // frame of the direction the light travels
+    float area;         // triangle area
     float intensity[3];
+    int kind;
+    float cos_angle;    // spot: cos of the cone half-angle
 };
 
 struct ShadingScene {
@@ -158,10 +167,13 @@ struct ShadingScene {
     const float* geom_normals;  // 3 floats per global triangle
     const float* inst_inv;      // 12 floats (3x4 row-major world-to-object) per instance
     const Material* materials;
-    const TriLight* lights;     // triangle lights, in light-list order after the environment
+    const LightSrc* lights;     // lights in light-list order after the environment
+    const float4* tex_pixels;   // texture texels (rgba), all textures back to back
+    const int4* tex_info;       // per texture: first texel, width, height
+    int n_textures;
     int n_materials;
-    int n_tri_lights;
-    int light_count;            // environment (if any) + triangle lights
+    int n_lights;
+    int light_count;            // environment (if any) + lights
     int has_env;
     float env_color[3];         // intensity * constant environment colour
     float bsphere[5];           // centre xyz, radius, 1/radius^2
@@ -170,6 +182,31 @@ struct ShadingScene {
 // ---------------------------------------------------------------------------------------
 // Intersection (integrator.h:71-123)
 // ---------------------------------------------------------------------------------------
+// TextureSampler::sample (texture_sampler.h:18-46): bilinear, wrapped, v flipped.
+__device__ __forceinline__ V3 texture_sample(const ShadingScene& s, int t, float uvx, float uvy) {
+    const int4 ti = s.tex_info[t];
+    const int w = ti.y, h = ti.z;
+    float u = clampf(uvx - (float)(int)uvx, -1.0f, 1.0f);
+    float v = clampf(uvy - (float)(int)uvy, -1.0f, 1.0f);
+    u += u < 0.0f ? 1.0f : 0.0f;
+    v += v < 0.0f ? 1.0f : 0.0f;
+    v = 1.0f - v;
+    const float kx = u * (float)(w - 1);
+    const float ky = v * (float)(h - 1);
+    const int x0 = (int)kx;
+    const int y0 = (int)ky;
+    const int x1 = (x0 + 1) % w;
+    const int y1 = (y0 + 1) % h;
+    const float gx = kx - floorf(kx);
+    const float gy = ky - floorf(ky);
+    const float hx = 1.0f - gx;
+    const float hy = 1.0f - gy;
+    const float4* px = s.tex_pixels + ti.x;
+    const float4 a = px[y0 * w + x0], b = px[y0 * w + x1], c = px[y1 * w + x0], d = px[y1 * w + x1];
+    const V3 i00(a.x, a.y, a.z), i10(b.x, b.y, b.z), i01(c.x, c.y, c.z), i11(d.x, d.y, d.z);
+    return hy * (hx * i00 + gx * i10) + gy * (hx * i01 + gx * i11);
+}
+
 struct Isect {
     V3 pos, out_dir, normal, geom_normal, u_tangent, v_tangent;
     float uv[2];
@@ -208,6 +245,22 @@ __device__ __forceinline__ Isect calculate_intersection(const ShadingScene& s, i
     r.out_dir = -normalize(out_dir);
     r.pos = pos;
     local_coordinates(r.normal, r.u_tangent, r.v_tangent);
+    // Material::bump (materials.h:32-53): finite differences of the bump map's red channel.
+    const int bump = s.materials[r.mat].bump;
+    if (bump >= 0) {
+        const float du = 0.001f, dv = 0.001f, vscale = 0.02f;
+        const V3 u_displace = texture_sample(s, bump, r.uv[0] + du, r.uv[1]);
+        const V3 v_displace = texture_sample(s, bump, r.uv[0], r.uv[1] + dv);
+        const V3 displace = texture_sample(s, bump, r.uv[0], r.uv[1]);
+        const float diff_u = vscale * (u_displace - displace).x / du;
+        const float diff_v = vscale * (v_displace - displace).x / dv;
+        const V3 nb = cross(r.v_tangent, r.u_tangent);
+        const V3 ub = r.u_tangent + diff_u * nb;
+        const V3 vb = r.v_tangent + diff_v * nb;
+        r.u_tangent = normalize(ub);
+        r.v_tangent = normalize(vb);
+        r.normal = cross(r.u_tangent, r.v_tangent);
+    }
     if (dot(r.geom_normal, r.normal) < 0.0f) r.normal = -r.normal;
     return r;
 }
@@ -240,12 +293,12 @@ __device__ __forceinline__ float fresnel_dielectric_eval(float cosi, float eta_o
 }
 
 // Lambertian (brdfs.h:8-21)
-__device__ __forceinline__ V3 lambert_eval(const float* c, V3 o, V3 i) {
-    return same_hemisphere(o, i) ? V3(c[0], c[1], c[2]) * (1.0f / kPi) : V3(0.0f);
+__device__ __forceinline__ V3 lambert_eval(V3 c, V3 o, V3 i) {
+    return same_hemisphere(o, i) ? c * (1.0f / kPi) : V3(0.0f);
 }
 __device__ __forceinline__ float default_pdf(V3 o, V3 i) { return same_hemisphere(o, i) ? cos_hemisphere_pdf(i.z) : 0.0f; }
 // BxDF::sample default (bsdf.h:54-64)
-__device__ __forceinline__ V3 lambert_sample(const float* c, V3 o, V3& in, Rng& rng, float* pdf) {
+__device__ __forceinline__ V3 lambert_sample(V3 c, V3 o, V3& in, Rng& rng, float* pdf) {
     float u1, u2;
     draw2(rng, u1, u2);
     in = sample_cos_hemisphere(u1, u2, pdf);
@@ -323,6 +376,7 @@ struct Bsdf {
     const Material* m;
     V3 n, ut, vt, gn;
     bool adjoint = false;   // light paths: the glass BTDF drops the (eta_in / eta_trans)^2 factor
+    V3 kd{0.0f};            // diffuse colour at the hit (the material's, or its texture's)
     __device__ V3 to_local(V3 d) const { return V3(dot(vt, d), dot(ut, d), dot(n, d)); }
     __device__ V3 to_world(V3 d) const {
         return V3(vt.x * d.x + ut.x * d.y + n.x * d.z, vt.y * d.x + ut.y * d.y + n.y * d.z,
@@ -339,9 +393,9 @@ struct Bsdf {
     __device__ V3 brdf_eval(V3 o, V3 i) const {
         switch (m->kind) {
             case kMirror: case kGlass: return V3(0.0f);
-            case kGlossy: return 0.5f * (ct_eval(m->spec, m->exponent, o, i) + lambert_eval(m->color, o, i));
-            case kPhong: return 0.5f * (phong_eval(m->spec, m->exponent, o, i) + lambert_eval(m->color, o, i));
-            default: return lambert_eval(m->color, o, i);
+            case kGlossy: return 0.5f * (ct_eval(m->spec, m->exponent, o, i) + lambert_eval(kd, o, i));
+            case kPhong: return 0.5f * (phong_eval(m->spec, m->exponent, o, i) + lambert_eval(kd, o, i));
+            default: return lambert_eval(kd, o, i);
         }
     }
     __device__ float brdf_pdf(V3 o, V3 i) const {
@@ -421,12 +475,12 @@ struct Bsdf {
                         value = m->kind == kGlossy ? ct_sample(m->spec, m->exponent, lo, li, rng, &pdf)
                                                    : phong_sample(m->spec, m->exponent, lo, li, rng, &pdf);
                     } else {
-                        value = lambert_sample(m->color, lo, li, rng, &pdf);
+                        value = lambert_sample(kd, lo, li, rng, &pdf);
                     }
                     break;
                 }
                 default:
-                    value = lambert_sample(m->color, lo, li, rng, &pdf);
+                    value = lambert_sample(kd, lo, li, rng, &pdf);
                     break;
             }
         }
@@ -460,7 +514,7 @@ struct EmitSample {
 };
 
 // TriangleLight::sample_direct (light.h:142-175)
-__device__ __forceinline__ DirectSample tri_light_sample(const TriLight& L, V3 from, Rng& rng) {
+__device__ __forceinline__ DirectSample tri_light_sample(const LightSrc& L, V3 from, Rng& rng) {
     DirectSample s;
     float r1, r2;
     draw2(rng, r1, r2);
@@ -513,7 +567,7 @@ __device__ __forceinline__ DirectSample env_light_sample(const ShadingScene& sc,
 }
 
 // TriangleLight::sample_emit (light.h:109-140)
-__device__ __forceinline__ EmitSample tri_light_emit(const TriLight& L, Rng& rng) {
+__device__ __forceinline__ EmitSample tri_light_emit(const LightSrc& L, Rng& rng) {
     EmitSample s;
     float r1, r2;
     draw2(rng, r1, r2);
@@ -570,6 +624,119 @@ __device__ __forceinline__ EmitSample env_light_emit(const ShadingScene& sc, Rng
     s.cos_out = 1.0f;
     s.radiance = color / s.pdf_emit_w;
     return s;
+}
+
+// DirectionalLight / PointLight / SpotLight::sample_direct (light.h:216-230, 265-282, 330-351):
+// no random numbers are drawn.
+__device__ __forceinline__ DirectSample delta_light_sample(const LightSrc& L, const ShadingScene& sc, V3 from) {
+    DirectSample s;
+    s.delta = true;
+    s.cos_out = 1.0f;
+    const V3 I(L.intensity[0], L.intensity[1], L.intensity[2]);
+    if (L.kind == kLightDirectional) {
+        s.dir = -V3(L.normal[0], L.normal[1], L.normal[2]);
+        s.distance = FLT_MAX;
+        s.radiance = I;
+        s.pdf_direct_w = 1.0f;
+        s.pdf_emit_w = concentric_disc_pdf() * sc.bsphere[4];
+        return s;
+    }
+    V3 dir = V3(L.v[0][0], L.v[0][1], L.v[0][2]) - from;
+    const float sqdist = dot(dir, dir);
+    const float dist = sqrtf(sqdist);
+    dir = dir * (1.0f / dist);
+    s.dir = dir;
+    s.distance = dist;
+    s.pdf_direct_w = sqdist;
+    if (L.kind == kLightPoint) {
+        s.radiance = I / (4.0f * kPi * sqdist);
+        s.pdf_emit_w = 1.0f / (4.0f * kPi);
+    } else {   // spot
+        const float cos_o = -dot(dir, V3(L.normal[0], L.normal[1], L.normal[2]));
+        if (cos_o < L.cos_angle) {
+            s.radiance = V3(0.0f);
+            s.pdf_emit_w = 0.0f;
+        } else {
+            s.radiance = I / sqdist;
+            s.pdf_emit_w = cos_o < L.cos_angle ? 0.0f : 1.0f / (2.0f * kPi * (1 - L.cos_angle));
+        }
+    }
+    return s;
+}
+
+// DirectionalLight / PointLight / SpotLight::sample_emit (light.h:201-214, 246-263, 304-328).
+__device__ __forceinline__ EmitSample delta_light_emit(const LightSrc& L, const ShadingScene& sc, Rng& rng) {
+    EmitSample s;
+    const V3 I(L.intensity[0], L.intensity[1], L.intensity[2]);
+    const V3 n(L.normal[0], L.normal[1], L.normal[2]), t(L.tangent[0], L.tangent[1], L.tangent[2]),
+        b(L.binormal[0], L.binormal[1], L.binormal[2]);
+    float u1, u2;
+    draw2(rng, u1, u2);
+    s.pdf_direct_a = 1.0f;
+    s.cos_out = 1.0f;
+    if (L.kind == kLightDirectional) {
+        float dx, dy;
+        sample_concentric_disc(u1, u2, dx, dy);
+        const V3 c(sc.bsphere[0], sc.bsphere[1], sc.bsphere[2]);
+        s.pos = c + sc.bsphere[3] * (-n + b * dx + t * dy);
+        s.dir = n;
+        s.pdf_emit_w = concentric_disc_pdf() * sc.bsphere[4];
+        s.radiance = I / s.pdf_emit_w;
+    } else if (L.kind == kLightPoint) {
+        // sample_uniform_sphere (random.h:120-127)
+        const float a = 2.0f * kPi * u1;
+        const float bb = 2.0f * sqrtf(u2 - sqr(u2));
+        s.pos = V3(L.v[0][0], L.v[0][1], L.v[0][2]);
+        s.radiance = I;
+        s.dir = spherical_dir(bb, 1.0f - 2.0f * u2, a);
+        s.pdf_emit_w = 1.0f / (4.0f * kPi);
+    } else {
+        // sample_uniform_cone (random.h:161-167)
+        const float phi = 2.0f * kPi * u1;
+        const float cos_t = 1.0f - u2 * (1.0f - L.cos_angle);
+        const float sin_t = sqrtf(1.0f - cos_t * cos_t);
+        const V3 d = spherical_dir(sin_t, cos_t, phi);
+        const float pdf = 1.0f / (2.0f * kPi * (1 - L.cos_angle));
+        s.pos = V3(L.v[0][0], L.v[0][1], L.v[0][2]);
+        s.dir = d.x * b + d.y * t + d.z * n;
+        s.radiance = I / pdf;
+        s.pdf_emit_w = pdf;
+    }
+    return s;
+}
+
+// Light l of the scene's list (the environment first when present).
+__device__ __forceinline__ DirectSample light_sample_direct(const ShadingScene& s, int l, V3 from, Rng& rng) {
+    if (s.has_env && l == 0) return env_light_sample(s, rng);
+    const LightSrc& L = s.lights[l - s.has_env];
+    return L.kind == kLightTri ? tri_light_sample(L, from, rng) : delta_light_sample(L, s, from);
+}
+
+__device__ __forceinline__ EmitSample light_emit(const ShadingScene& s, int l, Rng& rng) {
+    if (s.has_env && l == 0) return env_light_emit(s, rng);
+    const LightSrc& L = s.lights[l - s.has_env];
+    return L.kind == kLightTri ? tri_light_emit(L, rng) : delta_light_emit(L, s, rng);
+}
+
+// Light::is_delta / is_finite
+__device__ __forceinline__ bool light_is_delta(const ShadingScene& s, int l) {
+    return !(s.has_env && l == 0) && s.lights[l - s.has_env].kind != kLightTri;
+}
+__device__ __forceinline__ bool light_is_finite(const ShadingScene& s, int l) {
+    return !(s.has_env && l == 0) && s.lights[l - s.has_env].kind != kLightDirectional;
+}
+
+// The BSDF of a surface point of material m: the diffuse colour comes from the material's
+// texture when it has one (DiffuseMaterial / GlossyMaterial::get_bsdf, materials.h:76-84,
+// 170-181); light paths use the adjoint form.
+__device__ __forceinline__ Bsdf surface_bsdf(const ShadingScene& sc, const Material& m, V3 n, V3 ut, V3 vt, V3 gn,
+                                             float uvx, float uvy, bool adjoint) {
+    Bsdf b{&m, n, ut, vt, gn};
+    b.adjoint = adjoint;
+    b.kd = (m.tex >= 0 && (m.kind == kLambert || m.kind == kGlossy || m.kind == kPhong))
+               ? texture_sample(sc, m.tex, uvx, uvy)
+               : V3(m.color[0], m.color[1], m.color[2]);
+    return b;
 }
 
 // AreaEmitter::radiance (light.h:22-43) with both pdfs.

@@ -81,16 +81,6 @@ __device__ __forceinline__ float shading_normal_adjoint(V3 normal, V3 geom_norma
     return dot(out_dir, normal) * dot(in_dir, geom_normal) / dot(out_dir, geom_normal);
 }
 
-__device__ __forceinline__ DirectSample light_sample_direct(const ShadingScene& s, int l, V3 from, Rng& rng) {
-    return (s.has_env && l == 0) ? env_light_sample(s, rng) : tri_light_sample(s.lights[l - s.has_env], from, rng);
-}
-
-// The BSDF of a surface point; light paths use the adjoint form (materials.h:130-139).
-__device__ __forceinline__ Bsdf make_bsdf(const Material* m, V3 n, V3 ut, V3 vt, V3 gn, bool adjoint) {
-    Bsdf b{m, n, ut, vt, gn};
-    b.adjoint = adjoint;
-    return b;
-}
 
 // VCMIntegrator::bounce (vcm.cpp:132-190). Returns false when the path ends.
 __device__ __forceinline__ bool vcm_bounce(const VcmParams& p, Rng& rng, V3& thr, int& path_length, float& dVC,
@@ -147,17 +137,16 @@ __global__ void light_gen_kernel(VcmParams p, const LightTile* tiles, int n_tile
     const int i = j - t.first;
     Rng rng = seed_sample(t.seed, i, i);
     const ShadingScene& s = p.s;
-    const bool env = s.has_env && t.light == 0;
     const float pdf_lightpick = 1.0f / (float)s.light_count;
-    const EmitSample e = env ? env_light_emit(s, rng) : tri_light_emit(s.lights[t.light - s.has_env], rng);
+    const EmitSample e = light_emit(s, t.light, rng);
     rays[2 * j + 0] = make_float4(e.pos.x, e.pos.y, e.pos.z, 1e-3f);
     rays[2 * j + 1] = make_float4(e.dir.x, e.dir.y, e.dir.z, FLT_MAX);
     const V3 tp = e.radiance / pdf_lightpick;
     thr[j] = f4(tp, __int_as_float(1));
     const float dVCM = e.pdf_direct_a / e.pdf_emit_w;
-    const float dVC = e.cos_out / (e.pdf_emit_w * pdf_lightpick);   // lights here are never delta lights
+    const float dVC = light_is_delta(s, t.light) ? 0.0f : e.cos_out / (e.pdf_emit_w * pdf_lightpick);
     const float dVM = dVC * p.eta_vc;
-    w[j] = make_float4(dVC, dVCM, dVM, env ? 0.0f : 1.0f);           // w: finite light
+    w[j] = make_float4(dVC, dVCM, dVM, light_is_finite(s, t.light) ? 1.0f : 0.0f);   // w: finite light
     rng_out[j] = rng.state;
 }
 
@@ -234,7 +223,8 @@ __global__ void __launch_bounds__(128) light_shade_kernel(VcmParams p, int n, fl
                     dVM *= 1.0f / cos_theta_o;
                     V3 thr = v3(t4);
                     const Material& mat = s.materials[is.mat];
-                    const Bsdf bsdf = make_bsdf(&mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal, true);
+                    const Bsdf bsdf = surface_bsdf(s, mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal,
+                                                   is.uv[0], is.uv[1], true);
                     if (!is_specular_material(mat)) {
                         if (p.algo != kAlgoLt) {
                             float4* v = stage + 7 * (size_t)i;
@@ -435,7 +425,7 @@ __device__ __forceinline__ bool vcm_connect_one(const VcmParams& p, int cam_path
     const float4 q2 = __ldg(v + 2), q3 = __ldg(v + 3), q4 = __ldg(v + 4), q5 = __ldg(v + 5), q6 = __ldg(v + 6);
     const V3 lpos = v3(q0), lout = v3(q1), lnormal = v3(q2), lgn = v3(q3);
     const Material& lmat = p.s.materials[mi];
-    const Bsdf light_bsdf = make_bsdf(&lmat, lnormal, v3(q4), v3(q5), lgn, true);
+    const Bsdf light_bsdf = surface_bsdf(p.s, lmat, lnormal, v3(q4), v3(q5), lgn, q5.w, q6.w, true);
     V3 connect_dir = lpos - is.pos;
     const float connect_dist_sq = dot(connect_dir, connect_dir);
     const float connect_dist = sqrtf(connect_dist_sq);
@@ -505,7 +495,7 @@ __device__ __forceinline__ V3 vcm_merge(const VcmParams& p, V3 thr, float dVCM, 
 }
 
 // A camera vertex waiting for merging (7 float4): pos + pixel, out_dir + material, normal +
-// dVCM, geometric normal + dVM, u tangent, v tangent, throughput.
+// dVCM, geometric normal + dVM, u tangent + uv.x, v tangent + uv.y, throughput.
 constexpr int kMergeRec = 7;
 
 // Vertex merging for the camera vertices queued by the shading kernel (count on the device).
@@ -522,7 +512,8 @@ __global__ void __launch_bounds__(128) vcm_merge_kernel(VcmParams p, const int* 
     is.u_tangent = v3(m4);
     is.v_tangent = v3(m5);
     is.mat = __float_as_int(m1.w);
-    const Bsdf bsdf = make_bsdf(&p.s.materials[is.mat], is.normal, is.u_tangent, is.v_tangent, is.geom_normal, false);
+    const Bsdf bsdf = surface_bsdf(p.s, p.s.materials[is.mat], is.normal, is.u_tangent, is.v_tangent, is.geom_normal,
+                                   m4.w, m5.w, false);
     add_image(p.image, __float_as_int(m0.w), vcm_merge(p, v3(m6), m2.w, m3.w, is, bsdf));
 }
 
@@ -633,7 +624,7 @@ __global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const 
     }
     if (lane < count) {
         const Material& mat = p.s.materials[__float_as_int(m1.w)];
-        const Bsdf bsdf = make_bsdf(&mat, v3(m2), v3(m4), v3(m5), v3(m3), false);
+        const Bsdf bsdf = surface_bsdf(p.s, mat, v3(m2), v3(m4), v3(m5), v3(m3), m4.w, m5.w, false);
         const float4* v = p.cache + 7 * (size_t)my_id;
         const float4 q1 = __ldg(v + 1), q3 = __ldg(v + 3), q4 = __ldg(v + 4), q6 = __ldg(v + 6);
         const V3 photon_in_dir = v3(q1);
@@ -708,7 +699,8 @@ __global__ void __launch_bounds__(128) vcm_camera_shade_kernel(
                                         V3(rd.x, rd.y, rd.z));
             const float cos_theta_o = fabsf(dot(is.out_dir, is.normal));
             const Material& mat = s.materials[is.mat];
-            bsdf = make_bsdf(&mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal, false);
+            bsdf = surface_bsdf(s, mat, is.normal, is.u_tangent, is.v_tangent, is.geom_normal, is.uv[0], is.uv[1],
+                                false);
             dVCM *= sqr(tmax) / cos_theta_o;
             dVC *= 1.0f / cos_theta_o;
             dVM *= 1.0f / cos_theta_o;
@@ -771,8 +763,8 @@ __global__ void __launch_bounds__(128) vcm_camera_shade_kernel(
         r[1] = f4(is.out_dir, __int_as_float(is.mat));
         r[2] = f4(is.normal, dVCM);
         r[3] = f4(is.geom_normal, dVM);
-        r[4] = f4(is.u_tangent, 0.0f);
-        r[5] = f4(is.v_tangent, 0.0f);
+        r[4] = f4(is.u_tangent, is.uv[0]);
+        r[5] = f4(is.v_tangent, is.uv[1]);
         r[6] = f4(thr, 0.0f);
     }
     if (surface) {

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -98,30 +99,48 @@ using namespace imbart;
 
 extern "C" {
 
-imbart_shading* imbart_shading_create(int device, const float* vertices, int n_vertices, const float* normals,
-                                      const float* texcoords, const int* tris, const float* geom_normals, int n_tris,
-                                      const float* inst_inv, int n_inst, const int* mat_kind,
-                                      const float* mat_params, int n_mats, const float* tri_lights,
-                                      int n_tri_lights, const float* env_color, const float* bsphere) {
+imbart_shading* imbart_shading_create_ex(int device, const float* vertices, int n_vertices, const float* normals,
+                                         const float* texcoords, const int* tris, const float* geom_normals,
+                                         int n_tris, const float* inst_inv, int n_inst, const int* mat_kind,
+                                         const float* mat_params, int n_mats, const int* light_kinds,
+                                         const float* lights_in, int n_lights, const float* env_color,
+                                         const float* bsphere, const int* tex_dims, const float* tex_pixels,
+                                         int n_textures) {
     if (!vertices || !normals || !texcoords || !tris || !geom_normals || !inst_inv || !mat_kind || !mat_params ||
-        n_vertices <= 0 || n_tris <= 0 || n_inst <= 0 || n_mats <= 0 || n_tri_lights < 0 ||
-        (n_tri_lights > 0 && !tri_lights) || (n_tri_lights == 0 && !env_color)) {
+        n_vertices <= 0 || n_tris <= 0 || n_inst <= 0 || n_mats <= 0 || n_lights < 0 ||
+        (n_lights > 0 && !lights_in) || (n_lights == 0 && !env_color) || !valid_light_kinds(light_kinds, n_lights) ||
+        n_textures < 0 || (n_textures > 0 && (!tex_dims || !tex_pixels))) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_shading_create: invalid argument");
         return nullptr;
     }
+    std::vector<int4> tex_info(std::max(n_textures, 1), make_int4(0, 0, 0, 0));
+    long long texels = 0;
+    for (int t = 0; t < n_textures; ++t) {
+        if (tex_dims[2 * t] <= 0 || tex_dims[2 * t + 1] <= 0 || texels + (long long)tex_dims[2 * t] * tex_dims[2 * t + 1] > INT_MAX) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_shading_create: invalid texture size");
+            return nullptr;
+        }
+        tex_info[t] = make_int4((int)texels, tex_dims[2 * t], tex_dims[2 * t + 1], 0);
+        texels += (long long)tex_dims[2 * t] * tex_dims[2 * t + 1];
+    }
+    const std::vector<Material> mats = decode_materials(mat_kind, mat_params, n_mats, n_textures > 0);
+    for (const Material& m : mats)
+        if (m.tex >= n_textures || m.bump >= n_textures) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_shading_create: texture index out of range");
+            return nullptr;
+        }
+    const std::vector<LightSrc> lights = decode_lights(light_kinds, lights_in, n_lights);
     int prev = 0;
     cudaGetDevice(&prev);
     if (!ok(cudaSetDevice(device), "cudaSetDevice")) return nullptr;
     imbart_shading* h = new imbart_shading;
     h->device = device;
     ShadingScene& s = h->s;
-    const std::vector<Material> mats = decode_materials(mat_kind, mat_params, n_mats);
-    const std::vector<TriLight> lights = decode_lights(tri_lights, n_tri_lights);
     auto upl = [&](const void* src, size_t bytes) -> void* {
         void* d = nullptr;
-        if (!ok(cudaMalloc(&d, std::max<size_t>(bytes, 4)), "cudaMalloc")) return nullptr;
+        if (!ok(cudaMalloc(&d, std::max<size_t>(bytes, 16)), "cudaMalloc")) return nullptr;
         h->allocations.push_back(d);
-        if (!ok(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy")) return nullptr;
+        if (bytes > 0 && !ok(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy")) return nullptr;
         return d;
     };
     s.vertices = (const float*)upl(vertices, sizeof(float) * 3 * (size_t)n_vertices);
@@ -131,18 +150,22 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
     s.geom_normals = (const float*)upl(geom_normals, sizeof(float) * 3 * (size_t)n_tris);
     s.inst_inv = (const float*)upl(inst_inv, sizeof(float) * 12 * (size_t)n_inst);
     Material* dmats = (Material*)upl(mats.data(), sizeof(Material) * mats.size());
-    TriLight* dlights = (TriLight*)upl(lights.data(), sizeof(TriLight) * lights.size());
+    LightSrc* dlights = (LightSrc*)upl(lights.data(), sizeof(LightSrc) * lights.size());
+    s.tex_pixels = (const float4*)upl(tex_pixels, sizeof(float4) * (size_t)texels);
+    s.tex_info = (const int4*)upl(tex_info.data(), sizeof(int4) * tex_info.size());
+    s.n_textures = n_textures;
     s.materials = dmats;
     s.n_materials = n_mats;
     s.lights = dlights;
-    s.n_tri_lights = n_tri_lights;
+    s.n_lights = n_lights;
     s.has_env = env_color ? 1 : 0;
-    s.light_count = n_tri_lights + s.has_env;
+    s.light_count = n_lights + s.has_env;
     for (int k = 0; k < 3; ++k) s.env_color[k] = env_color ? env_color[k] : 0.0f;
     for (int k = 0; k < 5; ++k) s.bsphere[k] = bsphere ? bsphere[k] : 0.0f;
-    const bool good = s.vertices && s.normals && s.texcoords && s.tris && s.geom_normals && s.inst_inv && dmats && dlights;
+    const bool good = s.vertices && s.normals && s.texcoords && s.tris && s.geom_normals && s.inst_inv && dmats &&
+                      dlights && s.tex_pixels && s.tex_info;
     if (good) {
-        if (n_tri_lights > 0) setup_lights_kernel<<<(n_tri_lights + 127) / 128, 128>>>(dlights, n_tri_lights);
+        if (n_lights > 0) setup_lights_kernel<<<(n_lights + 127) / 128, 128>>>(dlights, n_lights);
         emitter_area_kernel<<<(n_tris + 127) / 128, 128>>>(s.vertices, s.tris, n_tris, dmats);
     }
     const bool synced = good && ok(cudaDeviceSynchronize(), "shading setup");
@@ -153,6 +176,16 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
         return nullptr;
     }
     return h;
+}
+
+imbart_shading* imbart_shading_create(int device, const float* vertices, int n_vertices, const float* normals,
+                                      const float* texcoords, const int* tris, const float* geom_normals, int n_tris,
+                                      const float* inst_inv, int n_inst, const int* mat_kind,
+                                      const float* mat_params, int n_mats, const float* tri_lights,
+                                      int n_tri_lights, const float* env_color, const float* bsphere) {
+    return imbart_shading_create_ex(device, vertices, n_vertices, normals, texcoords, tris, geom_normals, n_tris,
+                                    inst_inv, n_inst, mat_kind, mat_params, n_mats, nullptr, tri_lights, n_tri_lights,
+                                    env_color, bsphere, nullptr, nullptr, 0);
 }
 
 void imbart_shading_destroy(imbart_shading* h) {

@@ -49,12 +49,23 @@ class ShadingData:
             prm[i, 7] = m.eta
             prm[i, 8] = m.kappa
             prm[i, 9:12] = m.emission
+            prm[i, 12] = getattr(m, "texture", -1)
+            prm[i, 13] = getattr(m, "bump", -1)
         self.mat_params = prm
-        lights = np.zeros((max(len(desc.lights), 1), 12), np.float32)
+        n_tri, delta = len(desc.lights), list(getattr(desc, "delta_lights", []))
+        lights = np.zeros((max(n_tri + len(delta), 1), 12), np.float32)
         for i, (p0, p1, p2, e) in enumerate(desc.lights):
             lights[i] = np.concatenate([p0, p1, p2, e])
+        for i, (kind, prm12) in enumerate(delta):
+            lights[n_tri + i] = np.asarray(prm12, np.float32)
         self.lights = lights
-        self.n_lights = len(desc.lights)
+        self.n_lights = n_tri + len(delta)
+        self.light_kinds = np.array([0] * n_tri + [k for k, _ in delta] + [0], np.int32)[:max(self.n_lights, 1)]
+        tex = list(getattr(desc, "textures", []))
+        self.n_textures = len(tex)
+        self.tex_dims = np.array([[t.shape[1], t.shape[0]] for t in tex] or [[0, 0]], np.int32).reshape(-1)
+        self.tex_pixels = (np.ascontiguousarray(np.concatenate([np.asarray(t, np.float32).reshape(-1) for t in tex]))
+                           if tex else np.zeros(4, np.float32))
         self.env = None if desc.env_intensity is None else np.array(desc.env_intensity, np.float32)
         self.bsphere = bounding_sphere(desc)
 
@@ -97,11 +108,12 @@ class GpuScene:
         sd = ShadingData(desc)
         self.sd = sd
         lib = N.load()
-        h = lib.imbart_shading_create(device, N.ptr(sd.vertices), len(sd.vertices), N.ptr(sd.normals),
-                                      N.ptr(sd.texcoords), N.ptr(sd.tris), N.ptr(sd.geom_normals), len(sd.tris),
-                                      N.ptr(sd.inst_inv), len(sd.inst_inv), N.ptr(sd.mat_kind), N.ptr(sd.mat_params),
-                                      len(sd.mat_kind), N.ptr(sd.lights), sd.n_lights, N.ptr(sd.env),
-                                      N.ptr(sd.bsphere))
+        h = lib.imbart_shading_create_ex(device, N.ptr(sd.vertices), len(sd.vertices), N.ptr(sd.normals),
+                                         N.ptr(sd.texcoords), N.ptr(sd.tris), N.ptr(sd.geom_normals), len(sd.tris),
+                                         N.ptr(sd.inst_inv), len(sd.inst_inv), N.ptr(sd.mat_kind),
+                                         N.ptr(sd.mat_params), len(sd.mat_kind), N.ptr(sd.light_kinds),
+                                         N.ptr(sd.lights), sd.n_lights, N.ptr(sd.env), N.ptr(sd.bsphere),
+                                         N.ptr(sd.tex_dims), N.ptr(sd.tex_pixels), sd.n_textures)
         if not h:
             raise N.ImbartError("imbart_shading_create: " + N.last_error()[1])
         self.shading = h

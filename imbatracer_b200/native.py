@@ -67,7 +67,8 @@ class SceneSource(C.Structure):
                 ("mesh_tris", C.c_void_p), ("geom_normals", C.c_void_p), ("n_mesh_tris", C.c_int),
                 ("inst_inv", C.c_void_p), ("n_inst_inv", C.c_int), ("mat_kind", C.c_void_p),
                 ("mat_params", C.c_void_p), ("n_mats", C.c_int), ("tri_lights", C.c_void_p), ("n_tri_lights", C.c_int),
-                ("env_color", C.c_void_p), ("bsphere", C.c_void_p)]
+                ("env_color", C.c_void_p), ("bsphere", C.c_void_p), ("light_kinds", C.c_void_p),
+                ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int)]
 
 
 class RenderRequest(C.Structure):
@@ -130,6 +131,7 @@ _SIGNATURES = {
     "imbart_camera_rays": (I, [P, P, I, I, I, C.c_uint64, C.c_longlong, I, P, P, P, P, P]),
     "imbart_shading_create": (P, [I, P, I, P, P, P, P, I, P, I, P, P, I, P, I, P, P]),
     "imbart_shading_destroy": (None, [P]),
+    "imbart_shading_create_ex": (P, [I, P, I, P, P, P, P, I, P, I, P, P, I, P, P, I, P, P, P, P, I]),
     "imbart_pt_create": (P, [I]),
     "imbart_pt_destroy": (None, [P]),
     "imbart_pt_render": (I, [P, P, P, P, P, I, I, I, I, I, C.c_uint64, P, C.c_longlong, P, P]),

@@ -33,6 +33,8 @@ from .scene import Instance, Mesh
 # Material kinds (the reference's material classes, render/materials/materials.h, plus the
 # Phong class the configs ask for; brdfs.h:48-91 defines the Phong BxDF).
 LAMBERT, MIRROR, GLASS, GLOSSY, PHONG, EMISSIVE = 0, 1, 2, 3, 4, 5
+# Light kinds besides triangle lights (light.h: DirectionalLight, PointLight, SpotLight).
+DIRECTIONAL, POINT, SPOT = 1, 2, 3
 
 
 @dataclass
@@ -44,6 +46,8 @@ class Material:
     eta: float = 1.5                        # glass IOR / mirror eta
     kappa: float = 0.0                      # mirror conductor kappa
     emission: tuple = (0.0, 0.0, 0.0)       # area emitter intensity (emissive faces)
+    texture: int = -1                       # diffuse texture (Lambertian, glossy, Phong), index into textures
+    bump: int = -1                          # bump map, index into textures
 
 
 @dataclass
@@ -65,6 +69,11 @@ class SceneDesc:
     camera: Camera | None = None
     env_intensity: tuple | None = None               # constant environment light
     name: str = ""
+    # Lights of the other kinds, after the triangle lights: (kind, 12 floats) with kind
+    # DIRECTIONAL (direction of travel, -, -, intensity), POINT (position, -, -, intensity) or
+    # SPOT (position, axis, half-angle in radians + 2 unused, intensity).
+    delta_lights: list = field(default_factory=list)
+    textures: list = field(default_factory=list)     # (height, width, 4) float32 rgba, texel (x, y) at [y, x]
 
     @property
     def instanced_triangles(self) -> int:

@@ -50,6 +50,9 @@ class Server:
         src.mat_kind, src.mat_params, src.n_mats = N.ptr(sd.mat_kind), N.ptr(sd.mat_params), len(sd.mat_kind)
         src.tri_lights, src.n_tri_lights = N.ptr(sd.lights), sd.n_lights
         src.env_color, src.bsphere = N.ptr(sd.env), N.ptr(sd.bsphere)
+        src.light_kinds = N.ptr(sd.light_kinds)
+        src.tex_dims, src.tex_pixels, src.n_textures = N.ptr(sd.tex_dims), N.ptr(sd.tex_pixels), sd.n_textures
+        self._scenes.append((td, sd))   # the arrays the source points to stay alive during the call
         sid = self.lib.imbart_server_add_scene(self.h, C.byref(src))
         if sid < 0:
             raise N.ImbartError("imbart_server_add_scene: " + N.last_error()[1])

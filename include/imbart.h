@@ -326,6 +326,25 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
                                       int n_tri_lights, const float* env_color, const float* bsphere);
 void imbart_shading_destroy(imbart_shading* shading);
 
+/* imbart_shading_create with every light kind of the reference and textures.
+ * Lights (12 floats each, after the environment in the light list), light_kinds[i] (NULL: all
+ * triangles): 0 triangle {p0, p1, p2, intensity} (TriangleLight, light.h:94-190);
+ * 1 directional {direction of travel (normalized), 6 unused, intensity} (DirectionalLight,
+ * :192-237); 2 point {position, 6 unused, intensity} (PointLight, :239-290); 3 spot {position,
+ * axis (normalized), half-angle in radians, 2 unused, intensity} (SpotLight, :292-355).
+ * Textures (TextureSampler, texture_sampler.h:18-46): tex_dims[2t] = width, [2t+1] = height,
+ * tex_pixels = the textures' rgba texels back to back, rows bottom-up as the reference indexes
+ * them (texel (x, y) at y * width + x). Material params[12] = diffuse texture of a Lambertian,
+ * glossy or Phong material, params[13] = bump map of any material (Material::bump,
+ * materials.h:32-53); negative = none. */
+imbart_shading* imbart_shading_create_ex(int device, const float* vertices, int n_vertices, const float* normals,
+                                         const float* texcoords, const int* tris, const float* geom_normals,
+                                         int n_tris, const float* inst_inv, int n_inst, const int* mat_kind,
+                                         const float* mat_params, int n_mats, const int* light_kinds,
+                                         const float* lights, int n_lights, const float* env_color,
+                                         const float* bsphere, const int* tex_dims, const float* tex_pixels,
+                                         int n_textures);
+
 /* Wavefront path-tracing context (device queues, grown on demand). */
 typedef struct imbart_pt_context imbart_pt_context;
 imbart_pt_context* imbart_pt_create(int device);
@@ -490,6 +509,12 @@ typedef struct {
     const float* tri_lights; int n_tri_lights;
     const float* env_color;    /* NULL: no environment light */
     const float* bsphere;      /* NULL: zero */
+    /* Optional, as in imbart_shading_create_ex: kinds of the n_tri_lights lights (NULL: all
+     * triangles) and textures (n_textures = 0: none). */
+    const int* light_kinds;
+    const int* tex_dims;
+    const float* tex_pixels;
+    int n_textures;
 } imbart_scene_source;
 
 /* One path-traced frame (as imbart_pt_render with a fresh zeroed image). image_host: HOST

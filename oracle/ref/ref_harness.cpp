@@ -90,11 +90,13 @@ namespace {
 // Lambertian BxDFs (brdfs.h:8-91), built like GlossyMaterial (materials.h:151-189).
 class PhongMaterialRef : public Material {
 public:
-    PhongMaterialRef(float exponent, const rgb& spec, const rgb& diff) : exponent_(exponent), spec_(spec), diff_(diff) {}
-    Material* duplicate() const override { return new PhongMaterialRef(exponent_, spec_, diff_); }
+    PhongMaterialRef(float exponent, const rgb& spec, const rgb& diff, const TextureSampler* diff_sampler = nullptr,
+                     const TextureSampler* bump = nullptr)
+        : Material(bump), exponent_(exponent), spec_(spec), diff_(diff), diff_sampler_(diff_sampler) {}
+    Material* duplicate() const override { return new PhongMaterialRef(exponent_, spec_, diff_, diff_sampler_, bump_); }
     BSDF* get_bsdf(const Intersection& isect, MemoryArena& arena, bool) const override {
         auto a = arena.alloc<Phong>(spec_, exponent_);
-        auto b = arena.alloc<Lambertian>(diff_);
+        auto b = arena.alloc<Lambertian>(diff_sampler_ ? diff_sampler_->sample(isect.uv) : diff_);
         auto brdf = arena.alloc<CombineBxDF>(a, b);
         return arena.alloc<BSDF>(isect, brdf, nullptr);
     }
@@ -102,11 +104,14 @@ public:
 private:
     float exponent_;
     rgb spec_, diff_;
+    const TextureSampler* diff_sampler_;
 };
 
 struct RefScene {
     Scene scene{false, true};
     MaskBuffer masks;
+    std::vector<int> mat_kind;
+    std::vector<float> mat_params;
 };
 
 float3 f3(const float* p) { return float3(p[0], p[1], p[2]); }
@@ -249,6 +254,8 @@ void* ref_scene_create(int n_meshes, const int* mesh_nverts, const int* mesh_ntr
         scene.set_env_map(new EnvMap(img, 1.0f, scene.bounding_sphere()));
         scene.lights().emplace_back(new EnvLight(scene.env_map(), scene.bounding_sphere()));
     }
+    rs->mat_kind.assign(mat_kind, mat_kind + n_mats);
+    rs->mat_params.assign(mat_params, mat_params + 16 * (size_t)n_mats);
     for (int m = 0; m < n_mats; ++m) {
         const float* p = mat_params + 16 * m;
         const rgb color(p[0], p[1], p[2]), spec(p[3], p[4], p[5]), emit(p[9], p[10], p[11]);
@@ -291,6 +298,56 @@ void* ref_scene_create(int n_meshes, const int* mesh_nverts, const int* mesh_ntr
 }
 
 void ref_scene_destroy(void* h) { delete static_cast<RefScene*>(h); }
+
+// Adds the reference's other light kinds after the scene's lights (kinds 1 directional,
+// 2 point, 3 spot; 12 floats each, the layout of imbart_shading_create_ex) and textures
+// (TextureSampler over rgba texels, texel (x, y) at y * width + x), then rebuilds the
+// materials with a diffuse texture (mat_tex) or a bump map (mat_bump); -1 = none.
+int ref_scene_extend(void* h, int n_lights, const int* kinds, const float* lights, int n_tex, const int* tex_dims,
+                     const float* tex_pixels, const int* mat_tex, const int* mat_bump) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    Scene& scene = rs->scene;
+    for (int l = 0; l < n_lights; ++l) {
+        const float* q = lights + 12 * l;
+        const rgb intensity(q[9], q[10], q[11]);
+        switch (kinds[l]) {
+            case 1: scene.lights().emplace_back(new DirectionalLight(f3(q), intensity, scene.bounding_sphere())); break;
+            case 2: scene.lights().emplace_back(new PointLight(f3(q), intensity)); break;
+            case 3: scene.lights().emplace_back(new SpotLight(f3(q), f3(q + 3), q[6], intensity)); break;
+            default: return -1;
+        }
+    }
+    const int first_tex = (int)scene.textures().size();
+    size_t off = 0;
+    for (int t = 0; t < n_tex; ++t) {
+        const int w = tex_dims[2 * t], ht = tex_dims[2 * t + 1];
+        Image img(w, ht);
+        for (int i = 0; i < w * ht; ++i) {
+            const float* p = tex_pixels + 4 * (off + i);
+            img.pixels()[i] = float4(p[0], p[1], p[2], p[3]);
+        }
+        off += (size_t)w * ht;
+        scene.textures().emplace_back(new TextureSampler(std::move(img)));
+    }
+    for (int m = 0; mat_tex && mat_bump && m < (int)rs->mat_kind.size(); ++m) {
+        if (mat_tex[m] < 0 && mat_bump[m] < 0) continue;
+        const float* p = rs->mat_params.data() + 16 * m;
+        const rgb color(p[0], p[1], p[2]), spec(p[3], p[4], p[5]);
+        TextureSampler* tex = mat_tex[m] >= 0 ? scene.texture(first_tex + mat_tex[m]).get() : nullptr;
+        TextureSampler* bump = mat_bump[m] >= 0 ? scene.texture(first_tex + mat_bump[m]).get() : nullptr;
+        Material* mat = nullptr;
+        switch (rs->mat_kind[m]) {
+            case 1: mat = new MirrorMaterial(p[7], p[8], color, bump); break;
+            case 2: mat = new GlassMaterial(p[7], color, spec, bump); break;
+            case 3: mat = tex ? new GlossyMaterial(p[6], spec, tex, bump) : new GlossyMaterial(p[6], spec, color, bump); break;
+            case 4: mat = new PhongMaterialRef(p[6], spec, color, tex, bump); break;
+            case 5: return -2;   // emissive faces keep their plain material
+            default: mat = tex ? new DiffuseMaterial(tex, bump) : new DiffuseMaterial(color, bump); break;
+        }
+        scene.materials()[m].reset(mat);
+    }
+    return 0;
+}
 
 // Samplers of the reference evaluated with a fresh RNG(seed). Several of them take two
 // rng.random_float() calls as arguments of one call, whose evaluation order C++ leaves to

@@ -33,6 +33,7 @@ def load() -> C.CDLL:
             "ref_hashgrid_query": (I, [P, I, F, P, I, I, P, P]),
             "ref_scene_create": (P, [I, P, P, P, P, P, P, P, I, P, P, I, P, P, I, P, P]),
             "ref_scene_destroy": (None, [P]),
+            "ref_scene_extend": (I, [P, I, P, P, I, P, P, P, P]),
             "ref_scene_gpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
             "ref_scene_bsphere": (None, [P, P]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
@@ -133,6 +134,19 @@ class RefScene:
                                               _p(gn), len(im), _p(im), _p(mats), len(kinds), _p(kinds), _p(prm),
                                               len(desc.lights), _p(lights), _p(env))
         assert self.handle
+        delta, tex = list(getattr(desc, "delta_lights", [])), list(getattr(desc, "textures", []))
+        mtex = np.array([getattr(m, "texture", -1) for m in desc.materials], np.int32)
+        mbump = np.array([getattr(m, "bump", -1) for m in desc.materials], np.int32)
+        if delta or tex or (mtex >= 0).any() or (mbump >= 0).any():
+            kinds = np.array([k for k, _ in delta] or [0], np.int32)
+            lp = np.ascontiguousarray(np.array([p for _, p in delta] or [[0.0] * 12], np.float32))
+            dims = np.array([[t.shape[1], t.shape[0]] for t in tex] or [[0, 0]], np.int32)
+            px = (np.ascontiguousarray(np.concatenate([np.asarray(t, np.float32).reshape(-1) for t in tex]))
+                  if tex else np.zeros(4, np.float32))
+            self._keep2 = (kinds, lp, dims, px, mtex, mbump)
+            rc = load().ref_scene_extend(self.handle, len(delta), _p(kinds), _p(lp), len(tex), _p(dims), _p(px),
+                                         _p(mtex), _p(mbump))
+            assert rc == 0, rc
 
     def gpu_layout(self):
         """(root, nodes, instances, tris) copies of the reference adapters' output."""
