@@ -141,6 +141,7 @@ _SIGNATURES = {
     "imbart_set_trace_variant_any": (I, [I]),
     "imbart_get_trace_variant_any": (I, []),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
+    "imbart_build_mesh_node2_ex": (I, [P, I, I, P, I, I, I, C.c_float, P, I, P, P, I, P]),
     "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
     "imbart_camera_make": (I, [P, P, P, C.c_float, I, I, C.POINTER(Camera)]),
     "imbart_estimate_pixel_size": (I, [P, C.POINTER(Camera), P, P]),

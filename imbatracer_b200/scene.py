@@ -94,13 +94,19 @@ class TraversalData:
 
 
 def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_size: int = 2,
-                         masks: np.ndarray | None = None, mask_buffer: np.ndarray | None = None) -> TraversalData:
-    """Builds all bottom-level BVHs and the top-level BVH in the reference two-wide layout."""
+                         masks: np.ndarray | None = None, mask_buffer: np.ndarray | None = None,
+                         split_budget: float = 2.0) -> TraversalData:
+    """Builds all bottom-level BVHs and the top-level BVH in the reference two-wide layout.
+
+    The bottom levels use spatial splits (SBVH, as the reference's GPU adapter builds its
+    meshes with SplitBvhBuilder), allowing up to split_budget * triangles extra triangle
+    references per mesh; 0 builds object splits only."""
     lib = N.load()
     total_tris = sum(m.triangle_count for m in meshes)
-    node_cap = sum(m.triangle_count + 1 for m in meshes) + 2 * len(instances) + 1
+    total_refs = sum(int(m.triangle_count * (1.0 + split_budget)) for m in meshes)
+    node_cap = total_refs + len(meshes) + 2 * len(instances) + 1
     nodes = np.zeros(node_cap, N.NODE2_DTYPE)
-    tris = np.zeros((3 * total_tris, 4), np.float32)
+    tris = np.zeros((3 * total_refs, 4), np.float32)
     n_nodes = C.c_int(0)
     n_tv = C.c_int(0)
     layout, tri_layout = [], []
@@ -108,10 +114,10 @@ def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_siz
     for m in meshes:
         layout.append(n_nodes.value)
         tri_layout.append(tri_off)
-        rc = lib.imbart_build_mesh_node2(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices),
-                                         m.triangle_count, tri_off, leaf_size, N.ptr(nodes), node_cap,
-                                         C.byref(n_nodes), N.ptr(tris), len(tris), C.byref(n_tv))
-        N.check(rc, "imbart_build_mesh_node2")
+        rc = lib.imbart_build_mesh_node2_ex(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices),
+                                            m.triangle_count, tri_off, leaf_size, split_budget, N.ptr(nodes),
+                                            node_cap, C.byref(n_nodes), N.ptr(tris), len(tris), C.byref(n_tv))
+        N.check(rc, "imbart_build_mesh_node2_ex")
         tri_off += m.triangle_count
     node_count = n_nodes.value
     # Instance world boxes. The reference transforms the mesh box (centre +- |M| * half extent,

@@ -585,6 +585,17 @@ int imbart_build_mesh_node2(const float* vertices, int n_vertices, int vertex_st
                             imbart_node2* nodes_out, int nodes_cap, int* n_nodes,
                             imbart_vec4* tris_out, int tris_cap, int* n_tri_vec4);
 
+/* imbart_build_mesh_node2 with spatial splits (SBVH, Stich et al. 2009, as the reference's
+ * SplitBvhBuilder offers, sbvh_builder.h:29-165): where the two children of the best object
+ * split overlap, triangles may be split at a binned plane and referenced from both sides
+ * (each with its box clipped to its side). split_budget bounds the extra references as a
+ * fraction of n_tris (0: object splits only, the same tree as imbart_build_mesh_node2); the
+ * output capacities bound them too. Hits are the same as over any other tree. */
+int imbart_build_mesh_node2_ex(const float* vertices, int n_vertices, int vertex_stride,
+                               const int* indices, int n_tris, int tri_offset, int leaf_size, float split_budget,
+                               imbart_node2* nodes_out, int nodes_cap, int* n_nodes,
+                               imbart_vec4* tris_out, int tris_cap, int* n_tri_vec4);
+
 /* Builds the top-level BVH over instance boxes (binned SAH, one instance per leaf) and
  * APPENDS it in the reference two-wide layout at node index `*n_nodes` (the root is that
  * index), writing instance nodes to `inst_out` (`n_instances` of them). inv_mats are the

@@ -1,6 +1,7 @@
 """CPU tests of the traversal boundary: the oracle against brute force, the restated 8-wide
 walk against the oracle (which checks libimbart's layout conversion on the host), the
 library's exported symbols, and the builder's reference-layout output."""
+import ctypes as C
 import re
 import os
 
@@ -8,6 +9,7 @@ import numpy as np
 import pytest
 
 from imbatracer_b200 import native as N
+from imbatracer_b200 import scene as S
 from oracle import oracle as O
 from tests import helpers as H
 
@@ -68,6 +70,47 @@ def test_oracle_bvh_walk_matches_brute_force(name):
             assert np.array_equal(vb.view(np.int32), v2.view(np.int32))
 
 
+@pytest.mark.parametrize("name", ["config1", "config2"])
+def test_object_split_bvh_walk_matches_brute_force(name):
+    """Bottom levels built with object splits only (no duplicated references)."""
+    d = H.scene_desc(name)
+    td = S.build_traversal_data(d.meshes, d.instances, split_budget=0.0)
+    rays = H.ray_set(name, 1500 if name != "config2" else 600, seed=5)
+    hb, vb = O.trace_brute(d.meshes, d.instances, td.tri_layout, rays, with_v=True)
+    h2, v2 = O.trace_node2(td, rays, with_v=True)
+    assert H.hits_equal(hb, h2).all()
+    assert np.array_equal(vb.view(np.int32), v2.view(np.int32))
+
+
+def test_spatial_split_budget_bounds_references():
+    """The reference count never exceeds the budget or the output capacity; a capacity too
+    small for the triangles themselves is an error, not an overrun."""
+    lib = N.load()
+    m = H.scene_desc("config2").meshes[0]
+    n = m.triangle_count
+    for budget in (0.05, 0.5):
+        nodes = np.zeros(4 * n, N.NODE2_DTYPE)
+        tris = np.zeros((12 * n, 4), np.float32)
+        nn, nt = C.c_int(0), C.c_int(0)
+        rc = lib.imbart_build_mesh_node2_ex(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices), n, 0, 2,
+                                            C.c_float(budget), N.ptr(nodes), len(nodes), C.byref(nn), N.ptr(tris),
+                                            len(tris), C.byref(nt))
+        assert rc == 0
+        assert n <= nt.value // 3 <= int(n * (1.0 + budget))
+    cap = 3 * n + 30
+    tris = np.zeros((cap, 4), np.float32)
+    nn, nt = C.c_int(0), C.c_int(0)
+    rc = lib.imbart_build_mesh_node2_ex(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices), n, 0, 2,
+                                        C.c_float(2.0), N.ptr(nodes), len(nodes), C.byref(nn), N.ptr(tris),
+                                        cap, C.byref(nt))
+    assert rc == 0 and n <= nt.value // 3 <= n + 10
+    rc = lib.imbart_build_mesh_node2_ex(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices), n, 0, 2,
+                                        C.c_float(2.0), N.ptr(nodes), len(nodes), C.byref(nn), N.ptr(tris),
+                                        3 * n - 3, C.byref(nt))
+    assert rc != 0
+    lib.imbart_clear_error()
+
+
 @pytest.mark.parametrize("name", ["tiny", "config1", "config2"])
 def test_wide_layout_walk_matches_oracle(name):
     """The restated GPU walk over libimbart's converted 8-wide layout finds bit-identical
@@ -101,14 +144,22 @@ def test_wide_layout_invariants():
     assert 0 <= root < len(wn)
 
 
-def test_builder_writes_reference_layout():
+@pytest.mark.parametrize("split_budget", [0.0, 2.0])
+def test_builder_writes_reference_layout(split_budget):
     """Leaves end with the 0x80000000 sentinel in the last v2.w, ids sit in v1.w
-    (gpu_adapter.cpp:129-141), every triangle appears, node links are in range."""
+    (gpu_adapter.cpp:129-141), every triangle appears (exactly once without spatial splits,
+    at most 1 + split_budget references per triangle on average with them), node links are
+    in range."""
     d = H.scene_desc("config1")
-    td = H.traversal_data("config1")
+    td = S.build_traversal_data(d.meshes, d.instances, split_budget=split_budget)
     tris = td.tris
     ids = tris[1::3, 3].view(np.int32)
-    assert sorted(ids.tolist()) == list(range(d.meshes[0].triangle_count))
+    n = d.meshes[0].triangle_count
+    if split_budget == 0.0:
+        assert sorted(ids.tolist()) == list(range(n))
+    else:
+        assert np.array_equal(np.unique(ids), np.arange(n))
+        assert n < len(ids) <= int(n * (1.0 + split_budget))
     sent = tris[2::3, 3].view(np.int32)
     assert (sent == np.int32(-2 ** 31)).sum() > 0
     nodes = td.nodes
