@@ -43,6 +43,13 @@ SPP = 16
 MAX_PATH_LEN = 9        # 8 continuation bounces (path vertices incl. camera and light)
 RR_START = 3
 CPU_SAMPLE = (240, 135)  # bounded CPU sample: 1/64 of the pixels, same spp and bounces
+# DRAM bytes (read + write) per closest-hit ray inside this frame: 3,674 MB over the 78.3M
+# rays of the 18 closest-hit launches of one frame of this workload, captured with
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum
+#       --clock-control none -k regex:trace_persistent -s 36 -c 36
+#       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-serving --no-vcm
+# (1 pass per launch). roofline.traffic scales it by the rays of an average launch.
+CLOSEST_DRAM_BYTES_PER_RAY = 46.9
 
 
 def log(*a):
@@ -287,7 +294,10 @@ def run_pt(args):
                        "l2": "inputs larger than L2 (path + shadow queues ~2.5 GB per 16M paths in flight)",
                        "parallelism": f"replicas x{world} (independent frames per GPU, different seeds)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "frac": round(achieved / peak, 4),
+                         "traffic": int(CLOSEST_DRAM_BYTES_PER_RAY * work.closest_rays
+                                        / max(prof.closest_launches, 1)),
+                         "traffic_unit": "bytes per launch (ncu capture, scaled by rays per launch)",
                          "kernel": "trace_persistent (closest hit) inside the frame", "peak_source": peak_src,
                          "bytes_per_launch": int(per_launch_bytes), "launch_ms": round(per_launch_ms, 4),
                          "launches": int(prof.closest_launches),
