@@ -399,6 +399,13 @@ def serve_arm(mode, scenes, jobs, open_loop, ray_buf=None, hit_buf=None):
     ids = [srv.add_scene(d, td) for d, td in scenes]
     # Warm-up: every scene once (uploads it), so that both arms start with resident scenes.
     warm = [srv.submit_render(ids[k], scenes[k][0].camera, 64, 64, 1, SERVE_MAX_PATH_LEN, 1) for k in range(len(ids))]
+    vcm_sides = [j.width for j in jobs if isinstance(j, G.RenderJob) and j.integrator != "pt"]
+    if vcm_sides:
+        # One frame of the largest VCM-family size per VCM lane (4 in batched mode), so that
+        # every lane's buffers have their final size before the timed region.
+        side = max(vcm_sides)
+        warm += [srv.submit_vcm(ids[0], scenes[0][0].camera, side, side, "vcm", max_path_len=SERVE_MAX_PATH_LEN)
+                 for _ in range(4)]
     for t, _ in warm:
         srv.wait(t)
     s0 = srv.stats()
@@ -413,7 +420,13 @@ def serve_arm(mode, scenes, jobs, open_loop, ray_buf=None, hit_buf=None):
             delay = t_start + j.arrival_s - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-        if isinstance(j, G.RenderJob):
+        if isinstance(j, G.RenderJob) and j.integrator != "pt":
+            # BPT / VCM: spp iterations of one camera sample per pixel and width*height/2 light paths.
+            cam = scenes[j.scene][0].camera
+            t, _ = srv.submit_vcm(ids[j.scene], cam, j.width, j.height, j.integrator, iterations=j.spp,
+                                  max_path_len=SERVE_MAX_PATH_LEN, light_seed=j.seed, camera_seed=j.seed ^ 0x5BD1E995,
+                                  image=images[(j.width, j.height)])
+        elif isinstance(j, G.RenderJob):
             cam = scenes[j.scene][0].camera
             t, _ = srv.submit_render(ids[j.scene], cam, j.width, j.height, j.spp, SERVE_MAX_PATH_LEN, j.seed,
                                      image=images[(j.width, j.height)])
@@ -503,8 +516,10 @@ def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0):
            "max_path_len": SERVE_MAX_PATH_LEN, "paths_per_wavefront": SERVE_PATHS,
            "pool_bytes": SERVE_BUDGET}
     jobs4 = G.config4_requests()
-    c4 = {"workload": f"{len(jobs4)} renders at once, square, 64^2-1024^2 px log-uniform, spp in {{1,4,16,64}}, "
-                      f"path tracer (the 20% BPT / 10% VCM share of the mix is rendered with PT)"}
+    mix = {k: sum(1 for j in jobs4 if j.integrator == k) for k in ("pt", "bpt", "vcm")}
+    c4 = {"workload": f"{len(jobs4)} renders at once, square, 64^2-1024^2 px log-uniform, spp in {{1,4,16,64}}; "
+                      f"integrators {mix['pt']} PT / {mix['bpt']} BPT / {mix['vcm']} VCM (BPT and VCM: spp "
+                      f"iterations of one camera sample per pixel and width*height/2 light paths)"}
     for mode in ("plain", "batched"):
         c4[mode] = serve_arm(mode, scenes, jobs4, open_loop=False)
     c4["requests_per_s_ratio"] = round(c4["batched"]["requests_per_s"] / c4["plain"]["requests_per_s"], 3)

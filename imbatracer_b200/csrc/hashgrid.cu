@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cfloat>
 #include <mutex>
 #include <string>
@@ -235,14 +236,17 @@ int grid_for(int n) {
     return std::max(1, std::min((n + kBlock - 1) / kBlock, sms * 8));
 }
 
+// Grows geometrically: reallocation synchronizes the device, and a grid rebuilt every
+// iteration over a slowly growing photon count would otherwise reallocate every time.
 template <typename T>
 bool grow(T** p, int* cap, int need) {
     if (*cap >= need) return true;
+    const int n = (int)std::min<long long>(std::max<long long>(need, (long long)*cap * 3 / 2), INT_MAX);
     cudaFree(*p);
     *p = nullptr;
     *cap = 0;
-    if (!ok(cudaMalloc((void**)p, sizeof(T) * (size_t)std::max(need, 1)), "cudaMalloc")) return false;
-    *cap = need;
+    if (!ok(cudaMalloc((void**)p, sizeof(T) * (size_t)std::max(n, 1)), "cudaMalloc")) return false;
+    *cap = n;
     return true;
 }
 

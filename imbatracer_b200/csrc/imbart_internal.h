@@ -113,6 +113,13 @@ imbart_scene* upload_wide_scene(const HostWideScene& h, int device);
 // own record sizes (WideNode, WideTri, WideInst); the pool stays owned by the caller.
 imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes);
 void scene_pool_view_destroy(imbart_scene* s);
+// Root used by launches without a per-ray root array (single-scene work on the pool).
+void scene_pool_view_set_root(imbart_scene* s, int root);
+
+// imbart_estimate_pixel_size with the scratch buffers of a VCM context (kept between calls,
+// so that repeated estimates allocate nothing once the context has grown to the image size).
+int vcm_estimate_pixel_size(imbart_vcm* v, const imbart_scene* scene, const imbart_camera* cam, float* pixel_size,
+                            void* stream);
 
 inline int float_bits(float f) { union { float f; int i; } u; u.f = f; return u.i; }
 inline float bits_float(int i) { union { float f; int i; } u; u.i = i; return u.f; }

@@ -24,13 +24,22 @@
 //  * Completion. Finished images are copied to the caller's buffer by a completion thread on
 //    its own stream, overlapping the next wavefronts.
 //
+//  * VCM-family frames (VCM, BPT, PPM, LT, VCM-PT) keep a light-vertex cache and a photon
+//    grid per iteration, so they are not merged into the path-tracing wavefronts. Admitted
+//    ones are advanced by a few VCM lanes (threads, each with its own stream and VCM
+//    context): a lane takes the request at the head of the round robin, renders one iteration
+//    (imbart_vcm_render on the pool's copy of its scene) and puts it back. Small frames are
+//    latency-bound (one host synchronization per wavefront), so several lanes keep the GPU
+//    busy where one request alone cannot.
+//
 // The plain mode runs the same requests one at a time through imbart_pt_render /
-// imbart_trace, for comparison on the same GPU.
+// imbart_trace / imbart_vcm_render, for comparison on the same GPU.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -42,6 +51,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "hashgrid_query.cuh"
 #include "imbart_internal.h"
 #include "pt_kernels.cuh"
 
@@ -158,6 +168,12 @@ MemKind mem_kind(const void* p) {
     return MemKind::Pageable;
 }
 
+// VCM lanes of a batched server: IMBART_SERVE_VCM_LANES, default 4.
+int env_lanes() {
+    const char* e = std::getenv("IMBART_SERVE_VCM_LANES");
+    return e && *e ? std::atoi(e) : 4;
+}
+
 double now_ms(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -191,11 +207,15 @@ struct SceneRec {
 
 struct Request {
     long long ticket = 0;
-    int kind = 0;                  // 0 render, 1 ray batch
+    int kind = 0;                  // 0 render, 1 ray batch, 2 VCM-family frame
     int scene = 0;
     // render
     imbart_render_request rr{};
     long long total = 0, generated = 0;
+    // VCM-family frame
+    imbart_vcm_request vq{};
+    int iter_done = 0;
+    cudaEvent_t ready = nullptr;   // recorded on the worker stream after the scene upload and image clear
     // ray batch
     const imbart_ray* rays = nullptr;
     imbart_hit* hits = nullptr;
@@ -270,6 +290,19 @@ struct imbart_server {
     imbart_ray* stage_rays = nullptr;     // pinned
     imbart_hit* stage_hits = nullptr;     // pinned
 
+    // VCM-family frames: plain mode runs them on the worker thread with lane 0; batched mode
+    // runs them on `vcm_lanes` threads of their own, each with its own stream, VCM context and
+    // traversal view of the pool.
+    struct VcmLane {
+        cudaStream_t stream = nullptr;
+        imbart_vcm* vcm = nullptr;
+        imbart_scene* view = nullptr;
+    };
+    std::vector<VcmLane> vcm_lanes;
+    std::vector<std::thread> vcm_threads;
+    std::condition_variable cv_vcm;
+    int vcm_running = 0;                  // iterations in progress (their requests are off active_vcm)
+
     // Plain mode.
     imbart_pt_context* pt = nullptr;
     float* plain_image = nullptr;
@@ -298,10 +331,12 @@ struct imbart_server {
     std::deque<Request*> pending;
     std::vector<Request*> active_renders;
     std::deque<Request*> active_rays;
+    std::deque<Request*> active_vcm;
 
     // Completion thread.
     struct Job {
         Request* r;
+        float* dst;
         const float* src;
         size_t bytes;
     };
@@ -484,7 +519,8 @@ void admit(imbart_server* S) {
         if (rc > 1) { s.refs -= 1; S->broken = rc; return; }
         if (rc == 1) {
             s.refs -= 1;
-            const bool idle = S->active_renders.empty() && S->active_rays.empty() && S->n_cur == 0 && S->jobs.empty();
+            const bool idle = S->active_renders.empty() && S->active_rays.empty() && S->active_vcm.empty() &&
+                              S->vcm_running == 0 && S->n_cur == 0 && S->jobs.empty();
             if (idle) {
                 // Nothing left to finish or evict: the scene can never fit.
                 S->pending.pop_front();
@@ -494,13 +530,37 @@ void admit(imbart_server* S) {
             }
             break;
         }
-        if (r->kind == 0) {
+        if (r->kind == 2) {
+            const size_t bytes = (size_t)r->vq.camera.width * r->vq.camera.height * 3 * sizeof(float);
+            const size_t off = pool_alloc_locked(S, bytes, kArrayAlign);
+            if (off == SIZE_MAX) {
+                s.refs -= 1;
+                const bool idle = S->active_renders.empty() && S->active_rays.empty() && S->active_vcm.empty() &&
+                                  S->vcm_running == 0 && S->n_cur == 0 && S->jobs.empty();
+                if (idle) {
+                    S->pending.pop_front();
+                    complete_locked(S, r, IMBART_ERR_LIMIT);
+                    continue;
+                }
+                break;
+            }
+            r->img_off = off;
+            r->img_bytes = bytes;
+            if (!cuda_check(cudaMemsetAsync(S->pool + off, 0, bytes, S->stream), "cudaMemsetAsync") ||
+                !cuda_check(cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming), "cudaEventCreate") ||
+                !cuda_check(cudaEventRecord(r->ready, S->stream), "cudaEventRecord")) {
+                S->broken = IMBART_ERR_CUDA;
+                return;
+            }
+            S->active_vcm.push_back(r);
+            S->cv_vcm.notify_one();
+        } else if (r->kind == 0) {
             const size_t bytes = (size_t)r->rr.width * r->rr.height * 3 * sizeof(float);
             const size_t off = pool_alloc_locked(S, bytes, kArrayAlign);
             if (off == SIZE_MAX) {
                 s.refs -= 1;
-                const bool idle = S->active_renders.empty() && S->active_rays.empty() && S->n_cur == 0 &&
-                                  S->jobs.empty();
+                const bool idle = S->active_renders.empty() && S->active_rays.empty() && S->active_vcm.empty() &&
+                                  S->vcm_running == 0 && S->n_cur == 0 && S->jobs.empty();
                 if (idle) {
                     S->pending.pop_front();
                     complete_locked(S, r, IMBART_ERR_LIMIT);
@@ -620,6 +680,12 @@ void fail_all_active(imbart_server* S, int code) {
         complete_locked(S, r, code);
     }
     S->active_rays.clear();
+    for (Request* r : S->active_vcm) {
+        if (r->img_off != SIZE_MAX) S->alloc.release(r->img_off, r->img_bytes);
+        release_request_locked(S, r);
+        complete_locked(S, r, code);
+    }
+    S->active_vcm.clear();
     for (Request* r : S->pending) complete_locked(S, r, code);
     S->pending.clear();
     S->n_cur = 0;
@@ -749,7 +815,7 @@ bool batched_wave(imbart_server* S) {
         if (r->generated == r->total && (long long)S->h_terminated[r->slot] == r->total) {
             const float* img = reinterpret_cast<const float*>(S->pool + r->img_off);
             release_request_locked(S, r);
-            S->jobs.push_back(imbart_server::Job{r, img, r->img_bytes});
+            S->jobs.push_back(imbart_server::Job{r, r->rr.image_host, img, r->img_bytes});
             S->cv_jobs.notify_one();
             it = S->active_renders.erase(it);
         } else {
@@ -757,6 +823,92 @@ bool batched_wave(imbart_server* S) {
         }
     }
     return true;
+}
+
+// One iteration of a VCM-family request: its settings for iteration r->iter_done + 1
+// (seeds advanced by seed_step; the photon radius from the estimated pixel size when the
+// request gave none) rendered by imbart_vcm_render on `scene` / `sh` into `image`.
+int vcm_iteration(imbart_server* S, imbart_server::VcmLane& lane, Request* r, const imbart_scene* scene,
+                  const imbart_shading* sh, float* image, long long* stats) {
+    if (!lane.vcm) {
+        lane.vcm = imbart_vcm_create(S->device);
+        if (!lane.vcm) return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
+    }
+    imbart_vcm_request& q = r->vq;
+    if (!(q.settings.base_radius > 0.0f)) {
+        float pixel = 0.0f;
+        const int rc = vcm_estimate_pixel_size(lane.vcm, scene, &q.camera, &pixel, lane.stream);
+        if (rc) return rc;
+        q.settings.base_radius = pixel * q.radius_factor;
+        if (!(q.settings.base_radius > 0.0f)) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server: VCM photon radius is not positive");
+            return IMBART_ERR_INVALID_ARGUMENT;
+        }
+    }
+    imbart_vcm_settings st = q.settings;
+    const unsigned long long k = (unsigned long long)r->iter_done;
+    st.light_seed = q.settings.light_seed + k * q.seed_step;
+    st.camera_seed = q.settings.camera_seed + k * q.seed_step;
+    // Camera paths in flight: the frame's samples of one iteration, at most the server's cap.
+    const long long paths = std::min<long long>(S->cap, (long long)q.camera.width * q.camera.height * st.spp);
+    const int rc = imbart_vcm_render(lane.vcm, scene, sh, &q.camera, &st, r->iter_done + 1, image, paths, stats,
+                                     lane.stream);
+    if (!rc) r->iter_done += 1;
+    return rc;
+}
+
+// Batched mode: a VCM lane takes the admitted VCM-family request at the head of the round
+// robin, renders one iteration of it on the pool's copy of its scene, and puts it back (or
+// hands the finished image to the completion thread).
+void vcm_lane_main(imbart_server* S, int index) {
+    cudaSetDevice(S->device);
+    imbart_server::VcmLane& lane = S->vcm_lanes[index];
+    for (;;) {
+        Request* r;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_vcm.wait(lk, [&] { return S->stop || !S->active_vcm.empty(); });
+            if (S->active_vcm.empty()) return;
+            r = S->active_vcm.front();
+            S->active_vcm.pop_front();
+            S->vcm_running += 1;
+        }
+        SceneRec& s = *S->scenes[r->scene];
+        if (r->ready) {
+            // The lane's stream waits for the upload and the image clear on the worker stream.
+            cudaStreamWaitEvent(lane.stream, r->ready, 0);
+            cudaEventDestroy(r->ready);
+            r->ready = nullptr;
+        }
+        scene_pool_view_set_root(lane.view, s.root);
+        imbart_shading sh;
+        sh.device = S->device;
+        sh.s = S->h_scenes[s.slot];
+        long long stats[3] = {0, 0, 0};
+        int rc = vcm_iteration(S, lane, r, lane.view, &sh, reinterpret_cast<float*>(S->pool + r->img_off), stats);
+        if (!rc && !cuda_check(cudaStreamSynchronize(lane.stream), "cudaStreamSynchronize")) rc = IMBART_ERR_CUDA;
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->vcm_running -= 1;
+        S->stats.closest_rays += stats[0];
+        S->stats.shadow_rays += stats[1];
+        S->stats.waves += stats[2];
+        if (rc) {
+            // A failed request gives its memory back; the others go on.
+            S->alloc.release(r->img_off, r->img_bytes);
+            r->img_off = SIZE_MAX;
+            release_request_locked(S, r);
+            complete_locked(S, r, rc);
+            S->cv_work.notify_all();
+        } else if (r->iter_done < r->vq.iterations) {
+            S->active_vcm.push_back(r);
+            S->cv_vcm.notify_one();
+        } else {
+            release_request_locked(S, r);
+            S->jobs.push_back(imbart_server::Job{r, r->vq.image_host,
+                                                 reinterpret_cast<const float*>(S->pool + r->img_off), r->img_bytes});
+            S->cv_jobs.notify_one();
+        }
+    }
 }
 
 // Plain mode: one request through the single-request entry points.
@@ -776,8 +928,9 @@ int plain_request(imbart_server* S, Request* r) {
         if (!s.plain_shading) return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
         S->stats.scene_uploads += 1;
     }
-    if (r->kind == 0) {
-        const size_t bytes = (size_t)r->rr.width * r->rr.height * 3 * sizeof(float);
+    if (r->kind == 0 || r->kind == 2) {
+        const size_t bytes = r->kind == 0 ? (size_t)r->rr.width * r->rr.height * 3 * sizeof(float)
+                                          : (size_t)r->vq.camera.width * r->vq.camera.height * 3 * sizeof(float);
         if (bytes > S->plain_image_bytes) {
             cudaFree(S->plain_image);
             S->plain_image = nullptr;
@@ -787,11 +940,22 @@ int plain_request(imbart_server* S, Request* r) {
         }
         if (!cuda_check(cudaMemsetAsync(S->plain_image, 0, bytes, st), "cudaMemsetAsync")) return IMBART_ERR_CUDA;
         long long stats[3] = {0, 0, 0};
-        const int rc = imbart_pt_render(S->pt, s.plain_scene, s.plain_shading, r->rr.raster_to_world, r->rr.cam_pos,
-                                        r->rr.width, r->rr.height, r->rr.spp, r->rr.max_path_len, r->rr.rr_start,
-                                        r->rr.seed_base, S->plain_image, S->cap, stats, st);
-        if (rc) return rc;
-        if (!cuda_check(cudaMemcpyAsync(r->rr.image_host, S->plain_image, bytes, cudaMemcpyDeviceToHost, st),
+        if (r->kind == 0) {
+            const int rc = imbart_pt_render(S->pt, s.plain_scene, s.plain_shading, r->rr.raster_to_world,
+                                            r->rr.cam_pos, r->rr.width, r->rr.height, r->rr.spp, r->rr.max_path_len,
+                                            r->rr.rr_start, r->rr.seed_base, S->plain_image, S->cap, stats, st);
+            if (rc) return rc;
+        } else {
+            while (r->iter_done < r->vq.iterations) {
+                long long it[3] = {0, 0, 0};
+                const int rc = vcm_iteration(S, S->vcm_lanes[0], r, s.plain_scene, s.plain_shading, S->plain_image,
+                                             it);
+                if (rc) return rc;
+                for (int k = 0; k < 3; ++k) stats[k] += it[k];
+            }
+        }
+        float* dst = r->kind == 0 ? r->rr.image_host : r->vq.image_host;
+        if (!cuda_check(cudaMemcpyAsync(dst, S->plain_image, bytes, cudaMemcpyDeviceToHost, st),
                         "cudaMemcpyAsync") ||
             !cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize"))
             return IMBART_ERR_CUDA;
@@ -867,7 +1031,7 @@ void completer_main(imbart_server* S) {
             job = S->jobs.front();
         }
         const bool good =
-            cuda_check(cudaMemcpyAsync(job.r->rr.image_host, job.src, job.bytes, cudaMemcpyDeviceToHost,
+            cuda_check(cudaMemcpyAsync(job.dst, job.src, job.bytes, cudaMemcpyDeviceToHost,
                                        S->copy_stream), "cudaMemcpyAsync") &&
             cuda_check(cudaStreamSynchronize(S->copy_stream), "cudaStreamSynchronize");
         std::lock_guard<std::mutex> lk(S->mu);
@@ -887,6 +1051,11 @@ void free_server(imbart_server* S) {
     }
     if (S->pool_scene) scene_pool_view_destroy(S->pool_scene);
     if (S->pt) imbart_pt_destroy(S->pt);
+    for (auto& lane : S->vcm_lanes) {
+        if (lane.vcm) imbart_vcm_destroy(lane.vcm);
+        if (lane.view) scene_pool_view_destroy(lane.view);
+        if (lane.stream && lane.stream != S->stream) cudaStreamDestroy(lane.stream);
+    }
     void* dev[] = {S->pool, S->d_reqs, S->d_scenes, S->d_terminated, S->d_chunks, S->d_runs, S->d_counts,
                    S->hits, S->srays, S->shits, S->spixel, S->scontrib, S->sreq, S->sroot, S->b_rays, S->b_hits,
                    S->b_roots, S->plain_image, S->plain_rays, S->plain_hits};
@@ -926,6 +1095,8 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
     if (good && mode == IMBART_SERVE_PLAIN) {
         S->pt = imbart_pt_create(device);
         good = S->pt != nullptr;
+        S->vcm_lanes.resize(1);
+        S->vcm_lanes[0].stream = S->stream;
     } else if (good) {
         const long long budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (4ll << 30);
         S->pool_bytes = std::min<size_t>(align_up((size_t)budget, kBlockAlign), kMaxPoolBytes);
@@ -948,6 +1119,12 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
             S->pool_scene = scene_pool_view(device, S->pool, S->pool_bytes);
             good = S->pool_scene != nullptr;
         }
+        S->vcm_lanes.resize(std::max(1, std::min(env_lanes(), 16)));
+        for (auto& lane : S->vcm_lanes) {
+            if (!good) break;
+            good = cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate") &&
+                   (lane.view = scene_pool_view(device, S->pool, S->pool_bytes)) != nullptr;
+        }
         S->alloc.reset(S->pool_bytes);
         for (int i = kMaxReqSlots - 1; i >= 0; --i) S->free_req_slots.push_back(i);
         for (int i = kMaxSceneSlots - 1; i >= 0; --i) S->free_scene_slots.push_back(i);
@@ -960,6 +1137,8 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
     S->stats.pool_bytes = (long long)S->pool_bytes;
     S->worker = std::thread(worker_main, S);
     S->completer = std::thread(completer_main, S);
+    if (mode == IMBART_SERVE_BATCHED)
+        for (int k = 0; k < (int)S->vcm_lanes.size(); ++k) S->vcm_threads.emplace_back(vcm_lane_main, S, k);
     cudaSetDevice(prev);
     return S;
 }
@@ -973,8 +1152,10 @@ void imbart_server_destroy(imbart_server* S) {
     }
     S->cv_work.notify_all();
     S->cv_jobs.notify_all();
+    S->cv_vcm.notify_all();
     S->worker.join();
     S->completer.join();
+    for (auto& t : S->vcm_threads) t.join();
     int prev = 0;
     cudaGetDevice(&prev);
     free_server(S);
@@ -1109,6 +1290,29 @@ long long imbart_server_submit_rays(imbart_server* S, int scene, const imbart_ra
     r->rays_kind = mem_kind(rays);
     r->hits_kind = mem_kind(hits);
     cudaSetDevice(prev);
+    return submit(S, std::move(r));
+}
+
+long long imbart_server_submit_vcm(imbart_server* S, const imbart_vcm_request* q) {
+    if (!S || !q || !q->image_host || q->camera.width <= 0 || q->camera.height <= 0 || q->iterations <= 0 ||
+        (long long)q->camera.width * q->camera.height > 2147483647ll / 3) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_submit_vcm: invalid argument");
+        return -IMBART_ERR_INVALID_ARGUMENT;
+    }
+    // The settings are checked as imbart_vcm_begin_iteration checks them, with a positive
+    // radius (given, or radius_factor > 0 for the estimate).
+    imbart_vcm_settings st = q->settings;
+    if (!(st.base_radius > 0.0f)) st.base_radius = q->radius_factor > 0.0f ? 1.0f : 0.0f;
+    if (st.algorithm < IMBART_VCM || st.algorithm > IMBART_VCM_PT || st.spp <= 0 || st.max_path_len < 1 ||
+        st.light_path_count <= 0 || st.num_connections < 0 || st.num_knn < 1 || st.num_knn > kGridMaxK ||
+        st.light_tile_size < 0 || !(st.base_radius > 0.0f)) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_submit_vcm: invalid settings");
+        return -IMBART_ERR_INVALID_ARGUMENT;
+    }
+    auto r = std::make_unique<Request>();
+    r->kind = 2;
+    r->scene = q->scene;
+    r->vq = *q;
     return submit(S, std::move(r));
 }
 

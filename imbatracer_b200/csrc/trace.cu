@@ -462,6 +462,8 @@ imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes) {
 
 void scene_pool_view_destroy(imbart_scene* s) { free_scene(s); }
 
+void scene_pool_view_set_root(imbart_scene* s, int root) { s->info.root = root; }
+
 }  // namespace imbart
 
 using namespace imbart;

@@ -845,7 +845,26 @@ bool realloc_exact(T** ptr, size_t elems) {
 }  // namespace
 }  // namespace imbart
 
+namespace imbart {
+namespace {
+// Scratch of the pixel-size estimate: camera, probe rays and hits, per-query distances.
+struct PixelProbe {
+    float* cam = nullptr;
+    float4* rays = nullptr;
+    int4* hits = nullptr;
+    float4* dist = nullptr;
+    long long cap = 0;
+    std::vector<float4> host;
+    void release() {
+        cudaFree(cam); cudaFree(rays); cudaFree(hits); cudaFree(dist);
+        cam = nullptr; rays = nullptr; hits = nullptr; dist = nullptr; cap = 0;
+    }
+};
+}  // namespace
+}  // namespace imbart
+
 struct imbart_vcm {
+    imbart::PixelProbe probe;
     int device = 0;
     // light-path slots
     long long l_cap = 0;
@@ -900,6 +919,7 @@ void free_vcm(imbart_vcm* v) {
     }
     cudaFreeHost(v->host_counts);
     if (v->grid) imbart_hashgrid_destroy(v->grid);
+    v->probe.release();
 }
 
 bool valid_settings(const imbart_vcm_settings* st) {
@@ -910,6 +930,7 @@ bool valid_settings(const imbart_vcm_settings* st) {
 
 bool ensure_shadow(imbart_vcm* v, long long need) {
     if (v->s_cap >= need) return true;
+    need = std::max(need, v->s_cap * 3 / 2);   // geometric growth: reallocation synchronizes the device
     const bool good = realloc_exact(&v->s_rays, 2 * (size_t)need) && realloc_exact(&v->s_hits, (size_t)need) &&
                       realloc_exact(&v->s_pixel, (size_t)need) && realloc_exact(&v->s_contrib, (size_t)need);
     v->s_cap = good ? need : 0;
@@ -989,7 +1010,66 @@ int build_grid(imbart_vcm* v, const imbart_vcm_settings* st, cudaStream_t s) {
     return rc;
 }
 
+// Integrator::estimate_pixel_size (integrator.cpp:14-70) with caller-owned scratch buffers.
+int estimate_pixel_size(const imbart_scene* scene, const imbart_camera* cam, float* pixel_size, cudaStream_t s,
+                        PixelProbe& pb) {
+    if (!scene || !cam || !pixel_size || cam->width <= 0 || cam->height <= 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_estimate_pixel_size: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    const int nx = (cam->width + 7) / 8, ny = (cam->height + 7) / 8, nq = nx * ny;
+    bool good = true;
+    if (!pb.cam) good = ok(cudaMalloc((void**)&pb.cam, sizeof(float) * 19), "cudaMalloc");
+    if (good && pb.cap < nq) {
+        const long long c = std::max<long long>(nq, pb.cap * 3 / 2);
+        good = realloc_exact(&pb.rays, 8 * (size_t)c) && realloc_exact(&pb.hits, 4 * (size_t)c) &&
+               realloc_exact(&pb.dist, (size_t)c);
+        pb.cap = good ? c : 0;
+    }
+    pb.host.resize(nq);
+    float hcam[19];
+    std::memcpy(hcam, cam->raster_to_world, sizeof(float) * 16);
+    std::memcpy(hcam + 16, cam->pos, sizeof(float) * 3);
+    good = good && ok(cudaMemcpyAsync(pb.cam, hcam, sizeof(hcam), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+    if (good) {
+        pixel_probe_rays_kernel<<<(nq + 127) / 128, 128, 0, s>>>(pb.cam, pb.cam + 16, nx, ny, pb.rays);
+        note_launches(1);
+        good = launch_trace_internal(scene, pb.rays, pb.hits, nullptr, 4 * nq, IMBART_TRACE_CLOSEST, s, nullptr) == 0;
+    }
+    if (good) {
+        pixel_probe_dist_kernel<<<(nq + 127) / 128, 128, 0, s>>>(pb.rays, pb.hits, nq, pb.dist);
+        note_launches(1);
+        good = ok(cudaMemcpyAsync(pb.host.data(), pb.dist, sizeof(float4) * (size_t)nq, cudaMemcpyDeviceToHost, s),
+                  "cudaMemcpyAsync") &&
+               ok(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    }
+    if (!good) return IMBART_ERR_CUDA;
+    // The reference's reduction, in its order (one serial range, integrator.cpp:37-59).
+    float total = 0.0f;
+    int count = 0;
+    for (int q = 0; q < nq; ++q) {
+        if (pb.host[q].x < 0.0f) continue;
+        total += pb.host[q].x;
+        total += pb.host[q].y;
+        total += pb.host[q].z;
+        total += pb.host[q].w;
+        count += 4;
+    }
+    *pixel_size = count == 0 ? 1.0f : total / count;
+    return 0;
+}
+
 }  // namespace
+
+int vcm_estimate_pixel_size(imbart_vcm* v, const imbart_scene* scene, const imbart_camera* cam, float* pixel_size,
+                            void* stream) {
+    if (!v) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_estimate_pixel_size: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    return estimate_pixel_size(scene, cam, pixel_size, (cudaStream_t)stream, v->probe);
+}
+
 }  // namespace imbart
 
 using namespace imbart;
@@ -1067,11 +1147,13 @@ int imbart_vcm_light_pass(imbart_vcm* v, const imbart_scene* scene, const imbart
     const int n_blocks = (P + kScanTile - 1) / kScanTile;
     bool good = true;
     if (v->l_cap < P) {
-        good = realloc_exact(&v->l_rays, 2 * (size_t)P) && realloc_exact(&v->l_hits, (size_t)P) &&
-               realloc_exact(&v->l_rng, (size_t)P) && realloc_exact(&v->l_thr, (size_t)P) &&
-               realloc_exact(&v->l_w, (size_t)P) && realloc_exact(&v->stage, 7 * (size_t)P) &&
-               realloc_exact(&v->vflags, (size_t)P) && realloc_exact(&v->bsums, (size_t)n_blocks + 1);
-        v->l_cap = good ? P : 0;
+        const long long c = std::max<long long>(P, v->l_cap * 3 / 2);
+        const long long cb = (c + kScanTile - 1) / kScanTile;
+        good = realloc_exact(&v->l_rays, 2 * (size_t)c) && realloc_exact(&v->l_hits, (size_t)c) &&
+               realloc_exact(&v->l_rng, (size_t)c) && realloc_exact(&v->l_thr, (size_t)c) &&
+               realloc_exact(&v->l_w, (size_t)c) && realloc_exact(&v->stage, 7 * (size_t)c) &&
+               realloc_exact(&v->vflags, (size_t)c) && realloc_exact(&v->bsums, (size_t)cb + 1);
+        v->l_cap = good ? c : 0;
     }
     if (good && v->tiles_cap < (long long)tiles.size()) {
         good = realloc_exact(&v->d_tiles, tiles.size());
@@ -1206,13 +1288,13 @@ int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbar
     chunk = std::min(chunk, 0x7fffffffll / per);          // shadow rays of a wavefront fit an int
     bool good = true;
     if (v->c_cap < chunk) {
+        const long long c = std::max(chunk, v->c_cap * 3 / 2);
         for (int k = 0; k < 2 && good; ++k)
-            good = realloc_exact(&v->c_rays[k], 2 * (size_t)chunk) && realloc_exact(&v->c_pixel[k], (size_t)chunk) &&
-                   realloc_exact(&v->c_rng[k], (size_t)chunk) && realloc_exact(&v->c_thr[k], (size_t)chunk) &&
-                   realloc_exact(&v->c_w[k], (size_t)chunk);
-        good = good && realloc_exact(&v->c_hits, (size_t)chunk) &&
-               realloc_exact(&v->c_merge, (size_t)kMergeRec * chunk);
-        v->c_cap = good ? chunk : 0;
+            good = realloc_exact(&v->c_rays[k], 2 * (size_t)c) && realloc_exact(&v->c_pixel[k], (size_t)c) &&
+                   realloc_exact(&v->c_rng[k], (size_t)c) && realloc_exact(&v->c_thr[k], (size_t)c) &&
+                   realloc_exact(&v->c_w[k], (size_t)c);
+        good = good && realloc_exact(&v->c_hits, (size_t)c) && realloc_exact(&v->c_merge, (size_t)kMergeRec * c);
+        v->c_cap = good ? c : 0;
     }
     good = good && ensure_shadow(v, chunk * per);
     if (!good) { cudaSetDevice(prev); return IMBART_ERR_OUT_OF_MEMORY; }
@@ -1282,52 +1364,10 @@ int imbart_vcm_render(imbart_vcm* v, const imbart_scene* scene, const imbart_sha
 }
 
 int imbart_estimate_pixel_size(const imbart_scene* scene, const imbart_camera* cam, float* pixel_size, void* stream) {
-    if (!scene || !cam || !pixel_size || cam->width <= 0 || cam->height <= 0) {
-        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_estimate_pixel_size: invalid argument");
-        return IMBART_ERR_INVALID_ARGUMENT;
-    }
-    cudaStream_t s = (cudaStream_t)stream;
-    const int nx = (cam->width + 7) / 8, ny = (cam->height + 7) / 8, nq = nx * ny;
-    float* d_cam = nullptr;
-    float4* rays = nullptr;
-    int4* hits = nullptr;
-    float4* dist = nullptr;
-    bool good = ok(cudaMalloc((void**)&d_cam, sizeof(float) * 19), "cudaMalloc") &&
-                ok(cudaMalloc((void**)&rays, sizeof(float4) * 8 * (size_t)nq), "cudaMalloc") &&
-                ok(cudaMalloc((void**)&hits, sizeof(int4) * 4 * (size_t)nq), "cudaMalloc") &&
-                ok(cudaMalloc((void**)&dist, sizeof(float4) * (size_t)nq), "cudaMalloc");
-    std::vector<float4> host(nq);
-    float hcam[19];
-    std::memcpy(hcam, cam->raster_to_world, sizeof(float) * 16);
-    std::memcpy(hcam + 16, cam->pos, sizeof(float) * 3);
-    good = good && ok(cudaMemcpyAsync(d_cam, hcam, sizeof(hcam), cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
-    if (good) {
-        pixel_probe_rays_kernel<<<(nq + 127) / 128, 128, 0, s>>>(d_cam, d_cam + 16, nx, ny, rays);
-        note_launches(1);
-        good = launch_trace_internal(scene, rays, hits, nullptr, 4 * nq, IMBART_TRACE_CLOSEST, s, nullptr) == 0;
-    }
-    if (good) {
-        pixel_probe_dist_kernel<<<(nq + 127) / 128, 128, 0, s>>>(rays, hits, nq, dist);
-        note_launches(1);
-        good = ok(cudaMemcpyAsync(host.data(), dist, sizeof(float4) * (size_t)nq, cudaMemcpyDeviceToHost, s),
-                  "cudaMemcpyAsync") &&
-               ok(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    }
-    cudaFree(d_cam); cudaFree(rays); cudaFree(hits); cudaFree(dist);
-    if (!good) return IMBART_ERR_CUDA;
-    // The reference's reduction, in its order (one serial range, integrator.cpp:37-59).
-    float total = 0.0f;
-    int count = 0;
-    for (int q = 0; q < nq; ++q) {
-        if (host[q].x < 0.0f) continue;
-        total += host[q].x;
-        total += host[q].y;
-        total += host[q].z;
-        total += host[q].w;
-        count += 4;
-    }
-    *pixel_size = count == 0 ? 1.0f : total / count;
-    return 0;
+    PixelProbe probe;
+    const int rc = estimate_pixel_size(scene, cam, pixel_size, (cudaStream_t)stream, probe);
+    probe.release();
+    return rc;
 }
 
 }  // extern "C"

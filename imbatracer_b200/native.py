@@ -71,6 +71,11 @@ class SceneSource(C.Structure):
                 ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int)]
 
 
+class VcmRequest(C.Structure):
+    _fields_ = [("scene", C.c_int), ("camera", Camera), ("settings", VcmSettings), ("radius_factor", C.c_float),
+                ("iterations", C.c_int), ("seed_step", C.c_ulonglong), ("image_host", C.c_void_p)]
+
+
 class RenderRequest(C.Structure):
     _fields_ = [("scene", C.c_int), ("raster_to_world", C.c_float * 16), ("cam_pos", C.c_float * 3),
                 ("width", C.c_int), ("height", C.c_int), ("spp", C.c_int), ("max_path_len", C.c_int),
@@ -159,6 +164,7 @@ _SIGNATURES = {
     "imbart_server_add_scene": (I, [P, C.POINTER(SceneSource)]),
     "imbart_server_submit_render": (C.c_longlong, [P, C.POINTER(RenderRequest)]),
     "imbart_server_submit_rays": (C.c_longlong, [P, I, P, P, I, I]),
+    "imbart_server_submit_vcm": (C.c_longlong, [P, C.POINTER(VcmRequest)]),
     "imbart_server_wait": (I, [P, C.c_longlong, C.POINTER(RequestResult)]),
     "imbart_server_drain": (I, [P]),
     "imbart_server_get_stats": (I, [P, C.POINTER(ServerStats)]),

@@ -307,9 +307,10 @@ class RenderJob:
     scene: int
     width: int
     height: int
-    spp: int
+    spp: int          # samples per pixel (PT) or iterations (BPT, VCM: one camera sample each)
     seed: int
     arrival_s: float = 0.0
+    integrator: str = "pt"
 
 
 @dataclass
@@ -322,14 +323,18 @@ class RayJob:
 
 
 def config4_requests(seed: int = 1, n: int = 256, n_scenes: int = 12, min_side: int = 64,
-                     max_side: int = 1024) -> list[RenderJob]:
-    """All requests arrive at once (a closed batch)."""
+                     max_side: int = 1024, mix: tuple = (("pt", 0.7), ("bpt", 0.2), ("vcm", 0.1))) -> list[RenderJob]:
+    """All requests arrive at once (a closed batch): square frames with log-uniform sides,
+    spp (or iterations) in {1, 4, 16, 64}, integrators drawn from `mix`."""
     rng = np.random.default_rng(seed)
+    pick = np.random.default_rng(seed + 1000)
+    names, probs = [m[0] for m in mix], np.array([m[1] for m in mix], np.float64)
     jobs = []
     for i in range(n):
         side = int(round(np.exp(rng.uniform(np.log(min_side), np.log(max_side)))))
         jobs.append(RenderJob(int(rng.integers(n_scenes)), side, side, int(rng.choice([1, 4, 16, 64])),
-                              int(rng.integers(1, 2 ** 31))))
+                              int(rng.integers(1, 2 ** 31)),
+                              integrator=names[int(pick.choice(len(names), p=probs / probs.sum()))]))
     return jobs
 
 

@@ -19,7 +19,7 @@ import numpy as np
 from . import native as N
 from . import scene as S
 from . import scenegen as G
-from .integrators import ShadingData, camera_matrix
+from .integrators import ShadingData, camera_matrix, make_camera
 
 MODES = {"batched": N.SERVE_BATCHED, "plain": N.SERVE_PLAIN}
 
@@ -75,6 +75,43 @@ class Server:
         t = self.lib.imbart_server_submit_render(self.h, C.byref(q))
         if t < 0:
             raise N.ImbartError("imbart_server_submit_render: " + N.last_error()[1])
+        with self._lock:
+            self._keep[t] = image
+        return t, image
+
+    def submit_vcm(self, scene: int, cam: G.Camera, width: int, height: int, algorithm: str = "vcm",
+                   iterations: int = 1, max_path_len: int = 8, light_path_count: int | None = None,
+                   num_connections: int = 1, num_knn: int = 10, radius_factor: float = 2.0,
+                   base_radius: float = 0.0, light_seed: int = 1, camera_seed: int = 2, seed_step: int = 1,
+                   light_seed_step: int = 0x9E3779B9, light_tile_size: int = 0, image: np.ndarray | None = None):
+        """A VCM-family frame ("vcm", "bpt", "ppm", "lt", "pt"): `iterations` iterations into
+        one accumulated (height, width, 3) float32 host image. Returns (ticket, image).
+        base_radius 0 takes radius_factor times the camera's estimated pixel size."""
+        if image is None:
+            image = np.zeros((height, width, 3), np.float32)
+        assert image.dtype == np.float32 and image.flags.c_contiguous and image.size == width * height * 3
+        q = N.VcmRequest()
+        q.scene = scene
+        q.camera = make_camera(cam, width, height)
+        st = q.settings
+        st.algorithm = N.VCM_ALGORITHMS[algorithm]
+        st.spp = 1
+        st.max_path_len = max_path_len
+        st.light_path_count = light_path_count or (width * height // 2)
+        st.num_connections = num_connections
+        st.num_knn = num_knn
+        st.light_tile_size = light_tile_size
+        st.base_radius = base_radius
+        st.light_seed = light_seed & (2 ** 64 - 1)
+        st.light_seed_step = light_seed_step & (2 ** 64 - 1)
+        st.camera_seed = camera_seed & (2 ** 64 - 1)
+        q.radius_factor = radius_factor
+        q.iterations = iterations
+        q.seed_step = seed_step & (2 ** 64 - 1)
+        q.image_host = N.ptr(image)
+        t = self.lib.imbart_server_submit_vcm(self.h, C.byref(q))
+        if t < 0:
+            raise N.ImbartError("imbart_server_submit_vcm: " + N.last_error()[1])
         with self._lock:
             self._keep[t] = image
         return t, image

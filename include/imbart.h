@@ -528,12 +528,33 @@ typedef struct {
     float* image_host;
 } imbart_render_request;
 
+/* One VCM-family frame (VCM, BPT, PPM, LT, VCM-PT; VCMIntegrator::render, vcm.cpp:25-55, once
+ * per iteration) into a fresh zeroed image: iterations 1 .. `iterations` of imbart_vcm_render,
+ * so the photon radius shrinks as over one long render. Iteration i draws its light tiles
+ * from settings.light_seed + (i - 1) * seed_step and its camera samples from
+ * settings.camera_seed + (i - 1) * seed_step. settings.base_radius <= 0 selects
+ * radius_factor times imbart_estimate_pixel_size of the camera (the reference's default:
+ * radius factor 2). image_host: HOST width*height*3 floats, the sum over the iterations.
+ * In batched mode the request is admitted like a render (scene resident, image in the
+ * pool); its iterations then run on VCM lanes (host threads with their own CUDA streams and
+ * VCM contexts; IMBART_SERVE_VCM_LANES, default 4), one iteration at a time and round robin
+ * over the admitted VCM-family requests, concurrently with the merged wavefronts. */
+typedef struct {
+    int scene;
+    imbart_camera camera;
+    imbart_vcm_settings settings;
+    float radius_factor;
+    int iterations;
+    unsigned long long seed_step;
+    float* image_host;
+} imbart_vcm_request;
+
 /* Completion record. Times are milliseconds of the host steady clock since the server was
  * created: submission, admission (scene resident, memory granted) and completion (result in
  * the caller's buffer). */
 typedef struct {
     int status;          /* 0 or an IMBART_ERR_* code */
-    int kind;            /* 0 render, 1 ray batch */
+    int kind;            /* 0 render, 1 ray batch, 2 VCM-family frame */
     double submit_ms, start_ms, done_ms;
 } imbart_request_result;
 
@@ -557,6 +578,7 @@ void imbart_server_destroy(imbart_server* server);
 int imbart_server_add_scene(imbart_server* server, const imbart_scene_source* source);
 /* Submits a request; returns a ticket (> 0) or -(error code). */
 long long imbart_server_submit_render(imbart_server* server, const imbart_render_request* request);
+long long imbart_server_submit_vcm(imbart_server* server, const imbart_vcm_request* request);
 /* rays / hits: HOST (pageable or pinned) or DEVICE pointers of `count` records; flags
  * IMBART_TRACE_CLOSEST or IMBART_TRACE_ANY. */
 long long imbart_server_submit_rays(imbart_server* server, int scene, const imbart_ray* rays, imbart_hit* hits,

@@ -1,4 +1,5 @@
-"""The request server (imbart_server_*): merged wavefronts over several resident scenes.
+"""The request server (imbart_server_*): merged wavefronts over several resident scenes,
+VCM-family frames between them.
 
 A render served in a mix of other requests must give the image the single-request path
 (imbart_pt_render) gives alone: paths are seeded per sample and shaded by the same code, so
@@ -138,6 +139,79 @@ def test_ray_batches_bit_exact(cuda, scenes, where):
             assert H.hits_equal(got, want).all()
         else:
             assert np.array_equal(got["tri_id"] >= 0, want["tri_id"] >= 0)
+    srv.close()
+
+
+VCM_REQS = [  # (scene index, algorithm, width, height, iterations, max_path_len, light seed, camera seed)
+    (0, "vcm", 40, 32, 2, 5, 101, 201),
+    (1, "bpt", 32, 24, 2, 5, 102, 202),
+    (2, "ppm", 24, 24, 3, 5, 103, 203),
+    (0, "lt", 48, 32, 2, 4, 104, 204),
+    (1, "pt", 16, 12, 2, 4, 105, 205),
+]
+SEED_STEP = 7
+TILE_STEP = 0x9E3779B9
+
+
+def vcm_alone(d, td, algo, w, h, iters, ml, ls, cs):
+    """The same frame through VcmIntegrator alone: iteration i seeded ls / cs + (i - 1) * 7."""
+    from imbatracer_b200.integrators import GpuScene, VcmIntegrator
+    gs = GpuScene(d, td=td)
+    vi = VcmIntegrator(gs, algo, w, h, max_path_len=ml)
+    img = None
+    for i in range(iters):
+        img = vi.render(i + 1, ls + i * SEED_STEP, cs + i * SEED_STEP, TILE_STEP, image=img)
+    out = img.cpu().numpy()
+    vi.close()
+    gs.close()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_vcm_family_requests_in_a_mix(cuda, scenes, mode):
+    """VCM, BPT, PPM, LT and VCM-PT frames served between merged path-tracing wavefronts
+    give the images of VcmIntegrator alone, and the renders beside them are unchanged."""
+    from imbatracer_b200.serving import Server
+    srv = Server(mode=mode, hbm_budget=256 << 20, max_paths=20000)
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    vt, rt = [], []
+    for k, (si, algo, w, h, it, ml, ls, cs) in enumerate(VCM_REQS):
+        d = scenes[si][0]
+        vt.append(srv.submit_vcm(ids[si], d.camera, w, h, algo, iterations=it, max_path_len=ml, light_seed=ls,
+                                 camera_seed=cs, seed_step=SEED_STEP, light_seed_step=TILE_STEP))
+        si2, w2, h2, spp, ml2, seed, rr = REQS[k]
+        rt.append(srv.submit_render(ids[si2], scenes[si2][0].camera, w2, h2, spp, ml2, seed, rr_start=rr))
+    for (t, img), (si, algo, w, h, it, ml, ls, cs) in zip(vt, VCM_REQS):
+        res = srv.wait(t)
+        assert res["status"] == 0 and res["kind"] == 2
+        d, td = scenes[si]
+        ref = vcm_alone(d, td, algo, w, h, it, ml, ls, cs)
+        assert ref.sum() > 0
+        assert rel_rmse(img, ref) <= MIX_TOL, (algo, rel_rmse(img, ref))
+    for (t, img), (si, w, h, spp, ml, seed, rr) in zip(rt, REQS):
+        assert srv.wait(t)["status"] == 0
+        d, td = scenes[si]
+        assert rel_rmse(img, plain_image(d, td, w, h, spp, ml, seed, rr)) <= MIX_TOL
+    st = srv.stats()
+    assert st["completed"] == len(VCM_REQS) + len(REQS) and st["failed"] == 0
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_vcm_request_validation(cuda, scenes):
+    from imbatracer_b200.serving import Server
+    srv = Server(hbm_budget=64 << 20, max_paths=4096)
+    sid = srv.add_scene(*scenes[0])
+    d = scenes[0][0]
+    with pytest.raises(N.ImbartError):
+        srv.submit_vcm(sid, d.camera, 8, 8, "vcm", iterations=0)
+    with pytest.raises(N.ImbartError):
+        srv.submit_vcm(sid, d.camera, 8, 8, "vcm", num_knn=65)
+    with pytest.raises(N.ImbartError):
+        srv.submit_vcm(sid, d.camera, 8, 8, "vcm", radius_factor=0.0)
+    t, img = srv.submit_vcm(sid, d.camera, 8, 8, "bpt", base_radius=0.05)
+    assert srv.wait(t)["status"] == 0 and img.sum() > 0
     srv.close()
 
 
