@@ -20,7 +20,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
 SOURCES_CU = ["trace.cu", "hashgrid.cu", "wavefront.cu", "server.cu", "vcm.cu"]
-SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp"]
+SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp", "accel_file.cpp"]
 # Shading and sample generation mirror the reference's separately rounded single-precision
 # arithmetic: no fused multiply-add in device code, no contraction in the host camera set-up.
 # (The traversal kernels spell out their rounding with intrinsics and keep FMA elsewhere.)

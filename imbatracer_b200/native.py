@@ -57,6 +57,8 @@ class VcmSettings(C.Structure):
 
 
 VCM, BPT, PPM, LT, VCM_PT = 0, 1, 2, 3, 4
+ACCEL_GPU, ACCEL_CPU = 1, 2   # block types of the acceleration cache files
+
 VCM_ALGORITHMS = {"vcm": VCM, "bpt": BPT, "ppm": PPM, "lt": LT, "pt": VCM_PT}
 
 
@@ -147,6 +149,11 @@ _SIGNATURES = {
     "imbart_get_trace_variant_any": (I, []),
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_mesh_node2_ex": (I, [P, I, I, P, I, I, I, C.c_float, P, I, P, P, I, P]),
+    "imbart_accel_file_info": (I, [C.c_char_p, I, P, P]),
+    "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),
+    "imbart_load_accel_node4": (I, [C.c_char_p, I, P, I, P, P, I, P]),
+    "imbart_store_accel_node2": (I, [C.c_char_p, P, I, I, P, I, I, I]),
+    "imbart_store_accel_node4": (I, [C.c_char_p, P, I, I, P, I, I, I]),
     "imbart_build_top_node2": (I, [P, P, P, I, P, I, P, P]),
     "imbart_camera_make": (I, [P, P, P, C.c_float, I, I, C.POINTER(Camera)]),
     "imbart_estimate_pixel_size": (I, [P, C.POINTER(Camera), P, P]),

@@ -10,6 +10,7 @@ libimbart into the compressed 8-wide layout resident on the GPU.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -93,31 +94,59 @@ class TraversalData:
         self.tri_layout = tri_layout
 
 
+def accel_file_counts(path: str, block_type: int = N.ACCEL_GPU) -> tuple[int, int] | None:
+    """(nodes, Vec4s) of the file's block of `block_type`, or None when it has none or does
+    not exist; raises on a malformed file."""
+    if not path or not os.path.exists(path):
+        return None
+    nn, nv = C.c_int(0), C.c_int(0)
+    rc = N.load().imbart_accel_file_info(os.fsencode(path), block_type, C.byref(nn), C.byref(nv))
+    if rc == -1:
+        return None
+    N.check(rc, "imbart_accel_file_info")
+    return nn.value, nv.value
+
+
 def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_size: int = 2,
                          masks: np.ndarray | None = None, mask_buffer: np.ndarray | None = None,
-                         split_budget: float = 2.0) -> TraversalData:
+                         split_budget: float = 2.0, accel_files: list[str | None] | None = None) -> TraversalData:
     """Builds all bottom-level BVHs and the top-level BVH in the reference two-wide layout.
 
     The bottom levels use spatial splits (SBVH, as the reference's GPU adapter builds its
     meshes with SplitBvhBuilder), allowing up to split_budget * triangles extra triangle
-    references per mesh; 0 builds object splits only."""
+    references per mesh; 0 builds object splits only. accel_files[i] (optional) is mesh i's
+    acceleration cache file, as Scene::build_mesh_accels uses them (scene.cpp:51-68): the
+    mesh's BVH is loaded from it when it has a two-wide block, else built and appended to it."""
     lib = N.load()
-    total_tris = sum(m.triangle_count for m in meshes)
-    total_refs = sum(int(m.triangle_count * (1.0 + split_budget)) for m in meshes)
-    node_cap = total_refs + len(meshes) + 2 * len(instances) + 1
+    files = list(accel_files) if accel_files is not None else [None] * len(meshes)
+    assert len(files) == len(meshes)
+    cached = [accel_file_counts(f) for f in files]
+    node_need = [c[0] if c else int(m.triangle_count * (1.0 + split_budget)) + 1 for m, c in zip(meshes, cached)]
+    vec4_need = [c[1] if c else 3 * int(m.triangle_count * (1.0 + split_budget)) for m, c in zip(meshes, cached)]
+    node_cap = sum(node_need) + 2 * len(instances) + 1
     nodes = np.zeros(node_cap, N.NODE2_DTYPE)
-    tris = np.zeros((3 * total_refs, 4), np.float32)
+    tris = np.zeros((sum(vec4_need), 4), np.float32)
     n_nodes = C.c_int(0)
     n_tv = C.c_int(0)
     layout, tri_layout = [], []
     tri_off = 0
-    for m in meshes:
+    for m, path, c in zip(meshes, files, cached):
         layout.append(n_nodes.value)
         tri_layout.append(tri_off)
+        if c is not None:
+            N.check(lib.imbart_load_accel_node2(os.fsencode(path), tri_off, N.ptr(nodes), node_cap, C.byref(n_nodes),
+                                                N.ptr(tris), len(tris), C.byref(n_tv)), "imbart_load_accel_node2")
+            tri_off += m.triangle_count
+            continue
+        tris_first = n_tv.value
         rc = lib.imbart_build_mesh_node2_ex(N.ptr(m.vertices), len(m.vertices), 3, N.ptr(m.indices),
                                             m.triangle_count, tri_off, leaf_size, split_budget, N.ptr(nodes),
                                             node_cap, C.byref(n_nodes), N.ptr(tris), len(tris), C.byref(n_tv))
         N.check(rc, "imbart_build_mesh_node2_ex")
+        if path:
+            N.check(lib.imbart_store_accel_node2(os.fsencode(path), N.ptr(nodes), layout[-1], n_nodes.value,
+                                                 N.ptr(tris), tris_first, n_tv.value, tri_off),
+                    "imbart_store_accel_node2")
         tri_off += m.triangle_count
     node_count = n_nodes.value
     # Instance world boxes. The reference transforms the mesh box (centre +- |M| * half extent,

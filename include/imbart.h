@@ -627,6 +627,48 @@ int imbart_build_top_node2(const float* boxes, const float* inv_mats, const int*
                            int n_instances, imbart_node2* nodes_out, int nodes_cap, int* n_nodes,
                            imbart_instance_node* inst_out);
 
+/* ------------------------------------------------------------------------------------ */
+/* Acceleration-structure cache files (.bvh), as the reference reads and writes them      */
+/* (load_accel_gpu / load_accel_cpu / store_accel_gpu / store_accel_cpu,                   */
+/* src/imbatracer/loaders/load_bvh.cpp:44-304; used by Scene::build_mesh_accels,          */
+/* scene.cpp:37-70)                                                                       */
+/* ------------------------------------------------------------------------------------ */
+
+/* File: u32 magic 0x313F1A57, then blocks [u64 size][u32 type][u32 node_count][u32
+ * prim_count][nodes][prim_count Vec4s], size counting the bytes after the size field.
+ * Block type 1 holds two-wide GPU nodes (imbart_node2), type 2 four-wide CPU nodes
+ * (imbart_node4); a file holds at most one of each. Every size is checked: a malformed or
+ * truncated file returns IMBART_ERR_BAD_SCENE. */
+#define IMBART_ACCEL_GPU 1
+#define IMBART_ACCEL_CPU 2
+
+/* Node and Vec4 counts of the block of `block_type`. Returns 0, -1 when the file is valid
+ * but has no such block, or an error code. */
+int imbart_accel_file_info(const char* path, int block_type, int* node_count, int* vec4_count);
+
+/* Appends the file's two-wide block at nodes_out[*n_nodes] / tris_out[*n_tri_vec4] (both
+ * in/out counts, as the builders), rebasing node and leaf links when other nodes precede it
+ * and adding tri_id_offset to the triangle ids (v1.w), as load_accel_gpu does. The
+ * single-leaf wrapper's 0x76543210 marker is kept as it is (the reference shifts it with
+ * the node offset). The result goes to imbart_scene_from_node2 like a built BVH. */
+int imbart_load_accel_node2(const char* path, int tri_id_offset, imbart_node2* nodes_out, int nodes_cap,
+                            int* n_nodes, imbart_vec4* tris_out, int tris_cap, int* n_tri_vec4);
+
+/* The four-wide block (load_accel_cpu): ids are the last Vec4 of each 13-Vec4 packet. */
+int imbart_load_accel_node4(const char* path, int tri_id_offset, imbart_node4* nodes_out, int nodes_cap,
+                            int* n_nodes, imbart_vec4* tris_out, int tris_cap, int* n_vec4);
+
+/* Appends the mesh BVH nodes[node_offset, n_nodes) / tris[tris_offset, n_tri_vec4) to the
+ * file as a block with links relative to the mesh and ids minus tri_id_offset
+ * (store_accel_gpu); creates the file when it does not exist, refuses
+ * (IMBART_ERR_INVALID_ARGUMENT) when it has a two-wide block already. */
+int imbart_store_accel_node2(const char* path, const imbart_node2* nodes, int node_offset, int n_nodes,
+                             const imbart_vec4* tris, int tris_offset, int n_tri_vec4, int tri_id_offset);
+
+/* The four-wide block (store_accel_cpu). */
+int imbart_store_accel_node4(const char* path, const imbart_node4* nodes, int node_offset, int n_nodes,
+                             const imbart_vec4* tris, int tris_offset, int n_vec4, int tri_id_offset);
+
 #ifdef __cplusplus
 }
 #endif

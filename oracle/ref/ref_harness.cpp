@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "imbatracer/render/scene.h"
@@ -107,8 +108,14 @@ private:
     const TextureSampler* diff_sampler_;
 };
 
+// Options of the next ref_scene_create: the CPU (four-wide) layout too, and acceleration
+// cache file names per mesh (empty: none), as Scene::build_mesh_accels takes them.
+bool g_next_cpu_buffers = false;
+std::vector<std::string> g_next_accel_files;
+
 struct RefScene {
-    Scene scene{false, true};
+    RefScene() : scene(g_next_cpu_buffers, true) {}
+    Scene scene;
     MaskBuffer masks;
     std::vector<int> mat_kind;
     std::vector<float> mat_params;
@@ -288,6 +295,9 @@ void* ref_scene_create(int n_meshes, const int* mesh_nverts, const int* mesh_ntr
         io += 4 * (size_t)mesh_ntris[m];
     }
     std::vector<std::string> names(n_meshes, "");
+    if ((int)g_next_accel_files.size() == n_meshes) names = g_next_accel_files;
+    g_next_accel_files.clear();
+    g_next_cpu_buffers = false;
     scene.build_mesh_accels(names);
     scene.build_top_level_accel();
     scene.compute_bounding_sphere();
@@ -404,6 +414,61 @@ int ref_scene_gpu_layout(void* h, int* root, const void** nodes, const void** in
     sizes[1] = td.instances.size();
     sizes[2] = td.tris.size();
     return 0;
+}
+
+// The four-wide CPU layout (scenes created after ref_set_next_scene_options(1, ...)).
+int ref_scene_cpu_layout(void* h, int* root, const void** nodes, const void** insts, const void** tris,
+                         int64_t* sizes) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    if (!rs->scene.has_cpu_buffers()) return -1;
+    const auto& td = rs->scene.traversal_data_cpu();
+    *root = td.root;
+    *nodes = td.nodes.data();
+    *insts = td.instances.data();
+    *tris = td.tris.data();
+    sizes[0] = td.nodes.size();
+    sizes[1] = td.instances.size();
+    sizes[2] = td.tris.size();
+    return 0;
+}
+
+void ref_set_next_scene_options(int cpu_buffers, int n_files, const char* const* files) {
+    g_next_cpu_buffers = cpu_buffers != 0;
+    g_next_accel_files.clear();
+    for (int i = 0; i < n_files; ++i) g_next_accel_files.emplace_back(files[i] ? files[i] : "");
+}
+
+// The reference's load_accel_gpu / store_accel_gpu (load_bvh.cpp) on arrays: `pre` nodes and
+// Vec4s stand for other meshes already in the arrays.
+int ref_load_accel(int cpu, const char* path, int tri_id_offset, const void* pre_nodes, int n_pre_nodes,
+                   const float* pre_tris, int n_pre_tris, void* nodes_out, int nodes_cap, int* n_nodes,
+                   float* tris_out, int tris_cap, int* n_tris) {
+    auto run = [&](auto* node_tag, auto load) -> int {
+        using Node = std::remove_pointer_t<decltype(node_tag)>;
+        std::vector<Node> nodes((const Node*)pre_nodes, (const Node*)pre_nodes + n_pre_nodes);
+        std::vector<Vec4> tris((const Vec4*)pre_tris, (const Vec4*)pre_tris + n_pre_tris);
+        if (!load(path, nodes, tris, tri_id_offset)) return 1;
+        if ((int)nodes.size() > nodes_cap || (int)tris.size() > tris_cap) return 2;
+        std::memcpy(nodes_out, nodes.data(), sizeof(Node) * nodes.size());
+        std::memcpy(tris_out, tris.data(), sizeof(Vec4) * tris.size());
+        *n_nodes = (int)nodes.size();
+        *n_tris = (int)tris.size();
+        return 0;
+    };
+    if (cpu) return run((traversal_cpu::Node*)nullptr, imba::load_accel_cpu);
+    return run((traversal_gpu::Node*)nullptr, imba::load_accel_gpu);
+}
+
+int ref_store_accel(int cpu, const char* path, const void* nodes, int node_offset, int n_nodes, const float* tris,
+                    int tris_offset, int n_tris, int tri_id_offset) {
+    auto run = [&](auto* node_tag, auto store) -> int {
+        using Node = std::remove_pointer_t<decltype(node_tag)>;
+        std::vector<Node> nv((const Node*)nodes, (const Node*)nodes + n_nodes);
+        std::vector<Vec4> tv((const Vec4*)tris, (const Vec4*)tris + n_tris);
+        return store(path, nv, node_offset, tv, tris_offset, tri_id_offset) ? 0 : 1;
+    };
+    if (cpu) return run((traversal_cpu::Node*)nullptr, imba::store_accel_cpu);
+    return run((traversal_gpu::Node*)nullptr, imba::store_accel_gpu);
 }
 
 void ref_scene_bsphere(void* h, float* out4) {

@@ -36,6 +36,10 @@ def load() -> C.CDLL:
             "ref_scene_extend": (I, [P, I, P, P, I, P, P, P, P]),
             "ref_scene_gpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
             "ref_scene_bsphere": (None, [P, P]),
+            "ref_scene_cpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
+            "ref_set_next_scene_options": (None, [I, I, P]),
+            "ref_load_accel": (I, [I, C.c_char_p, I, P, I, P, I, P, I, P, P, I, P]),
+            "ref_store_accel": (I, [I, C.c_char_p, P, I, I, P, I, I, I]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
             "ref_render_pt_threads": (I, [P, I, I, P, P, P, F, I, I, U64, I, I, P, P]),
             "ref_vcm_create": (P, [P, I, I, I, P, P, P, F, I, I, I, I, I, F, I, U64]),
@@ -108,12 +112,47 @@ def material_arrays(materials):
     return kinds, prm
 
 
+def load_accel(path, tri_id_offset, pre_nodes, pre_tris, cpu=False):
+    """The reference's load_accel_gpu / _cpu appending to copies of pre_nodes / pre_tris;
+    None when it returns false."""
+    from imbatracer_b200.native import NODE2_DTYPE, NODE4_DTYPE
+    dt = NODE4_DTYPE if cpu else NODE2_DTYPE
+    pre_nodes = np.ascontiguousarray(pre_nodes, dtype=dt)
+    pre_tris = np.ascontiguousarray(pre_tris, dtype=np.float32).reshape(-1, 4)
+    cap_n, cap_t = len(pre_nodes) + (1 << 22), len(pre_tris) + (1 << 24)
+    nodes = np.zeros(cap_n, dt)
+    tris = np.zeros((cap_t, 4), np.float32)
+    nn, nt = C.c_int(0), C.c_int(0)
+    rc = load().ref_load_accel(1 if cpu else 0, os.fsencode(path), tri_id_offset, _p(pre_nodes), len(pre_nodes),
+                               _p(pre_tris), len(pre_tris), _p(nodes), cap_n, C.byref(nn), _p(tris), cap_t,
+                               C.byref(nt))
+    if rc != 0:
+        return None
+    return nodes[: nn.value].copy(), tris[: nt.value].copy()
+
+
+def store_accel(path, nodes, node_offset, tris, tris_offset, tri_id_offset, cpu=False) -> bool:
+    """The reference's store_accel_gpu / _cpu."""
+    from imbatracer_b200.native import NODE2_DTYPE, NODE4_DTYPE
+    nodes = np.ascontiguousarray(nodes, dtype=NODE4_DTYPE if cpu else NODE2_DTYPE)
+    tris = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 4)
+    return load().ref_store_accel(1 if cpu else 0, os.fsencode(path), _p(nodes), node_offset, len(nodes), _p(tris),
+                                  tris_offset, len(tris), tri_id_offset) == 0
+
+
 class RefScene:
     """The reference's Scene built from a SceneDesc with the reference's adapters (SBVH
-    bottom level, binned top level) into its GPU two-wide layout."""
+    bottom level, binned top level) into its GPU two-wide layout (and its CPU four-wide
+    layout with cpu_buffers). accel_files: per-mesh acceleration cache files, loaded or
+    written by the reference's Scene::build_mesh_accels."""
 
-    def __init__(self, desc):
+    def __init__(self, desc, cpu_buffers: bool = False, accel_files=None):
         self.desc = desc
+        names = None
+        if accel_files is not None:
+            enc = [os.fsencode(f) if f else None for f in accel_files]
+            names = (C.c_char_p * len(enc))(*enc)
+        load().ref_set_next_scene_options(1 if cpu_buffers else 0, len(accel_files or []), names)
         meshes = desc.meshes
         nv = np.array([len(m.vertices) for m in meshes], np.int32)
         nt = np.array([m.triangle_count for m in meshes], np.int32)
@@ -165,6 +204,22 @@ class RefScene:
         insts = grab(pi.value, sizes[1], INST_DTYPE)
         tris = grab(pt.value, sizes[2], np.dtype((np.float32, 4)))
         return root.value, nodes, insts, tris
+
+    def cpu_layout(self):
+        """(root, nodes, instances, tris) of the reference CPU adapters (cpu_buffers=True)."""
+        from imbatracer_b200.native import INST_DTYPE, NODE4_DTYPE
+        root = C.c_int(0)
+        pn, pi, pt = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        sizes = np.zeros(3, np.int64)
+        assert load().ref_scene_cpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt),
+                                           _p(sizes)) == 0
+
+        def grab(ptr, n, dtype):
+            buf = (C.c_char * (int(n) * dtype.itemsize)).from_address(ptr)
+            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+
+        return (root.value, grab(pn.value, sizes[0], NODE4_DTYPE), grab(pi.value, sizes[1], INST_DTYPE),
+                grab(pt.value, sizes[2], np.dtype((np.float32, 4))))
 
     def render_pt(self, w, h, spp, max_path_len, seed_base, cam=None):
         cam = cam or self.desc.camera
