@@ -53,14 +53,17 @@ class ShadingData:
             prm[i, 13] = getattr(m, "bump", -1)
         self.mat_params = prm
         n_tri, delta = len(desc.lights), list(getattr(desc, "delta_lights", []))
-        lights = np.zeros((max(n_tri + len(delta), 1), 12), np.float32)
-        for i, (p0, p1, p2, e) in enumerate(desc.lights):
-            lights[i] = np.concatenate([p0, p1, p2, e])
-        for i, (kind, prm12) in enumerate(delta):
-            lights[n_tri + i] = np.asarray(prm12, np.float32)
+        rows = [(0, np.concatenate([p0, p1, p2, e]).astype(np.float32)) for p0, p1, p2, e in desc.lights]
+        drows = [(k, np.asarray(prm12, np.float32)) for k, prm12 in delta]
+        # Light order = the reference's light list: delta lights first for scenes read from
+        # files (parse order), after the triangle lights otherwise.
+        rows = drows + rows if getattr(desc, "delta_first", False) else rows + drows
+        lights = np.zeros((max(len(rows), 1), 12), np.float32)
+        for i, (_, r) in enumerate(rows):
+            lights[i] = r
         self.lights = lights
-        self.n_lights = n_tri + len(delta)
-        self.light_kinds = np.array([0] * n_tri + [k for k, _ in delta] + [0], np.int32)[:max(self.n_lights, 1)]
+        self.n_lights = len(rows)
+        self.light_kinds = np.array([k for k, _ in rows] or [0], np.int32)
         tex = list(getattr(desc, "textures", []))
         self.n_textures = len(tex)
         self.tex_dims = np.array([[t.shape[1], t.shape[0]] for t in tex] or [[0, 0]], np.int32).reshape(-1)
@@ -103,7 +106,9 @@ class GpuScene:
     def __init__(self, desc: G.SceneDesc, device: int = 0, td: S.TraversalData | None = None):
         self.desc = desc
         self.device = device
-        self.td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances)
+        self.td = td if td is not None else S.build_traversal_data(
+            desc.meshes, desc.instances, masks=getattr(desc, "masks", None),
+            mask_buffer=getattr(desc, "mask_buffer", None), accel_files=getattr(desc, "accel_files", None))
         self.trace_scene = S.DeviceScene(self.td, device)
         sd = ShadingData(desc)
         self.sd = sd

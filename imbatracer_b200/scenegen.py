@@ -74,6 +74,10 @@ class SceneDesc:
     # SPOT (position, axis, half-angle in radians + 2 unused, intensity).
     delta_lights: list = field(default_factory=list)
     textures: list = field(default_factory=list)     # (height, width, 4) float32 rgba, texel (x, y) at [y, x]
+    delta_first: bool = False        # list the delta lights before the triangle lights
+    masks: np.ndarray | None = None  # opacity masks per material (MASK_DTYPE), None: all opaque
+    mask_buffer: np.ndarray | None = None
+    accel_files: list | None = None  # per-mesh acceleration cache files
 
     @property
     def instanced_triangles(self) -> int:

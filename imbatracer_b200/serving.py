@@ -36,7 +36,11 @@ class Server:
         self._lock = threading.Lock()
 
     def add_scene(self, desc: G.SceneDesc, td: S.TraversalData | None = None) -> int:
-        td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances)
+        masks = getattr(desc, "masks", None)
+        if masks is not None and (np.asarray(masks["width"]) * np.asarray(masks["height"]) > 1).any():
+            raise N.ImbartError("imbart_server_add_scene: opacity masks are not supported by the server")
+        td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances,
+                                                              accel_files=getattr(desc, "accel_files", None))
         sd = ShadingData(desc)
         src = N.SceneSource()
         src.root = td.root

@@ -24,8 +24,13 @@ REF_SOURCES = [
     "src/imbatracer/render/integrators/pt.cpp",
     "src/imbatracer/render/integrators/vcm.cpp",
     "src/imbatracer/render/integrators/light_vertices.cpp",
+    "src/imbatracer/frontend/build_scene.cpp",
+    "src/imbatracer/loaders/load_obj.cpp",
+    "src/imbatracer/loaders/load_tga.cpp",
+    "src/imbatracer/loaders/load_hdr.cpp",
 ]
-OWN_SOURCES = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_vcm.cpp")]
+OWN_SOURCES = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_vcm.cpp"),
+               os.path.join(HERE, "ref_scene_io.cpp")]
 ORACLE_C = [os.path.join(ORACLE, "traversal.c")]
 
 FLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-w"]

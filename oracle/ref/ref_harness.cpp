@@ -76,13 +76,6 @@ extern "C" void occluded_cpu_masked_instanced(int, traversal_cpu::Node*, travers
     for (int i = 0; i < count; ++i) hits[i].tri_id = -1;
 }
 
-// Loaders the reference's Scene links against; the harness never uses accel cache files.
-namespace imba {
-bool load_png(const Path&, Image&) { return false; }
-bool load_tga(const Path&, Image&) { return false; }
-bool load_hdr(const Path&, Image&) { return false; }
-}  // namespace imba
-
 using namespace imba;
 
 namespace {
@@ -126,6 +119,9 @@ float3 f3(const float* p) { return float3(p[0], p[1], p[2]); }
 }  // namespace
 
 imba::Scene* ref_scene_of(void* h) { return &static_cast<RefScene*>(h)->scene; }
+
+// An empty scene (GPU layout only) for the scene-file loader harness (ref_scene_io.cpp).
+void* ref_scene_new_empty() { return new RefScene; }
 
 extern "C" {
 

@@ -38,6 +38,14 @@ def load() -> C.CDLL:
             "ref_scene_bsphere": (None, [P, P]),
             "ref_scene_cpu_layout": (I, [P, C.POINTER(I), C.POINTER(P), C.POINTER(P), C.POINTER(P), P]),
             "ref_set_next_scene_options": (None, [I, I, P]),
+            "ref_scene_load": (P, [C.c_char_p, P]),
+            "ref_scene_counts": (None, [P, P]),
+            "ref_scene_meshes": (None, [P, P, P, P, P, P, P]),
+            "ref_scene_instances": (None, [P, P, P]),
+            "ref_scene_materials": (I, [P, P, P]),
+            "ref_scene_lights": (I, [P, P, P]),
+            "ref_scene_textures": (None, [P, P, P]),
+            "ref_scene_masks": (None, [P, P, P]),
             "ref_load_accel": (I, [I, C.c_char_p, I, P, I, P, I, P, I, P, P, I, P]),
             "ref_store_accel": (I, [I, C.c_char_p, P, I, I, P, I, I, I]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
@@ -204,6 +212,50 @@ class RefScene:
         insts = grab(pi.value, sizes[1], INST_DTYPE)
         tris = grab(pt.value, sizes[2], np.dtype((np.float32, 4)))
         return root.value, nodes, insts, tris
+
+    @classmethod
+    def from_file(cls, path, width=512, height=512, fov=60.0):
+        """A scene built by the reference's own frontend (build_scene.cpp) from a .scene file."""
+        from types import SimpleNamespace
+
+        from imbatracer_b200 import scenegen as G
+        self = cls.__new__(cls)
+        cam9 = np.zeros(9, np.float32)
+        self.handle = load().ref_scene_load(os.fsencode(path), _p(cam9))
+        if not self.handle:
+            raise RuntimeError(f"the reference could not load {path}")
+        cam = G.Camera(tuple(map(float, cam9[0:3])), tuple(map(float, cam9[3:6])), tuple(map(float, cam9[6:9])),
+                       fov, width, height)
+        self.desc = SimpleNamespace(camera=cam)
+        return self
+
+    def export(self) -> dict:
+        """The arrays of the reference's scene (ref_scene_io.cpp): meshes, instances,
+        materials, lights, textures, masks."""
+        cnt = np.zeros(10, np.int64)
+        lib = load()
+        lib.ref_scene_counts(self.handle, _p(cnt))
+        n_mesh, nv, nt, ni, nm, nl, ntex, texels, nmask, nbuf = (int(c) for c in cnt)
+        out = {"mesh_counts": np.zeros((n_mesh, 2), np.int32), "vertices": np.zeros((nv, 3), np.float32),
+               "normals": np.zeros((nv, 3), np.float32), "texcoords": np.zeros((nv, 2), np.float32),
+               "indices": np.zeros((nt, 4), np.int32), "geom_normals": np.zeros((nt, 3), np.float32),
+               "inst_mesh": np.zeros(ni, np.int32), "inst_mats": np.zeros((ni, 4, 4), np.float32),
+               "mat_kind": np.zeros(nm, np.int32), "mat_params": np.zeros((nm, 16), np.float32),
+               "light_kind": np.zeros(nl, np.int32), "light_params": np.zeros((nl, 12), np.float32),
+               "tex_dims": np.zeros((max(ntex, 1), 2), np.int32), "texels": np.zeros((max(texels, 1), 4), np.float32),
+               "masks": np.zeros((max(nmask, 1), 3), np.int32), "mask_buffer": np.zeros(max(nbuf, 1), np.uint8)}
+        lib.ref_scene_meshes(self.handle, _p(out["mesh_counts"]), _p(out["vertices"]), _p(out["normals"]),
+                             _p(out["texcoords"]), _p(out["indices"]), _p(out["geom_normals"]))
+        lib.ref_scene_instances(self.handle, _p(out["inst_mesh"]), _p(out["inst_mats"]))
+        assert lib.ref_scene_materials(self.handle, _p(out["mat_kind"]), _p(out["mat_params"])) == 0
+        assert lib.ref_scene_lights(self.handle, _p(out["light_kind"]), _p(out["light_params"])) == 0
+        lib.ref_scene_textures(self.handle, _p(out["tex_dims"]), _p(out["texels"]))
+        lib.ref_scene_masks(self.handle, _p(out["masks"]), _p(out["mask_buffer"]))
+        out["tex_dims"] = out["tex_dims"][:ntex]
+        out["texels"] = out["texels"][:texels]
+        out["masks"] = out["masks"][:nmask]
+        out["mask_buffer"] = out["mask_buffer"][:nbuf]
+        return out
 
     def cpu_layout(self):
         """(root, nodes, instances, tris) of the reference CPU adapters (cpu_buffers=True)."""
