@@ -116,6 +116,11 @@ void scene_pool_view_destroy(imbart_scene* s);
 // Root used by launches without a per-ray root array (single-scene work on the pool).
 void scene_pool_view_set_root(imbart_scene* s, int root);
 
+// A scene over device arrays built on the GPU; the scene takes ownership (cudaFree on
+// destroy). NULL on error (the arrays are then still the caller's).
+imbart_scene* scene_adopt_device_arrays(int device, WideNode* nodes, int64_t n_nodes, int64_t top_nodes,
+                                        WideTri* tris, int64_t n_tris, WideInst* insts, int64_t n_insts, int root);
+
 // imbart_estimate_pixel_size with the scratch buffers of a VCM context (kept between calls,
 // so that repeated estimates allocate nothing once the context has grown to the image size).
 int vcm_estimate_pixel_size(imbart_vcm* v, const imbart_scene* scene, const imbart_camera* cam, float* pixel_size,

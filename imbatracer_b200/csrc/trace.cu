@@ -464,6 +464,31 @@ void scene_pool_view_destroy(imbart_scene* s) { free_scene(s); }
 
 void scene_pool_view_set_root(imbart_scene* s, int root) { s->info.root = root; }
 
+imbart_scene* scene_adopt_device_arrays(int device, WideNode* nodes, int64_t n_nodes, int64_t top_nodes,
+                                        WideTri* tris, int64_t n_tris, WideInst* insts, int64_t n_insts, int root) {
+    imbart_scene* s = new imbart_scene;
+    s->device = device;
+    s->nodes = nodes;
+    s->tris = tris;
+    s->insts = insts;
+    s->owns_arrays = false;
+    if (!cuda_ok(cudaMalloc((void**)&s->error_flags, 4 * sizeof(int)), "cudaMalloc") ||
+        !cuda_ok(cudaMemset(s->error_flags, 0, 4 * sizeof(int)), "cudaMemset")) {
+        free_scene(s);
+        return nullptr;
+    }
+    s->owns_arrays = true;
+    s->info.wide_nodes = n_nodes;
+    s->info.top_nodes = top_nodes;
+    s->info.triangles = n_tris;
+    s->info.instances = n_insts;
+    s->info.device_bytes = n_nodes * (int64_t)sizeof(WideNode) + n_tris * (int64_t)sizeof(WideTri) +
+                           n_insts * (int64_t)sizeof(WideInst);
+    s->info.root = root;
+    s->info.masked = 0;
+    return s;
+}
+
 }  // namespace imbart
 
 using namespace imbart;

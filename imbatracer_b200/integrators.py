@@ -103,13 +103,22 @@ def bounding_sphere(desc) -> np.ndarray:
 class GpuScene:
     """A SceneDesc resident on one GPU: traversal scene + shading data."""
 
-    def __init__(self, desc: G.SceneDesc, device: int = 0, td: S.TraversalData | None = None):
+    def __init__(self, desc: G.SceneDesc, device: int = 0, td: S.TraversalData | None = None,
+                 gpu_build: bool = False):
+        """gpu_build: build the BVHs on the GPU (imbart_scene_build_gpu; unmasked scenes)
+        instead of the host SBVH builder and layout conversion."""
         self.desc = desc
         self.device = device
-        self.td = td if td is not None else S.build_traversal_data(
-            desc.meshes, desc.instances, masks=getattr(desc, "masks", None),
-            mask_buffer=getattr(desc, "mask_buffer", None), accel_files=getattr(desc, "accel_files", None))
-        self.trace_scene = S.DeviceScene(self.td, device)
+        if gpu_build:
+            if getattr(desc, "masks", None) is not None and (desc.masks["width"] * desc.masks["height"] > 1).any():
+                raise N.ImbartError("GpuScene: the GPU builder does not take opacity masks")
+            self.td = None
+            self.trace_scene = S.DeviceScene.build_gpu(desc.meshes, desc.instances, device)
+        else:
+            self.td = td if td is not None else S.build_traversal_data(
+                desc.meshes, desc.instances, masks=getattr(desc, "masks", None),
+                mask_buffer=getattr(desc, "mask_buffer", None), accel_files=getattr(desc, "accel_files", None))
+            self.trace_scene = S.DeviceScene(self.td, device)
         sd = ShadingData(desc)
         self.sd = sd
         lib = N.load()

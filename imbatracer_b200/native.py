@@ -73,6 +73,16 @@ class SceneSource(C.Structure):
                 ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int)]
 
 
+class MeshDesc(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("n_vertices", C.c_int), ("indices", C.c_void_p), ("n_tris", C.c_int),
+                ("tri_offset", C.c_int)]
+
+
+class InstanceDesc(C.Structure):
+    _fields_ = [("obj_to_world", C.c_float * 12), ("world_to_obj", C.c_float * 12), ("mesh", C.c_int),
+                ("id", C.c_int)]
+
+
 class VcmRequest(C.Structure):
     _fields_ = [("scene", C.c_int), ("camera", Camera), ("settings", VcmSettings), ("radius_factor", C.c_float),
                 ("iterations", C.c_int), ("seed_step", C.c_ulonglong), ("image_host", C.c_void_p)]
@@ -150,6 +160,7 @@ _SIGNATURES = {
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_mesh_node2_ex": (I, [P, I, I, P, I, I, I, C.c_float, P, I, P, P, I, P]),
     "imbart_accel_file_info": (I, [C.c_char_p, I, P, P]),
+    "imbart_scene_build_gpu": (P, [C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, I, P, C.POINTER(C.c_float)]),
     "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),
     "imbart_load_accel_node4": (I, [C.c_char_p, I, P, I, P, P, I, P]),
     "imbart_store_accel_node2": (I, [C.c_char_p, P, I, I, P, I, I, I]),

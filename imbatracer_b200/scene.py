@@ -195,6 +195,42 @@ def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_siz
 class DeviceScene:
     """A prepared scene resident on one GPU (imbart_scene)."""
 
+    @classmethod
+    def build_gpu(cls, meshes: list[Mesh], instances: list[Instance], device: int = 0, stream=None) -> "DeviceScene":
+        """The scene built on the GPU (imbart_scene_build_gpu) from its meshes and instances;
+        triangle ids are numbered mesh after mesh as build_traversal_data numbers them.
+        `build_ms` holds the build's wall time."""
+        lib = N.load()
+        md = (N.MeshDesc * len(meshes))()
+        keep, off = [], 0
+        for k, m in enumerate(meshes):
+            v = np.ascontiguousarray(m.vertices, np.float32)
+            ix = np.ascontiguousarray(m.indices, np.int32)
+            keep += [v, ix]
+            md[k].vertices, md[k].n_vertices = N.ptr(v), len(v)
+            md[k].indices, md[k].n_tris = N.ptr(ix), len(ix)
+            md[k].tri_offset = off
+            off += m.triangle_count
+        idesc = (N.InstanceDesc * len(instances))()
+        for i, inst in enumerate(instances):
+            idesc[i].obj_to_world[:] = [float(x) for x in inst.mat[:3].reshape(-1)]
+            idesc[i].world_to_obj[:] = [float(x) for x in inst.inv_mat.reshape(-1)]
+            idesc[i].mesh = inst.mesh_id
+            idesc[i].id = i
+        ms = C.c_float(0.0)
+        st = None if stream is None else stream.cuda_stream
+        h = lib.imbart_scene_build_gpu(md, len(meshes), idesc, len(instances), device, st, C.byref(ms))
+        if not h:
+            code, msg = N.last_error()
+            raise N.ImbartError(f"imbart_scene_build_gpu failed ({code}): {msg}")
+        self = cls.__new__(cls)
+        self.handle, self.device, self.td = h, device, None
+        info = N.SceneInfo()
+        N.check(lib.imbart_scene_get_info(h, C.byref(info)), "imbart_scene_get_info")
+        self.info = info
+        self.build_ms = ms.value
+        return self
+
     def __init__(self, td: TraversalData, device: int = 0):
         lib = N.load()
         h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),

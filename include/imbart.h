@@ -628,6 +628,37 @@ int imbart_build_top_node2(const float* boxes, const float* inv_mats, const int*
                            imbart_instance_node* inst_out);
 
 /* ------------------------------------------------------------------------------------ */
+/* GPU scene build (no counterpart in the reference, which builds on the CPU with SBVH)    */
+/* ------------------------------------------------------------------------------------ */
+
+/* A triangle mesh: HOST arrays of n_vertices xyz floats and n_tris {v0, v1, v2, material}
+ * ints; tri_offset is the global id of its first triangle (hits report tri_offset + local
+ * index, as Scene::build_mesh_accels numbers triangles, scene.cpp:75-97). */
+typedef struct {
+    const float* vertices; int n_vertices;
+    const int* indices; int n_tris;
+    int tri_offset;
+} imbart_mesh_desc;
+
+/* An instance: row-major 3x4 object-to-world and world-to-object matrices, the mesh it
+ * instances and the id its hits report. */
+typedef struct {
+    float obj_to_world[12];
+    float world_to_obj[12];
+    int mesh;
+    int id;
+} imbart_instance_desc;
+
+/* Builds a scene entirely on the GPU (PLOC clustering over Morton-sorted primitives, a
+ * surface-area leaf pass, a collapse into the compressed 8-wide layout) and returns it ready
+ * for imbart_trace and the renderers, like imbart_scene_from_node2 (unmasked). One BVH per
+ * mesh, a top-level BVH over the instances. Synchronizes `stream`; build_ms (may be NULL)
+ * receives the wall time. NULL on error (imbart_last_error). */
+imbart_scene* imbart_scene_build_gpu(const imbart_mesh_desc* meshes, int n_meshes,
+                                     const imbart_instance_desc* instances, int n_instances, int device,
+                                     void* stream, float* build_ms);
+
+/* ------------------------------------------------------------------------------------ */
 /* Acceleration-structure cache files (.bvh), as the reference reads and writes them      */
 /* (load_accel_gpu / load_accel_cpu / store_accel_gpu / store_accel_cpu,                   */
 /* src/imbatracer/loaders/load_bvh.cpp:44-304; used by Scene::build_mesh_accels,          */
