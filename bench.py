@@ -162,6 +162,20 @@ def reference_cpu(desc, steps, threads, w, h, seed=7):
     return tot_rays / tot_s / 1e6, tot_rays // max(steps, 1), tot_s / max(steps, 1)
 
 
+def job_totals(ms: float, units: float, device, world: int) -> tuple[float, float]:
+    """Whole-job figures of a multi-rank timing: the slowest rank's device time (max over
+    ranks) and the units all ranks processed (sum); the rank's own values when world == 1."""
+    if world <= 1:
+        return float(ms), float(units)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, float(units)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(t[1])
+
+
 def run_pt(args):
     import torch
     import torch.distributed as dist
@@ -213,14 +227,7 @@ def run_pt(args):
     clk = clocks.stop()
     launches = lib.imbart_kernel_launch_count() - launches0
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms, float(rays)], dtype=torch.float64, device=dev)
-    if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms_max, all_rays = float(tmax[0]), float(t[1])
-    else:
-        ms_max, all_rays = ms, float(rays)
+    ms_max, all_rays = job_totals(ms, rays, dev, world)
 
     # e2e through the public API: render + image copied to pinned host memory per frame.
     host_img = torch.empty((H, W, 3), dtype=torch.float32).pin_memory()
@@ -238,15 +245,7 @@ def run_pt(args):
         host_img.copy_(image, non_blocking=True)
     q1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = q0.elapsed_time(q1)
-    te = torch.tensor([e2e_ms, float(e2e_rays)], dtype=torch.float64, device=dev)
-    if world > 1:
-        temax = te.clone()
-        dist.all_reduce(temax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(te, op=dist.ReduceOp.SUM)
-        e2e_ms, e2e_all = float(temax[0]), float(te[1])
-    else:
-        e2e_all = float(e2e_rays)
+    e2e_ms, e2e_all = job_totals(q0.elapsed_time(q1), e2e_rays, dev, world)
 
     # Roofline of the dominant kernel (closest-hit traversal): one frame with every traversal
     # launch timed by CUDA events on the launching stream, one frame with the statistics

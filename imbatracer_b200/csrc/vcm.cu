@@ -123,18 +123,21 @@ __device__ __forceinline__ bool vcm_bounce(const VcmParams& p, Rng& rng, V3& thr
 // The light-sample function of trace_light_paths (vcm.cpp:64-101) for LightRayGen sample i of
 // a tile: RNG seeded as in ray_gen.h:128-141 (the tile-local index scrambles the seed and
 // sets the discard).
-__global__ void light_gen_kernel(VcmParams p, const LightTile* tiles, int n_tiles, int n, float4* rays,
+// Light paths first + j for the n slots j (a rank of a multi-GPU iteration traces a range of
+// the iteration's paths; every path is seeded by its global index).
+__global__ void light_gen_kernel(VcmParams p, const LightTile* tiles, int n_tiles, int first, int n, float4* rays,
                                  unsigned long long* rng_out, float4* thr, float4* w) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
+    const int g = first + j;
     int lo = 0, hi = n_tiles - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (tiles[mid].first <= j) lo = mid;
+        if (tiles[mid].first <= g) lo = mid;
         else hi = mid - 1;
     }
     const LightTile t = tiles[lo];
-    const int i = j - t.first;
+    const int i = g - t.first;
     Rng rng = seed_sample(t.seed, i, i);
     const ShadingScene& s = p.s;
     const float pdf_lightpick = 1.0f / (float)s.light_count;
@@ -1127,23 +1130,33 @@ int imbart_vcm_begin_iteration(imbart_vcm* v, const imbart_vcm_settings* st, int
 int imbart_vcm_light_pass(imbart_vcm* v, const imbart_scene* scene, const imbart_shading* sh,
                           const imbart_camera* cam, const imbart_vcm_settings* st, float* image, long long* stats,
                           void* stream) {
+    return imbart_vcm_light_pass_range(v, scene, sh, cam, st, 0, st ? st->light_path_count : 0, image, nullptr, 0,
+                                       stats, stream);
+}
+
+int imbart_vcm_light_pass_range(imbart_vcm* v, const imbart_scene* scene, const imbart_shading* sh,
+                                const imbart_camera* cam, const imbart_vcm_settings* st, int first_path, int n_paths,
+                                float* image, int* wave_counts, int wave_cap, long long* stats, void* stream) {
     if (!v || !scene || !sh || !cam || !image || !valid_settings(st) || cam->width <= 0 || cam->height <= 0 ||
-        v->iteration < 1 || sh->s.light_count <= 0) {
+        v->iteration < 1 || sh->s.light_count <= 0 || first_path < 0 || n_paths < 0 ||
+        (long long)first_path + n_paths > st->light_path_count || wave_cap < 0 || (wave_cap > 0 && !wave_counts)) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_vcm_light_pass: invalid argument (begin the iteration first)");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
     if (stats) { stats[0] = 0; stats[1] = 0; stats[2] = 0; }
+    for (int k = 0; k < wave_cap; ++k) wave_counts[k] = 0;
     v->cache_count = 0;
     v->grid_built = false;
-    if (st->algorithm == IMBART_VCM_PT) return 0;   // the VCM path tracer traces no light paths
+    if (st->algorithm == IMBART_VCM_PT || n_paths == 0) return 0;   // the VCM path tracer traces no light paths
     cudaStream_t s = (cudaStream_t)stream;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(v->device);
-    const int P = st->light_path_count;
-    const int desired = st->light_tile_size > 0 ? st->light_tile_size : P;
+    const int P_total = st->light_path_count;
+    const int P = n_paths;        // slots of this call: paths first_path + slot
+    const int desired = st->light_tile_size > 0 ? st->light_tile_size : P_total;
     const std::vector<LightTile> tiles =
-        light_tiles(sh->s.light_count, P, desired, st->light_seed, st->light_seed_step);
+        light_tiles(sh->s.light_count, P_total, desired, st->light_seed, st->light_seed_step);
     const int n_blocks = (P + kScanTile - 1) / kScanTile;
     bool good = true;
     if (v->l_cap < P) {
@@ -1168,7 +1181,8 @@ int imbart_vcm_light_pass(imbart_vcm* v, const imbart_scene* scene, const imbart
     }
     VcmParams p = make_params(v, sh, cam, st, image);
     const int grid = (P + 127) / 128;
-    light_gen_kernel<<<grid, 128, 0, s>>>(p, v->d_tiles, (int)tiles.size(), P, v->l_rays, v->l_rng, v->l_thr, v->l_w);
+    light_gen_kernel<<<grid, 128, 0, s>>>(p, v->d_tiles, (int)tiles.size(), first_path, P, v->l_rays, v->l_rng,
+                                          v->l_thr, v->l_w);
     note_launches(1);
     int rc = 0;
     long long n_closest = 0, n_shadow = 0, n_waves = 0;
@@ -1208,6 +1222,7 @@ int imbart_vcm_light_pass(imbart_vcm* v, const imbart_scene* scene, const imbart
         }
         n_shadow += v->host_counts[1];
         v->cache_count += v->host_counts[3];
+        if (n_waves <= wave_cap) wave_counts[n_waves - 1] = v->host_counts[3];
         live = v->host_counts[2];
     }
     if (!rc) rc = build_grid(v, st, s);
@@ -1269,8 +1284,17 @@ int imbart_vcm_load_light_vertices(imbart_vcm* v, const imbart_vcm_settings* st,
 int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbart_shading* sh,
                            const imbart_camera* cam, const imbart_vcm_settings* st, float* image,
                            long long max_paths_in_flight, long long* stats, void* stream) {
+    const long long total = cam && st ? (long long)cam->width * cam->height * st->spp : 0;
+    return imbart_vcm_camera_pass_range(v, scene, sh, cam, st, 0, total, image, max_paths_in_flight, stats, stream);
+}
+
+int imbart_vcm_camera_pass_range(imbart_vcm* v, const imbart_scene* scene, const imbart_shading* sh,
+                                 const imbart_camera* cam, const imbart_vcm_settings* st, long long first_sample,
+                                 long long n_samples, float* image, long long max_paths_in_flight, long long* stats,
+                                 void* stream) {
     if (!v || !scene || !sh || !cam || !image || !valid_settings(st) || cam->width <= 0 || cam->height <= 0 ||
-        v->iteration < 1) {
+        v->iteration < 1 || first_sample < 0 || n_samples < 0 ||
+        first_sample + n_samples > (long long)cam->width * cam->height * st->spp) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_vcm_camera_pass: invalid argument (begin the iteration first)");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
@@ -1280,7 +1304,7 @@ int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbar
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(v->device);
-    const long long total = (long long)cam->width * cam->height * st->spp;
+    const long long total = n_samples;
     const int per = 1 + st->num_connections;
     long long chunk = max_paths_in_flight > 0 ? max_paths_in_flight : (8ll << 20);
     chunk = std::min(chunk, total);
@@ -1304,7 +1328,8 @@ int imbart_vcm_camera_pass(imbart_vcm* v, const imbart_scene* scene, const imbar
     for (long long first = 0; first < total && !rc; first += chunk) {
         int n = (int)std::min(chunk, total - first);
         int cur = 0;
-        vcm_camera_kernel<<<(n + 127) / 128, 128, 0, s>>>(p, st->camera_seed, st->spp, first, n, v->c_rays[cur],
+        vcm_camera_kernel<<<(n + 127) / 128, 128, 0, s>>>(p, st->camera_seed, st->spp, first_sample + first, n,
+                                                         v->c_rays[cur],
                                                          v->c_pixel[cur], v->c_rng[cur], v->c_thr[cur], v->c_w[cur]);
         note_launches(1);
         while (n > 0 && !rc) {

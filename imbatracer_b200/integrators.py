@@ -312,11 +312,55 @@ class VcmIntegrator:
             raise N.ImbartError("imbart_vcm_copy_light_vertices: " + N.last_error()[1])
         return out
 
-    def load_light_vertices(self, vertices: np.ndarray) -> None:
-        """Replaces the cache (e.g. with the reference's) and rebuilds the photon grid."""
-        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 28)
-        N.check(N.load().imbart_vcm_load_light_vertices(self.ctx, C.byref(self.settings), N.ptr(v), len(v), None),
-                "imbart_vcm_load_light_vertices")
+    def load_light_vertices(self, vertices) -> None:
+        """Replaces the cache (e.g. with the reference's, or the vertices of several GPUs) and
+        rebuilds the photon grid. vertices: (count, 28) float32 host array or CUDA tensor."""
+        if isinstance(vertices, np.ndarray):
+            vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1, 28)
+        else:
+            vertices = vertices.contiguous().view(-1, 28)
+        N.check(N.load().imbart_vcm_load_light_vertices(self.ctx, C.byref(self.settings), N.ptr(vertices),
+                                                        int(vertices.shape[0]), None), "imbart_vcm_load_light_vertices")
+
+    def light_pass_range(self, first_path: int, n_paths: int, light_seed: int, light_seed_step: int = 0,
+                         image=None):
+        """The light pass over paths [first_path, first_path + n_paths) of the iteration; returns
+        (image, vertices added per wavefront)."""
+        image = self._image(image)
+        self.settings.light_seed = light_seed & (2 ** 64 - 1)
+        self.settings.light_seed_step = light_seed_step & (2 ** 64 - 1)
+        stats = np.zeros(3, np.int64)
+        waves = np.zeros(self.settings.max_path_len + 1, np.int32)
+        N.check(N.load().imbart_vcm_light_pass_range(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                                     C.byref(self.camera), C.byref(self.settings), first_path,
+                                                     n_paths, N.ptr(image), N.ptr(waves), len(waves), N.ptr(stats),
+                                                     None), "imbart_vcm_light_pass_range")
+        self.last_stats[:3] = stats
+        return image, waves
+
+    def camera_pass_range(self, first_sample: int, n_samples: int, camera_seed: int, image=None):
+        image = self._image(image)
+        self.settings.camera_seed = camera_seed & (2 ** 64 - 1)
+        stats = np.zeros(3, np.int64)
+        N.check(N.load().imbart_vcm_camera_pass_range(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                                      C.byref(self.camera), C.byref(self.settings), first_sample,
+                                                      n_samples, N.ptr(image), self.max_paths, N.ptr(stats), None),
+                "imbart_vcm_camera_pass_range")
+        self.last_stats[3:] = stats
+        return image
+
+    def light_vertices_device(self):
+        """The cache as a (count, 28) float32 CUDA tensor (a copy)."""
+        import torch
+        ptr, n = C.c_void_p(), C.c_int(0)
+        N.check(N.load().imbart_vcm_light_vertices(self.ctx, C.byref(ptr), C.byref(n)), "imbart_vcm_light_vertices")
+        out = torch.empty((n.value, 28), dtype=torch.float32, device=torch.device("cuda", self.scene.device))
+        if n.value > 0:
+            class _View:
+                __cuda_array_interface__ = {"shape": (n.value, 28), "typestr": "<f4", "data": (ptr.value, False),
+                                            "version": 3}
+            out.copy_(torch.as_tensor(_View(), device=out.device))
+        return out
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -173,6 +173,9 @@ _SIGNATURES = {
     "imbart_vcm_begin_iteration": (I, [P, C.POINTER(VcmSettings), I, P]),
     "imbart_vcm_light_pass": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), P, P, P]),
     "imbart_vcm_camera_pass": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), P, C.c_longlong, P, P]),
+    "imbart_vcm_light_pass_range": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), I, I, P, P, I, P, P]),
+    "imbart_vcm_camera_pass_range": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), C.c_longlong,
+                                         C.c_longlong, P, C.c_longlong, P, P]),
     "imbart_vcm_render": (I, [P, P, P, C.POINTER(Camera), C.POINTER(VcmSettings), I, P, C.c_longlong, P, P]),
     "imbart_vcm_light_vertices": (I, [P, C.POINTER(P), C.POINTER(I)]),
     "imbart_vcm_copy_light_vertices": (I, [P, P, I]),

@@ -441,10 +441,29 @@ int imbart_vcm_light_pass(imbart_vcm* vcm, const imbart_scene* scene, const imba
                           const imbart_camera* camera, const imbart_vcm_settings* settings, float* image,
                           long long* stats, void* stream);
 
+/* The light pass over paths [first_path, first_path + n_paths) of the iteration's
+ * light_path_count (each path seeded by its global index, so the ranges of several GPUs
+ * together trace exactly the single-GPU paths). The cache then holds this range's vertices
+ * in (wavefront, path) order; wave_counts (HOST, may be NULL) receives the vertices each
+ * wavefront added, at most wave_cap entries. With the ranges' caches concatenated wavefront
+ * by wavefront in range order, imbart_vcm_load_light_vertices restores the single-GPU
+ * cache. */
+int imbart_vcm_light_pass_range(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
+                                const imbart_camera* camera, const imbart_vcm_settings* settings, int first_path,
+                                int n_paths, float* image, int* wave_counts, int wave_cap, long long* stats,
+                                void* stream);
+
 /* Camera pass (trace_camera_paths, vcm.cpp:106-130, 322-611) against the current cache. */
 int imbart_vcm_camera_pass(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
                            const imbart_camera* camera, const imbart_vcm_settings* settings, float* image,
                            long long max_paths_in_flight, long long* stats, void* stream);
+
+/* The camera pass over camera samples [first_sample, first_sample + n_samples) of the
+ * width * height * spp samples (sample index as in PixelRayGen: pixel-major per spp). */
+int imbart_vcm_camera_pass_range(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
+                                 const imbart_camera* camera, const imbart_vcm_settings* settings,
+                                 long long first_sample, long long n_samples, float* image,
+                                 long long max_paths_in_flight, long long* stats, void* stream);
 
 /* begin_iteration + light pass + camera pass into `image` (accumulated). */
 int imbart_vcm_render(imbart_vcm* vcm, const imbart_scene* scene, const imbart_shading* shading,
