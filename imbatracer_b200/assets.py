@@ -15,9 +15,10 @@ bump maps (map_bump / bump) and opacity masks (map_d). Arithmetic that decides r
 (instance matrices, normals, light vertices) is done in single precision in the
 reference's order of operations, so the arrays equal the reference's.
 
-Not supported: environment maps from HDR images (`env`; the shading code has a constant
-environment only) and emissive materials whose base is not diffuse (they become emissive
-diffuse). Both raise or are documented where they occur.
+An `env <file.hdr> <intensity>` command gives an image environment light (load_hdr.cpp;
+EnvMap, light.h:361-544); it is light 0 here, so a scene listing other lights before it
+samples them in another order than the reference (same estimate, other random numbers).
+Emissive materials whose base is not diffuse become emissive diffuse.
 """
 from __future__ import annotations
 
@@ -213,6 +214,58 @@ def load_tga(path: str) -> np.ndarray | None:
                 img[cur:cur + chunk] = np.array([one[2], one[1], one[0], one[3]], np.float32) / inv
             cur += chunk
     return img.reshape(h, w, 4)
+
+
+def load_hdr(path: str) -> np.ndarray:
+    """Radiance RGBE images with run-length encoded scanlines (load_hdr.cpp:174-229): header
+    lines up to an empty line, a "-Y height +X width" resolution line, one scanline per row;
+    texel = ((byte + 0.5) * 2^(e - 136)) per channel, alpha 0. Scanlines in the older flat or
+    RLE formats are refused: the reference's decoder does not store their pixels."""
+    data = open(path, "rb").read()
+    pos = data.index(b"\n") + 1                    # the signature line (not checked)
+    while True:
+        end = data.index(b"\n", pos)
+        line = data[pos:end]
+        pos = end + 1
+        if line == b"":
+            break
+    end = data.index(b"\n", pos)
+    res = data[pos:end].split()
+    pos = end + 1
+    if len(res) != 4 or res[0] != b"-Y" or res[2] != b"+X":
+        raise ValueError(f"hdr: unsupported axis configuration in {path}")
+    h, w = int(res[1]), int(res[3])
+    img = np.zeros((h, w, 4), np.float32)
+    buf = np.frombuffer(data, np.uint8)
+    for y in range(h):
+        if pos + 4 > len(buf):
+            raise ValueError(f"hdr: unexpected end of file in {path}")
+        r, g, b, e = (int(v) for v in buf[pos:pos + 4])
+        pos += 4
+        if not (r == 2 and g == 2 and not (b & 128)):
+            raise ValueError(f"hdr: only adaptive run-length scanlines are supported ({path})")
+        if ((b << 8) | e) != w:
+            raise ValueError(f"hdr: scanline length mismatch in {path}")
+        px = np.zeros((w, 4), np.uint8)
+        for comp in range(4):
+            i = 0
+            while i < w:
+                code = int(buf[pos]); pos += 1
+                if code > 128:
+                    code &= 127
+                    if i + code > w:
+                        raise ValueError("hdr: overrun in a scanline run")
+                    px[i:i + code, comp] = buf[pos]; pos += 1
+                    i += code
+                else:
+                    if code == 0 or i + code > w:
+                        raise ValueError("hdr: bad scanline dump")
+                    px[i:i + code, comp] = buf[pos:pos + code]; pos += code
+                    i += code
+        scale = np.ldexp(1.0, px[:, 3].astype(np.int64) - 136)
+        for c in range(3):
+            img[y, :, c] = ((px[:, c].astype(np.float64) + 0.5) * scale).astype(np.float32)
+    return img
 
 
 def load_image(path: str) -> np.ndarray | None:
@@ -516,7 +569,7 @@ class SceneFileInfo:
     cam_up: tuple | None = None
     instances: list = field(default_factory=list)   # (mesh index, 4x4 matrix)
     lights: list = field(default_factory=list)      # (kind, 12 floats) in file order
-    env: tuple | None = None
+    env: tuple | None = None        # (image path, intensity)
 
 
 def parse_scene_file(path: str) -> SceneFileInfo:
@@ -533,6 +586,11 @@ def parse_scene_file(path: str) -> SceneFileInfo:
             toks.append(t)
     info = SceneFileInfo()
     i = 0
+
+    def nums_after(j):
+        if j >= len(toks):
+            raise ValueError(f"scene: unexpected end of file in {path}")
+        return float(np.float32(toks[j]))
 
     def nums(k):
         nonlocal i
@@ -586,7 +644,10 @@ def parse_scene_file(path: str) -> SceneFileInfo:
                     break
             info.instances.append((idx, instance_matrix(pos, scale, rot)))
         elif cmd == "env":
-            raise ValueError("scene: environment maps from HDR images are not supported")
+            if info.env is not None:
+                continue                            # the reference ignores further maps
+            info.env = (os.path.join(base, toks[i]), nums_after(i + 1))
+            i += 2
         # unknown commands are skipped, as the reference's loop does
     if info.cam_pos is None or info.cam_dir is None or info.cam_up is None:
         raise ValueError("scene: camera settings not specified")
@@ -763,10 +824,15 @@ def load_scene_file(path: str, width: int = 512, height: int = 512, fov: float =
         for (p0, p1, p2), e in mesh_lights[mesh_id]:
             lights.append((_xform_point(mat, p0), _xform_point(mat, p1), _xform_point(mat, p2),
                            np.asarray(e, np.float32)))
-    if not lights and not info.lights:
+    env_map, env_intensity = -1, 1.0
+    if info.env is not None:
+        img = load_hdr(info.env[0])
+        env_map, env_intensity = len(tex.images), info.env[1]
+        tex.images.append(img)
+    if not lights and not info.lights and env_map < 0:
         raise ValueError("scene: there are no lights in the scene")
     cam = G.Camera(info.cam_pos, info.cam_dir, info.cam_up, fov, width, height)
     return G.SceneDesc(meshes, instances, materials, lights, cam, None, os.path.basename(path),
                        delta_lights=list(info.lights), textures=tex.images, delta_first=True,
                        masks=np.array(masks.descs, N.MASK_DTYPE), mask_buffer=np.concatenate(masks.buffer),
-                       accel_files=info.accel_files)
+                       accel_files=info.accel_files, env_map=env_map, env_map_intensity=env_intensity)

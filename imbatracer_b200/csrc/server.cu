@@ -189,6 +189,8 @@ struct SceneRec {
     int n_textures = 0;
     bool has_env = false;
     float env[3] = {0, 0, 0};
+    int env_map = 0;              // 1 + environment image texture, 0: constant
+    float env_intensity = 0.0f;
     float bsphere[5] = {0, 0, 0, 0, 0};
     // Block layout (byte offsets from the block start).
     size_t bytes = 0, o_nodes = 0, o_tris = 0, o_insts = 0, o_vert = 0, o_nrm = 0, o_tc = 0, o_mtris = 0,
@@ -482,6 +484,8 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
     ss.has_env = s.has_env ? 1 : 0;
     ss.light_count = s.n_tri_lights + ss.has_env;
     for (int k = 0; k < 3; ++k) ss.env_color[k] = s.env[k];
+    ss.env_map = s.env_map;
+    ss.env_intensity = s.env_intensity;
     for (int k = 0; k < 5; ++k) ss.bsphere[k] = s.bsphere[k];
     if (!cuda_check(cudaMemcpyAsync(S->d_scenes + slot, &ss, sizeof(ShadingScene), cudaMemcpyHostToDevice, st),
                     "upload") ||
@@ -926,6 +930,10 @@ int plain_request(imbart_server* S, Request* r) {
             s.n_tri_lights, s.has_env ? s.env : nullptr, s.bsphere, s.tex_dims.empty() ? nullptr : s.tex_dims.data(),
             s.tex_pixels.empty() ? nullptr : s.tex_pixels.data(), s.n_textures);
         if (!s.plain_shading) return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
+        if (s.env_map > 0) {
+            const int rc = imbart_shading_set_env_map(s.plain_shading, s.env_map - 1, s.env_intensity);
+            if (rc) return rc;
+        }
         S->stats.scene_uploads += 1;
     }
     if (r->kind == 0 || r->kind == 2) {
@@ -1167,7 +1175,7 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         src->n_tri_vec4 <= 0 || !src->vertices || src->n_vertices <= 0 || !src->normals || !src->texcoords ||
         !src->mesh_tris || !src->geom_normals || src->n_mesh_tris <= 0 || !src->inst_inv || src->n_inst_inv <= 0 ||
         !src->mat_kind || !src->mat_params || src->n_mats <= 0 || src->n_tri_lights < 0 ||
-        (src->n_tri_lights > 0 && !src->tri_lights) || (src->n_tri_lights == 0 && !src->env_color) ||
+        (src->n_tri_lights > 0 && !src->tri_lights) || (src->n_tri_lights == 0 && !src->env_color && src->env_map <= 0) ||
         !valid_light_kinds(src->light_kinds, src->n_tri_lights) || src->n_textures < 0 ||
         (src->n_textures > 0 && (!src->tex_dims || !src->tex_pixels))) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: invalid argument");
@@ -1215,8 +1223,14 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         }
     s->lights = decode_lights(src->light_kinds, src->tri_lights, src->n_tri_lights);
     s->n_tri_lights = src->n_tri_lights;
-    s->has_env = src->env_color != nullptr;
+    s->has_env = src->env_color != nullptr || src->env_map > 0;
     for (int k = 0; k < 3; ++k) s->env[k] = src->env_color ? src->env_color[k] : 0.0f;
+    if (src->env_map < 0 || src->env_map > src->n_textures || !(src->env_intensity >= 0.0f)) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: invalid environment image");
+        return -IMBART_ERR_INVALID_ARGUMENT;
+    }
+    s->env_map = src->env_map;
+    s->env_intensity = src->env_intensity;
     for (int k = 0; k < 5; ++k) s->bsphere[k] = src->bsphere ? src->bsphere[k] : 0.0f;
     for (int i = 0; i < src->n_mesh_tris; ++i) {
         const int* t = src->mesh_tris + 4 * i;

@@ -177,6 +177,8 @@ struct ShadingScene {
     int has_env;
     float env_color[3];         // intensity * constant environment colour
     float bsphere[5];           // centre xyz, radius, 1/radius^2
+    int env_map;                // 0: constant environment; else 1 + texture index of its image
+    float env_intensity;        // scale of the environment image
 };
 
 // ---------------------------------------------------------------------------------------
@@ -543,14 +545,36 @@ __device__ __forceinline__ DirectSample tri_light_sample(const LightSrc& L, V3 f
     return s;
 }
 
-// EnvLight::sample_direct with a constant 1x1 map (light.h:446-485, 525-539).
+// The environment image's size (1 x 1 for a constant environment) and its texel at
+// (x, y) = (int)(s * (w - 1)), (int)(t * (h - 1)) times its intensity: EnvMap's image lookup
+// img_(s * (width - 1), t * (height - 1)) (light.h:413-424, 458-470; Image::operator()
+// truncates the coordinates).
+__device__ __forceinline__ void env_size(const ShadingScene& sc, int& w, int& h) {
+    if (sc.env_map == 0) { w = 1; h = 1; return; }
+    const int4 ti = sc.tex_info[sc.env_map - 1];
+    w = ti.y;
+    h = ti.z;
+}
+
+__device__ __forceinline__ V3 env_lookup(const ShadingScene& sc, float s, float t) {
+    if (sc.env_map == 0) return V3(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    const int4 ti = sc.tex_info[sc.env_map - 1];
+    const int x = (int)(s * (float)(ti.y - 1)), y = (int)(t * (float)(ti.z - 1));
+    const float4 c = sc.tex_pixels[ti.x + y * ti.y + x];
+    return sc.env_intensity * V3(c.x, c.y, c.z);
+}
+
+// EnvLight::sample_direct (light.h:446-485, 525-539): a uniform (u, v) on the map (the
+// reference does not importance-sample the image).
 __device__ __forceinline__ DirectSample env_light_sample(const ShadingScene& sc, Rng& rng) {
     DirectSample s;
-    float pdf = 1.0f / float(1 * 1);
+    int w, h;
+    env_size(sc, w, h);
+    float pdf = 1.0f / float(w * h);
     const float ux = rng.next_float();
     const float uy = rng.next_float();
-    pdf *= float(1 * 1);
-    const V3 color(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    pdf *= float(w * h);
+    const V3 color = env_lookup(sc, ux, uy);
     const float theta = kPi * uy;
     const float sin_theta = sinf(theta);
     const float phi = 2.0f * kPi * ux;
@@ -595,15 +619,17 @@ __device__ __forceinline__ EmitSample tri_light_emit(const LightSrc& L, Rng& rng
     return s;
 }
 
-// EnvLight::sample_emit with a constant map (light.h:494-523, 446-485): a direction from the
-// map, then a point on the disc of the scene's bounding sphere facing it.
+// EnvLight::sample_emit (light.h:494-523, 446-485): a direction from the map, then a point
+// on the disc of the scene's bounding sphere facing it.
 __device__ __forceinline__ EmitSample env_light_emit(const ShadingScene& sc, Rng& rng) {
     EmitSample s;
-    float pdf = 1.0f / float(1 * 1);
+    int w, h;
+    env_size(sc, w, h);
+    float pdf = 1.0f / float(w * h);
     const float ux = rng.next_float();
     const float uy = rng.next_float();
-    pdf *= float(1 * 1);
-    const V3 color(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    pdf *= float(w * h);
+    const V3 color = env_lookup(sc, ux, uy);
     const float theta = kPi * uy;
     const float sin_theta = sinf(theta);
     const float phi = 2.0f * kPi * ux;
@@ -756,14 +782,14 @@ __device__ __forceinline__ V3 area_emitter_radiance(const Material& m, V3 out_di
     return V3(m.emission[0], m.emission[1], m.emission[2]);
 }
 
-// EnvMap::radiance with a constant map (light.h:413-424): pdf_direct_w = 1 / (2 pi^2 sin t).
+// EnvMap::radiance (light.h:413-424): pdf_direct_w = 1 / (2 pi^2 sin t).
 __device__ __forceinline__ V3 env_radiance(const ShadingScene& sc, V3 out_dir, float* pdf_direct_w) {
     float phi = atan2f(out_dir.x, out_dir.z);
     phi = (phi < 0.0f) ? (phi + 2.0f * kPi) : phi;
+    const float s = phi / (2.0f * kPi);
     const float t = acosf(out_dir.y) / kPi;
     *pdf_direct_w = 1.0f / (2.0f * kPi * kPi * sinf(t));
-    (void)phi;
-    return V3(sc.env_color[0], sc.env_color[1], sc.env_color[2]);
+    return env_lookup(sc, s, t);
 }
 
 __device__ __forceinline__ V3 env_radiance_emit(const ShadingScene& sc, V3 out_dir, float* pdf_direct_w,

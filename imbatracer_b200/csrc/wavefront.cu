@@ -188,6 +188,20 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
                                     env_color, bsphere, nullptr, nullptr, 0);
 }
 
+int imbart_shading_set_env_map(imbart_shading* h, int texture, float intensity) {
+    if (!h || texture < 0 || texture >= h->s.n_textures || !(intensity >= 0.0f)) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_shading_set_env_map: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (!h->s.has_env) {
+        h->s.has_env = 1;
+        h->s.light_count += 1;
+    }
+    h->s.env_map = texture + 1;
+    h->s.env_intensity = intensity;
+    return 0;
+}
+
 void imbart_shading_destroy(imbart_shading* h) {
     if (!h) return;
     int prev = 0;

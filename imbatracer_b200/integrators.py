@@ -70,6 +70,10 @@ class ShadingData:
         self.tex_pixels = (np.ascontiguousarray(np.concatenate([np.asarray(t, np.float32).reshape(-1) for t in tex]))
                            if tex else np.zeros(4, np.float32))
         self.env = None if desc.env_intensity is None else np.array(desc.env_intensity, np.float32)
+        self.env_map = int(getattr(desc, "env_map", -1))
+        self.env_map_intensity = float(getattr(desc, "env_map_intensity", 1.0))
+        if self.env_map >= 0 and self.env is None:
+            self.env = np.zeros(3, np.float32)     # the environment light exists; its image is set after
         self.bsphere = bounding_sphere(desc)
 
 
@@ -131,6 +135,8 @@ class GpuScene:
         if not h:
             raise N.ImbartError("imbart_shading_create: " + N.last_error()[1])
         self.shading = h
+        if sd.env_map >= 0:
+            N.check(lib.imbart_shading_set_env_map(h, sd.env_map, sd.env_map_intensity), "imbart_shading_set_env_map")
 
     def close(self):
         if getattr(self, "shading", None):

@@ -70,7 +70,8 @@ class SceneSource(C.Structure):
                 ("inst_inv", C.c_void_p), ("n_inst_inv", C.c_int), ("mat_kind", C.c_void_p),
                 ("mat_params", C.c_void_p), ("n_mats", C.c_int), ("tri_lights", C.c_void_p), ("n_tri_lights", C.c_int),
                 ("env_color", C.c_void_p), ("bsphere", C.c_void_p), ("light_kinds", C.c_void_p),
-                ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int)]
+                ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int),
+                ("env_map", C.c_int), ("env_intensity", C.c_float)]
 
 
 class MeshDesc(C.Structure):
@@ -160,6 +161,7 @@ _SIGNATURES = {
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_mesh_node2_ex": (I, [P, I, I, P, I, I, I, C.c_float, P, I, P, P, I, P]),
     "imbart_accel_file_info": (I, [C.c_char_p, I, P, P]),
+    "imbart_shading_set_env_map": (I, [P, I, C.c_float]),
     "imbart_scene_build_gpu": (P, [C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, I, P, C.POINTER(C.c_float)]),
     "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),
     "imbart_load_accel_node4": (I, [C.c_char_p, I, P, I, P, P, I, P]),

@@ -78,6 +78,8 @@ class SceneDesc:
     masks: np.ndarray | None = None  # opacity masks per material (MASK_DTYPE), None: all opaque
     mask_buffer: np.ndarray | None = None
     accel_files: list | None = None  # per-mesh acceleration cache files
+    env_map: int = -1                # texture index of an environment image (-1: none)
+    env_map_intensity: float = 1.0
 
     @property
     def instanced_triangles(self) -> int:

@@ -56,6 +56,7 @@ class Server:
         src.env_color, src.bsphere = N.ptr(sd.env), N.ptr(sd.bsphere)
         src.light_kinds = N.ptr(sd.light_kinds)
         src.tex_dims, src.tex_pixels, src.n_textures = N.ptr(sd.tex_dims), N.ptr(sd.tex_pixels), sd.n_textures
+        src.env_map, src.env_intensity = sd.env_map + 1, sd.env_map_intensity
         self._scenes.append((td, sd))   # the arrays the source points to stay alive during the call
         sid = self.lib.imbart_server_add_scene(self.h, C.byref(src))
         if sid < 0:

@@ -324,6 +324,11 @@ imbart_shading* imbart_shading_create(int device, const float* vertices, int n_v
                                       int n_tris, const float* inst_inv, int n_inst, const int* mat_kind,
                                       const float* mat_params, int n_mats, const float* tri_lights,
                                       int n_tri_lights, const float* env_color, const float* bsphere);
+/* Makes the environment light an image (EnvMap / EnvLight, light.h:361-544): texture
+ * `texture` of the shading data (latitude-longitude, rgba) times `intensity`, looked up at
+ * the texel the reference's EnvMap reads (no filtering; directions sampled uniformly over
+ * the map, as the reference does). Adds the environment as light 0 when the scene had none. */
+int imbart_shading_set_env_map(imbart_shading* shading, int texture, float intensity);
 void imbart_shading_destroy(imbart_shading* shading);
 
 /* imbart_shading_create with every light kind of the reference and textures.
@@ -534,6 +539,10 @@ typedef struct {
     const int* tex_dims;
     const float* tex_pixels;
     int n_textures;
+    /* Optional: 1 + the texture holding an environment image (0: none) and its intensity,
+     * as imbart_shading_set_env_map. */
+    int env_map;
+    float env_intensity;
 } imbart_scene_source;
 
 /* One path-traced frame (as imbart_pt_render with a fresh zeroed image). image_host: HOST

@@ -42,6 +42,19 @@ namespace {
 int g_masks_active = 0;
 int g_n_masks = 0;
 int g_trace_threads = 1;
+
+// The alpha-mask test is active for scenes whose uploaded masks are not all the default
+// opaque 1x1 descriptor (scenes read from files with map_d), as the reference's traversal
+// applies them.
+void use_scene_masks(const imba::Scene& scene) {
+    const auto& td = scene.traversal_data_gpu();
+    g_masks_active = 0;
+    g_n_masks = (int)td.masks.size();
+    for (size_t i = 0; i < td.masks.size(); ++i) {
+        const auto& m = td.masks.data()[i];
+        if (m.width * m.height > 1) g_masks_active = 1;
+    }
+}
 }
 
 // The reference's GPU entry points, served on the CPU by the oracle.
@@ -478,6 +491,7 @@ void ref_scene_bsphere(void* h, float* out4) {
 int ref_render_pt(void* h, int w, int ht, const float* pos, const float* dir, const float* up, float fov, int spp,
                   int max_path_len, uint64_t seed_base, float* image_out) {
     RefScene* rs = static_cast<RefScene*>(h);
+    use_scene_masks(rs->scene);
     PerspectiveCamera cam((float)w, (float)ht, fov);
     cam.move(f3(pos), f3(dir), f3(up));
     const int tile = w > ht ? w : ht;
@@ -504,6 +518,7 @@ int ref_render_pt_threads(void* h, int w, int ht, const float* pos, const float*
                           int spp, int max_path_len, uint64_t seed_base, int tile, int threads, float* image_out,
                           long long* counts) {
     RefScene* rs = static_cast<RefScene*>(h);
+    use_scene_masks(rs->scene);
     PerspectiveCamera cam((float)w, (float)ht, fov);
     cam.move(f3(pos), f3(dir), f3(up));
     DefaultTileGen<PTState> gen(w, ht, spp, tile);

@@ -158,7 +158,8 @@ int ref_scene_materials(void* h, int* kinds, float* params) {
     return 0;
 }
 
-// Lights in the reference's order: kind (0 triangle, 1 directional, 2 point, 3 spot) and 12
+// Lights in the reference's order: kind (0 triangle, 1 directional, 2 point, 3 spot,
+// 4 environment) and 12
 // floats as the product's light records (triangle: p0, p1, p2, intensity; directional:
 // direction, 6 zero, intensity; point: position, 6 zero, intensity; spot: position, axis,
 // half-angle, 2 zero, intensity).
@@ -186,6 +187,8 @@ int ref_scene_lights(void* h, int* kinds, float* params) {
             put3(p + 3, sp->normal_);
             p[6] = sp->angle_;
             put_rgb(p + 9, sp->intensity_);
+        } else if (dynamic_cast<EnvLight*>(l)) {
+            kinds[i] = 4;
         } else {
             return -1;
         }
@@ -207,6 +210,25 @@ void ref_scene_textures(void* h, int* dims, float* texels) {
                 texels += 4;
             }
     }
+}
+
+// The environment image (EnvMap, light.h:361-486): returns 0 and fills dims (width,
+// height), texels (rgba rows) and the intensity when the scene has one, else -1.
+int ref_scene_env(void* h, int* dims, float* texels, float* intensity) {
+    const Scene* s = ref_scene_of(h);
+    const EnvMap* e = s->env_map();
+    if (!e) return -1;
+    dims[0] = e->img_.width();
+    dims[1] = e->img_.height();
+    *intensity = e->intensity_;
+    if (texels)
+        for (int y = 0; y < e->img_.height(); ++y)
+            for (int x = 0; x < e->img_.width(); ++x) {
+                const float4& c = e->img_(x, y);
+                texels[0] = c.x; texels[1] = c.y; texels[2] = c.z; texels[3] = c.w;
+                texels += 4;
+            }
+    return 0;
 }
 
 // Opacity masks as uploaded for traversal: descriptors (width, height, offset) and bytes.

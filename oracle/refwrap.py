@@ -46,6 +46,7 @@ def load() -> C.CDLL:
             "ref_scene_lights": (I, [P, P, P]),
             "ref_scene_textures": (None, [P, P, P]),
             "ref_scene_masks": (None, [P, P, P]),
+            "ref_scene_env": (I, [P, P, P, P]),
             "ref_load_accel": (I, [I, C.c_char_p, I, P, I, P, I, P, I, P, P, I, P]),
             "ref_store_accel": (I, [I, C.c_char_p, P, I, I, P, I, I, I]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
@@ -251,6 +252,11 @@ class RefScene:
         assert lib.ref_scene_lights(self.handle, _p(out["light_kind"]), _p(out["light_params"])) == 0
         lib.ref_scene_textures(self.handle, _p(out["tex_dims"]), _p(out["texels"]))
         lib.ref_scene_masks(self.handle, _p(out["masks"]), _p(out["mask_buffer"]))
+        dims, inten = np.zeros(2, np.int32), np.zeros(1, np.float32)
+        if lib.ref_scene_env(self.handle, _p(dims), None, _p(inten)) == 0:
+            tex = np.zeros((int(dims[1]) * int(dims[0]), 4), np.float32)
+            lib.ref_scene_env(self.handle, _p(dims), _p(tex), _p(inten))
+            out["env_dims"], out["env_texels"], out["env_intensity"] = dims, tex, float(inten[0])
         out["tex_dims"] = out["tex_dims"][:ntex]
         out["texels"] = out["texels"][:texels]
         out["masks"] = out["masks"][:nmask]

@@ -90,18 +90,29 @@ def compare_with_reference(path):
     kinds, prm = material_records(d)
     assert np.array_equal(kinds, e["mat_kind"])
     assert np.array_equal(bits(prm[:, :14]), bits(e["mat_params"][:, :14]))
-    # Light list in the reference's order: the file's lights, then the triangle lights.
-    lk = [k for k, _ in d.delta_lights] + [0] * len(d.lights)
-    lp = [np.asarray(p, np.float32) for _, p in d.delta_lights] + \
+    # Light list in the reference's order: the file's lights (the environment first in these
+    # files), then the triangle lights.
+    env = [4] if d.env_map >= 0 else []
+    lk = env + [k for k, _ in d.delta_lights] + [0] * len(d.lights)
+    lp = [np.zeros(12, np.float32) for _ in env] + [np.asarray(p, np.float32) for _, p in d.delta_lights] + \
          [np.concatenate([a, b, c, x]).astype(np.float32) for a, b, c, x in d.lights]
     assert np.array_equal(np.array(lk, np.int32), e["light_kind"])
     if lp:
         assert np.array_equal(bits(np.stack(lp)), bits(e["light_params"]))
-    assert len(d.textures) == len(e["tex_dims"])
-    for k, t in enumerate(d.textures):
+    if d.env_map >= 0:
+        img = d.textures[d.env_map]
+        assert tuple(e["env_dims"]) == (img.shape[1], img.shape[0])
+        assert np.array_equal(bits(img.reshape(-1, 4)), bits(e["env_texels"]))
+        assert np.float32(d.env_map_intensity) == np.float32(e["env_intensity"])
+    else:
+        assert "env_dims" not in e
+    # Textures (the environment image is kept with the reference's EnvMap, not its textures).
+    tex = [t for k, t in enumerate(d.textures) if k != d.env_map]
+    assert len(tex) == len(e["tex_dims"])
+    for k, t in enumerate(tex):
         assert (t.shape[1], t.shape[0]) == tuple(e["tex_dims"][k])
-    if d.textures:
-        assert np.array_equal(bits(np.concatenate([t.reshape(-1, 4) for t in d.textures])), bits(e["texels"]))
+    if tex:
+        assert np.array_equal(bits(np.concatenate([t.reshape(-1, 4) for t in tex])), bits(e["texels"]))
     assert np.array_equal(d.masks.view(np.int32).reshape(-1, 3), e["masks"])
     assert np.array_equal(d.mask_buffer, e["mask_buffer"])
     return d, e
@@ -140,6 +151,38 @@ def write_tga(path, img, rle=False):
     open(path, "wb").write(head + bytes(out))
 
 
+def write_hdr(path, rgb):
+    """Radiance RGBE with adaptive run-length scanlines (runs for repeated bytes, dumps
+    otherwise)."""
+    h, w, _ = rgb.shape
+    m = rgb.max(-1)
+    mant, ex = np.frexp(np.maximum(m, 1e-38))
+    e = np.where(m > 1e-32, ex + 128, 0).astype(np.int64)
+    scale = np.where(m > 1e-32, 256.0 / np.ldexp(1.0, ex), 0.0)
+    px = np.zeros((h, w, 4), np.uint8)
+    px[..., :3] = np.clip(rgb * scale[..., None], 0, 255).astype(np.uint8)
+    px[..., 3] = np.clip(e, 0, 255)
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+    for y in range(h):
+        out += bytes([2, 2, w >> 8, w & 255])
+        for c in range(4):
+            row, i = px[y, :, c], 0
+            while i < w:
+                run = 1
+                while i + run < w and run < 127 and row[i + run] == row[i]:
+                    run += 1
+                if run >= 3:
+                    out += bytes([128 + run, int(row[i])])
+                    i += run
+                else:
+                    j = i
+                    while j < w and j - i < 128 and not (j + 2 < w and row[j] == row[j + 1] == row[j + 2]):
+                        j += 1
+                    out += bytes([j - i]) + row[i:j].tobytes()
+                    i = j
+    open(path, "wb").write(bytes(out))
+
+
 def feature_scene(tmp):
     rng = np.random.default_rng(5)
     tex = rng.uniform(0, 1, (6, 8, 3)).astype(np.float32)
@@ -152,6 +195,11 @@ def feature_scene(tmp):
     mask = np.zeros((4, 4, 3), np.float32)
     mask[1:3, 1:3] = 1
     write_tga(os.path.join(tmp, "mask.tga"), mask)
+    sky = np.zeros((16, 32, 3), np.float32)
+    sky[:8] = (0.6, 0.7, 1.4)                                     # bright upper half
+    sky[8:] = rng.uniform(0.0, 0.3, (8, 32, 3))
+    sky[3:5, 20:24] = (40.0, 35.0, 20.0)                           # a sun
+    write_hdr(os.path.join(tmp, "sky.hdr"), sky)
     open(os.path.join(tmp, "feat.mtl"), "w").write("""# every material kind
 newmtl wall
   Kd 0.5 0.4 0.3
@@ -244,6 +292,7 @@ rot 10 45 -30
 instance 0
 rot 0 90 0
 scale 1.5 1.5 1.5
+env sky.hdr 0.7
 dir_light 0.3 -1 0.2 1 1 1
 point_light 1 3 1 20 20 20
 spot_light -1 4 2 0.2 -1 -0.3 35 50 40 30
@@ -256,7 +305,8 @@ def test_feature_scene_loads_as_the_reference_loads_it(tmp_path):
     d, e = compare_with_reference(feature_scene(str(tmp_path)))
     kinds = set(m.kind for m in d.materials)
     assert {G.LAMBERT, G.GLOSSY, G.MIRROR, G.GLASS, G.EMISSIVE} <= kinds
-    assert len(d.textures) == 4 and (d.masks["width"] > 1).any() and len(d.delta_lights) == 3
+    assert len(d.textures) == 5 and (d.masks["width"] > 1).any() and len(d.delta_lights) == 3
+    assert d.env_map == 4 and "env_dims" in e
     assert any(m.texture >= 0 for m in d.materials) and any(m.bump >= 0 for m in d.materials)
     assert any(tuple(m.color) == (1.0, 0.0, 1.0) for m in d.materials)      # missing texture
 
@@ -292,9 +342,9 @@ def test_malformed_scene_files_are_errors(tmp_path):
     p.write_text("mesh a.obj\n")
     with pytest.raises(ValueError):
         A.load_scene_file(str(p))                   # no camera
-    p.write_text("pos 0 0 0\ndir 0 0 -1\nup 0 1 0\nenv sky.hdr 1\nmesh a.obj\n")
+    (tmp_path / "sky.hdr").write_bytes(b"#?RADIANCE\n\n-Y 1 +X 2\n" + bytes([10, 20, 30, 128] * 2))
     with pytest.raises(ValueError):
-        A.load_scene_file(str(p))                   # image environment maps are not supported
+        A.load_hdr(str(tmp_path / "sky.hdr"))        # flat scanlines: the reference stores none of them
     (tmp_path / "a.obj").write_text("v 0 0 0\nv 1 0 0\nf 1 2\n")
     p.write_text("pos 0 0 0\ndir 0 0 -1\nup 0 1 0\nmesh a.obj\n")
     with pytest.raises(ValueError):
@@ -364,3 +414,22 @@ def test_cornell_converges_to_the_reference_image(cuda, name, algo):
     err = rel_rmse(img[ok], z["golden"][ok])
     ratio = float(img[ok].mean() / z["golden"][ok].mean())
     assert err <= tol and abs(ratio - 1.0) <= 0.03, (err, ratio)
+
+
+needs_ref_lib = pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+
+
+@pytest.mark.gpu
+@needs_ref_lib
+@pytest.mark.parametrize("w,h,spp,max_len,seed", [(64, 48, 8, 6, 31), (40, 30, 4, 3, 32)])
+def test_feature_scene_path_traced_like_the_reference(cuda, tmp_path, w, h, spp, max_len, seed):
+    """Every feature the asset path carries (environment image, all light kinds, raw / RLE
+    TGA textures, bump maps, opacity masks, glass / mirror / glossy / emissive materials,
+    rotated and scaled instances) rendered by the reference from the same files."""
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    path = feature_scene(str(tmp_path))
+    ref = R.RefScene.from_file(path, w, h).render_pt(w, h, spp, max_len, seed)
+    d = A.load_scene_file(path, w, h)
+    img = PathTracer(GpuScene(d), max_path_len=max_len).render(spp, seed, w, h).cpu().numpy()
+    assert ref.sum() > 0
+    assert rel_rmse(img, ref) <= RMSE_TOL, rel_rmse(img, ref)
