@@ -236,6 +236,7 @@ struct ShadeParams {
     const int* req; const int* root;
     int* o_req; int* o_root; int* s_req; int* s_root;
     int* terminated;         // per request slot: paths that ended
+    const int* perm;         // optional: shade path perm[i] in thread i (paths grouped by material)
 };
 
 __device__ __forceinline__ void add_image(float* img, int pixel, V3 c) {
@@ -346,15 +347,62 @@ __device__ __forceinline__ void shade_path(const ShadingScene& s, int max_path_l
     }
 }
 
+// RayQueue::sort_by_material (ray_queue.h:211-244) for the device queue: the paths of a
+// wavefront grouped by what shading will run for them (material kind of the hit, or a miss),
+// so that the warps of the shading kernel follow one code path each. The reference sorts the
+// queue itself with a two-pass counting sort; here a permutation is built (keys with a
+// per-block histogram, then a scatter with warp-aggregated cursors) and the shading kernel
+// reads through it. Results per path do not depend on the order.
+constexpr int kShadeKeys = 8;   // material kinds 0..5, 6: miss
+
+__device__ __forceinline__ int shade_key(const ShadingScene& s, int4 h) {
+    if (h.x < 0) return 6;
+    return s.materials[s.tris[h.x].w].kind & 7;
+}
+
+__global__ void __launch_bounds__(256) shade_key_kernel(ShadingScene s, const int4* __restrict__ hits, int n,
+                                                        uint8_t* keys, int* counts) {
+    __shared__ int hist[kShadeKeys];
+    if (threadIdx.x < kShadeKeys) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int k = shade_key(s, hits[i]);
+        keys[i] = (uint8_t)k;
+        atomicAdd(&hist[k], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+}
+
+// counts[0..7]: keys per bucket; counts[8..15]: running cursors (zeroed before).
+__global__ void __launch_bounds__(256) shade_scatter_kernel(const uint8_t* __restrict__ keys, int n, int* counts,
+                                                            int* perm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const int k = valid ? keys[i] : kShadeKeys;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned group = __match_any_sync(0xffffffffu, k);
+    if (!valid) return;
+    const int leader = __ffs(group) - 1;
+    int base = 0;
+    if ((int)lane == leader) base = atomicAdd(counts + kShadeKeys + k, __popc(group));
+    base = __shfl_sync(group, base, leader);
+    int off = 0;
+    for (int b = 0; b < k; ++b) off += __ldg(counts + b);
+    perm[off + base + __popc(group & ((1u << lane) - 1u))] = i;
+}
+
 // One wavefront of shading: continuations go to the next path queue, shadow rays to the
 // shadow queue (both appended in warp order). In the merged form every path that ends adds
 // one to its request's `terminated` counter.
 template <bool kMulti>
 __global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     ShadeOut o;
     int pixel = 0, req = 0, root = 0;
-    if (i < p.n) {
+    if (t < p.n) {
+        const int i = p.perm ? p.perm[t] : t;
         pixel = p.pixel[i];
         const float4 ro = p.rays[2 * i], rd = p.rays[2 * i + 1];
         const int4 h = p.hits[i];
@@ -389,7 +437,7 @@ __global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
         if (kMulti) { p.s_req[sslot] = req; p.s_root[sslot] = root; }
     }
     if (kMulti) {
-        const bool ended = i < p.n && !o.alive;
+        const bool ended = t < p.n && !o.alive;
         const unsigned m = __ballot_sync(__activemask(), ended);
         if (ended) {
             const unsigned peers = __match_any_sync(m, req);

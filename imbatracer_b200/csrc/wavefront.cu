@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -48,6 +49,9 @@ struct imbart_pt_context {
     imbart_pt_profile* profile = nullptr;    // measurement of the traversal launches
     cudaEvent_t ev[2] = {nullptr, nullptr};
     unsigned long long* work = nullptr;      // device: closest nodes/tris/insts, shadow nodes/tris/insts
+    uint8_t* keys = nullptr;                 // material grouping: key per path
+    int* perm = nullptr;                     // shading order
+    int* key_counts = nullptr;               // 8 bucket sizes + 8 cursors
 };
 
 namespace imbart {
@@ -75,7 +79,19 @@ void free_ctx_buffers(imbart_pt_context* c) {
     }
     cudaFree(c->hits); cudaFree(c->srays); cudaFree(c->shits); cudaFree(c->spixel); cudaFree(c->scontrib);
     c->hits = nullptr; c->srays = nullptr; c->shits = nullptr; c->spixel = nullptr; c->scontrib = nullptr;
+    cudaFree(c->keys); cudaFree(c->perm); cudaFree(c->key_counts);
+    c->keys = nullptr; c->perm = nullptr; c->key_counts = nullptr;
     c->cap = 0;
+}
+
+// Grouping of each wavefront's paths by material before shading: IMBART_PT_SORT=0 turns it
+// off (for comparison); on by default.
+bool sort_by_material() {
+    static const int v = [] {
+        const char* e = std::getenv("IMBART_PT_SORT");
+        return e && *e ? std::atoi(e) : 1;
+    }();
+    return v != 0;
 }
 
 bool ensure_capacity(imbart_pt_context* c, long long n) {
@@ -86,7 +102,8 @@ bool ensure_capacity(imbart_pt_context* c, long long n) {
         good = dev_alloc(&c->rays[k], 2 * n) && dev_alloc(&c->pixel[k], n) && dev_alloc(&c->rng[k], n) &&
                dev_alloc(&c->thr[k], n) && dev_alloc(&c->bounces[k], n);
     good = good && dev_alloc(&c->hits, n) && dev_alloc(&c->srays, 2 * n) && dev_alloc(&c->shits, n) &&
-           dev_alloc(&c->spixel, n) && dev_alloc(&c->scontrib, n);
+           dev_alloc(&c->spixel, n) && dev_alloc(&c->scontrib, n) && dev_alloc(&c->keys, n) &&
+           dev_alloc(&c->perm, n) && dev_alloc(&c->key_counts, 2 * kShadeKeys);
     if (!good) { free_ctx_buffers(c); return false; }
     c->cap = n;
     return true;
@@ -339,6 +356,17 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
             p.s_rays = ctx->srays; p.s_pixel = ctx->spixel; p.s_contrib = ctx->scontrib;
             p.counts = ctx->counts;
             p.image = image;
+            if (sort_by_material()) {
+                // Group the wavefront's paths by material kind before shading.
+                if (!ok(cudaMemsetAsync(ctx->key_counts, 0, sizeof(int) * 2 * kShadeKeys, st), "cudaMemsetAsync")) {
+                    rc = IMBART_ERR_CUDA;
+                    break;
+                }
+                shade_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(sh->s, ctx->hits, n, ctx->keys, ctx->key_counts);
+                shade_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(ctx->keys, n, ctx->key_counts, ctx->perm);
+                note_launches(2);
+                p.perm = ctx->perm;
+            }
             pt_shade_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(p);
             note_launches(1);
             if (!ok(cudaGetLastError(), "shade kernel") ||
