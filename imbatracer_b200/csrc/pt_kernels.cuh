@@ -27,6 +27,7 @@ struct imbart_shading {
     int device = 0;
     imbart::sh::ShadingScene s{};
     std::vector<void*> allocations;
+    unsigned kind_mask = 0;     // bit k: some material has kind k (grouping pays only for several)
 };
 
 namespace imbart {
@@ -86,6 +87,15 @@ __global__ void emitter_area_kernel(const float* vertices, const int4* tris, int
 
 // Host-side decoding of the material / light arrays of imbart_shading_create(_ex). With
 // textures, params[12] / params[13] are the diffuse-texture / bump-map indices (< 0: none).
+// Bit k set when some material has kind k. Emitters are left out: a path that hits one
+// ends after a few instructions, so they add no divergence worth grouping for.
+inline unsigned material_kind_mask(const std::vector<Material>& mats) {
+    unsigned m = 0;
+    for (const Material& x : mats)
+        if (x.kind != kEmissive) m |= 1u << (x.kind & 7);
+    return m;
+}
+
 inline std::vector<Material> decode_materials(const int* kind, const float* params, int n, bool textured) {
     std::vector<Material> mats(n);
     for (int m = 0; m < n; ++m) {
@@ -368,6 +378,24 @@ __global__ void __launch_bounds__(256) shade_key_kernel(ShadingScene s, const in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const int k = shade_key(s, hits[i]);
+        keys[i] = (uint8_t)k;
+        atomicAdd(&hist[k], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+}
+
+// The same keys for a merged wavefront: each path's hit is looked up in its request's scene.
+__global__ void __launch_bounds__(256) shade_key_multi_kernel(const ReqDev* __restrict__ reqs,
+                                                              const ShadingScene* __restrict__ scenes,
+                                                              const int* __restrict__ req, const int4* __restrict__ hits,
+                                                              int n, uint8_t* keys, int* counts) {
+    __shared__ int hist[kShadeKeys];
+    if (threadIdx.x < kShadeKeys) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int k = shade_key(scenes[reqs[req[i]].scene_slot], hits[i]);
         keys[i] = (uint8_t)k;
         atomicAdd(&hist[k], 1);
     }

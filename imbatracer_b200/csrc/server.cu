@@ -66,6 +66,9 @@ constexpr size_t kBlockAlign = 3840;        // lcm(80, 48, 64, 256)
 constexpr size_t kArrayAlign = 256;
 constexpr int kMaxReqSlots = 4096;          // admitted requests at once
 constexpr int kMaxSceneSlots = 1024;        // resident scenes at once
+// Registered scenes. The record vector is reserved once, so the worker threads can read it
+// while scenes are added (a push_back never reallocates).
+constexpr size_t kMaxScenes = 1 << 16;
 constexpr size_t kMaxPoolBytes = 160ull << 30;   // node indices of the pool stay below 2^31
 
 bool cuda_check(cudaError_t e, const char* what) {
@@ -190,6 +193,7 @@ struct SceneRec {
     bool has_env = false;
     float env[3] = {0, 0, 0};
     int env_map = 0;              // 1 + environment image texture, 0: constant
+    unsigned kind_mask = 0;       // material kinds present (bit per kind)
     float env_intensity = 0.0f;
     float bsphere[5] = {0, 0, 0, 0, 0};
     // Block layout (byte offsets from the block start).
@@ -265,6 +269,9 @@ struct imbart_server {
     RootRun* h_runs = nullptr;            // pinned
     int* d_counts = nullptr;
     int* h_counts = nullptr;              // pinned
+    uint8_t* keys = nullptr;              // material grouping of a wavefront
+    int* perm = nullptr;
+    int* key_counts = nullptr;
     std::vector<int> free_req_slots, free_scene_slots;
 
     // Path queues (double-buffered), shadow queue, hits.
@@ -738,9 +745,26 @@ bool batched_wave(imbart_server* S) {
             p.req = S->req[cur]; p.root = S->root[cur];
             p.o_req = S->req[nxt]; p.o_root = S->root[nxt]; p.s_req = S->sreq; p.s_root = S->sroot;
             p.terminated = S->d_terminated;
-            pt_shade_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(p);
-            note_launches(1);
-            good = cuda_check(cudaGetLastError(), "shade kernel") &&
+            // Group the paths by material kind (RayQueue::sort_by_material) before shading.
+            // Only when the active renders' scenes hold more than one material kind.
+            unsigned kinds = 0;
+            for (Request* r : S->active_renders) kinds |= S->scenes[r->scene]->kind_mask;
+            const bool group = __builtin_popcount(kinds) > 1;
+            const bool zeroed =
+                !group ||
+                cuda_check(cudaMemsetAsync(S->key_counts, 0, sizeof(int) * 2 * kShadeKeys, st), "cudaMemsetAsync");
+            if (zeroed) {
+                if (group) {
+                    shade_key_multi_kernel<<<(n + 255) / 256, 256, 0, st>>>(S->d_reqs, S->d_scenes, S->req[cur],
+                                                                             S->hits, n, S->keys, S->key_counts);
+                    shade_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(S->keys, n, S->key_counts, S->perm);
+                    note_launches(2);
+                    p.perm = S->perm;
+                }
+                pt_shade_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(p);
+                note_launches(1);
+            }
+            good = zeroed && cuda_check(cudaGetLastError(), "shade kernel") &&
                    launch_trace_internal(S->pool_scene, S->srays, S->shits, nullptr, n, IMBART_TRACE_ANY, st, nullptr,
                                          S->sroot, S->d_counts + 1) == 0;
             if (good) {
@@ -1065,6 +1089,7 @@ void free_server(imbart_server* S) {
         if (lane.stream && lane.stream != S->stream) cudaStreamDestroy(lane.stream);
     }
     void* dev[] = {S->pool, S->d_reqs, S->d_scenes, S->d_terminated, S->d_chunks, S->d_runs, S->d_counts,
+                   S->keys, S->perm, S->key_counts,
                    S->hits, S->srays, S->shits, S->spixel, S->scontrib, S->sreq, S->sroot, S->b_rays, S->b_hits,
                    S->b_roots, S->plain_image, S->plain_rays, S->plain_hits};
     for (void* p : dev) cudaFree(p);
@@ -1097,6 +1122,7 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
     S->device = device;
     S->mode = mode;
     S->t0 = std::chrono::steady_clock::now();
+    S->scenes.reserve(kMaxScenes);
     S->cap = max_paths_in_flight > 0 ? std::min(max_paths_in_flight, (long long)(1 << 30)) : (4ll << 20);
     bool good = cuda_check(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking), "cudaStreamCreate") &&
                 cuda_check(cudaStreamCreateWithFlags(&S->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -1116,6 +1142,7 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
                dalloc(&S->d_runs, kMaxReqSlots) && halloc(&S->h_runs, kMaxReqSlots) &&
                dalloc(&S->d_counts, 4) && halloc(&S->h_counts, 4) &&
                dalloc(&S->hits, cap) && dalloc(&S->srays, 2 * cap) && dalloc(&S->shits, cap) &&
+               dalloc(&S->keys, cap) && dalloc(&S->perm, cap) && dalloc(&S->key_counts, 2 * kShadeKeys) &&
                dalloc(&S->spixel, cap) && dalloc(&S->scontrib, cap) && dalloc(&S->sreq, cap) &&
                dalloc(&S->sroot, cap) && dalloc(&S->b_rays, cap) && dalloc(&S->b_hits, cap) &&
                dalloc(&S->b_roots, cap) && halloc(&S->stage_rays, cap) && halloc(&S->stage_hits, cap);
@@ -1216,6 +1243,7 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         s->tex_pixels = vec(src->tex_pixels, 4 * (size_t)texels);
     }
     s->mats = decode_materials(src->mat_kind, src->mat_params, src->n_mats, src->n_textures > 0);
+    s->kind_mask = material_kind_mask(s->mats);
     for (const Material& m : s->mats)
         if (m.tex >= src->n_textures || m.bump >= src->n_textures) {
             set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: texture index out of range");
@@ -1244,6 +1272,10 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->mode == IMBART_SERVE_BATCHED && s->bytes > S->pool_bytes) {
         set_error(IMBART_ERR_LIMIT, "imbart_server_add_scene: scene larger than the pool");
+        return -IMBART_ERR_LIMIT;
+    }
+    if (S->scenes.size() >= kMaxScenes) {
+        set_error(IMBART_ERR_LIMIT, "imbart_server_add_scene: too many scenes");
         return -IMBART_ERR_LIMIT;
     }
     S->scenes.push_back(std::move(s));

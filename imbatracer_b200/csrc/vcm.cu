@@ -153,6 +153,23 @@ __global__ void light_gen_kernel(VcmParams p, const LightTile* tiles, int n_tile
     rng_out[j] = rng.state;
 }
 
+// Material grouping keys of light-path slots (pt::shade_key; finished slots get key 7).
+__global__ void __launch_bounds__(256) light_key_kernel(ShadingScene s, const int4* __restrict__ hits,
+                                                        const float4* __restrict__ thrs, int n, uint8_t* keys,
+                                                        int* counts) {
+    __shared__ int hist[pt::kShadeKeys];
+    if (threadIdx.x < pt::kShadeKeys) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int k = __float_as_int(thrs[i].w) < 0 ? 7 : pt::shade_key(s, hits[i]);
+        keys[i] = (uint8_t)k;
+        atomicAdd(&hist[k], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < pt::kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+}
+
 // connect_to_camera (vcm.cpp:260-320): a shadow ray towards the camera. Returns false when the
 // vertex does not project into the image or the BSDF cannot reach the camera.
 __device__ __forceinline__ bool camera_connection(const VcmParams& p, V3 thr, float dVC, float dVCM, const Isect& is,
@@ -198,8 +215,10 @@ __device__ __forceinline__ bool camera_connection(const VcmParams& p, V3 thr, fl
 __global__ void __launch_bounds__(128) light_shade_kernel(VcmParams p, int n, float4* rays, const int4* hits,
                                                           unsigned long long* rngs, float4* thrs, float4* ws,
                                                           float4* stage, int* vflags, float4* s_rays, int* s_pixel,
-                                                          float4* s_contrib) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                          float4* s_contrib, const int* perm) {
+    // Thread t shades slot perm[t] (slots grouped by material); every write goes to the slot.
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (perm && t < n) ? perm[t] : t;
     bool alive = false, vertex = false, shadow = false;
     float4 s_org = make_float4(0, 0, 0, 0), s_dir = s_org;
     int s_pix = 0;
@@ -661,8 +680,9 @@ __global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const 
 __global__ void __launch_bounds__(128) vcm_camera_shade_kernel(
     VcmParams p, int n, const float4* rays, const int4* hits, const int* pixels, const unsigned long long* rngs,
     const float4* thrs, const float4* ws, float4* o_rays, int* o_pixel, unsigned long long* o_rng, float4* o_thr,
-    float4* o_w, float4* s_rays, int* s_pixel, float4* s_contrib, float4* merge_recs) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float4* o_w, float4* s_rays, int* s_pixel, float4* s_contrib, float4* merge_recs, const int* perm) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (perm && t < n) ? perm[t] : t;
     bool alive = false;
     float4 o_org = make_float4(0, 0, 0, 0), o_dir = o_org;
     Rng rng{0};
@@ -896,6 +916,12 @@ struct imbart_vcm {
     float4* c_w[2] = {nullptr, nullptr};
     int4* c_hits = nullptr;
     float4* c_merge = nullptr;      // queued camera vertices for merging (7 float4 each)
+    // Material grouping of a wavefront (keys, shading order, 8 bucket sizes + 8 cursors).
+    long long sort_cap = 0;
+    bool use_perm = false;
+    uint8_t* keys = nullptr;
+    int* perm = nullptr;
+    int* key_counts = nullptr;
     // shadow queue
     long long s_cap = 0;
     float4* s_rays = nullptr;
@@ -913,7 +939,8 @@ namespace imbart {
 namespace {
 
 void free_vcm(imbart_vcm* v) {
-    void* ptrs[] = {v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage, v->vflags, v->bsums, v->d_tiles,
+    void* ptrs[] = {v->keys, v->perm, v->key_counts,
+                    v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage, v->vflags, v->bsums, v->d_tiles,
                     v->cache, v->c_hits, v->c_merge, v->s_rays, v->s_hits, v->s_pixel, v->s_contrib, v->counts};
     for (void* p : ptrs) cudaFree(p);
     for (int k = 0; k < 2; ++k) {
@@ -938,6 +965,26 @@ bool ensure_shadow(imbart_vcm* v, long long need) {
                       realloc_exact(&v->s_pixel, (size_t)need) && realloc_exact(&v->s_contrib, (size_t)need);
     v->s_cap = good ? need : 0;
     return good;
+}
+
+// The shading order of a wavefront of n paths: keys from `key_launch(keys, counts)`, then the
+// counting-sort scatter into v->perm (pt::shade_scatter_kernel).
+template <typename KeyLaunch>
+bool group_paths(imbart_vcm* v, const imbart_shading* sh, int n, cudaStream_t s, KeyLaunch key_launch) {
+    v->use_perm = __builtin_popcount(sh->kind_mask) > 1;    // one kind: nothing to group
+    if (!v->use_perm) return true;
+    if (v->sort_cap < n) {
+        const long long c = std::max<long long>(n, v->sort_cap * 3 / 2);
+        const bool good = realloc_exact(&v->keys, (size_t)c) && realloc_exact(&v->perm, (size_t)c) &&
+                          realloc_exact(&v->key_counts, 2 * pt::kShadeKeys);
+        v->sort_cap = good ? c : 0;
+        if (!good) return false;
+    }
+    if (!ok(cudaMemsetAsync(v->key_counts, 0, sizeof(int) * 2 * pt::kShadeKeys, s), "cudaMemsetAsync")) return false;
+    key_launch(v->keys, v->key_counts);
+    pt::shade_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(v->keys, n, v->key_counts, v->perm);
+    note_launches(2);
+    return ok(cudaGetLastError(), "grouping kernels");
 }
 
 VcmParams make_params(const imbart_vcm* v, const imbart_shading* sh, const imbart_camera* cam,
@@ -1199,8 +1246,14 @@ int imbart_vcm_light_pass_range(imbart_vcm* v, const imbart_scene* scene, const 
         }
         p.cache = v->cache;
         if (!ok(cudaMemsetAsync(v->counts, 0, sizeof(int) * 4, s), "cudaMemsetAsync")) { rc = IMBART_ERR_CUDA; break; }
+        if (!group_paths(v, sh, P, s, [&](uint8_t* keys, int* counts) {
+                light_key_kernel<<<(P + 255) / 256, 256, 0, s>>>(p.s, v->l_hits, v->l_thr, P, keys, counts);
+            })) {
+            rc = IMBART_ERR_CUDA;
+            break;
+        }
         light_shade_kernel<<<grid, 128, 0, s>>>(p, P, v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage,
-                                                v->vflags, v->s_rays, v->s_pixel, v->s_contrib);
+                                                v->vflags, v->s_rays, v->s_pixel, v->s_contrib, v->use_perm ? v->perm : nullptr);
         flag_count_kernel<<<n_blocks, kScanBlock, 0, s>>>(v->vflags, P, v->bsums);
         block_scan_kernel<<<1, kScanBlock, 0, s>>>(v->bsums, n_blocks);
         vertex_scatter_kernel<<<n_blocks, kScanBlock, 0, s>>>(v->vflags, P, v->bsums, v->stage, v->cache,
@@ -1339,10 +1392,16 @@ int imbart_vcm_camera_pass_range(imbart_vcm* v, const imbart_scene* scene, const
             ++n_waves;
             if (!ok(cudaMemsetAsync(v->counts, 0, sizeof(int) * 4, s), "cudaMemsetAsync")) { rc = IMBART_ERR_CUDA; break; }
             const int nxt = 1 - cur;
+            if (!group_paths(v, sh, n, s, [&](uint8_t* keys, int* counts) {
+                    pt::shade_key_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.s, v->c_hits, n, keys, counts);
+                })) {
+                rc = IMBART_ERR_CUDA;
+                break;
+            }
             vcm_camera_shade_kernel<<<(n + 127) / 128, 128, 0, s>>>(
                 p, n, v->c_rays[cur], v->c_hits, v->c_pixel[cur], v->c_rng[cur], v->c_thr[cur], v->c_w[cur],
                 v->c_rays[nxt], v->c_pixel[nxt], v->c_rng[nxt], v->c_thr[nxt], v->c_w[nxt], v->s_rays, v->s_pixel,
-                v->s_contrib, v->c_merge);
+                v->s_contrib, v->c_merge, v->use_perm ? v->perm : nullptr);
             note_launches(1);
             if (p.merging && (st->algorithm == IMBART_VCM || st->algorithm == IMBART_PPM)) {
                 if (st->num_knn <= 32)   // one warp per queued vertex

@@ -152,6 +152,7 @@ imbart_shading* imbart_shading_create_ex(int device, const float* vertices, int 
     if (!ok(cudaSetDevice(device), "cudaSetDevice")) return nullptr;
     imbart_shading* h = new imbart_shading;
     h->device = device;
+    h->kind_mask = material_kind_mask(mats);
     ShadingScene& s = h->s;
     auto upl = [&](const void* src, size_t bytes) -> void* {
         void* d = nullptr;
@@ -356,7 +357,7 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
             p.s_rays = ctx->srays; p.s_pixel = ctx->spixel; p.s_contrib = ctx->scontrib;
             p.counts = ctx->counts;
             p.image = image;
-            if (sort_by_material()) {
+            if (sort_by_material() && __builtin_popcount(sh->kind_mask) > 1) {
                 // Group the wavefront's paths by material kind before shading.
                 if (!ok(cudaMemsetAsync(ctx->key_counts, 0, sizeof(int) * 2 * kShadeKeys, st), "cudaMemsetAsync")) {
                     rc = IMBART_ERR_CUDA;
