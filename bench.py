@@ -198,6 +198,18 @@ def run_pt(args):
     pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
     W, H = desc.camera.width, desc.camera.height
     stream = torch.cuda.current_stream(dev)
+    # Autotuner (untimed): the kernel configuration of each query class on this scene's rays.
+    tuning = {}
+    if not args.no_autotune:
+        sets = make_wavefront(desc, gs.trace_scene, torch, dev, 4321)
+        for (rays, any_hit), name, flags in zip(sets, ("camera", "bounce", "shadow"),
+                                                (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)):
+            hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
+            t = gs.trace_scene.autotune(rays, hits, flags, stream=stream)
+            tuning[name] = {"variant": t["variant"], "refill": t["refill"],
+                            "speedup": round(t["default_ms"] / max(t["ms"], 1e-9), 3)}
+        del sets
+        torch.cuda.synchronize()
     image = torch.zeros((H, W, 3), dtype=torch.float32, device=dev)
     base_seed = 1000 * (rank + 1)
 
@@ -310,6 +322,7 @@ def run_pt(args):
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 16 * 4 + 12,
                     "d2h_bytes_per_step": W * H * 12},
             "gpu_launches": int(launches),
+            "autotune": tuning,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
@@ -649,6 +662,7 @@ def main():
     ap.add_argument("--mode", default="pt", choices=["pt", "trace", "serve", "vcm"])
     ap.add_argument("--no-vcm", action="store_true", help="pt mode: skip the VCM-family iterations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="pt mode: keep the default kernel configurations")
     ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
     ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
                     help="serve mode: config 5 arrival rates (req/s)")

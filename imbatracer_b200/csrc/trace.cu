@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <climits>
 #include <cstring>
 #include <map>
@@ -130,13 +131,17 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 // imbart_set_trace_variant_any, or IMBART_TRACE_VARIANT, IMBART_TRACE_VARIANT_ANY,
 // IMBART_TRACE_REFILL and IMBART_TRACE_POSTPONE in the environment).
 // ---------------------------------------------------------------------------------------
+// Three query classes keep their own variant and refill threshold: incoherent closest hit,
+// any hit, and closest hit over coherent rays (camera rays, flag IMBART_TRACE_COHERENT),
+// which traverse best in static batches (refill only when the whole warp is idle).
 struct TraceConfig {
     int variant, refill, postpone, variant_any;
+    int refill_any, variant_coh, refill_coh;
 };
 
 std::mutex g_cfg_mutex;
 bool g_cfg_init = false;
-TraceConfig g_cfg{4, 24, 0, 6};
+TraceConfig g_cfg{4, 12, 0, 6, 24, 4, 32};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -149,6 +154,9 @@ TraceConfig current_config() {
         g_cfg.variant = env_int("IMBART_TRACE_VARIANT", g_cfg.variant);
         g_cfg.variant_any = env_int("IMBART_TRACE_VARIANT_ANY", g_cfg.variant_any);
         g_cfg.refill = env_int("IMBART_TRACE_REFILL", g_cfg.refill);
+        g_cfg.refill_any = env_int("IMBART_TRACE_REFILL_ANY", g_cfg.refill_any);
+        g_cfg.variant_coh = env_int("IMBART_TRACE_VARIANT_COHERENT", g_cfg.variant_coh);
+        g_cfg.refill_coh = env_int("IMBART_TRACE_REFILL_COHERENT", g_cfg.refill_coh);
         g_cfg.postpone = env_int("IMBART_TRACE_POSTPONE", g_cfg.postpone);
         g_cfg_init = true;
     }
@@ -263,9 +271,11 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
     p.error_flags = s->error_flags;
     p.stats = stats;
     const bool any = (flags & IMBART_TRACE_ANY) != 0;
+    const bool coherent = !any && (flags & IMBART_TRACE_COHERENT) != 0;
     const bool masked = s->info.masked != 0;
     const TraceConfig cfg = current_config();
-    const int variant = any ? cfg.variant_any : cfg.variant;
+    const int variant = any ? cfg.variant_any : coherent ? cfg.variant_coh : cfg.variant;
+    const int refill = any ? cfg.refill_any : coherent ? cfg.refill_coh : cfg.refill;
     bool launched;
     if (variant == 0) {
         const int block = 128;
@@ -276,7 +286,7 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
         int* work = work_slot(s->device);
         if (!work) return IMBART_ERR_CUDA;
         p.work = work;
-        p.refill_lanes = std::min(std::max(cfg.refill, 1), 32);
+        p.refill_lanes = std::min(std::max(refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
         if (stats) launched = dispatch_persistent<true>(variant, any, masked, count, s->device, stream, p);
         else launched = dispatch_persistent<false>(variant, any, masked, count, s->device, stream, p);
@@ -610,8 +620,87 @@ int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
     }
     current_config();
     std::lock_guard<std::mutex> lk(g_cfg_mutex);
-    g_cfg = TraceConfig{variant, refill_lanes, postpone_lanes, variant};
+    g_cfg.variant = variant;
+    g_cfg.refill = refill_lanes;
+    g_cfg.postpone = postpone_lanes;
+    g_cfg.variant_any = variant;
+    g_cfg.variant_coh = variant;
     return 0;
+}
+
+int imbart_set_trace_class(int flags, int variant, int refill_lanes) {
+    if (variant < 0 || variant > 7 || refill_lanes < 1 || refill_lanes > 32 || flags < 0 || flags > 3) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_class: out of range");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    current_config();
+    std::lock_guard<std::mutex> lk(g_cfg_mutex);
+    if (flags & IMBART_TRACE_ANY) { g_cfg.variant_any = variant; g_cfg.refill_any = refill_lanes; }
+    else if (flags & IMBART_TRACE_COHERENT) { g_cfg.variant_coh = variant; g_cfg.refill_coh = refill_lanes; }
+    else { g_cfg.variant = variant; g_cfg.refill = refill_lanes; }
+    return 0;
+}
+
+int imbart_get_trace_class(int flags, int* variant, int* refill_lanes) {
+    const TraceConfig c = current_config();
+    const bool any = (flags & IMBART_TRACE_ANY) != 0, coh = !any && (flags & IMBART_TRACE_COHERENT) != 0;
+    if (variant) *variant = any ? c.variant_any : coh ? c.variant_coh : c.variant;
+    if (refill_lanes) *refill_lanes = any ? c.refill_any : coh ? c.refill_coh : c.refill;
+    return 0;
+}
+
+int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count, int flags,
+                          void* stream, imbart_trace_tuning* out) {
+    if (!scene || !rays || !hits || count <= 0 || flags < 0 || flags > 3) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace_autotune: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(scene->device);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int v0 = 0, r0 = 0;
+    imbart_get_trace_class(flags, &v0, &r0);
+    // Time one configuration: a warm-up launch, then the mean of three.
+    auto time_config = [&](int variant, int refill, float* ms) -> int {
+        int rc = imbart_set_trace_class(flags, variant, refill);
+        for (int k = 0; k < 4 && !rc; ++k) {
+            if (k == 1) cudaEventRecord(e0, st);
+            rc = launch_trace(scene, rays, hits, nullptr, count, flags, st);
+        }
+        if (rc) return rc;
+        cudaEventRecord(e1, st);
+        if (!cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize")) return IMBART_ERR_CUDA;
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= 3.0f;
+        return 0;
+    };
+    static const int kRefills[] = {8, 16, 24, 32};
+    float default_ms = 0.0f, best_ms = FLT_MAX;
+    int best_v = v0, best_r = r0;
+    int rc = time_config(v0, r0, &default_ms);
+    if (!rc) { best_ms = default_ms; }
+    for (int v = 1; v <= 7 && !rc; ++v)
+        for (int r : kRefills) {
+            float ms = 0.0f;
+            rc = time_config(v, r, &ms);
+            if (rc) break;
+            if (ms < best_ms) { best_ms = ms; best_v = v; best_r = r; }
+        }
+    imbart_set_trace_class(flags, rc ? v0 : best_v, rc ? r0 : best_r);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaSetDevice(prev);
+    if (!rc && out) {
+        out->variant = best_v;
+        out->refill = best_r;
+        out->ms = best_ms;
+        out->default_ms = default_ms;
+    }
+    return rc;
 }
 
 int imbart_set_trace_variant_any(int variant) {

@@ -315,7 +315,7 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     }
     // One traversal launch, timed / counted when profiling.
     auto trace = [&](const void* rays, void* hits, int count, int flags) -> int {
-        const bool any = flags == IMBART_TRACE_ANY;
+        const bool any = (flags & IMBART_TRACE_ANY) != 0;
         unsigned long long* work = (prof && prof->work) ? ctx->work + (any ? 3 : 0) : nullptr;
         if (prof && prof->events) cudaEventRecord(ctx->ev[0], st);
         const int r = launch_trace_internal(scene, rays, hits, nullptr, count, flags, st, work);
@@ -338,8 +338,11 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
         camera_kernel<<<(n + 127) / 128, 128, 0, st>>>(c, first, n, ctx->rays[cur], ctx->pixel[cur], ctx->rng[cur],
                                                        ctx->thr[cur], ctx->bounces[cur], nullptr);
         note_launches(1);
+        bool camera_rays = true;   // the first wavefront of a sample range: coherent camera rays
         while (n > 0) {
-            rc = trace(ctx->rays[cur], ctx->hits, n, IMBART_TRACE_CLOSEST);
+            rc = trace(ctx->rays[cur], ctx->hits, n,
+                       camera_rays ? (IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT) : IMBART_TRACE_CLOSEST);
+            camera_rays = false;
             if (rc) break;
             n_closest += n;
             ++n_waves;

@@ -29,6 +29,7 @@ assert NODE2_DTYPE.itemsize == 64 and NODE4_DTYPE.itemsize == 112 and INST_DTYPE
 
 TRACE_CLOSEST = 0
 TRACE_ANY = 1
+TRACE_COHERENT = 2
 
 
 class SceneInfo(C.Structure):
@@ -72,6 +73,10 @@ class SceneSource(C.Structure):
                 ("env_color", C.c_void_p), ("bsphere", C.c_void_p), ("light_kinds", C.c_void_p),
                 ("tex_dims", C.c_void_p), ("tex_pixels", C.c_void_p), ("n_textures", C.c_int),
                 ("env_map", C.c_int), ("env_intensity", C.c_float)]
+
+
+class TraceTuning(C.Structure):
+    _fields_ = [("variant", C.c_int), ("refill", C.c_int), ("ms", C.c_float), ("default_ms", C.c_float)]
 
 
 class MeshDesc(C.Structure):
@@ -161,6 +166,9 @@ _SIGNATURES = {
     "imbart_build_mesh_node2": (I, [P, I, I, P, I, I, I, P, I, P, P, I, P]),
     "imbart_build_mesh_node2_ex": (I, [P, I, I, P, I, I, I, C.c_float, P, I, P, P, I, P]),
     "imbart_accel_file_info": (I, [C.c_char_p, I, P, P]),
+    "imbart_set_trace_class": (I, [I, I, I]),
+    "imbart_get_trace_class": (I, [I, P, P]),
+    "imbart_trace_autotune": (I, [P, P, P, I, I, P, C.POINTER(TraceTuning)]),
     "imbart_shading_set_env_map": (I, [P, I, C.c_float]),
     "imbart_scene_build_gpu": (P, [C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, I, P, C.POINTER(C.c_float)]),
     "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),

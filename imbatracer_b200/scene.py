@@ -266,6 +266,15 @@ class DeviceScene:
                                    N.TRACE_ANY if any_hit else N.TRACE_CLOSEST, st)
         N.check(rc, "imbart_trace_host")
 
+    def autotune(self, rays, hits, flags: int, stream=None) -> dict:
+        """imbart_trace_autotune on device tensors: picks the kernel configuration of the query
+        class `flags` (TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST | TRACE_COHERENT) for these rays."""
+        t = N.TraceTuning()
+        st = None if stream is None else stream.cuda_stream
+        N.check(N.load().imbart_trace_autotune(self.handle, N.ptr(rays), N.ptr(hits), rays.shape[0], flags, st,
+                                               C.byref(t)), "imbart_trace_autotune")
+        return {"variant": t.variant, "refill": t.refill, "ms": t.ms, "default_ms": t.default_ms}
+
     def device_arrays(self):
         lib = N.load()
         a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()

@@ -194,8 +194,10 @@ int imbart_scene_get_info(const imbart_scene* scene, imbart_scene_info* out);
 int imbart_scene_get_device_arrays(const imbart_scene* scene, const void** nodes,
                                    const void** tris, const void** instances);
 
-/* Trace flags. */
-enum { IMBART_TRACE_CLOSEST = 0, IMBART_TRACE_ANY = 1 };
+/* Trace flags. IMBART_TRACE_COHERENT (with closest hit) marks coherent rays, such as camera
+ * rays in pixel order: they run with their own kernel configuration (see
+ * imbart_set_trace_class). Hits never depend on the flags. */
+enum { IMBART_TRACE_CLOSEST = 0, IMBART_TRACE_ANY = 1, IMBART_TRACE_COHERENT = 2 };
 
 /* Traces `count` rays from DEVICE buffers, stream-ordered on `stream` (a cudaStream_t,
  * NULL = legacy default stream). Returns 0 or an error code; does not synchronize. */
@@ -238,6 +240,27 @@ int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes);
 int imbart_set_trace_variant_any(int variant);
 int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes);
 int imbart_get_trace_variant_any(void);
+
+/* The configuration of one query class: flags IMBART_TRACE_CLOSEST (incoherent closest hit),
+ * IMBART_TRACE_ANY, or IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT. variant 1..7 (threads
+ * per block x blocks per SM x shared stack entries of the persistent kernel, 0: one ray per
+ * thread), refill_lanes: idle lanes a warp waits for before it fetches new rays. */
+int imbart_set_trace_class(int flags, int variant, int refill_lanes);
+int imbart_get_trace_class(int flags, int* variant, int* refill_lanes);
+
+/* Autotuner: times every persistent-kernel configuration of the query class of `flags`
+ * (variants 1..7 x refill 8, 16, 24, 32; one warm-up and three timed launches each, CUDA
+ * events on `stream`) on `count` DEVICE rays, keeps the fastest as the class's configuration
+ * and reports it with the time of the configuration it replaced. Hits are written to `hits`.
+ * Run it on rays like those the class will trace (camera rays, bounce rays, shadow rays). */
+typedef struct {
+    int variant;
+    int refill;
+    float ms;          /* per launch, the chosen configuration */
+    float default_ms;  /* per launch, the configuration before tuning */
+} imbart_trace_tuning;
+int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count, int flags,
+                          void* stream, imbart_trace_tuning* out);
 
 /* ------------------------------------------------------------------------------------ */
 /* Photon hash grid (replaces HashGrid::build / HashGrid::query, rangesearch.h:25-129,     */

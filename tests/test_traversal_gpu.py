@@ -202,3 +202,42 @@ def test_empty_and_zero_count(cuda):
     d = torch.zeros(64, dtype=torch.uint8, device="cuda")
     assert lib.imbart_trace(ds.handle, N.ptr(d), N.ptr(d), 0, 0, None) == 0
     assert lib.imbart_trace(ds.handle, N.ptr(d), N.ptr(d), -1, 0, None) == 1
+
+
+def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
+    """imbart_trace_autotune times the persistent-kernel configurations of a query class and
+    keeps the fastest; the hits of every class stay bit-exact afterwards."""
+    import ctypes as C
+    import torch
+    lib = N.load()
+    saved = {}
+    for flags in (N.TRACE_CLOSEST, N.TRACE_ANY, N.TRACE_CLOSEST | N.TRACE_COHERENT):
+        v, r = C.c_int(0), C.c_int(0)
+        lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
+        saved[flags] = (v.value, r.value)
+    try:
+        td = H.traversal_data("config2")
+        ds = S.DeviceScene(td)
+        rays = H.ray_set("config2", 50000, seed=12)
+        dev = torch.device("cuda:0")
+        d_rays = to_dev(rays, torch, dev)
+        d_hits = torch.zeros(len(rays) * 16, dtype=torch.uint8, device=dev)
+        for flags in saved:
+            t = N.TraceTuning()
+            N.check(lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), len(rays), flags, None,
+                                              C.byref(t)), "autotune")
+            assert 1 <= t.variant <= 7 and t.refill in (8, 16, 24, 32) and 0 < t.ms <= t.default_ms * 1.0001
+            v, r = C.c_int(0), C.c_int(0)
+            lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
+            assert (v.value, r.value) == (t.variant, t.refill)
+        ref = O.trace_node2(td, rays)
+        hits, _, _ = run_gpu(ds, rays)
+        assert H.hits_equal(ref, hits).all()
+        refa = O.trace_node2(td, rays, any_hit=True)
+        hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
+        assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0)
+        assert lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), 0, 0, None, None) != 0
+        lib.imbart_clear_error()
+    finally:
+        for flags, (v, r) in saved.items():
+            lib.imbart_set_trace_class(flags, v, r)
