@@ -17,7 +17,8 @@ void set_error(int code, const std::string& msg) {
     g_msg = msg;
 }
 
-// Process-wide count of kernel launches issued by libimbart.
+// Process-wide count of kernel launches issued by libimbart (a CUDA graph's kernels are
+// counted when the graph is launched).
 static std::atomic<long long> g_launches{0};
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launches_total() { return g_launches.load(std::memory_order_relaxed); }

@@ -2,6 +2,7 @@
 // sm_100a kernels. Nothing here is part of the C ABI.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
 #include <vector>
@@ -97,9 +98,24 @@ long long launches_total();
 // a cudaStream_t; rays are imbart_ray records, hits imbart_hit records.
 // `roots` (optional): per-ray root node for batches over several scenes of one pool;
 // `count_ptr` (optional): device-resident ray count, `count` being its upper bound.
+// `work` (optional): the persistent kernel's (next, done) counter pair, zeroed, owned by the
+// caller (a launch inside a CUDA graph keeps its own); otherwise one of the device's ring.
 int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
                           int flags, void* stream, unsigned long long* stats, const int* roots = nullptr,
-                          const int* count_ptr = nullptr);
+                          const int* count_ptr = nullptr, int* work = nullptr);
+
+// Adds one traversal launch (as launch_trace_internal with count_ptr and work) to `graph`
+// after `deps`, under the configuration in force; `count` > 0.
+int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, cudaGraphNode_t* node,
+                   const imbart_scene* scene, const void* rays, void* hits, int count, int flags,
+                   const int* count_ptr, int* work);
+
+// The traversal configuration in force (variant, refill, postpone, any-hit variant and refill,
+// coherent variant and refill): a captured launch is stale once it changes.
+void trace_config_snapshot(int out[7]);
+// Every scene value a traversal launch takes into its parameters (array pointers, root,
+// masks, device): two launches with equal keys and arguments are the same launch.
+void scene_launch_key(const imbart_scene* s, unsigned long long out[12]);
 
 // Device arrays of a built photon grid (hashgrid.cu): photons in bucket order (float4 xyz +
 // index bits), inclusive bucket ends, the 10 grid parameters; false before the first build.

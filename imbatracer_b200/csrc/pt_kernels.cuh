@@ -206,6 +206,21 @@ __global__ void camera_kernel(CameraParams c, long long first, int n, float4* ra
     if (sample_out) sample_out[j] = i % c.spp;
 }
 
+// camera_kernel with the camera and the sample range read on the device (`*cam`, `*first`,
+// `*n`: the state of a frame captured as a CUDA graph), walked with a grid stride.
+__global__ void camera_range_kernel(const CameraParams* cam, const long long* first, const int* n_ptr, float4* rays,
+                                    int* pixel, unsigned long long* rng_out, float4* thr, int* bounces) {
+    const CameraParams& c = *cam;
+    const long long f = *first;
+    const int n = *n_ptr;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        camera_sample(c.r2w, c.pos, c.spp, c.tile_left, c.tile_top, c.tile_w, c.full_w, c.seed_base, (int)(f + j),
+                      rays + 2 * j, pixel + j, rng_out + j);
+        thr[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        bounces[j] = 0;
+    }
+}
+
 // Camera samples of several requests, appended at queue position `offset`: thread j finds its
 // chunk by binary search over the chunks' out_begin.
 __global__ void camera_multi_kernel(const ReqDev* reqs, const GenChunk* chunks, int n_chunks, int n, int offset,
@@ -247,6 +262,7 @@ struct ShadeParams {
     int* o_req; int* o_root; int* s_req; int* s_root;
     int* terminated;         // per request slot: paths that ended
     const int* perm;         // optional: shade path perm[i] in thread i (paths grouped by material)
+    const int* n_ptr;        // optional: queue size read on the device (`n` is then its bound)
 };
 
 __device__ __forceinline__ void add_image(float* img, int pixel, V3 c) {
@@ -360,76 +376,168 @@ __device__ __forceinline__ void shade_path(const ShadingScene& s, int max_path_l
 // RayQueue::sort_by_material (ray_queue.h:211-244) for the device queue: the paths of a
 // wavefront grouped by what shading will run for them (material kind of the hit, or a miss),
 // so that the warps of the shading kernel follow one code path each. The reference sorts the
-// queue itself with a two-pass counting sort; here a permutation is built (keys with a
-// per-block histogram, then a scatter with warp-aggregated cursors) and the shading kernel
-// reads through it. Results per path do not depend on the order.
-constexpr int kShadeKeys = 8;   // material kinds 0..5, 6: miss
+// queue itself with a two-pass counting sort; here a permutation is built and the shading
+// kernel reads through it. The sort is a stable counting sort over tiles of kGroupTile
+// entries: per-tile key counts, one scan (key-major, tile-minor), then each tile places its
+// entries in index order. Stable, so paths that were neighbours in the queue (neighbouring
+// samples) stay neighbours within their group, and the permutation is deterministic. Results
+// per path do not depend on the order.
+constexpr int kShadeKeys = 8;   // material kinds 0..5, 6: miss (7: a finished light-path slot)
+constexpr int kGroupTile = 2048;
+
+inline int group_tiles(long long n) { return (int)((n + kGroupTile - 1) / kGroupTile); }
 
 __device__ __forceinline__ int shade_key(const ShadingScene& s, int4 h) {
     if (h.x < 0) return 6;
     return s.materials[s.tris[h.x].w].kind & 7;
 }
 
+// The grouping kernels take the queue size from `n`, or with `n_ptr` set read it on the
+// device (`n` then bounds it), so a launch sized for the bound can sit in a CUDA graph.
+__device__ __forceinline__ int queue_size(const int* n_ptr, int n) { return n_ptr ? min(*n_ptr, n) : n; }
+
 __global__ void __launch_bounds__(256) shade_key_kernel(ShadingScene s, const int4* __restrict__ hits, int n,
-                                                        uint8_t* keys, int* counts) {
-    __shared__ int hist[kShadeKeys];
-    if (threadIdx.x < kShadeKeys) hist[threadIdx.x] = 0;
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const int k = shade_key(s, hits[i]);
-        keys[i] = (uint8_t)k;
-        atomicAdd(&hist[k], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+                                                        const int* n_ptr, uint8_t* keys) {
+    n = queue_size(n_ptr, n);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        keys[i] = (uint8_t)shade_key(s, hits[i]);
 }
 
 // The same keys for a merged wavefront: each path's hit is looked up in its request's scene.
 __global__ void __launch_bounds__(256) shade_key_multi_kernel(const ReqDev* __restrict__ reqs,
                                                               const ShadingScene* __restrict__ scenes,
                                                               const int* __restrict__ req, const int4* __restrict__ hits,
-                                                              int n, uint8_t* keys, int* counts) {
-    __shared__ int hist[kShadeKeys];
-    if (threadIdx.x < kShadeKeys) hist[threadIdx.x] = 0;
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const int k = shade_key(scenes[reqs[req[i]].scene_slot], hits[i]);
-        keys[i] = (uint8_t)k;
-        atomicAdd(&hist[k], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+                                                              int n, const int* n_ptr, uint8_t* keys) {
+    n = queue_size(n_ptr, n);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        keys[i] = (uint8_t)shade_key(scenes[reqs[req[i]].scene_slot], hits[i]);
 }
 
-// counts[0..7]: keys per bucket; counts[8..15]: running cursors (zeroed before).
-__global__ void __launch_bounds__(256) shade_scatter_kernel(const uint8_t* __restrict__ keys, int n, int* counts,
-                                                            int* perm) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const int k = valid ? keys[i] : kShadeKeys;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned group = __match_any_sync(0xffffffffu, k);
-    if (!valid) return;
-    const int leader = __ffs(group) - 1;
-    int base = 0;
-    if ((int)lane == leader) base = atomicAdd(counts + kShadeKeys + k, __popc(group));
-    base = __shfl_sync(group, base, leader);
-    int off = 0;
-    for (int b = 0; b < k; ++b) off += __ldg(counts + b);
-    perm[off + base + __popc(group & ((1u << lane) - 1u))] = i;
+// Keys of tile blockIdx.x (8 rounds of 256 entries): tile_counts[8 * tile + k] = entries with
+// key k.
+__global__ void __launch_bounds__(256) group_count_kernel(const uint8_t* __restrict__ keys, int n, const int* n_ptr,
+                                                          int* __restrict__ tile_counts) {
+    n = queue_size(n_ptr, n);
+    const int base = blockIdx.x * kGroupTile;
+    if (base >= n) return;
+    __shared__ int warp_counts[8][kShadeKeys];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int mine = 0;   // lane k < 8: this warp's entries with key k
+    for (int r = 0; r < kGroupTile / 256; ++r) {
+        const int i = base + r * 256 + threadIdx.x;
+        const int k = i < n ? keys[i] : kShadeKeys;
+        for (int kk = 0; kk < kShadeKeys; ++kk) {
+            const int c = __popc(__ballot_sync(0xffffffffu, k == kk));
+            if (lane == kk) mine += c;
+        }
+    }
+    if (lane < kShadeKeys) warp_counts[warp][lane] = mine;
+    __syncthreads();
+    if (threadIdx.x < kShadeKeys) {
+        int total = 0;
+        for (int w = 0; w < 8; ++w) total += warp_counts[w][threadIdx.x];
+        tile_counts[kShadeKeys * blockIdx.x + threadIdx.x] = total;
+    }
+}
+
+// Exclusive scan of the tile counts in key-major order, in place: tile_counts[8 * t + k]
+// becomes the first position of tile t's key-k entries in the permutation. One block.
+__global__ void __launch_bounds__(1024) group_scan_kernel(int* tile_counts, int n, const int* n_ptr) {
+    n = queue_size(n_ptr, n);
+    const int tiles = (n + kGroupTile - 1) / kGroupTile;
+    const int per = (tiles + 1023) / 1024;
+    const int t0 = min((int)threadIdx.x * per, tiles), t1 = min(t0 + per, tiles);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int k = 0; k < kShadeKeys; ++k) {
+        int local = 0;
+        for (int t = t0; t < t1; ++t) local += tile_counts[kShadeKeys * t + k];
+        int incl = local;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int w = warp_sums[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, w, d);
+                if (lane >= d) w += v;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        int run = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + incl - local;
+        for (int t = t0; t < t1; ++t) {
+            const int c = tile_counts[kShadeKeys * t + k];
+            tile_counts[kShadeKeys * t + k] = run;
+            run += c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_sums[31];
+        __syncthreads();
+    }
+}
+
+// Places the entries of tile blockIdx.x at their scanned offsets, in index order within each
+// key (round by round, warp by warp, lane by lane).
+__global__ void __launch_bounds__(256) group_scatter_kernel(const uint8_t* __restrict__ keys, int n, const int* n_ptr,
+                                                            const int* __restrict__ tile_offsets, int* __restrict__ perm) {
+    n = queue_size(n_ptr, n);
+    const int base = blockIdx.x * kGroupTile;
+    if (base >= n) return;
+    __shared__ int run[kShadeKeys];                 // entries of each key placed so far (+ tile offset)
+    __shared__ int warp_counts[8][kShadeKeys];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    if (threadIdx.x < kShadeKeys) run[threadIdx.x] = tile_offsets[kShadeKeys * blockIdx.x + threadIdx.x];
+    for (int r = 0; r < kGroupTile / 256; ++r) {
+        const int i = base + r * 256 + threadIdx.x;
+        const bool valid = i < n;
+        const int k = valid ? keys[i] : kShadeKeys;
+        unsigned same = 0;
+        for (int kk = 0; kk < kShadeKeys; ++kk) {
+            const unsigned m = __ballot_sync(0xffffffffu, k == kk);
+            if (lane == kk) warp_counts[warp][kk] = __popc(m);
+            if (k == kk) same = m;
+        }
+        __syncthreads();
+        if (valid) {
+            int off = run[k] + __popc(same & lt_mask);
+            for (int w = 0; w < warp; ++w) off += warp_counts[w][k];
+            perm[off] = i;
+        }
+        int total = 0;
+        if (threadIdx.x < kShadeKeys)
+            for (int w = 0; w < 8; ++w) total += warp_counts[w][threadIdx.x];
+        __syncthreads();
+        if (threadIdx.x < kShadeKeys) run[threadIdx.x] += total;
+    }
+}
+
+// The permutation of a queue of n entries (n_ptr: size read on the device, n its bound) from
+// its keys; tile_counts holds 8 ints per tile (group_tiles(n) tiles).
+inline void launch_grouping(const uint8_t* keys, int n, const int* n_ptr, int* tile_counts, int* perm,
+                            cudaStream_t st) {
+    const int tiles = group_tiles(n);
+    group_count_kernel<<<tiles, 256, 0, st>>>(keys, n, n_ptr, tile_counts);
+    group_scan_kernel<<<1, 1024, 0, st>>>(tile_counts, n, n_ptr);
+    group_scatter_kernel<<<tiles, 256, 0, st>>>(keys, n, n_ptr, tile_counts, perm);
+    note_launches(3);
 }
 
 // One wavefront of shading: continuations go to the next path queue, shadow rays to the
 // shadow queue (both appended in warp order). In the merged form every path that ends adds
 // one to its request's `terminated` counter.
 template <bool kMulti>
-__global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void shade_queue_entry(const ShadeParams& p, int t, int n) {
     ShadeOut o;
     int pixel = 0, req = 0, root = 0;
-    if (t < p.n) {
+    if (t < n) {
         const int i = p.perm ? p.perm[t] : t;
         pixel = p.pixel[i];
         const float4 ro = p.rays[2 * i], rd = p.rays[2 * i + 1];
@@ -465,7 +573,7 @@ __global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
         if (kMulti) { p.s_req[sslot] = req; p.s_root[sslot] = root; }
     }
     if (kMulti) {
-        const bool ended = t < p.n && !o.alive;
+        const bool ended = t < n && !o.alive;
         const unsigned m = __ballot_sync(__activemask(), ended);
         if (ended) {
             const unsigned peers = __match_any_sync(m, req);
@@ -474,18 +582,26 @@ __global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
     }
 }
 
+// One queue entry per thread: the launch covers the queue (or its bound, when the size is read
+// on the device; threads past the size only take part in the warp-wide appends).
+template <bool kMulti>
+__global__ void __launch_bounds__(128) pt_shade_kernel(ShadeParams p) {
+    shade_queue_entry<kMulti>(p, blockIdx.x * blockDim.x + threadIdx.x, queue_size(p.n_ptr, p.n));
+}
+
 // Integrator::process_shadow_rays (integrator.h:49-63): unoccluded shadow rays add their
 // contribution to the image. The ray count is read from the device (`count`), `bound` sizes
 // the launch.
 template <bool kMulti>
 __global__ void shadow_accumulate_kernel(const int* count, const int4* hits, const int* pixel, const float4* contrib,
                                          float* image, const int* sreq, const ReqDev* reqs) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *count) return;
-    if (hits[i].x >= 0) return;
-    const float4 c = contrib[i];
-    float* img = kMulti ? reqs[sreq[i]].image : image;
-    add_image(img, pixel[i], V3(c.x, c.y, c.z));
+    const int n = *count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (hits[i].x >= 0) continue;
+        const float4 c = contrib[i];
+        float* img = kMulti ? reqs[sreq[i]].image : image;
+        add_image(img, pixel[i], V3(c.x, c.y, c.z));
+    }
 }
 
 }  // namespace

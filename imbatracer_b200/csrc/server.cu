@@ -271,7 +271,7 @@ struct imbart_server {
     int* h_counts = nullptr;              // pinned
     uint8_t* keys = nullptr;              // material grouping of a wavefront
     int* perm = nullptr;
-    int* key_counts = nullptr;
+    int* tile_counts = nullptr;           // grouping sort: 8 counts (then offsets) per tile
     std::vector<int> free_req_slots, free_scene_slots;
 
     // Path queues (double-buffered), shadow queue, hits.
@@ -750,21 +750,16 @@ bool batched_wave(imbart_server* S) {
             unsigned kinds = 0;
             for (Request* r : S->active_renders) kinds |= S->scenes[r->scene]->kind_mask;
             const bool group = __builtin_popcount(kinds) > 1;
-            const bool zeroed =
-                !group ||
-                cuda_check(cudaMemsetAsync(S->key_counts, 0, sizeof(int) * 2 * kShadeKeys, st), "cudaMemsetAsync");
-            if (zeroed) {
-                if (group) {
-                    shade_key_multi_kernel<<<(n + 255) / 256, 256, 0, st>>>(S->d_reqs, S->d_scenes, S->req[cur],
-                                                                             S->hits, n, S->keys, S->key_counts);
-                    shade_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(S->keys, n, S->key_counts, S->perm);
-                    note_launches(2);
-                    p.perm = S->perm;
-                }
-                pt_shade_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(p);
+            if (group) {
+                shade_key_multi_kernel<<<(n + 255) / 256, 256, 0, st>>>(S->d_reqs, S->d_scenes, S->req[cur], S->hits,
+                                                                         n, nullptr, S->keys);
+                launch_grouping(S->keys, n, nullptr, S->tile_counts, S->perm, st);
                 note_launches(1);
+                p.perm = S->perm;
             }
-            good = zeroed && cuda_check(cudaGetLastError(), "shade kernel") &&
+            pt_shade_kernel<true><<<(n + 127) / 128, 128, 0, st>>>(p);
+            note_launches(1);
+            good = cuda_check(cudaGetLastError(), "shade kernel") &&
                    launch_trace_internal(S->pool_scene, S->srays, S->shits, nullptr, n, IMBART_TRACE_ANY, st, nullptr,
                                          S->sroot, S->d_counts + 1) == 0;
             if (good) {
@@ -1089,7 +1084,7 @@ void free_server(imbart_server* S) {
         if (lane.stream && lane.stream != S->stream) cudaStreamDestroy(lane.stream);
     }
     void* dev[] = {S->pool, S->d_reqs, S->d_scenes, S->d_terminated, S->d_chunks, S->d_runs, S->d_counts,
-                   S->keys, S->perm, S->key_counts,
+                   S->keys, S->perm, S->tile_counts,
                    S->hits, S->srays, S->shits, S->spixel, S->scontrib, S->sreq, S->sroot, S->b_rays, S->b_hits,
                    S->b_roots, S->plain_image, S->plain_rays, S->plain_hits};
     for (void* p : dev) cudaFree(p);
@@ -1142,7 +1137,7 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
                dalloc(&S->d_runs, kMaxReqSlots) && halloc(&S->h_runs, kMaxReqSlots) &&
                dalloc(&S->d_counts, 4) && halloc(&S->h_counts, 4) &&
                dalloc(&S->hits, cap) && dalloc(&S->srays, 2 * cap) && dalloc(&S->shits, cap) &&
-               dalloc(&S->keys, cap) && dalloc(&S->perm, cap) && dalloc(&S->key_counts, 2 * kShadeKeys) &&
+               dalloc(&S->keys, cap) && dalloc(&S->perm, cap) && dalloc(&S->tile_counts, (size_t)kShadeKeys * group_tiles(cap)) &&
                dalloc(&S->spixel, cap) && dalloc(&S->scontrib, cap) && dalloc(&S->sreq, cap) &&
                dalloc(&S->sroot, cap) && dalloc(&S->b_rays, cap) && dalloc(&S->b_hits, cap) &&
                dalloc(&S->b_roots, cap) && halloc(&S->stage_rays, cap) && halloc(&S->stage_hits, cap);

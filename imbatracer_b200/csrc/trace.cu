@@ -194,13 +194,18 @@ int* work_slot(int device) {
     return pool + 2 * slot;
 }
 
+// A traversal launch: kernel, grid, block (the parameters are the TraceParams beside it).
+struct LaunchSpec {
+    const void* func = nullptr;
+    dim3 grid, block;
+};
+
 template <bool kStats>
-bool dispatch_simple(bool any, bool masked, int grid, int block, cudaStream_t stream, const TraceParams& p) {
-    if (any && masked) trace_kernel<true, true, kStats><<<grid, block, 0, stream>>>(p);
-    else if (any) trace_kernel<true, false, kStats><<<grid, block, 0, stream>>>(p);
-    else if (masked) trace_kernel<false, true, kStats><<<grid, block, 0, stream>>>(p);
-    else trace_kernel<false, false, kStats><<<grid, block, 0, stream>>>(p);
-    return true;
+const void* simple_kernel(bool any, bool masked) {
+    if (any && masked) return (const void*)trace_kernel<true, true, kStats>;
+    if (any) return (const void*)trace_kernel<true, false, kStats>;
+    if (masked) return (const void*)trace_kernel<false, true, kStats>;
+    return (const void*)trace_kernel<false, false, kStats>;
 }
 
 template <typename Kernel>
@@ -219,46 +224,48 @@ int max_grid(Kernel k, int block, int device) {
     return g;
 }
 
+// One persistent block per resident slot (fewer for short queues).
 template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
-void launch_persistent(int count, int device, cudaStream_t stream, TraceParams p) {
+LaunchSpec persistent_spec(int count, int device, TraceParams& p) {
     auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh>;
     const int grid = std::min(max_grid(k, kBlock, device), (count + kBlock - 1) / kBlock);
     p.total_warps = grid * (kBlock / 32);
-    k<<<grid, kBlock, 0, stream>>>(p);
+    return {(const void*)k, dim3(grid), dim3(kBlock)};
 }
 
 template <bool kAny, bool kMasked, bool kStats>
-bool dispatch_variant(int variant, int count, int device, cudaStream_t stream, const TraceParams& p) {
+LaunchSpec variant_spec(int variant, int count, int device, TraceParams& p) {
     switch (variant) {
-        case 1: launch_persistent<kAny, kMasked, kStats, 128, 4, 16>(count, device, stream, p); return true;
-        case 2: launch_persistent<kAny, kMasked, kStats, 128, 6, 12>(count, device, stream, p); return true;
-        case 3: launch_persistent<kAny, kMasked, kStats, 256, 2, 16>(count, device, stream, p); return true;
-        case 4: launch_persistent<kAny, kMasked, kStats, 256, 3, 12>(count, device, stream, p); return true;
-        case 5: launch_persistent<kAny, kMasked, kStats, 64, 8, 16>(count, device, stream, p); return true;
-        case 6: launch_persistent<kAny, kMasked, kStats, 256, 4, 8>(count, device, stream, p); return true;
-        case 7: launch_persistent<kAny, kMasked, kStats, 128, 7, 10>(count, device, stream, p); return true;
-        default: return false;
+        case 1: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16>(count, device, p);
+        case 2: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12>(count, device, p);
+        case 3: return persistent_spec<kAny, kMasked, kStats, 256, 2, 16>(count, device, p);
+        case 4: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12>(count, device, p);
+        case 5: return persistent_spec<kAny, kMasked, kStats, 64, 8, 16>(count, device, p);
+        case 6: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8>(count, device, p);
+        case 7: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10>(count, device, p);
+        default: return {};
     }
 }
 
 template <bool kStats>
-bool dispatch_persistent(int variant, bool any, bool masked, int count, int device, cudaStream_t stream,
-                         const TraceParams& p) {
-    if (any && masked) return dispatch_variant<true, true, kStats>(variant, count, device, stream, p);
-    if (any) return dispatch_variant<true, false, kStats>(variant, count, device, stream, p);
-    if (masked) return dispatch_variant<false, true, kStats>(variant, count, device, stream, p);
-    return dispatch_variant<false, false, kStats>(variant, count, device, stream, p);
+LaunchSpec persistent_kernel_spec(int variant, bool any, bool masked, int count, int device, TraceParams& p) {
+    if (any && masked) return variant_spec<true, true, kStats>(variant, count, device, p);
+    if (any) return variant_spec<true, false, kStats>(variant, count, device, p);
+    if (masked) return variant_spec<false, true, kStats>(variant, count, device, p);
+    return variant_spec<false, false, kStats>(variant, count, device, p);
 }
 
-int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out,
-                 int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr,
-                 const int* roots = nullptr, const int* count_ptr = nullptr) {
+// The launch of one traversal query (kernel, grid, block and parameters) under the current
+// configuration; false with the error set on invalid arguments. `count` = 0: nothing to launch.
+bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out, int count, int flags,
+                unsigned long long* stats, const int* roots, const int* count_ptr, int* work_override, TraceParams& p,
+                LaunchSpec& spec) {
     if (!s || (!rays && count > 0) || (!hits && count > 0) || count < 0 || (roots && s->info.masked)) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: invalid argument");
-        return IMBART_ERR_INVALID_ARGUMENT;
+        return false;
     }
-    if (count == 0) return 0;
-    TraceParams p;
+    spec = LaunchSpec{};
+    if (count == 0) return true;
     p.nodes = s->nodes; p.tris = s->tris; p.insts = s->insts; p.root = s->info.root;
     p.indices = s->indices; p.texcoords = s->texcoords; p.masks = s->masks; p.mask_buffer = s->mask_buffer;
     p.n_masks = s->n_masks;
@@ -276,27 +283,39 @@ int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits
     const TraceConfig cfg = current_config();
     const int variant = any ? cfg.variant_any : coherent ? cfg.variant_coh : cfg.variant;
     const int refill = any ? cfg.refill_any : coherent ? cfg.refill_coh : cfg.refill;
-    bool launched;
     if (variant == 0) {
         const int block = 128;
-        const int grid = (count + block - 1) / block;
-        if (stats) launched = dispatch_simple<true>(any, masked, grid, block, stream, p);
-        else launched = dispatch_simple<false>(any, masked, grid, block, stream, p);
+        spec.func = stats ? simple_kernel<true>(any, masked) : simple_kernel<false>(any, masked);
+        spec.grid = dim3((count + block - 1) / block);
+        spec.block = dim3(block);
     } else {
-        int* work = work_slot(s->device);
-        if (!work) return IMBART_ERR_CUDA;
+        int* work = work_override ? work_override : work_slot(s->device);
+        if (!work) return false;
         p.work = work;
         p.refill_lanes = std::min(std::max(refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
-        if (stats) launched = dispatch_persistent<true>(variant, any, masked, count, s->device, stream, p);
-        else launched = dispatch_persistent<false>(variant, any, masked, count, s->device, stream, p);
+        spec = stats ? persistent_kernel_spec<true>(variant, any, masked, count, s->device, p)
+                     : persistent_kernel_spec<false>(variant, any, masked, count, s->device, p);
     }
-    if (!launched) {
+    if (!spec.func) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");
-        return IMBART_ERR_INVALID_ARGUMENT;
+        return false;
     }
+    return true;
+}
+
+int launch_trace(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits, float* v_out,
+                 int count, int flags, cudaStream_t stream, unsigned long long* stats = nullptr,
+                 const int* roots = nullptr, const int* count_ptr = nullptr, int* work_override = nullptr) {
+    TraceParams p;
+    LaunchSpec spec;
+    if (!trace_spec(s, rays, hits, v_out, count, flags, stats, roots, count_ptr, work_override, p, spec))
+        return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
+    if (!spec.func) return 0;
+    void* args[] = {&p};
+    if (!cuda_ok(cudaLaunchKernel(spec.func, spec.grid, spec.block, args, 0, stream), "trace kernel launch"))
+        return IMBART_ERR_CUDA;
     note_launches(1);
-    if (!cuda_ok(cudaGetLastError(), "trace kernel launch")) return IMBART_ERR_CUDA;
     return 0;
 }
 
@@ -445,9 +464,49 @@ void dropin_host(bool any, int root, imbart_node4* nodes, imbart_instance_node* 
 
 int launch_trace_internal(const imbart_scene* scene, const void* rays, void* hits, float* v_out, int count,
                           int flags, void* stream, unsigned long long* stats, const int* roots,
-                          const int* count_ptr) {
+                          const int* count_ptr, int* work) {
     return launch_trace(scene, reinterpret_cast<const imbart_ray*>(rays), reinterpret_cast<imbart_hit*>(hits), v_out,
-                        count, flags, (cudaStream_t)stream, stats, roots, count_ptr);
+                        count, flags, (cudaStream_t)stream, stats, roots, count_ptr, work);
+}
+
+int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, cudaGraphNode_t* node,
+                   const imbart_scene* scene, const void* rays, void* hits, int count, int flags,
+                   const int* count_ptr, int* work) {
+    TraceParams p;
+    LaunchSpec spec;
+    if (!trace_spec(scene, reinterpret_cast<const imbart_ray*>(rays), reinterpret_cast<imbart_hit*>(hits), nullptr,
+                    count, flags, nullptr, nullptr, count_ptr, work, p, spec))
+        return imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA;
+    if (!spec.func) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "add_trace_node: empty launch");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    void* args[] = {&p};
+    cudaKernelNodeParams np{};
+    np.func = const_cast<void*>(spec.func);
+    np.gridDim = spec.grid;
+    np.blockDim = spec.block;
+    np.sharedMemBytes = 0;
+    np.kernelParams = args;
+    np.extra = nullptr;
+    return cuda_ok(cudaGraphAddKernelNode(node, graph, deps, (size_t)n_deps, &np), "cudaGraphAddKernelNode")
+               ? 0
+               : IMBART_ERR_CUDA;
+}
+
+void scene_launch_key(const imbart_scene* s, unsigned long long out[12]) {
+    out[0] = (unsigned long long)(uintptr_t)s->nodes; out[1] = (unsigned long long)(uintptr_t)s->tris;
+    out[2] = (unsigned long long)(uintptr_t)s->insts; out[3] = (unsigned long long)(uintptr_t)s->indices;
+    out[4] = (unsigned long long)(uintptr_t)s->texcoords; out[5] = (unsigned long long)(uintptr_t)s->masks;
+    out[6] = (unsigned long long)(uintptr_t)s->mask_buffer; out[7] = (unsigned long long)(uintptr_t)s->error_flags;
+    out[8] = (unsigned long long)s->n_masks; out[9] = (unsigned long long)(unsigned)s->info.root;
+    out[10] = (unsigned long long)s->info.masked; out[11] = (unsigned long long)s->device;
+}
+
+void trace_config_snapshot(int out[7]) {
+    const TraceConfig c = current_config();
+    out[0] = c.variant; out[1] = c.refill; out[2] = c.postpone; out[3] = c.variant_any;
+    out[4] = c.refill_any; out[5] = c.variant_coh; out[6] = c.refill_coh;
 }
 
 imbart_scene* upload_wide_scene(const HostWideScene& h, int device) { return upload_scene(h, device); }

@@ -155,19 +155,9 @@ __global__ void light_gen_kernel(VcmParams p, const LightTile* tiles, int n_tile
 
 // Material grouping keys of light-path slots (pt::shade_key; finished slots get key 7).
 __global__ void __launch_bounds__(256) light_key_kernel(ShadingScene s, const int4* __restrict__ hits,
-                                                        const float4* __restrict__ thrs, int n, uint8_t* keys,
-                                                        int* counts) {
-    __shared__ int hist[pt::kShadeKeys];
-    if (threadIdx.x < pt::kShadeKeys) hist[threadIdx.x] = 0;
-    __syncthreads();
+                                                        const float4* __restrict__ thrs, int n, uint8_t* keys) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const int k = __float_as_int(thrs[i].w) < 0 ? 7 : pt::shade_key(s, hits[i]);
-        keys[i] = (uint8_t)k;
-        atomicAdd(&hist[k], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < pt::kShadeKeys && hist[threadIdx.x] > 0) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+    if (i < n) keys[i] = (uint8_t)(__float_as_int(thrs[i].w) < 0 ? 7 : pt::shade_key(s, hits[i]));
 }
 
 // connect_to_camera (vcm.cpp:260-320): a shadow ray towards the camera. Returns false when the
@@ -916,12 +906,12 @@ struct imbart_vcm {
     float4* c_w[2] = {nullptr, nullptr};
     int4* c_hits = nullptr;
     float4* c_merge = nullptr;      // queued camera vertices for merging (7 float4 each)
-    // Material grouping of a wavefront (keys, shading order, 8 bucket sizes + 8 cursors).
+    // Material grouping of a wavefront (keys, shading order, 8 counts then offsets per tile).
     long long sort_cap = 0;
     bool use_perm = false;
     uint8_t* keys = nullptr;
     int* perm = nullptr;
-    int* key_counts = nullptr;
+    int* tile_counts = nullptr;
     // shadow queue
     long long s_cap = 0;
     float4* s_rays = nullptr;
@@ -939,7 +929,7 @@ namespace imbart {
 namespace {
 
 void free_vcm(imbart_vcm* v) {
-    void* ptrs[] = {v->keys, v->perm, v->key_counts,
+    void* ptrs[] = {v->keys, v->perm, v->tile_counts,
                     v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage, v->vflags, v->bsums, v->d_tiles,
                     v->cache, v->c_hits, v->c_merge, v->s_rays, v->s_hits, v->s_pixel, v->s_contrib, v->counts};
     for (void* p : ptrs) cudaFree(p);
@@ -967,8 +957,8 @@ bool ensure_shadow(imbart_vcm* v, long long need) {
     return good;
 }
 
-// The shading order of a wavefront of n paths: keys from `key_launch(keys, counts)`, then the
-// counting-sort scatter into v->perm (pt::shade_scatter_kernel).
+// The shading order of a wavefront of n paths: keys from `key_launch(keys)`, then the stable
+// counting sort into v->perm (pt::launch_grouping).
 template <typename KeyLaunch>
 bool group_paths(imbart_vcm* v, const imbart_shading* sh, int n, cudaStream_t s, KeyLaunch key_launch) {
     v->use_perm = __builtin_popcount(sh->kind_mask) > 1;    // one kind: nothing to group
@@ -976,14 +966,13 @@ bool group_paths(imbart_vcm* v, const imbart_shading* sh, int n, cudaStream_t s,
     if (v->sort_cap < n) {
         const long long c = std::max<long long>(n, v->sort_cap * 3 / 2);
         const bool good = realloc_exact(&v->keys, (size_t)c) && realloc_exact(&v->perm, (size_t)c) &&
-                          realloc_exact(&v->key_counts, 2 * pt::kShadeKeys);
+                          realloc_exact(&v->tile_counts, (size_t)pt::kShadeKeys * pt::group_tiles(c));
         v->sort_cap = good ? c : 0;
         if (!good) return false;
     }
-    if (!ok(cudaMemsetAsync(v->key_counts, 0, sizeof(int) * 2 * pt::kShadeKeys, s), "cudaMemsetAsync")) return false;
-    key_launch(v->keys, v->key_counts);
-    pt::shade_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(v->keys, n, v->key_counts, v->perm);
-    note_launches(2);
+    key_launch(v->keys);
+    pt::launch_grouping(v->keys, n, nullptr, v->tile_counts, v->perm, s);
+    note_launches(1);
     return ok(cudaGetLastError(), "grouping kernels");
 }
 
@@ -1246,8 +1235,8 @@ int imbart_vcm_light_pass_range(imbart_vcm* v, const imbart_scene* scene, const 
         }
         p.cache = v->cache;
         if (!ok(cudaMemsetAsync(v->counts, 0, sizeof(int) * 4, s), "cudaMemsetAsync")) { rc = IMBART_ERR_CUDA; break; }
-        if (!group_paths(v, sh, P, s, [&](uint8_t* keys, int* counts) {
-                light_key_kernel<<<(P + 255) / 256, 256, 0, s>>>(p.s, v->l_hits, v->l_thr, P, keys, counts);
+        if (!group_paths(v, sh, P, s, [&](uint8_t* keys) {
+                light_key_kernel<<<(P + 255) / 256, 256, 0, s>>>(p.s, v->l_hits, v->l_thr, P, keys);
             })) {
             rc = IMBART_ERR_CUDA;
             break;
@@ -1392,8 +1381,8 @@ int imbart_vcm_camera_pass_range(imbart_vcm* v, const imbart_scene* scene, const
             ++n_waves;
             if (!ok(cudaMemsetAsync(v->counts, 0, sizeof(int) * 4, s), "cudaMemsetAsync")) { rc = IMBART_ERR_CUDA; break; }
             const int nxt = 1 - cur;
-            if (!group_paths(v, sh, n, s, [&](uint8_t* keys, int* counts) {
-                    pt::shade_key_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.s, v->c_hits, n, keys, counts);
+            if (!group_paths(v, sh, n, s, [&](uint8_t* keys) {
+                    pt::shade_key_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.s, v->c_hits, n, nullptr, keys);
                 })) {
                 rc = IMBART_ERR_CUDA;
                 break;

@@ -21,7 +21,10 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "imbart_internal.h"
@@ -51,7 +54,22 @@ struct imbart_pt_context {
     unsigned long long* work = nullptr;      // device: closest nodes/tris/insts, shadow nodes/tris/insts
     uint8_t* keys = nullptr;                 // material grouping: key per path
     int* perm = nullptr;                     // shading order
-    int* key_counts = nullptr;               // 8 bucket sizes + 8 cursors
+    int* tile_counts = nullptr;              // grouping sort: 8 counts (then offsets) per tile
+    // The bounce loop of one sample range as a CUDA graph, replayed once per range.
+    int graphs = -1;                         // -1: IMBART_PT_GRAPH (default 2); 0 host loop, 1 graph, 2 forked graph
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> graph_key;    // the launch parameters the graph was captured with
+    int graph_kernels = 0;                   // kernel launches per replay
+    int graph_bounces = 0;                   // range state sized for this many bounces
+    long long* range_state = nullptr;        // next sample, per-slot totals, waves; then the range's counts
+    int* graph_work = nullptr;               // (next, done) counters of the graph's traversal launches
+    CameraParams* camera = nullptr;          // the frame's camera and seeding, copied in before the replays
+    // Forked form: a second shadow queue, so that a bounce's shadow rays are traced beside the
+    // next bounce's closest hits.
+    float4* srays2 = nullptr;
+    int4* shits2 = nullptr;
+    int* spixel2 = nullptr;
+    float4* scontrib2 = nullptr;
 };
 
 namespace imbart {
@@ -79,8 +97,10 @@ void free_ctx_buffers(imbart_pt_context* c) {
     }
     cudaFree(c->hits); cudaFree(c->srays); cudaFree(c->shits); cudaFree(c->spixel); cudaFree(c->scontrib);
     c->hits = nullptr; c->srays = nullptr; c->shits = nullptr; c->spixel = nullptr; c->scontrib = nullptr;
-    cudaFree(c->keys); cudaFree(c->perm); cudaFree(c->key_counts);
-    c->keys = nullptr; c->perm = nullptr; c->key_counts = nullptr;
+    cudaFree(c->keys); cudaFree(c->perm); cudaFree(c->tile_counts);
+    c->keys = nullptr; c->perm = nullptr; c->tile_counts = nullptr;
+    cudaFree(c->srays2); cudaFree(c->shits2); cudaFree(c->spixel2); cudaFree(c->scontrib2);
+    c->srays2 = nullptr; c->shits2 = nullptr; c->spixel2 = nullptr; c->scontrib2 = nullptr;
     c->cap = 0;
 }
 
@@ -103,10 +123,292 @@ bool ensure_capacity(imbart_pt_context* c, long long n) {
                dev_alloc(&c->thr[k], n) && dev_alloc(&c->bounces[k], n);
     good = good && dev_alloc(&c->hits, n) && dev_alloc(&c->srays, 2 * n) && dev_alloc(&c->shits, n) &&
            dev_alloc(&c->spixel, n) && dev_alloc(&c->scontrib, n) && dev_alloc(&c->keys, n) &&
-           dev_alloc(&c->perm, n) && dev_alloc(&c->key_counts, 2 * kShadeKeys);
+           dev_alloc(&c->perm, n) && dev_alloc(&c->tile_counts, (size_t)kShadeKeys * group_tiles(n));
     if (!good) { free_ctx_buffers(c); return false; }
     c->cap = n;
+    c->graph_key.clear();   // the captured frame names the old buffers
     return true;
+}
+
+// How the bounce loop runs: 0 driven from the host, 1 as a CUDA graph (one chain of
+// launches), 2 as a CUDA graph whose shadow-ray work (each bounce's any-hit launch and
+// accumulation) runs on a branch beside the next bounce's closest-hit launch (measured best:
+// the launches fill each other's tails). The caller's choice, else IMBART_PT_GRAPH, else 2.
+int graph_mode(const imbart_pt_context* c) {
+    if (c->graphs >= 0) return c->graphs;
+    static const int v = [] {
+        const char* e = std::getenv("IMBART_PT_GRAPH");
+        const int x = e && *e ? std::atoi(e) : 2;
+        return x < 0 || x > 2 ? 2 : x;
+    }();
+    return v;
+}
+
+// ---------------------------------------------------------------------------------------
+// The bounce loop as a CUDA graph. The host loop reads each wavefront's queue sizes back
+// before it launches the next wavefront (one synchronization per bounce). Captured, every
+// kernel of a sample range reads its queue size on the device instead and walks its queue
+// with a grid stride: camera samples, then per bounce b < max_path_len the closest-hit
+// launch, the material grouping, the shading launch, the any-hit launch and the shadow
+// accumulation, each sized for the largest queue; a bounce whose queue is empty costs a few
+// microseconds of launches that exit at once. The range state (next sample index, the
+// range's queue sizes, totals for the statistics) lives on the device, so the same graph is
+// replayed once per range and the frame runs without host synchronization.
+//
+// Range state: [0] first sample of the next range, [1 + k] total of count slot k over the
+// ranges, [1 + n_slots] wavefronts traced; then n_slots ints: slot 2b = paths entering
+// bounce b, slot 2b + 3 = shadow rays of bounce b.
+// ---------------------------------------------------------------------------------------
+__global__ void range_begin_kernel(const long long* first, int* counts, int n_slots, long long total,
+                                   long long chunk) {
+    const long long left = total - *first;
+    const int n = (int)(left < chunk ? left : chunk);
+    for (int k = threadIdx.x; k < n_slots; k += blockDim.x) counts[k] = k == 0 ? n : 0;
+}
+
+__global__ void range_end_kernel(long long* state, const int* counts, int n_slots, int bounces, long long chunk) {
+    for (int k = threadIdx.x; k < n_slots; k += blockDim.x) state[1 + k] += counts[k];
+    if (threadIdx.x == 0) {
+        int waves = 0;
+        for (int b = 0; b < bounces; ++b) waves += counts[2 * b] > 0;
+        state[1 + n_slots] += waves;
+        state[0] += chunk;
+    }
+}
+
+// Everything the captured kernels take into their parameters: equal keys, same graph. The
+// camera and the seed are read on the device, so a new view or seed replays the same graph.
+struct FrameGraphKey {
+    unsigned long long scene[12];
+    ShadingScene s;
+    float* image;
+    long long total, chunk;
+    int max_path_len, rr_start, group, fork, trace_cfg[7];
+};
+
+std::vector<unsigned char> frame_key(const imbart_scene* scene, const imbart_shading* sh, float* image, long long total,
+                                     long long chunk, int max_path_len, int rr_start, bool group, bool fork) {
+    FrameGraphKey k;
+    std::memset(&k, 0, sizeof(k));
+    scene_launch_key(scene, k.scene);
+    std::memcpy(&k.s, &sh->s, sizeof(k.s));
+    k.image = image;
+    k.total = total;
+    k.chunk = chunk;
+    k.max_path_len = max_path_len;
+    k.rr_start = rr_start;
+    k.group = group ? 1 : 0;
+    k.fork = fork ? 1 : 0;
+    trace_config_snapshot(k.trace_cfg);
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&k);
+    return std::vector<unsigned char>(b, b + sizeof(k));
+}
+
+bool ensure_range_state(imbart_pt_context* c, int bounces, cudaStream_t st) {
+    if (!c->camera && !ok(cudaMalloc((void**)&c->camera, sizeof(CameraParams)), "cudaMalloc")) return false;
+    if (c->graph_bounces >= bounces) return true;
+    cudaFree(c->range_state);
+    cudaFree(c->graph_work);
+    c->range_state = nullptr;
+    c->graph_work = nullptr;
+    c->graph_bounces = 0;
+    c->graph_key.clear();
+    const int n_slots = 2 * bounces + 2;
+    const size_t state_bytes = sizeof(long long) * (n_slots + 2) + sizeof(int) * n_slots;
+    if (!ok(cudaMalloc((void**)&c->range_state, state_bytes), "cudaMalloc") ||
+        !ok(cudaMalloc((void**)&c->graph_work, sizeof(int) * 4 * bounces), "cudaMalloc") ||
+        !ok(cudaMemsetAsync(c->graph_work, 0, sizeof(int) * 4 * bounces, st), "cudaMemsetAsync"))
+        return false;
+    c->graph_bounces = bounces;
+    return true;
+}
+
+int device_sms(int device) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return std::max(sms, 1);
+}
+
+// Explicit construction of a graph's kernel nodes. The graph is built with the graph API, not
+// by stream capture: a capture in progress would make device-wide synchronization by any other
+// thread of the process (cudaDeviceSynchronize, cudaFree) fail and invalidate the capture.
+struct GraphBuilder {
+    cudaGraph_t graph = nullptr;
+    int kernels = 0;
+    bool good = true;
+
+    // Adds kernel `k` with the given arguments after `deps` (null nodes are skipped).
+    template <typename... KArgs, typename... Args>
+    cudaGraphNode_t kernel(std::initializer_list<cudaGraphNode_t> deps, void (*k)(KArgs...), dim3 grid, dim3 block,
+                           Args&&... args) {
+        if (!good) return nullptr;
+        return add(deps, (const void*)k, grid, block, std::tuple<KArgs...>(std::forward<Args>(args)...),
+                   std::index_sequence_for<KArgs...>{});
+    }
+
+    template <typename Tuple, size_t... I>
+    cudaGraphNode_t add(std::initializer_list<cudaGraphNode_t> deps, const void* func, dim3 grid, dim3 block,
+                        Tuple args, std::index_sequence<I...>) {
+        void* ptrs[] = {(void*)&std::get<I>(args)..., nullptr};
+        std::vector<cudaGraphNode_t> d;
+        for (cudaGraphNode_t x : deps)
+            if (x) d.push_back(x);
+        cudaKernelNodeParams np{};
+        np.func = const_cast<void*>(func);
+        np.gridDim = grid;
+        np.blockDim = block;
+        np.kernelParams = ptrs;
+        cudaGraphNode_t node = nullptr;
+        good = ok(cudaGraphAddKernelNode(&node, graph, d.data(), d.size(), &np), "cudaGraphAddKernelNode");
+        kernels += good ? 1 : 0;
+        return good ? node : nullptr;
+    }
+
+    cudaGraphNode_t trace(std::initializer_list<cudaGraphNode_t> deps, const imbart_scene* scene, const void* rays,
+                          void* hits, int bound, int flags, const int* count_ptr, int* work) {
+        if (!good) return nullptr;
+        std::vector<cudaGraphNode_t> d;
+        for (cudaGraphNode_t x : deps)
+            if (x) d.push_back(x);
+        cudaGraphNode_t node = nullptr;
+        good = add_trace_node(graph, d.data(), (int)d.size(), &node, scene, rays, hits, bound, flags, count_ptr,
+                              work) == 0;
+        kernels += good ? 1 : 0;
+        return good ? node : nullptr;
+    }
+};
+
+// Builds the bounce loop of one sample range (`chunk` samples at most) into ctx->exec.
+int capture_range(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh, int max_path_len,
+                  int rr_start, float* image, long long total, long long chunk, bool group, bool fork) {
+    const int sms = device_sms(ctx->device);
+    // Shading: one thread per entry of the queue's bound, blocks past the queue's size doing
+    // nothing. (A block-stride loop over one wave measured no faster: the loop costs the
+    // shading kernel registers, 86 instead of 71, or spills under a 7-block bound.)
+    const int shade_grid = (int)((chunk + 127) / 128);
+    const int small_grid = 16 * sms;
+    const int n = (int)chunk;
+    const int n_slots = 2 * max_path_len + 2;
+    long long* state = ctx->range_state;
+    int* counts = reinterpret_cast<int*>(state + n_slots + 2);
+    if (fork && !ctx->srays2 &&
+        !(dev_alloc(&ctx->srays2, 2 * chunk) && dev_alloc(&ctx->shits2, chunk) && dev_alloc(&ctx->spixel2, chunk) &&
+          dev_alloc(&ctx->scontrib2, chunk)))
+        return IMBART_ERR_OUT_OF_MEMORY;
+    GraphBuilder gb;
+    if (!ok(cudaGraphCreate(&gb.graph, 0), "cudaGraphCreate")) return IMBART_ERR_CUDA;
+    cudaGraphNode_t main = gb.kernel({}, range_begin_kernel, dim3(1), dim3(64), state, counts, n_slots, total, chunk);
+    main = gb.kernel({main}, camera_range_kernel, dim3(small_grid), dim3(128), ctx->camera, state, counts,
+                     ctx->rays[0], ctx->pixel[0], ctx->rng[0], ctx->thr[0], ctx->bounces[0]);
+    // Shadow-ray work: on the main chain, or (forked) on a branch of its own beside the next
+    // bounce's closest hits; acc[b] = accumulation node of bounce b.
+    std::vector<cudaGraphNode_t> acc(max_path_len, nullptr);
+    cudaGraphNode_t side = nullptr;
+    int cur = 0;
+    for (int b = 0; b < max_path_len && gb.good; ++b) {
+        const int* n_in = counts + 2 * b;
+        int* out = counts + 2 * b + 2;   // [0] next paths, [1] shadow rays
+        main = gb.trace({main}, scene, ctx->rays[cur], ctx->hits, n,
+                        b == 0 ? (IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT) : IMBART_TRACE_CLOSEST, n_in,
+                        ctx->graph_work + 4 * b);
+        ShadeParams p{};
+        p.s = sh->s;
+        p.n = n;
+        p.n_ptr = n_in;
+        p.max_path_len = max_path_len;
+        p.rr_start = rr_start;
+        p.rays = ctx->rays[cur]; p.hits = ctx->hits; p.pixel = ctx->pixel[cur]; p.rng = ctx->rng[cur];
+        p.thr = ctx->thr[cur]; p.bounces = ctx->bounces[cur];
+        const int nxt = 1 - cur;
+        p.o_rays = ctx->rays[nxt]; p.o_pixel = ctx->pixel[nxt]; p.o_rng = ctx->rng[nxt];
+        p.o_thr = ctx->thr[nxt]; p.o_bounces = ctx->bounces[nxt];
+        // Shadow queue of this bounce (the forked form alternates two).
+        const bool second = fork && (b & 1);
+        float4* srays = second ? ctx->srays2 : ctx->srays;
+        int4* shits = second ? ctx->shits2 : ctx->shits;
+        int* spixel = second ? ctx->spixel2 : ctx->spixel;
+        float4* scontrib = second ? ctx->scontrib2 : ctx->scontrib;
+        p.s_rays = srays; p.s_pixel = spixel; p.s_contrib = scontrib;
+        p.counts = out;
+        p.image = image;
+        if (group) {
+            main = gb.kernel({main}, shade_key_kernel, dim3(small_grid), dim3(256), sh->s, ctx->hits, n, n_in,
+                             ctx->keys);
+            const int tiles = group_tiles(n);
+            main = gb.kernel({main}, group_count_kernel, dim3(tiles), dim3(256), ctx->keys, n, n_in, ctx->tile_counts);
+            main = gb.kernel({main}, group_scan_kernel, dim3(1), dim3(1024), ctx->tile_counts, n, n_in);
+            main = gb.kernel({main}, group_scatter_kernel, dim3(tiles), dim3(256), ctx->keys, n, n_in,
+                             ctx->tile_counts, ctx->perm);
+            p.perm = ctx->perm;
+        }
+        // The shadow queue this bounce fills was last read by the shadow work of bounce b - 2
+        // (forked), or of bounce b - 1 (on the main chain already).
+        const cudaGraphNode_t reuse = fork && b >= 2 ? acc[b - 2] : nullptr;
+        main = gb.kernel({main, reuse}, pt_shade_kernel<false>, dim3(shade_grid), dim3(128), p);
+        const cudaGraphNode_t shaded = main;
+        cudaGraphNode_t t = gb.trace({shaded, fork ? side : nullptr}, scene, srays, shits, n, IMBART_TRACE_ANY,
+                                     out + 1, ctx->graph_work + 4 * b + 2);
+        t = gb.kernel({t}, shadow_accumulate_kernel<false>, dim3(small_grid), dim3(128), (const int*)(out + 1),
+                      (const int4*)shits, (const int*)spixel, (const float4*)scontrib, image, (const int*)nullptr,
+                      (const ReqDev*)nullptr);
+        acc[b] = t;
+        if (fork) side = t;
+        else main = t;
+        cur = nxt;
+    }
+    gb.kernel({main, side}, range_end_kernel, dim3(1), dim3(64), state, (const int*)counts, n_slots, max_path_len,
+              chunk);
+    int rc = gb.good ? 0 : (imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA);
+    if (!rc && ctx->exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ctx->exec, gb.graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ctx->exec);
+            ctx->exec = nullptr;
+        }
+    }
+    if (!rc && !ctx->exec && !ok(cudaGraphInstantiate(&ctx->exec, gb.graph, 0), "cudaGraphInstantiate")) {
+        ctx->exec = nullptr;
+        rc = IMBART_ERR_CUDA;
+    }
+    cudaGraphDestroy(gb.graph);
+    ctx->graph_kernels = gb.kernels;
+    return rc;
+}
+
+// A frame through the bounce-loop graph: the graph is (re)built when a launch parameter
+// changed, then replayed once per sample range.
+int render_graph(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh, const CameraParams& c,
+                 int max_path_len, int rr_start, float* image, long long total, long long chunk, bool group,
+                 bool fork, long long* stats, cudaStream_t st) {
+    if (!ensure_range_state(ctx, max_path_len, st)) return IMBART_ERR_OUT_OF_MEMORY;
+    std::vector<unsigned char> key = frame_key(scene, sh, image, total, chunk, max_path_len, rr_start, group, fork);
+    if (!ctx->exec || key != ctx->graph_key) {
+        ctx->graph_key.clear();
+        const int rc = capture_range(ctx, scene, sh, max_path_len, rr_start, image, total, chunk, group, fork);
+        if (rc) return rc;
+        ctx->graph_key = std::move(key);
+    }
+    const int n_slots = 2 * max_path_len + 2;
+    // A copy from pageable memory is staged before the call returns: `c` may go out of scope.
+    if (!ok(cudaMemcpyAsync(ctx->camera, &c, sizeof(CameraParams), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync") ||
+        !ok(cudaMemsetAsync(ctx->range_state, 0, sizeof(long long) * (n_slots + 2), st), "cudaMemsetAsync"))
+        return IMBART_ERR_CUDA;
+    const long long ranges = (total + chunk - 1) / chunk;
+    for (long long r = 0; r < ranges; ++r)
+        if (!ok(cudaGraphLaunch(ctx->exec, st), "cudaGraphLaunch")) return IMBART_ERR_CUDA;
+    note_launches((int)(ctx->graph_kernels * ranges));
+    if (stats) {
+        std::vector<long long> tot(n_slots + 2);
+        if (!ok(cudaMemcpyAsync(tot.data(), ctx->range_state, sizeof(long long) * tot.size(), cudaMemcpyDeviceToHost,
+                                st), "cudaMemcpyAsync") ||
+            !ok(cudaStreamSynchronize(st), "cudaStreamSynchronize"))
+            return IMBART_ERR_CUDA;
+        long long closest = 0, shadow = 0;
+        for (int b = 0; b < max_path_len; ++b) { closest += tot[1 + 2 * b]; shadow += tot[1 + 2 * b + 3]; }
+        stats[0] = closest; stats[1] = shadow; stats[2] = tot[1 + n_slots];
+    }
+    return 0;
 }
 
 }  // namespace
@@ -253,6 +555,10 @@ void imbart_pt_destroy(imbart_pt_context* c) {
     cudaFreeHost(c->host_counts);
     cudaFree(c->work);
     if (c->ev[0]) { cudaEventDestroy(c->ev[0]); cudaEventDestroy(c->ev[1]); }
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    cudaFree(c->range_state);
+    cudaFree(c->graph_work);
+    cudaFree(c->camera);
     cudaSetDevice(prev);
     delete c;
 }
@@ -297,6 +603,7 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     cudaSetDevice(ctx->device);
     if (!ensure_capacity(ctx, chunk)) { cudaSetDevice(prev); return IMBART_ERR_OUT_OF_MEMORY; }
     CameraParams c;
+    std::memset(&c, 0, sizeof(c));
     std::memcpy(c.r2w, raster_to_world, sizeof(c.r2w));
     std::memcpy(c.pos, cam_pos, sizeof(c.pos));
     c.width = width; c.height = height; c.spp = spp;
@@ -305,6 +612,14 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     long long n_closest = 0, n_shadow = 0, n_waves = 0;
     int rc = 0;
     imbart_pt_profile* prof = ctx->profile;
+    const bool group = sort_by_material() && __builtin_popcount(sh->kind_mask) > 1;
+    const int mode = graph_mode(ctx);
+    if (!prof && mode > 0) {
+        // Measurement (per-launch events, host-side ray counts) keeps the host-driven loop.
+        rc = render_graph(ctx, scene, sh, c, max_path_len, rr_start, image, total, chunk, group, mode == 2, stats, st);
+        cudaSetDevice(prev);
+        return rc;
+    }
     if (prof) {
         if (!ctx->ev[0]) { cudaEventCreate(&ctx->ev[0]); cudaEventCreate(&ctx->ev[1]); }
         if (prof->work && !ctx->work && !ok(cudaMalloc((void**)&ctx->work, sizeof(unsigned long long) * 6), "cudaMalloc")) {
@@ -360,15 +675,11 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
             p.s_rays = ctx->srays; p.s_pixel = ctx->spixel; p.s_contrib = ctx->scontrib;
             p.counts = ctx->counts;
             p.image = image;
-            if (sort_by_material() && __builtin_popcount(sh->kind_mask) > 1) {
+            if (group) {
                 // Group the wavefront's paths by material kind before shading.
-                if (!ok(cudaMemsetAsync(ctx->key_counts, 0, sizeof(int) * 2 * kShadeKeys, st), "cudaMemsetAsync")) {
-                    rc = IMBART_ERR_CUDA;
-                    break;
-                }
-                shade_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(sh->s, ctx->hits, n, ctx->keys, ctx->key_counts);
-                shade_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(ctx->keys, n, ctx->key_counts, ctx->perm);
-                note_launches(2);
+                shade_key_kernel<<<(n + 255) / 256, 256, 0, st>>>(sh->s, ctx->hits, n, nullptr, ctx->keys);
+                launch_grouping(ctx->keys, n, nullptr, ctx->tile_counts, ctx->perm, st);
+                note_launches(1);
                 p.perm = ctx->perm;
             }
             pt_shade_kernel<false><<<(n + 127) / 128, 128, 0, st>>>(p);
@@ -407,6 +718,31 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     }
     cudaSetDevice(prev);
     return rc;
+}
+
+int imbart_group_by_key(const unsigned char* keys, int n, int* perm, void* stream) {
+    if (n < 0 || (n > 0 && (!keys || !perm))) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_group_by_key: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (n == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    int* tiles = nullptr;
+    if (!ok(cudaMallocAsync((void**)&tiles, sizeof(int) * kShadeKeys * group_tiles(n), st), "cudaMallocAsync"))
+        return IMBART_ERR_OUT_OF_MEMORY;
+    launch_grouping(keys, n, nullptr, tiles, perm, st);
+    const bool good = ok(cudaGetLastError(), "grouping kernels");
+    cudaFreeAsync(tiles, st);
+    return good ? 0 : IMBART_ERR_CUDA;
+}
+
+int imbart_pt_set_graphs(imbart_pt_context* ctx, int enable) {
+    if (!ctx || enable < -1 || enable > 2) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_pt_set_graphs: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    ctx->graphs = enable;
+    return 0;
 }
 
 int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile) {

@@ -166,7 +166,11 @@ def camera_matrix(cam: G.Camera, width: int | None = None, height: int | None = 
 class PathTracer:
     """Wavefront path tracer (pt.cpp) on the GPU."""
 
-    def __init__(self, scene: GpuScene, max_path_len: int = 10, rr_start: int = 0, max_paths_in_flight: int = 0):
+    def __init__(self, scene: GpuScene, max_path_len: int = 10, rr_start: int = 0, max_paths_in_flight: int = 0,
+                 graphs: int | None = None):
+        """graphs: each sample range's bounce loop driven from the host (0), as a CUDA graph
+        (1), as a CUDA graph with the shadow-ray work on a branch of its own (2), or as
+        IMBART_PT_GRAPH says (None; default 2)."""
         self.scene = scene
         self.max_path_len = max_path_len
         self.rr_start = rr_start
@@ -175,6 +179,8 @@ class PathTracer:
         self.ctx = lib.imbart_pt_create(scene.device)
         if not self.ctx:
             raise N.ImbartError("imbart_pt_create: " + N.last_error()[1])
+        N.check(lib.imbart_pt_set_graphs(self.ctx, -1 if graphs is None else int(graphs)),
+                "imbart_pt_set_graphs")
         self.last_stats = np.zeros(3, np.int64)
 
     def render(self, spp: int, seed_base: int, width: int | None = None, height: int | None = None, image=None,

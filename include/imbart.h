@@ -384,7 +384,12 @@ void imbart_pt_destroy(imbart_pt_context* ctx);
  * max_path_len); Russian roulette from bounce `rr_start` on (0 = the reference). At most
  * max_paths_in_flight paths (<= 0: 16M) are in flight; larger frames run in consecutive
  * sample ranges with unchanged seeding. stats (host, may be NULL): closest-hit rays, shadow
- * rays, wavefronts. Synchronizes `stream` once per wavefront. */
+ * rays, wavefronts. By default the bounce loop of a sample range runs as a CUDA graph (built
+ * on the first call, rebuilt when a launch parameter other than the camera or the seed
+ * changes, replayed once per range; kernels read their queue sizes on the device): the call
+ * then returns without synchronizing, unless stats are asked for (one synchronization at the
+ * end). With graphs off (imbart_pt_set_graphs) or a profile set, the loop is driven from the
+ * host and synchronizes `stream` once per wavefront. */
 int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* shading,
                      const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
                      int max_path_len, int rr_start, unsigned long long seed_base, float* image,
@@ -406,6 +411,19 @@ typedef struct {
 
 /* Makes the following imbart_pt_render calls of `ctx` fill `profile` (NULL: stop). */
 int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile);
+
+/* How imbart_pt_render runs its bounce loop: 0 driven from the host (one synchronization per
+ * wavefront), 1 a CUDA graph (one chain of launches), 2 a CUDA graph whose shadow-ray work
+ * runs on a branch beside the next bounce's closest-hit launch, -1 the environment's choice
+ * (IMBART_PT_GRAPH, default 2). */
+int imbart_pt_set_graphs(imbart_pt_context* ctx, int enable);
+
+/* The queue order of RayQueue::sort_by_material (ray_queue.h:211-244) as a permutation:
+ * perm (DEVICE, n ints) lists the indices of keys (DEVICE, n bytes, each < 8) grouped by key
+ * in increasing key order, stably (indices increasing within a key). The path tracer, the
+ * VCM passes and the server group every wavefront this way before shading (key = material
+ * kind of the hit, 6 = miss, 7 = finished light-path slot). Stream-ordered. */
+int imbart_group_by_key(const unsigned char* keys, int n, int* perm, void* stream);
 
 /* ------------------------------------------------------------------------------------ */
 /* VCM family: VCM, BPT, PPM, LT and the VCM path tracer (VCMIntegrator<algo>, vcm.cpp)    */

@@ -114,3 +114,60 @@ def test_path_tracer_image_matches_reference(cuda, name, w, h, spp, max_len):
     err = rel_rmse(img, ref)
     assert err <= RMSE_TOL, f"relative RMSE {err:.2e}"
     assert pt.last_stats[0] >= w * h * spp and pt.last_stats[1] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,max_paths,mode", [("mixed", 0, 1), ("mixed", 0, 2), ("mixed", 10000, 2),
+                                                 ("config1", 7000, 1), ("config1", 7000, 2)])
+def test_graph_frames_equal_the_host_driven_loop(cuda, name, max_paths, mode):
+    """The bounce loop as a CUDA graph (queue sizes read on the device, one replay per sample
+    range; mode 2 with the shadow-ray work on a branch of its own) traces the same rays as the
+    host-driven loop: equal ray and wavefront counts, the image equal up to the order of the
+    float additions. Replays with a new seed (camera and seed are read on the device),
+    rebuilds into the same executable graph (a new Russian-roulette start) and into a new one
+    (a new path length) all stay equal."""
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    d = small_mixed_scene() if name == "mixed" else H.scene_desc("config1")
+    gs = GpuScene(d)
+    w, h, spp, max_len = 96, 64, 8, 6
+    host = PathTracer(gs, max_path_len=max_len, rr_start=2, max_paths_in_flight=max_paths, graphs=0)
+    graph = PathTracer(gs, max_path_len=max_len, rr_start=2, max_paths_in_flight=max_paths, graphs=mode)
+    for seed in (11, 12, 11):
+        a = host.render(spp, seed, w, h).cpu().numpy()
+        b = graph.render(spp, seed, w, h).cpu().numpy()
+        assert np.array_equal(host.last_stats, graph.last_stats), (host.last_stats, graph.last_stats)
+        assert a.sum() > 0 and rel_rmse(b, a) <= 1e-6
+    for rr, max_len in ((1, 6), (1, 4)):
+        host.rr_start = graph.rr_start = rr
+        host.max_path_len = graph.max_path_len = max_len
+        a = host.render(spp, 13, w, h).cpu().numpy()
+        b = graph.render(spp, 13, w, h).cpu().numpy()
+        assert np.array_equal(host.last_stats, graph.last_stats), (host.last_stats, graph.last_stats)
+        assert a.sum() > 0 and rel_rmse(b, a) <= 1e-6
+    # An image accumulated over two replays equals two host frames.
+    acc_h = host.render(spp, 5, w, h)
+    host.render(spp, 6, w, h, image=acc_h)
+    acc_g = graph.render(spp, 5, w, h)
+    graph.render(spp, 6, w, h, image=acc_g)
+    assert rel_rmse(acc_g.cpu().numpy(), acc_h.cpu().numpy()) <= 1e-6
+    host.close()
+    graph.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,kinds", [(0, 8), (1, 8), (2047, 3), (2048, 8), (2049, 2), (100003, 8), (5_000_000, 7)])
+def test_group_by_key_is_a_stable_counting_sort(cuda, n, kinds):
+    """sort_by_material's order (ray_queue.h:211-244) as the permutation the wavefront
+    kernels shade through: equal to a stable sort of the keys, on ragged tile counts, a
+    single entry, empty queues and keys absent from the queue."""
+    import torch
+    rng = np.random.default_rng(n + kinds)
+    keys = rng.integers(0, kinds, n).astype(np.uint8)
+    if n > 10:
+        keys[rng.random(n) < 0.6] = kinds - 1          # one dominant key, as in real wavefronts
+    k = torch.from_numpy(keys).cuda()
+    perm = torch.full((max(n, 1),), -1, dtype=torch.int32, device="cuda")
+    N.check(N.load().imbart_group_by_key(N.ptr(k) if n else None, n, N.ptr(perm), None), "imbart_group_by_key")
+    torch.cuda.synchronize()
+    got = perm.cpu().numpy()[:n]
+    assert np.array_equal(got, np.argsort(keys, kind="stable").astype(np.int32))
