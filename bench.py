@@ -4,9 +4,11 @@ Default workload (`--mode pt`): the wavefront path tracer on the 1920x1080 insta
 (200 instances of 8 seeded meshes, ~1.30M instanced triangles, materials Lambertian / Phong /
 Cook-Torrance / glass / mirror, 16 triangle area lights + constant environment), 16 samples
 per pixel, up to 8 bounces (max_path_len 9), Russian roulette from bounce 3. One step = one
-frame rendered entirely on the GPU (sample generation, traversal, shading, shadow rays).
-Scene data is resident in HBM; the path and shadow queues (~2.5 GB per 16M paths) exceed the
-126 MB L2. `value` counts every closest-hit and shadow ray the frame traced.
+frame rendered entirely on the GPU (sample generation, traversal, shading, shadow rays), its
+bounce loop replayed as a CUDA graph. Scene data is resident in HBM; the path and shadow
+queues (~285 B per path in flight, several GB) exceed the 126 MB L2. Before timing, the
+autotuner picks the traversal kernel of each query class and the wavefront size (untimed).
+`value` counts every closest-hit and shadow ray the frame traced.
 
 `e2e`: the same frames through the public API with the image copied back to pinned host
 memory every frame (the camera set-up goes host -> device per frame).
@@ -50,6 +52,10 @@ CPU_SAMPLE = (240, 135)  # bounded CPU sample: 1/64 of the pixels, same spp and 
 #       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-serving --no-vcm
 # (1 pass per launch). roofline.traffic scales it by the rays of an average launch.
 CLOSEST_DRAM_BYTES_PER_RAY = 46.9
+# Device queues per path in flight: two path queues (ray 32 B, pixel 4, RNG 8, throughput 16,
+# bounce 4), hit 16, two shadow queues (ray 32, hit 16, pixel 4, contribution 16), grouping
+# key 1 and permutation entry 4.
+QUEUE_BYTES_PER_PATH = 2 * 64 + 16 + 2 * 68 + 5
 
 
 def log(*a):
@@ -210,6 +216,14 @@ def run_pt(args):
                             "speedup": round(t["default_ms"] / max(t["ms"], 1e-9), 3)}
         del sets
         torch.cuda.synchronize()
+        # Wavefront size (paths in flight) for this frame shape, with the tuned kernels.
+        if not args.paths_in_flight:
+            wf = pt.autotune_wavefront(SPP, seed_base=777, stream=stream)
+            tuning["wavefront"] = {"paths_in_flight": pt.max_paths,
+                                   "ms_per_frame": {str(k): round(v, 2) for k, v in wf.items()}}
+        torch.cuda.synchronize()
+    if args.paths_in_flight:
+        pt.max_paths = args.paths_in_flight
     image = torch.zeros((H, W, 3), dtype=torch.float32, device=dev)
     base_seed = 1000 * (rank + 1)
 
@@ -281,6 +295,7 @@ def run_pt(args):
     peak, peak_src = peak_hbm()
 
     if rank == 0:
+        paths = min(pt.max_paths or (16 << 20), W * H * SPP)
         value = all_rays / (ms_max * 1e-3) / 1e6
         e2e_value = e2e_all / (e2e_ms * 1e-3) / 1e6
         cpu = None
@@ -302,7 +317,8 @@ def run_pt(args):
                        "rr_start_bounce": RR_START, "instances": len(desc.instances), "meshes": len(desc.meshes),
                        "instanced_triangles": desc.instanced_triangles, "lights": len(desc.lights) + 1,
                        "rays_per_step": int(all_rays / world / args.steps),
-                       "l2": "inputs larger than L2 (path + shadow queues ~2.5 GB per 16M paths in flight)",
+                       "l2": f"inputs larger than L2 (path + shadow queues ~{QUEUE_BYTES_PER_PATH * paths / 1e9:.1f} GB "
+                             f"for {paths} paths in flight)",
                        "parallelism": f"replicas x{world} (independent frames per GPU, different seeds)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
@@ -663,6 +679,8 @@ def main():
     ap.add_argument("--no-vcm", action="store_true", help="pt mode: skip the VCM-family iterations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="pt mode: keep the default kernel configurations")
+    ap.add_argument("--paths-in-flight", type=int, default=0,
+                    help="pt mode: wavefront size (paths in flight) instead of the autotuner's pick")
     ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
     ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
                     help="serve mode: config 5 arrival rates (req/s)")

@@ -123,7 +123,7 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 }
 
 // ---------------------------------------------------------------------------------------
-// Kernel variants. Variant 0 is the one-ray-per-thread kernel; variants 1..7 are the
+// Kernel variants. Variant 0 is the one-ray-per-thread kernel; variants 1..10 are the
 // persistent-warp kernel at different block sizes / register budgets / shared stack depths.
 // Closest-hit and any-hit queries pick their variants separately (measured on the B200:
 // persistent warps win on incoherent closest-hit rays, the one-ray-per-thread kernel on
@@ -134,6 +134,8 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 // Three query classes keep their own variant and refill threshold: incoherent closest hit,
 // any hit, and closest hit over coherent rays (camera rays, flag IMBART_TRACE_COHERENT),
 // which traverse best in static batches (refill only when the whole warp is idle).
+constexpr int kTraceVariants = 10;   // persistent-kernel shapes 1..10 (0: one ray per thread)
+
 struct TraceConfig {
     int variant, refill, postpone, variant_any;
     int refill_any, variant_coh, refill_coh;
@@ -243,6 +245,9 @@ LaunchSpec variant_spec(int variant, int count, int device, TraceParams& p) {
         case 5: return persistent_spec<kAny, kMasked, kStats, 64, 8, 16>(count, device, p);
         case 6: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8>(count, device, p);
         case 7: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10>(count, device, p);
+        case 8: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12>(count, device, p);
+        case 9: return persistent_spec<kAny, kMasked, kStats, 256, 4, 16>(count, device, p);
+        case 10: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12>(count, device, p);
         default: return {};
     }
 }
@@ -672,7 +677,7 @@ int imbart_scene_error_count(const imbart_scene* scene) {
 int64_t imbart_kernel_launch_count(void) { return launches_total(); }
 
 int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
-    if (variant < 0 || variant > 7 || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||
+    if (variant < 0 || variant > kTraceVariants || refill_lanes < 1 || refill_lanes > 32 || postpone_lanes < 0 ||
         postpone_lanes > 32) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_config: out of range");
         return IMBART_ERR_INVALID_ARGUMENT;
@@ -688,7 +693,7 @@ int imbart_set_trace_config(int variant, int refill_lanes, int postpone_lanes) {
 }
 
 int imbart_set_trace_class(int flags, int variant, int refill_lanes) {
-    if (variant < 0 || variant > 7 || refill_lanes < 1 || refill_lanes > 32 || flags < 0 || flags > 3) {
+    if (variant < 0 || variant > kTraceVariants || refill_lanes < 1 || refill_lanes > 32 || flags < 0 || flags > 3) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_class: out of range");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
@@ -737,12 +742,12 @@ int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imb
         *ms /= 3.0f;
         return 0;
     };
-    static const int kRefills[] = {8, 16, 24, 32};
+    static const int kRefills[] = {4, 8, 16, 24, 32};
     float default_ms = 0.0f, best_ms = FLT_MAX;
     int best_v = v0, best_r = r0;
     int rc = time_config(v0, r0, &default_ms);
     if (!rc) { best_ms = default_ms; }
-    for (int v = 1; v <= 7 && !rc; ++v)
+    for (int v = 1; v <= kTraceVariants && !rc; ++v)
         for (int r : kRefills) {
             float ms = 0.0f;
             rc = time_config(v, r, &ms);
@@ -763,7 +768,7 @@ int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imb
 }
 
 int imbart_set_trace_variant_any(int variant) {
-    if (variant < 0 || variant > 7) {
+    if (variant < 0 || variant > kTraceVariants) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_trace_variant_any: out of range");
         return IMBART_ERR_INVALID_ARGUMENT;
     }

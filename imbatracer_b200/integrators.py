@@ -203,6 +203,36 @@ class PathTracer:
         self.last_stats = stats
         return image
 
+    def autotune_wavefront(self, spp: int, seed_base: int = 0, width: int | None = None, height: int | None = None,
+                           sizes=(4 << 20, 8 << 20, 16 << 20, 32 << 20), repeats: int = 2, stream=None):
+        """Picks the wavefront size (paths in flight) for frames of this shape: one untimed
+        frame per size (it grows the queues and builds the graph), then `repeats` frames timed
+        with CUDA events on the stream; keeps the fastest in max_paths_in_flight. Returns
+        {size: ms per frame}."""
+        import torch
+        cam = self.scene.desc.camera
+        w, h = width or cam.width, height or cam.height
+        dev = torch.device("cuda", self.scene.device)
+        st = stream or torch.cuda.current_stream(dev)
+        image = torch.zeros((h, w, 3), dtype=torch.float32, device=dev)
+        total = w * h * spp
+        times = {}
+        for size in sizes:
+            size = int(min(size, total))
+            if size in times:
+                continue
+            self.max_paths = size
+            self.render(spp, seed_base, w, h, image=image, stream=st)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for k in range(repeats):
+                self.render(spp, seed_base + 1 + k, w, h, image=image, stream=st)
+            e1.record(st)
+            e1.synchronize()
+            times[size] = e0.elapsed_time(e1) / repeats
+        self.max_paths = min(times, key=times.get)
+        return times
+
     def close(self):
         if getattr(self, "ctx", None):
             N.load().imbart_pt_destroy(self.ctx)

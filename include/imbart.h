@@ -228,9 +228,9 @@ int imbart_scene_error_count(const imbart_scene* scene);
 int64_t imbart_kernel_launch_count(void);
 
 /* Process-wide traversal kernel configuration (the tuning knobs of the autotuner):
- * variant 0 = one ray per thread; 1..7 = persistent warps (1: 128 threads x 4 blocks/SM,
+ * variant 0 = one ray per thread; 1..10 = persistent warps (1: 128 threads x 4 blocks/SM,
  * 16-entry shared stack; 2: 128 x 6, 12; 3: 256 x 2, 16; 4: 256 x 3, 12; 5: 64 x 8, 16;
- * 6: 256 x 4, 8; 7: 128 x 7, 10); refill_lanes (1..32): a warp fetches new rays once this
+ * 6: 256 x 4, 8; 7: 128 x 7, 10; 8: 256 x 4, 12; 9: 256 x 4, 16; 10: 128 x 8, 12); refill_lanes (1..32): a warp fetches new rays once this
  * many lanes are idle; postpone_lanes (0..32): triangle tests are postponed while fewer than
  * postpone_lanes/32 of the live lanes would test together (0 = never).
  * imbart_set_trace_config sets the variant of both query types; imbart_set_trace_variant_any
@@ -242,14 +242,14 @@ int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes
 int imbart_get_trace_variant_any(void);
 
 /* The configuration of one query class: flags IMBART_TRACE_CLOSEST (incoherent closest hit),
- * IMBART_TRACE_ANY, or IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT. variant 1..7 (threads
+ * IMBART_TRACE_ANY, or IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT. variant 1..10 (threads
  * per block x blocks per SM x shared stack entries of the persistent kernel, 0: one ray per
  * thread), refill_lanes: idle lanes a warp waits for before it fetches new rays. */
 int imbart_set_trace_class(int flags, int variant, int refill_lanes);
 int imbart_get_trace_class(int flags, int* variant, int* refill_lanes);
 
 /* Autotuner: times every persistent-kernel configuration of the query class of `flags`
- * (variants 1..7 x refill 8, 16, 24, 32; one warm-up and three timed launches each, CUDA
+ * (variants 1..10 x refill 4, 8, 16, 24, 32; one warm-up and three timed launches each, CUDA
  * events on `stream`) on `count` DEVICE rays, keeps the fastest as the class's configuration
  * and reports it with the time of the configuration it replaced. Hits are written to `hits`.
  * Run it on rays like those the class will trace (camera rays, bounce rays, shadow rays). */

@@ -226,7 +226,7 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
             t = N.TraceTuning()
             N.check(lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), len(rays), flags, None,
                                               C.byref(t)), "autotune")
-            assert 1 <= t.variant <= 7 and t.refill in (8, 16, 24, 32) and 0 < t.ms <= t.default_ms * 1.0001
+            assert 1 <= t.variant <= 10 and t.refill in (4, 8, 16, 24, 32) and 0 < t.ms <= t.default_ms * 1.0001
             v, r = C.c_int(0), C.c_int(0)
             lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
             assert (v.value, r.value) == (t.variant, t.refill)
@@ -237,6 +237,38 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
         hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
         assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0)
         assert lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), 0, 0, None, None) != 0
+        lib.imbart_clear_error()
+    finally:
+        for flags, (v, r) in saved.items():
+            lib.imbart_set_trace_class(flags, v, r)
+
+
+@pytest.mark.gpu
+def test_every_kernel_variant_is_exact(cuda):
+    """Each traversal kernel shape the autotuner may pick (0: one ray per thread, 1..10:
+    persistent warps at different block sizes, blocks per SM and shared stack depths) gives
+    the oracle's closest hits bit for bit and its occlusion answers."""
+    import ctypes as C
+    lib = N.load()
+    saved = {}
+    for flags in (N.TRACE_CLOSEST, N.TRACE_ANY):
+        v, r = C.c_int(0), C.c_int(0)
+        lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
+        saved[flags] = (v.value, r.value)
+    try:
+        td = H.traversal_data("config2")
+        ds = S.DeviceScene(td)
+        rays = H.ray_set("config2", 20000, seed=21)
+        ref = O.trace_node2(td, rays)
+        refa = O.trace_node2(td, rays, any_hit=True)
+        for variant in range(11):
+            for flags in saved:
+                N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
+            hits, _, _ = run_gpu(ds, rays)
+            assert H.hits_equal(ref, hits).all(), variant
+            hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
+            assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0), variant
+        assert lib.imbart_set_trace_class(N.TRACE_CLOSEST, 11, 16) != 0
         lib.imbart_clear_error()
     finally:
         for flags, (v, r) in saved.items():
