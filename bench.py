@@ -136,6 +136,67 @@ def trace_bytes(rays: int, work) -> int:
     return 48 * rays + 80 * int(work[0]) + 48 * int(work[1]) + 64 * int(work[2])
 
 
+def frame_roofline(pt, frame):
+    """Closest-hit traversal inside path-traced frames: one frame with every traversal
+    launch timed by CUDA events on the launching stream (the host-driven loop, so each launch
+    is timed alone), one with the statistics variant (identical hits) for the node / triangle
+    / instance counts. `frame(seed)` renders one frame. Returns (profile, work, GB/s)."""
+    from imbatracer_b200 import native as N
+    lib = N.load()
+    prof = N.PtProfile()
+    prof.events = 1
+    lib.imbart_pt_set_profile(pt.ctx, C_ref(prof))
+    frame(30_000)
+    lib.imbart_pt_set_profile(pt.ctx, None)
+    work = N.PtProfile()
+    work.work = 1
+    lib.imbart_pt_set_profile(pt.ctx, C_ref(work))
+    frame(30_000)
+    lib.imbart_pt_set_profile(pt.ctx, None)
+    closest_bytes = trace_bytes(work.closest_rays, work.closest_work)
+    achieved = closest_bytes / max(prof.closest_launches, 1) / (prof.closest_ms / max(prof.closest_launches, 1) * 1e-3) / 1e9
+    return prof, work, achieved
+
+
+def config3_roofline(torch, dev, stream, peak):
+    """The same roofline on the config-3 scene (2M triangles, 400 displaced spheres, one
+    level): path-traced 1280x720 frames at 4 spp, max_path_len 9, traversal kernels tuned on
+    the scene's own rays first (untimed)."""
+    import ctypes
+    from imbatracer_b200 import native as N
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    lib = N.load()
+    classes = (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)
+    saved = []
+    for flags in classes:
+        v, r = ctypes.c_int(0), ctypes.c_int(0)
+        lib.imbart_get_trace_class(flags, ctypes.byref(v), ctypes.byref(r))
+        saved.append((flags, v.value, r.value))
+    desc = G.config3()
+    gs = GpuScene(desc, device=dev.index or 0)
+    sets = make_wavefront(desc, gs.trace_scene, torch, dev, 99)
+    for (rays, _), flags in zip(sets, classes):
+        hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
+        gs.trace_scene.autotune(rays, hits, flags, stream=stream)
+    del sets
+    pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
+    image = torch.zeros((desc.camera.height, desc.camera.width, 3), dtype=torch.float32, device=dev)
+    for k in range(2):
+        pt.render(4, 500 + k, image=image, stream=stream)
+    prof, work, achieved = frame_roofline(pt, lambda seed: pt.render(4, seed, image=image, stream=stream))
+    torch.cuda.synchronize()
+    out = {"workload": f"config 3: {desc.instanced_triangles} triangles, 1280x720 at 4 spp, max_path_len {MAX_PATH_LEN}",
+           "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+           "closest_mrays_s": round(work.closest_rays / max(prof.closest_ms, 1e-9) / 1e3, 1),
+           "bytes_per_ray": round(trace_bytes(work.closest_rays, work.closest_work) / max(work.closest_rays, 1), 1),
+           "launches": int(prof.closest_launches)}
+    pt.close()
+    for flags, v, r in saved:   # the main frame's tuning again for what follows
+        lib.imbart_set_trace_class(flags, v, r)
+    return out
+
+
 class _StdoutToStderr:
     """Sends file descriptor 1 to stderr while the reference's C++ code prints its progress, so
     that the bench's stdout carries only the JSON line."""
@@ -212,7 +273,7 @@ def run_pt(args):
                                                 (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)):
             hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
             t = gs.trace_scene.autotune(rays, hits, flags, stream=stream)
-            tuning[name] = {"variant": t["variant"], "refill": t["refill"],
+            tuning[name] = {"variant": t["variant"], "refill": t["refill"], "tri_batch": t["tri_batch"],
                             "speedup": round(t["default_ms"] / max(t["ms"], 1e-9), 3)}
         del sets
         torch.cuda.synchronize()
@@ -273,26 +334,15 @@ def run_pt(args):
     torch.cuda.synchronize()
     e2e_ms, e2e_all = job_totals(q0.elapsed_time(q1), e2e_rays, dev, world)
 
-    # Roofline of the dominant kernel (closest-hit traversal): one frame with every traversal
-    # launch timed by CUDA events on the launching stream, one frame with the statistics
-    # variant (identical hits) for the node / triangle / instance counts.
-    prof = N.PtProfile()
-    prof.events = 1
-    lib.imbart_pt_set_profile(pt.ctx, C_ref(prof))
-    frame(30_000)
-    lib.imbart_pt_set_profile(pt.ctx, None)
-    work = N.PtProfile()
-    work.work = 1
-    lib.imbart_pt_set_profile(pt.ctx, C_ref(work))
-    frame(30_000)
-    lib.imbart_pt_set_profile(pt.ctx, None)
+    # Roofline of the dominant kernel (closest-hit traversal) inside the frame.
+    prof, work, achieved = frame_roofline(pt, frame)
     torch.cuda.synchronize()
     closest_bytes = trace_bytes(work.closest_rays, work.closest_work)
     shadow_bytes = trace_bytes(work.shadow_rays, work.shadow_work)
     per_launch_bytes = closest_bytes / max(prof.closest_launches, 1)
     per_launch_ms = prof.closest_ms / max(prof.closest_launches, 1)
-    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, peak_src = peak_hbm()
+    roof3 = config3_roofline(torch, dev, stream, peak) if world == 1 and not args.no_config3 else None
 
     if rank == 0:
         paths = min(pt.max_paths or (16 << 20), W * H * SPP)
@@ -337,6 +387,7 @@ def run_pt(args):
                          "shadow_mrays_s": round(work.shadow_rays / max(prof.shadow_ms, 1e-9) / 1e3, 1)},
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 16 * 4 + 12,
                     "d2h_bytes_per_step": W * H * 12},
+            "roofline_config3": roof3,
             "gpu_launches": int(launches),
             "autotune": tuning,
             "clocks": clk,
@@ -682,6 +733,7 @@ def main():
     ap.add_argument("--paths-in-flight", type=int, default=0,
                     help="pt mode: wavefront size (paths in flight) instead of the autotuner's pick")
     ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
+    ap.add_argument("--no-config3", action="store_true", help="pt mode: skip the config-3 traversal roofline")
     ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
                     help="serve mode: config 5 arrival rates (req/s)")
     args = ap.parse_args()

@@ -111,8 +111,9 @@ int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, c
                    const int* count_ptr, int* work);
 
 // The traversal configuration in force (variant, refill, postpone, any-hit variant and refill,
-// coherent variant and refill): a captured launch is stale once it changes.
-void trace_config_snapshot(int out[7]);
+// coherent variant and refill, triangle batches of the three classes): a launch recorded in a
+// graph is stale once it changes.
+void trace_config_snapshot(int out[10]);
 // Every scene value a traversal launch takes into its parameters (array pointers, root,
 // masks, device): two launches with equal keys and arguments are the same launch.
 void scene_launch_key(const imbart_scene* s, unsigned long long out[12]);

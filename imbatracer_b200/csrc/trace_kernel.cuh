@@ -56,6 +56,7 @@ struct TraceParams {
     int total_warps;                        // warps in the launch
     int refill_lanes;                       // refill a warp's idle lanes once this many are idle
     int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
+    int tri_batch;                          // triangles a lane tests per loop trip (0: its whole group)
 };
 
 constexpr uint32_t kEntryTri = 3u;      // triangle group (postponed): x = prim base, y = prim mask
@@ -488,7 +489,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
         if (t_mask != 0) {
             if (bottom) {
                 bool stop = false;
+                int tested = 0;
                 while (t_mask != 0) {
+                    // The rest of the group waits for the next trip (the lanes with node work
+                    // take their node step meanwhile).
+                    if (p.tri_batch > 0 && tested == p.tri_batch) break;
+                    ++tested;
                     // Postpone only while node work remains, so that a ray with nothing
                     // but triangles left always makes progress.
                     if (g_hits != 0 && __popc(__activemask()) * 32 < n_live * p.postpone_lanes) {

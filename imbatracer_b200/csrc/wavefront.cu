@@ -183,7 +183,7 @@ struct FrameGraphKey {
     ShadingScene s;
     float* image;
     long long total, chunk;
-    int max_path_len, rr_start, group, fork, trace_cfg[7];
+    int max_path_len, rr_start, group, fork, trace_cfg[10];
 };
 
 std::vector<unsigned char> frame_key(const imbart_scene* scene, const imbart_shading* sh, float* image, long long total,

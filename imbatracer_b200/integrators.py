@@ -184,7 +184,10 @@ class PathTracer:
         self.last_stats = np.zeros(3, np.int64)
 
     def render(self, spp: int, seed_base: int, width: int | None = None, height: int | None = None, image=None,
-               stream=None, cam: G.Camera | None = None):
+               stream=None, cam: G.Camera | None = None, stats: bool = True):
+        """Adds one frame to `image` (a new zeroed image when None) on `stream`. With stats,
+        last_stats holds the frame's closest-hit rays, shadow rays and wavefronts (one
+        synchronization at the end); without, a graph-driven frame returns unsynchronized."""
         import torch
         cam = cam or self.scene.desc.camera
         w = width or cam.width
@@ -195,12 +198,14 @@ class PathTracer:
         if image is None:
             image = torch.zeros((h, w, 3), dtype=torch.float32, device=dev)
         st = None if stream is None else stream.cuda_stream
-        stats = np.zeros(3, np.int64)
+        out = np.zeros(3, np.int64)
         N.check(N.load().imbart_pt_render(self.ctx, self.scene.trace_scene.handle, self.scene.shading, N.ptr(r2w),
                                           N.ptr(pos), w, h, spp, self.max_path_len, self.rr_start,
-                                          seed_base & (2 ** 64 - 1), N.ptr(image), self.max_paths, N.ptr(stats), st),
+                                          seed_base & (2 ** 64 - 1), N.ptr(image), self.max_paths,
+                                          N.ptr(out) if stats else None, st),
                 "imbart_pt_render")
-        self.last_stats = stats
+        if stats:
+            self.last_stats = out
         return image
 
     def autotune_wavefront(self, spp: int, seed_base: int = 0, width: int | None = None, height: int | None = None,

@@ -76,7 +76,8 @@ class SceneSource(C.Structure):
 
 
 class TraceTuning(C.Structure):
-    _fields_ = [("variant", C.c_int), ("refill", C.c_int), ("ms", C.c_float), ("default_ms", C.c_float)]
+    _fields_ = [("variant", C.c_int), ("refill", C.c_int), ("ms", C.c_float), ("default_ms", C.c_float),
+                ("tri_batch", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -171,6 +172,8 @@ _SIGNATURES = {
     "imbart_set_trace_class": (I, [I, I, I]),
     "imbart_get_trace_class": (I, [I, P, P]),
     "imbart_trace_autotune": (I, [P, P, P, I, I, P, C.POINTER(TraceTuning)]),
+    "imbart_set_trace_tri_batch": (I, [I, I]),
+    "imbart_get_trace_tri_batch": (I, [I]),
     "imbart_shading_set_env_map": (I, [P, I, C.c_float]),
     "imbart_scene_build_gpu": (P, [C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, I, P, C.POINTER(C.c_float)]),
     "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),

@@ -273,7 +273,8 @@ class DeviceScene:
         st = None if stream is None else stream.cuda_stream
         N.check(N.load().imbart_trace_autotune(self.handle, N.ptr(rays), N.ptr(hits), rays.shape[0], flags, st,
                                                C.byref(t)), "imbart_trace_autotune")
-        return {"variant": t.variant, "refill": t.refill, "ms": t.ms, "default_ms": t.default_ms}
+        return {"variant": t.variant, "refill": t.refill, "tri_batch": t.tri_batch, "ms": t.ms,
+                "default_ms": t.default_ms}
 
     def device_arrays(self):
         lib = N.load()

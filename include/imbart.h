@@ -248,16 +248,24 @@ int imbart_get_trace_variant_any(void);
 int imbart_set_trace_class(int flags, int variant, int refill_lanes);
 int imbart_get_trace_class(int flags, int* variant, int* refill_lanes);
 
+/* Triangle batch of a query class (persistent kernels): the triangles a lane tests per loop
+ * trip before the warp's lanes with node work take their next node step; 0 = the whole leaf
+ * group at once. 0..24, default 2 (IMBART_TRACE_TRI_BATCH). Hits do not depend on it. */
+int imbart_set_trace_tri_batch(int flags, int tri_batch);
+int imbart_get_trace_tri_batch(int flags);
+
 /* Autotuner: times every persistent-kernel configuration of the query class of `flags`
- * (variants 1..10 x refill 4, 8, 16, 24, 32; one warm-up and three timed launches each, CUDA
- * events on `stream`) on `count` DEVICE rays, keeps the fastest as the class's configuration
- * and reports it with the time of the configuration it replaced. Hits are written to `hits`.
+ * (variants 1..10 x refill 4, 8, 16, 24, 32, then triangle batches 0..4 of the best; one
+ * warm-up and three timed launches each, CUDA events on `stream`) on `count` DEVICE rays,
+ * keeps the fastest as the class's configuration and reports it with the time of the
+ * configuration it replaced. Hits are written to `hits`.
  * Run it on rays like those the class will trace (camera rays, bounce rays, shadow rays). */
 typedef struct {
     int variant;
     int refill;
     float ms;          /* per launch, the chosen configuration */
     float default_ms;  /* per launch, the configuration before tuning */
+    int tri_batch;     /* the chosen triangle batch (imbart_set_trace_tri_batch) */
 } imbart_trace_tuning;
 int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imbart_hit* hits, int count, int flags,
                           void* stream, imbart_trace_tuning* out);

@@ -171,3 +171,65 @@ def test_group_by_key_is_a_stable_counting_sort(cuda, n, kinds):
     torch.cuda.synchronize()
     got = perm.cpu().numpy()[:n]
     assert np.array_equal(got, np.argsort(keys, kind="stable").astype(np.int32))
+
+
+@pytest.mark.gpu
+def test_graph_frames_edge_cases(cuda):
+    """Graph-driven frames at the edges: one pixel and one sample, camera rays only
+    (max_path_len 1: no continuation, shadow rays only), wavefronts of one path, and a
+    frame whose last sample range holds a single path; each equals the host-driven loop."""
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    gs = GpuScene(small_mixed_scene())
+    cases = [(1, 1, 1, 6, 0), (16, 8, 2, 1, 0), (5, 3, 2, 4, 1), (9, 7, 3, 5, 47), (9, 7, 3, 5, 94)]
+    for w, h, spp, max_len, max_paths in cases:
+        host = PathTracer(gs, max_path_len=max_len, max_paths_in_flight=max_paths, graphs=0)
+        graph = PathTracer(gs, max_path_len=max_len, max_paths_in_flight=max_paths, graphs=2)
+        a = host.render(spp, 3, w, h).cpu().numpy()
+        b = graph.render(spp, 3, w, h).cpu().numpy()
+        assert np.array_equal(host.last_stats, graph.last_stats), (w, h, spp, max_len, max_paths)
+        den = max(float(np.sqrt(np.mean(a.astype(np.float64) ** 2))), 1e-30)
+        assert float(np.sqrt(np.mean((b.astype(np.float64) - a) ** 2))) / den <= 1e-6
+        host.close()
+        graph.close()
+    # Without statistics the call does not synchronize; the stream orders the image read.
+    pt = PathTracer(gs, max_path_len=5, graphs=2)
+    a = pt.render(4, 8, 40, 30).cpu().numpy()
+    b = pt.render(4, 8, 40, 30, stats=False).cpu().numpy()
+    assert a.sum() > 0 and rel_rmse(b, a) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_graph_frames_beside_device_wide_synchronization(cuda):
+    """A thread that renders graph-driven frames while another thread creates scenes (whose
+    set-up synchronizes the whole device): both succeed, and the frames equal the same frames
+    rendered alone. (Graphs are built with the graph API, not by stream capture, which such a
+    synchronization would invalidate.)"""
+    import threading
+    import torch
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    d = small_mixed_scene()
+    gs = GpuScene(d)
+    alone = [PathTracer(gs, max_path_len=5, graphs=2).render(2, 100 + k, 48, 32).cpu().numpy() for k in range(6)]
+    out, errors = [], []
+
+    def render():
+        try:
+            torch.cuda.set_device(0)
+            pt = PathTracer(gs, max_path_len=5, graphs=2)
+            for k in range(6):
+                pt.render(2, 100 + k, 48, 32, cam=None)   # a fresh image (new graph) every frame
+                out.append(pt.render(2, 100 + k, 48, 32).cpu().numpy())
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    t = threading.Thread(target=render)
+    t.start()
+    scenes = []
+    while t.is_alive():
+        scenes.append(GpuScene(d))
+        torch.cuda.synchronize()
+    t.join()
+    assert not errors, errors
+    assert len(scenes) >= 1 and len(out) == 6
+    for a, b in zip(alone, out):
+        assert rel_rmse(b, a) <= 1e-6

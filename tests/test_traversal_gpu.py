@@ -214,7 +214,7 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
     for flags in (N.TRACE_CLOSEST, N.TRACE_ANY, N.TRACE_CLOSEST | N.TRACE_COHERENT):
         v, r = C.c_int(0), C.c_int(0)
         lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
-        saved[flags] = (v.value, r.value)
+        saved[flags] = (v.value, r.value, lib.imbart_get_trace_tri_batch(flags))
     try:
         td = H.traversal_data("config2")
         ds = S.DeviceScene(td)
@@ -230,6 +230,7 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
             v, r = C.c_int(0), C.c_int(0)
             lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
             assert (v.value, r.value) == (t.variant, t.refill)
+            assert lib.imbart_get_trace_tri_batch(flags) == t.tri_batch and 0 <= t.tri_batch <= 4
         ref = O.trace_node2(td, rays)
         hits, _, _ = run_gpu(ds, rays)
         assert H.hits_equal(ref, hits).all()
@@ -239,22 +240,24 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
         assert lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), 0, 0, None, None) != 0
         lib.imbart_clear_error()
     finally:
-        for flags, (v, r) in saved.items():
+        for flags, (v, r, b) in saved.items():
             lib.imbart_set_trace_class(flags, v, r)
+            lib.imbart_set_trace_tri_batch(flags, b)
 
 
 @pytest.mark.gpu
 def test_every_kernel_variant_is_exact(cuda):
     """Each traversal kernel shape the autotuner may pick (0: one ray per thread, 1..10:
-    persistent warps at different block sizes, blocks per SM and shared stack depths) gives
-    the oracle's closest hits bit for bit and its occlusion answers."""
+    persistent warps at different block sizes, blocks per SM and shared stack depths; with
+    triangle batches 0, 1 and 2) gives the oracle's closest hits bit for bit and its
+    occlusion answers."""
     import ctypes as C
     lib = N.load()
     saved = {}
     for flags in (N.TRACE_CLOSEST, N.TRACE_ANY):
         v, r = C.c_int(0), C.c_int(0)
         lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
-        saved[flags] = (v.value, r.value)
+        saved[flags] = (v.value, r.value, lib.imbart_get_trace_tri_batch(flags))
     try:
         td = H.traversal_data("config2")
         ds = S.DeviceScene(td)
@@ -262,14 +265,18 @@ def test_every_kernel_variant_is_exact(cuda):
         ref = O.trace_node2(td, rays)
         refa = O.trace_node2(td, rays, any_hit=True)
         for variant in range(11):
-            for flags in saved:
-                N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
-            hits, _, _ = run_gpu(ds, rays)
-            assert H.hits_equal(ref, hits).all(), variant
-            hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
-            assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0), variant
+            for tri_batch in (0, 1, 2):
+                for flags in saved:
+                    N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
+                    N.check(lib.imbart_set_trace_tri_batch(flags, tri_batch), "imbart_set_trace_tri_batch")
+                hits, _, _ = run_gpu(ds, rays)
+                assert H.hits_equal(ref, hits).all(), (variant, tri_batch)
+                hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
+                assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0), (variant, tri_batch)
         assert lib.imbart_set_trace_class(N.TRACE_CLOSEST, 11, 16) != 0
+        assert lib.imbart_set_trace_tri_batch(N.TRACE_CLOSEST, -1) != 0
         lib.imbart_clear_error()
     finally:
-        for flags, (v, r) in saved.items():
+        for flags, (v, r, b) in saved.items():
             lib.imbart_set_trace_class(flags, v, r)
+            lib.imbart_set_trace_tri_batch(flags, b)
