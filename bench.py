@@ -45,13 +45,15 @@ SPP = 16
 MAX_PATH_LEN = 9        # 8 continuation bounces (path vertices incl. camera and light)
 RR_START = 3
 CPU_SAMPLE = (240, 135)  # bounded CPU sample: 1/64 of the pixels, same spp and bounces
-# DRAM bytes (read + write) per closest-hit ray inside this frame: 3,674 MB over the 78.3M
-# rays of the 18 closest-hit launches of one frame of this workload, captured with
+# DRAM bytes (read + write) per closest-hit ray inside this frame: 3,755 MB over the 78.3M
+# rays of the 9 closest-hit launches of one frame of this workload (one wavefront of all
+# samples), captured with
 #   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum
-#       --clock-control none -k regex:trace_persistent -s 36 -c 36
-#       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-serving --no-vcm
+#       --clock-control none -k regex:trace_persistent -s 54 -c 18
+#       python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-serving --no-vcm --no-config3
+#       --no-autotune --paths-in-flight 33177600
 # (1 pass per launch). roofline.traffic scales it by the rays of an average launch.
-CLOSEST_DRAM_BYTES_PER_RAY = 46.9
+CLOSEST_DRAM_BYTES_PER_RAY = 48.0
 # Device queues per path in flight: two path queues (ray 32 B, pixel 4, RNG 8, throughput 16,
 # bounce 4), hit 16, two shadow queues (ray 32, hit 16, pixel 4, contribution 16), grouping
 # key 1 and permutation entry 4.
