@@ -455,7 +455,7 @@ def run_reference(args):
 # Serving: the request server (batched) against the same requests one at a time (plain)
 # ---------------------------------------------------------------------------------------
 SERVE_MAX_PATH_LEN = 5        # 4 bounces, as the sphere-field renders
-SERVE_PATHS = 4 << 20         # paths per merged wavefront (and per single-request wavefront)
+SERVE_PATHS = int(os.environ.get("IMBART_SERVE_PATHS", 4 << 20))   # paths per merged (and single-request) wavefront
 SERVE_BUDGET = 16 << 30       # device pool of the batched server
 
 

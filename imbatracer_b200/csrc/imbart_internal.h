@@ -114,6 +114,10 @@ int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, c
 // coherent variant and refill, triangle batches of the three classes): a launch recorded in a
 // graph is stale once it changes.
 void trace_config_snapshot(int out[10]);
+// Persistent traversal launches on `s` use this share (0.05..1) of the resident block slots,
+// leaving the rest of the SMs to concurrent work on other streams.
+void scene_set_grid_share(imbart_scene* s, float share);
+
 // Every scene value a traversal launch takes into its parameters (array pointers, root,
 // masks, device): two launches with equal keys and arguments are the same launch.
 void scene_launch_key(const imbart_scene* s, unsigned long long out[12]);

@@ -220,7 +220,10 @@ struct Request {
     long long total = 0, generated = 0;
     // VCM-family frame
     imbart_vcm_request vq{};
-    int iter_done = 0;
+    int iter_done = 0;             // iterations finished
+    int iter_claimed = 0;          // iterations handed to lanes (several lanes may run one request)
+    int iter_running = 0;          // iterations in progress
+    int failed = 0;                // first error of an iteration (the last running lane completes it)
     cudaEvent_t ready = nullptr;   // recorded on the worker stream after the scene upload and image clear
     // ray batch
     const imbart_ray* rays = nullptr;
@@ -692,6 +695,11 @@ void fail_all_active(imbart_server* S, int code) {
     }
     S->active_rays.clear();
     for (Request* r : S->active_vcm) {
+        if (r->iter_running > 0) {   // a lane still renders into its image: that lane completes it
+            if (!r->failed) r->failed = code;
+            continue;
+        }
+        if (r->ready) { cudaEventDestroy(r->ready); r->ready = nullptr; }
         if (r->img_off != SIZE_MAX) S->alloc.release(r->img_off, r->img_bytes);
         release_request_locked(S, r);
         complete_locked(S, r, code);
@@ -700,6 +708,14 @@ void fail_all_active(imbart_server* S, int code) {
     for (Request* r : S->pending) complete_locked(S, r, code);
     S->pending.clear();
     S->n_cur = 0;
+}
+
+float serve_grid_share() {
+    static const float v = [] {
+        const char* e = std::getenv("IMBART_SERVE_GRID_SHARE");
+        return e && *e ? (float)std::atof(e) : 0.75f;
+    }();
+    return v;
 }
 
 // One merged wavefront. Returns false when there was nothing to do.
@@ -723,6 +739,18 @@ bool batched_wave(imbart_server* S) {
         note_launches(1);
     }
     const int n = (int)(S->n_cur + n_gen);
+    // While VCM-family iterations run on the lanes, the merged wavefront's persistent
+    // traversal launches leave a share of the SMs to the lanes' launches, which would
+    // otherwise wait for whole persistent launches to drain (config-4 mix: 177 -> 188 req/s
+    // at a share of 0.75; IMBART_SERVE_GRID_SHARE).
+    {
+        bool lanes_busy;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            lanes_busy = S->vcm_running > 0 || !S->active_vcm.empty();
+        }
+        scene_set_grid_share(S->pool_scene, lanes_busy ? serve_grid_share() : 1.0f);
+    }
     std::vector<BatchPiece> pieces;
     int n_bc = 0, n_ba = 0;
     plan_batches(S, pieces, n_bc, n_ba);
@@ -848,10 +876,12 @@ bool batched_wave(imbart_server* S) {
     return true;
 }
 
-// One iteration of a VCM-family request: its settings for iteration r->iter_done + 1
-// (seeds advanced by seed_step; the photon radius from the estimated pixel size when the
-// request gave none) rendered by imbart_vcm_render on `scene` / `sh` into `image`.
-int vcm_iteration(imbart_server* S, imbart_server::VcmLane& lane, Request* r, const imbart_scene* scene,
+// Iteration k + 1 (k = 0, 1, ...) of a VCM-family request: its settings (seeds advanced by
+// k * seed_step; the photon radius from the estimated pixel size when the request gave none,
+// estimated by the lane that runs iteration 1 before any other lane takes the request)
+// rendered by imbart_vcm_render on `scene` / `sh` into `image`. Iterations depend on their
+// index only, so several lanes may render iterations of one request at once.
+int vcm_iteration(imbart_server* S, imbart_server::VcmLane& lane, Request* r, int k_iter, const imbart_scene* scene,
                   const imbart_shading* sh, float* image, long long* stats) {
     if (!lane.vcm) {
         lane.vcm = imbart_vcm_create(S->device);
@@ -869,62 +899,77 @@ int vcm_iteration(imbart_server* S, imbart_server::VcmLane& lane, Request* r, co
         }
     }
     imbart_vcm_settings st = q.settings;
-    const unsigned long long k = (unsigned long long)r->iter_done;
+    const unsigned long long k = (unsigned long long)k_iter;
     st.light_seed = q.settings.light_seed + k * q.seed_step;
     st.camera_seed = q.settings.camera_seed + k * q.seed_step;
     // Camera paths in flight: the frame's samples of one iteration, at most the server's cap.
     const long long paths = std::min<long long>(S->cap, (long long)q.camera.width * q.camera.height * st.spp);
-    const int rc = imbart_vcm_render(lane.vcm, scene, sh, &q.camera, &st, r->iter_done + 1, image, paths, stats,
-                                     lane.stream);
-    if (!rc) r->iter_done += 1;
-    return rc;
+    return imbart_vcm_render(lane.vcm, scene, sh, &q.camera, &st, k_iter + 1, image, paths, stats, lane.stream);
 }
 
 // Batched mode: a VCM lane takes the admitted VCM-family request at the head of the round
-// robin, renders one iteration of it on the pool's copy of its scene, and puts it back (or
-// hands the finished image to the completion thread).
+// robin, claims its next iteration and puts it back at once (so that other lanes can run
+// later iterations of it meanwhile: a long request near the end of a batch is spread over
+// every lane), renders the iteration on the pool's copy of its scene, and the lane that ends
+// the last running iteration hands the finished image to the completion thread. Iteration 1
+// goes first alone when the photon radius still has to be estimated.
 void vcm_lane_main(imbart_server* S, int index) {
     cudaSetDevice(S->device);
     imbart_server::VcmLane& lane = S->vcm_lanes[index];
     for (;;) {
         Request* r;
+        int k = 0;
+        bool estimate = false;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv_vcm.wait(lk, [&] { return S->stop || !S->active_vcm.empty(); });
             if (S->active_vcm.empty()) return;
             r = S->active_vcm.front();
             S->active_vcm.pop_front();
+            if (r->failed || r->iter_claimed >= r->vq.iterations) continue;   // the running lanes complete it
+            k = r->iter_claimed++;
+            estimate = !(r->vq.settings.base_radius > 0.0f);
+            r->iter_running += 1;
             S->vcm_running += 1;
+            if (!estimate && r->iter_claimed < r->vq.iterations) {
+                S->active_vcm.push_back(r);
+                S->cv_vcm.notify_one();
+            }
         }
         SceneRec& s = *S->scenes[r->scene];
-        if (r->ready) {
-            // The lane's stream waits for the upload and the image clear on the worker stream.
-            cudaStreamWaitEvent(lane.stream, r->ready, 0);
-            cudaEventDestroy(r->ready);
-            r->ready = nullptr;
-        }
+        // The lane's stream waits for the upload and the image clear on the worker stream.
+        if (r->ready) cudaStreamWaitEvent(lane.stream, r->ready, 0);
         scene_pool_view_set_root(lane.view, s.root);
         imbart_shading sh;
         sh.device = S->device;
         sh.s = S->h_scenes[s.slot];
         long long stats[3] = {0, 0, 0};
-        int rc = vcm_iteration(S, lane, r, lane.view, &sh, reinterpret_cast<float*>(S->pool + r->img_off), stats);
+        int rc = vcm_iteration(S, lane, r, k, lane.view, &sh, reinterpret_cast<float*>(S->pool + r->img_off), stats);
         if (!rc && !cuda_check(cudaStreamSynchronize(lane.stream), "cudaStreamSynchronize")) rc = IMBART_ERR_CUDA;
         std::lock_guard<std::mutex> lk(S->mu);
         S->vcm_running -= 1;
+        r->iter_running -= 1;
         S->stats.closest_rays += stats[0];
         S->stats.shadow_rays += stats[1];
         S->stats.waves += stats[2];
-        if (rc) {
+        if (rc && !r->failed) r->failed = rc;
+        if (!rc) r->iter_done += 1;
+        if (estimate && !r->failed && r->iter_claimed < r->vq.iterations) {
+            S->active_vcm.push_back(r);   // the radius is known now: the other lanes may join
+            S->cv_vcm.notify_all();
+        }
+        if (r->iter_running > 0 || (!r->failed && r->iter_done < r->vq.iterations)) continue;
+        // The last running iteration of a finished or failed request (a failed one may still
+        // sit in the round robin).
+        S->active_vcm.erase(std::remove(S->active_vcm.begin(), S->active_vcm.end(), r), S->active_vcm.end());
+        if (r->ready) { cudaEventDestroy(r->ready); r->ready = nullptr; }
+        if (r->failed) {
             // A failed request gives its memory back; the others go on.
             S->alloc.release(r->img_off, r->img_bytes);
             r->img_off = SIZE_MAX;
             release_request_locked(S, r);
-            complete_locked(S, r, rc);
+            complete_locked(S, r, r->failed);
             S->cv_work.notify_all();
-        } else if (r->iter_done < r->vq.iterations) {
-            S->active_vcm.push_back(r);
-            S->cv_vcm.notify_one();
         } else {
             release_request_locked(S, r);
             S->jobs.push_back(imbart_server::Job{r, r->vq.image_host,
@@ -975,9 +1020,10 @@ int plain_request(imbart_server* S, Request* r) {
         } else {
             while (r->iter_done < r->vq.iterations) {
                 long long it[3] = {0, 0, 0};
-                const int rc = vcm_iteration(S, S->vcm_lanes[0], r, s.plain_scene, s.plain_shading, S->plain_image,
-                                             it);
+                const int rc = vcm_iteration(S, S->vcm_lanes[0], r, r->iter_done, s.plain_scene, s.plain_shading,
+                                             S->plain_image, it);
                 if (rc) return rc;
+                r->iter_done += 1;
                 for (int k = 0; k < 3; ++k) stats[k] += it[k];
             }
         }

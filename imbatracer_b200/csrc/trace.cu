@@ -31,6 +31,7 @@ struct imbart_scene {
     int* error_flags = nullptr;
     imbart_scene_info info{};
     bool owns_arrays = true;   // false for views into a node pool shared by several scenes
+    float grid_share = 1.0f;   // persistent launches use this share of the resident block slots
 };
 
 namespace imbart {
@@ -234,36 +235,38 @@ int max_grid(Kernel k, int block, int device) {
 
 // One persistent block per resident slot (fewer for short queues).
 template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
-LaunchSpec persistent_spec(int count, int device, TraceParams& p) {
+LaunchSpec persistent_spec(int count, int device, float share, TraceParams& p) {
     auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh>;
-    const int grid = std::min(max_grid(k, kBlock, device), (count + kBlock - 1) / kBlock);
+    const int slots = std::max(1, (int)(max_grid(k, kBlock, device) * share));
+    const int grid = std::min(slots, (count + kBlock - 1) / kBlock);
     p.total_warps = grid * (kBlock / 32);
     return {(const void*)k, dim3(grid), dim3(kBlock)};
 }
 
 template <bool kAny, bool kMasked, bool kStats>
-LaunchSpec variant_spec(int variant, int count, int device, TraceParams& p) {
+LaunchSpec variant_spec(int variant, int count, int device, float share, TraceParams& p) {
     switch (variant) {
-        case 1: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16>(count, device, p);
-        case 2: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12>(count, device, p);
-        case 3: return persistent_spec<kAny, kMasked, kStats, 256, 2, 16>(count, device, p);
-        case 4: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12>(count, device, p);
-        case 5: return persistent_spec<kAny, kMasked, kStats, 64, 8, 16>(count, device, p);
-        case 6: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8>(count, device, p);
-        case 7: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10>(count, device, p);
-        case 8: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12>(count, device, p);
-        case 9: return persistent_spec<kAny, kMasked, kStats, 256, 4, 16>(count, device, p);
-        case 10: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12>(count, device, p);
+        case 1: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16>(count, device, share, p);
+        case 2: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12>(count, device, share, p);
+        case 3: return persistent_spec<kAny, kMasked, kStats, 256, 2, 16>(count, device, share, p);
+        case 4: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12>(count, device, share, p);
+        case 5: return persistent_spec<kAny, kMasked, kStats, 64, 8, 16>(count, device, share, p);
+        case 6: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8>(count, device, share, p);
+        case 7: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10>(count, device, share, p);
+        case 8: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12>(count, device, share, p);
+        case 9: return persistent_spec<kAny, kMasked, kStats, 256, 4, 16>(count, device, share, p);
+        case 10: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12>(count, device, share, p);
         default: return {};
     }
 }
 
 template <bool kStats>
-LaunchSpec persistent_kernel_spec(int variant, bool any, bool masked, int count, int device, TraceParams& p) {
-    if (any && masked) return variant_spec<true, true, kStats>(variant, count, device, p);
-    if (any) return variant_spec<true, false, kStats>(variant, count, device, p);
-    if (masked) return variant_spec<false, true, kStats>(variant, count, device, p);
-    return variant_spec<false, false, kStats>(variant, count, device, p);
+LaunchSpec persistent_kernel_spec(int variant, bool any, bool masked, int count, int device, float share,
+                                  TraceParams& p) {
+    if (any && masked) return variant_spec<true, true, kStats>(variant, count, device, share, p);
+    if (any) return variant_spec<true, false, kStats>(variant, count, device, share, p);
+    if (masked) return variant_spec<false, true, kStats>(variant, count, device, share, p);
+    return variant_spec<false, false, kStats>(variant, count, device, share, p);
 }
 
 // The launch of one traversal query (kernel, grid, block and parameters) under the current
@@ -306,8 +309,8 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
         p.refill_lanes = std::min(std::max(refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
         p.tri_batch = std::max(any ? cfg.tri_batch_any : coherent ? cfg.tri_batch_coh : cfg.tri_batch, 0);
-        spec = stats ? persistent_kernel_spec<true>(variant, any, masked, count, s->device, p)
-                     : persistent_kernel_spec<false>(variant, any, masked, count, s->device, p);
+        spec = stats ? persistent_kernel_spec<true>(variant, any, masked, count, s->device, s->grid_share, p)
+                     : persistent_kernel_spec<false>(variant, any, masked, count, s->device, s->grid_share, p);
     }
     if (!spec.func) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");
@@ -506,13 +509,20 @@ int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, c
                : IMBART_ERR_CUDA;
 }
 
+void scene_set_grid_share(imbart_scene* s, float share) {
+    s->grid_share = std::min(std::max(share, 0.05f), 1.0f);
+}
+
 void scene_launch_key(const imbart_scene* s, unsigned long long out[12]) {
     out[0] = (unsigned long long)(uintptr_t)s->nodes; out[1] = (unsigned long long)(uintptr_t)s->tris;
     out[2] = (unsigned long long)(uintptr_t)s->insts; out[3] = (unsigned long long)(uintptr_t)s->indices;
     out[4] = (unsigned long long)(uintptr_t)s->texcoords; out[5] = (unsigned long long)(uintptr_t)s->masks;
     out[6] = (unsigned long long)(uintptr_t)s->mask_buffer; out[7] = (unsigned long long)(uintptr_t)s->error_flags;
     out[8] = (unsigned long long)s->n_masks; out[9] = (unsigned long long)(unsigned)s->info.root;
-    out[10] = (unsigned long long)s->info.masked; out[11] = (unsigned long long)s->device;
+    uint32_t share_bits;
+    std::memcpy(&share_bits, &s->grid_share, sizeof(share_bits));
+    out[10] = (unsigned long long)s->info.masked | ((unsigned long long)share_bits << 32);
+    out[11] = (unsigned long long)s->device;
 }
 
 void trace_config_snapshot(int out[10]) {

@@ -199,6 +199,27 @@ def test_vcm_family_requests_in_a_mix(cuda, scenes, mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["vcm", "bpt"])
+def test_one_long_vcm_request_spread_over_lanes(cuda, scenes, algo):
+    """A VCM-family request with many iterations and nothing beside it: the server's lanes
+    render its iterations concurrently (iterations depend on their index only), and the image
+    equals VcmIntegrator's iterations run one after another (up to the order of the float
+    additions); its photon radius is estimated once, before the other lanes join."""
+    from imbatracer_b200.serving import Server
+    srv = Server(mode="batched", hbm_budget=256 << 20, max_paths=20000)
+    ids = [srv.add_scene(d, td) for d, td in scenes]
+    d, td = scenes[1]
+    t, img = srv.submit_vcm(ids[1], d.camera, 40, 30, algo, iterations=12, max_path_len=5, light_seed=11,
+                            camera_seed=22, seed_step=SEED_STEP, light_seed_step=TILE_STEP)
+    res = srv.wait(t)
+    assert res["status"] == 0 and res["kind"] == 2
+    ref = vcm_alone(d, td, algo, 40, 30, 12, 5, 11, 22)
+    assert ref.sum() > 0 and rel_rmse(img, ref) <= MIX_TOL, rel_rmse(img, ref)
+    assert srv.stats()["failed"] == 0
+    srv.close()
+
+
+@pytest.mark.gpu
 def test_vcm_request_validation(cuda, scenes):
     from imbatracer_b200.serving import Server
     srv = Server(hbm_budget=64 << 20, max_paths=4096)
