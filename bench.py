@@ -177,7 +177,7 @@ def config3_roofline(torch, dev, stream, peak):
         saved.append((flags, v.value, r.value))
     desc = G.config3()
     gs = GpuScene(desc, device=dev.index or 0)
-    sets = make_wavefront(desc, gs.trace_scene, torch, dev, 99)
+    sets = make_wavefront(desc, gs.trace_scene, torch, dev, 99, shadow_from_bounce=True)
     for (rays, _), flags in zip(sets, classes):
         hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
         gs.trace_scene.autotune(rays, hits, flags, stream=stream)
@@ -270,7 +270,7 @@ def run_pt(args):
     # Autotuner (untimed): the kernel configuration of each query class on this scene's rays.
     tuning = {}
     if not args.no_autotune:
-        sets = make_wavefront(desc, gs.trace_scene, torch, dev, 4321)
+        sets = make_wavefront(desc, gs.trace_scene, torch, dev, 4321, shadow_from_bounce=True)
         for (rays, any_hit), name, flags in zip(sets, ("camera", "bounce", "shadow"),
                                                 (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)):
             hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
@@ -637,9 +637,11 @@ def make_scene():
     return desc, td
 
 
-def make_wavefront(desc, ds, torch, dev, seed: int):
+def make_wavefront(desc, ds, torch, dev, seed: int, shadow_from_bounce: bool = False):
     """Primary camera rays, one bounce of incoherent secondary rays from their hits, and one
-    shadow ray per hit towards a random light point (untimed set-up on the device)."""
+    shadow ray per hit towards a random light point (untimed set-up on the device). With
+    shadow_from_bounce the shadow set also holds one shadow ray per hit of the secondary rays
+    (as in a frame, where most shadow rays start at bounce hits)."""
     cam = desc.camera
     w, h = cam.width, cam.height
     g = torch.Generator(device=dev)
@@ -694,7 +696,36 @@ def make_wavefront(desc, ds, torch, dev, seed: int):
     sh[:, 3] = off
     sh[:, 4:7] = dv / dist[:, None]
     sh[:, 7] = dist - off
+    if shadow_from_bounce:
+        shits = torch.zeros((m, 4), dtype=torch.int32, device=dev)
+        ds.trace(sec.contiguous(), shits)
+        torch.cuda.synchronize()
+        sh2 = shadow_rays_from(sec, shits, lights, g, torch, dev)
+        sh = torch.cat([sh, sh2], 0)
     return [(prim.contiguous(), False), (sec.contiguous(), False), (sh.contiguous(), True)]
+
+
+def shadow_rays_from(rays, hits, lights, g, torch, dev):
+    """One shadow ray per hit of `rays` towards a random point of a random light triangle."""
+    hit = hits[:, 0] >= 0
+    t = hits[:, 2].view(torch.float32)
+    p = (rays[:, :3] + t[:, None] * rays[:, 4:7])[hit]
+    m = p.shape[0]
+    li = torch.randint(0, lights.shape[0], (m,), generator=g, device=dev)
+    r1 = torch.rand(m, generator=g, device=dev).sqrt()
+    r2 = torch.rand(m, generator=g, device=dev)
+    bu, bv = 1 - r1, r2 * r1
+    tri = lights[li]
+    lp = bu[:, None] * tri[:, 0] + bv[:, None] * tri[:, 1] + (1 - bu - bv)[:, None] * tri[:, 2]
+    dv = lp - p
+    dist = dv.norm(dim=-1)
+    off = 1e-3 * dist
+    out = torch.zeros((m, 8), dtype=torch.float32, device=dev)
+    out[:, :3] = p
+    out[:, 3] = off
+    out[:, 4:7] = dv / dist[:, None]
+    out[:, 7] = dist - off
+    return out
 
 
 def run_trace(args):

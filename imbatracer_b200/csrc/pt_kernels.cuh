@@ -383,7 +383,7 @@ __device__ __forceinline__ void shade_path(const ShadingScene& s, int max_path_l
 // samples) stay neighbours within their group, and the permutation is deterministic. Results
 // per path do not depend on the order.
 constexpr int kShadeKeys = 8;   // material kinds 0..5, 6: miss (7: a finished light-path slot)
-constexpr int kGroupTile = 2048;
+constexpr int kGroupTile = 8192;
 
 inline int group_tiles(long long n) { return (int)((n + kGroupTile - 1) / kGroupTile); }
 

@@ -155,7 +155,8 @@ def test_graph_frames_equal_the_host_driven_loop(cuda, name, max_paths, mode):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,kinds", [(0, 8), (1, 8), (2047, 3), (2048, 8), (2049, 2), (100003, 8), (5_000_000, 7)])
+@pytest.mark.parametrize("n,kinds", [(0, 8), (1, 8), (2047, 3), (8191, 3), (8192, 8), (8193, 2), (100003, 8),
+                                     (5_000_000, 7)])
 def test_group_by_key_is_a_stable_counting_sort(cuda, n, kinds):
     """sort_by_material's order (ray_queue.h:211-244) as the permutation the wavefront
     kernels shade through: equal to a stable sort of the keys, on ragged tile counts, a
