@@ -641,7 +641,8 @@ def make_wavefront(desc, ds, torch, dev, seed: int, shadow_from_bounce: bool = F
     """Primary camera rays, one bounce of incoherent secondary rays from their hits, and one
     shadow ray per hit towards a random light point (untimed set-up on the device). With
     shadow_from_bounce the shadow set also holds one shadow ray per hit of the secondary rays
-    (as in a frame, where most shadow rays start at bounce hits)."""
+    and the secondary set a second bounce from those hits (as in a frame, where most rays
+    start at bounce hits)."""
     cam = desc.camera
     w, h = cam.width, cam.height
     g = torch.Generator(device=dev)
@@ -702,6 +703,22 @@ def make_wavefront(desc, ds, torch, dev, seed: int, shadow_from_bounce: bool = F
         torch.cuda.synchronize()
         sh2 = shadow_rays_from(sec, shits, lights, g, torch, dev)
         sh = torch.cat([sh, sh2], 0)
+        # A second bounce: uniform directions in the hemisphere facing back along each hit ray.
+        hit2 = shits[:, 0] >= 0
+        t2 = shits[:, 2].view(torch.float32)
+        p2 = (sec[:, :3] + t2[:, None] * sec[:, 4:7])[hit2]
+        d2 = sec[hit2, 4:7]
+        k = p2.shape[0]
+        nd = torch.randn((k, 3), generator=g, device=dev)
+        nd = nd / nd.norm(dim=-1, keepdim=True)
+        flip2 = (nd * d2).sum(-1) > 0
+        nd[flip2] = -nd[flip2]
+        ter = torch.zeros((k, 8), dtype=torch.float32, device=dev)
+        ter[:, :3] = p2
+        ter[:, 3] = 1e-3 * t2[hit2]
+        ter[:, 4:7] = nd
+        ter[:, 7] = 3.0e38
+        sec = torch.cat([sec, ter], 0)
     return [(prim.contiguous(), False), (sec.contiguous(), False), (sh.contiguous(), True)]
 
 
