@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(256) group_count_kernel(const uint8_t* __restr
     int mine = 0;   // lane k < 8: this warp's entries with key k
     for (int r = 0; r < kGroupTile / 256; ++r) {
         const int i = base + r * 256 + threadIdx.x;
-        const int k = i < n ? keys[i] : kShadeKeys;
+        const int k = i < n ? min((int)keys[i], kShadeKeys - 1) : kShadeKeys;   // keys above 7 group as 7
         for (int kk = 0; kk < kShadeKeys; ++kk) {
             const int c = __popc(__ballot_sync(0xffffffffu, k == kk));
             if (lane == kk) mine += c;
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(256) group_scatter_kernel(const uint8_t* __res
     for (int r = 0; r < kGroupTile / 256; ++r) {
         const int i = base + r * 256 + threadIdx.x;
         const bool valid = i < n;
-        const int k = valid ? keys[i] : kShadeKeys;
+        const int k = valid ? min((int)keys[i], kShadeKeys - 1) : kShadeKeys;
         unsigned same = 0;
         for (int kk = 0; kk < kShadeKeys; ++kk) {
             const unsigned m = __ballot_sync(0xffffffffu, k == kk);

@@ -427,8 +427,8 @@ int imbart_pt_set_profile(imbart_pt_context* ctx, imbart_pt_profile* profile);
 int imbart_pt_set_graphs(imbart_pt_context* ctx, int enable);
 
 /* The queue order of RayQueue::sort_by_material (ray_queue.h:211-244) as a permutation:
- * perm (DEVICE, n ints) lists the indices of keys (DEVICE, n bytes, each < 8) grouped by key
- * in increasing key order, stably (indices increasing within a key). The path tracer, the
+ * perm (DEVICE, n ints) lists the indices of keys (DEVICE, n bytes; keys above 7 count as 7)
+ * grouped by key in increasing key order, stably (indices increasing within a key). The path tracer, the
  * VCM passes and the server group every wavefront this way before shading (key = material
  * kind of the hit, 6 = miss, 7 = finished light-path slot). Stream-ordered. */
 int imbart_group_by_key(const unsigned char* keys, int n, int* perm, void* stream);

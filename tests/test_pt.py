@@ -172,6 +172,14 @@ def test_group_by_key_is_a_stable_counting_sort(cuda, n, kinds):
     torch.cuda.synchronize()
     got = perm.cpu().numpy()[:n]
     assert np.array_equal(got, np.argsort(keys, kind="stable").astype(np.int32))
+    if n > 10:
+        # Keys above 7 are grouped with 7: still a permutation, nothing written out of range.
+        wild = keys.copy()
+        wild[::7] = 200
+        k2 = torch.from_numpy(wild).cuda()
+        N.check(N.load().imbart_group_by_key(N.ptr(k2), n, N.ptr(perm), None), "imbart_group_by_key")
+        torch.cuda.synchronize()
+        assert np.array_equal(perm.cpu().numpy()[:n], np.argsort(np.minimum(wild, 7), kind="stable").astype(np.int32))
 
 
 @pytest.mark.gpu
