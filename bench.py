@@ -174,7 +174,7 @@ def config3_roofline(torch, dev, stream, peak):
     for flags in classes:
         v, r = ctypes.c_int(0), ctypes.c_int(0)
         lib.imbart_get_trace_class(flags, ctypes.byref(v), ctypes.byref(r))
-        saved.append((flags, v.value, r.value))
+        saved.append((flags, v.value, r.value, lib.imbart_get_trace_tri_batch(flags)))
     desc = G.config3()
     gs = GpuScene(desc, device=dev.index or 0)
     sets = make_wavefront(desc, gs.trace_scene, torch, dev, 99, shadow_from_bounce=True)
@@ -194,8 +194,9 @@ def config3_roofline(torch, dev, stream, peak):
            "bytes_per_ray": round(trace_bytes(work.closest_rays, work.closest_work) / max(work.closest_rays, 1), 1),
            "launches": int(prof.closest_launches)}
     pt.close()
-    for flags, v, r in saved:   # the main frame's tuning again for what follows
+    for flags, v, r, b in saved:   # the main frame's tuning again for what follows
         lib.imbart_set_trace_class(flags, v, r)
+        lib.imbart_set_trace_tri_batch(flags, b)
     return out
 
 
