@@ -11,7 +11,9 @@
 // queue and unoccluded contributions are added to the image. Each path carries its own
 // MWC64X state, consumed in the reference's order, so the image is independent of queue
 // order; samples are indexed globally (one tile covering the image), as in the reference
-// run with a tile at least as large as the image.
+// run with a tile at least as large as the image. By default the bounce loop of a sample
+// range runs as a CUDA graph whose kernels read their queue sizes on the device (see
+// build_range_graph); the host-driven loop remains for measurement and on request.
 //
 // This file is compiled with -fmad=false (see build.py): the shading arithmetic rounds like
 // the reference's.
@@ -279,7 +281,7 @@ struct GraphBuilder {
 };
 
 // Builds the bounce loop of one sample range (`chunk` samples at most) into ctx->exec.
-int capture_range(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh, int max_path_len,
+int build_range_graph(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh, int max_path_len,
                   int rr_start, float* image, long long total, long long chunk, bool group, bool fork) {
     const int sms = device_sms(ctx->device);
     // Shading: one thread per entry of the queue's bound, blocks past the queue's size doing
@@ -385,7 +387,7 @@ int render_graph(imbart_pt_context* ctx, const imbart_scene* scene, const imbart
     std::vector<unsigned char> key = frame_key(scene, sh, image, total, chunk, max_path_len, rr_start, group, fork);
     if (!ctx->exec || key != ctx->graph_key) {
         ctx->graph_key.clear();
-        const int rc = capture_range(ctx, scene, sh, max_path_len, rr_start, image, total, chunk, group, fork);
+        const int rc = build_range_graph(ctx, scene, sh, max_path_len, rr_start, image, total, chunk, group, fork);
         if (rc) return rc;
         ctx->graph_key = std::move(key);
     }
