@@ -60,7 +60,7 @@ struct imbart_pt_context {
     // The bounce loop of one sample range as a CUDA graph, replayed once per range.
     int graphs = -1;                         // -1: IMBART_PT_GRAPH (default 2); 0 host loop, 1 graph, 2 forked graph
     cudaGraphExec_t exec = nullptr;
-    std::vector<unsigned char> graph_key;    // the launch parameters the graph was captured with
+    std::vector<unsigned char> graph_key;    // the launch parameters the graph was built with
     int graph_kernels = 0;                   // kernel launches per replay
     int graph_bounces = 0;                   // range state sized for this many bounces
     long long* range_state = nullptr;        // next sample, per-slot totals, waves; then the range's counts
@@ -128,7 +128,7 @@ bool ensure_capacity(imbart_pt_context* c, long long n) {
            dev_alloc(&c->perm, n) && dev_alloc(&c->tile_counts, (size_t)kShadeKeys * group_tiles(n));
     if (!good) { free_ctx_buffers(c); return false; }
     c->cap = n;
-    c->graph_key.clear();   // the captured frame names the old buffers
+    c->graph_key.clear();   // the frame graph names the old buffers
     return true;
 }
 
@@ -178,7 +178,7 @@ __global__ void range_end_kernel(long long* state, const int* counts, int n_slot
     }
 }
 
-// Everything the captured kernels take into their parameters: equal keys, same graph. The
+// Everything the graph's kernels take into their parameters: equal keys, same graph. The
 // camera and the seed are read on the device, so a new view or seed replays the same graph.
 struct FrameGraphKey {
     unsigned long long scene[12];
