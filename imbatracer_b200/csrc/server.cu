@@ -1200,6 +1200,12 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
             if (!good) break;
             good = cuda_check(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate") &&
                    (lane.view = scene_pool_view(device, S->pool, S->pool_bytes)) != nullptr;
+            // Share of the resident block slots a lane's persistent traversal launches take
+            // (IMBART_SERVE_LANE_GRID_SHARE, default all).
+            if (good) {
+                const char* e = std::getenv("IMBART_SERVE_LANE_GRID_SHARE");
+                scene_set_grid_share(lane.view, e && *e ? (float)std::atof(e) : 1.0f);
+            }
         }
         S->alloc.reset(S->pool_bytes);
         for (int i = kMaxReqSlots - 1; i >= 0; --i) S->free_req_slots.push_back(i);
