@@ -42,6 +42,41 @@ def test_library_loads_and_exports_every_header_symbol():
     assert lib.imbart_version().startswith(b"imbart")
 
 
+def header_arities():
+    """Parameter count of every function the headers declare."""
+    out = {}
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if not f.endswith(".h"):
+            continue
+        text = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, f)).read(), flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b((?:imbart|intersect|occluded)_[a-z0-9_]*)\s*\(", text, flags=re.M):
+            depth, i, params = 1, m.end(), ""
+            while depth:
+                c = text[i]
+                depth += (c == "(") - (c == ")")
+                params += c if depth else ""
+                i += 1
+            params = params.strip()
+            out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_bindings_take_the_declared_number_of_arguments():
+    """native.py's ctypes signatures match the C declarations in include/*.h, argument for
+    argument (a missing or extra argument would pass garbage through the C ABI)."""
+    lib = N.load()
+    arity = header_arities()
+    wrong = {}
+    for name in N.exported_symbols():
+        if name in arity:
+            got = len(getattr(lib, name).argtypes or [])
+            if got != arity[name]:
+                wrong[name] = (arity[name], got)
+    assert len(arity) > 50
+    assert not wrong, f"declared vs bound argument counts: {wrong}"
+
+
 def test_error_reporting_without_gpu():
     lib = N.load()
     lib.imbart_clear_error()
