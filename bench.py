@@ -124,6 +124,19 @@ class ClockSampler:
                 "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the CPU baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def peak_hbm():
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -337,6 +350,30 @@ def run_pt(args):
     torch.cuda.synchronize()
     e2e_ms, e2e_all = job_totals(q0.elapsed_time(q1), e2e_rays, dev, world)
 
+    # The same frames under the reference's Russian-roulette policy (from bounce 0,
+    # pt.cpp:53-57), which the reference arm runs: device time and end to end.
+    pt.rr_start = 0
+    for k in range(2):
+        frame(40_000 + k)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    r0, r1, r2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    r0.record(stream)
+    rr0_rays = 0
+    for k in range(args.steps):
+        rr0_rays += frame(50_000 + k)
+    r1.record(stream)
+    rr0_e2e_rays = 0
+    for k in range(args.steps):
+        rr0_e2e_rays += frame(60_000 + k)
+        host_img.copy_(image, non_blocking=True)
+    r2.record(stream)
+    torch.cuda.synchronize()
+    rr0_ms, rr0_all = job_totals(r0.elapsed_time(r1), rr0_rays, dev, world)
+    rr0_e2e_ms, rr0_e2e_all = job_totals(r1.elapsed_time(r2), rr0_e2e_rays, dev, world)
+    pt.rr_start = RR_START
+
     # Roofline of the dominant kernel (closest-hit traversal) inside the frame.
     prof, work, achieved = frame_roofline(pt, frame)
     torch.cuda.synchronize()
@@ -358,6 +395,7 @@ def run_pt(args):
                 threads = os.cpu_count() or 1
                 mr, rps, sps = reference_cpu(desc, 2, threads, *CPU_SAMPLE)
                 cpu = {"value": round(mr, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                       "cpu_model": cpu_model(), "rr_start_bounce": 0,
                        "sample": f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]} at {SPP} spp, max_path_len {MAX_PATH_LEN} "
                                  f"(1/64 of the frame's pixels), 2 frames, {rps} rays/frame: the reference's "
                                  f"PathTracer+TileScheduler ({threads} tile threads) with the oracle CPU traversal"}
@@ -370,8 +408,9 @@ def run_pt(args):
                        "rr_start_bounce": RR_START, "instances": len(desc.instances), "meshes": len(desc.meshes),
                        "instanced_triangles": desc.instanced_triangles, "lights": len(desc.lights) + 1,
                        "rays_per_step": int(all_rays / world / args.steps),
-                       "l2": f"inputs larger than L2 (path + shadow queues ~{QUEUE_BYTES_PER_PATH * paths / 1e9:.1f} GB "
-                             f"for {paths} paths in flight)",
+                       "l2": f"path + shadow queues larger than L2 (~{QUEUE_BYTES_PER_PATH * paths / 1e9:.1f} GB "
+                             f"for {paths} paths in flight); the scene itself (8-wide BVH ~11 MB, triangles, "
+                             f"instances) stays L2-resident",
                        "parallelism": f"replicas x{world} (independent frames per GPU, different seeds)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
@@ -390,6 +429,15 @@ def run_pt(args):
                          "shadow_mrays_s": round(work.shadow_rays / max(prof.shadow_ms, 1e-9) / 1e3, 1)},
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 16 * 4 + 12,
                     "d2h_bytes_per_step": W * H * 12},
+            "equal_policy": {
+                "rr_start_bounce": 0, "unit": "Mrays/s",
+                "value": round(rr0_all / (rr0_ms * 1e-3) / 1e6, 2),
+                "ms_per_step": round(rr0_ms / args.steps, 2),
+                "e2e": round(rr0_e2e_all / (rr0_e2e_ms * 1e-3) / 1e6, 2),
+                "rays_per_step": int(rr0_all / world / args.steps),
+                "note": "the same frames with Russian roulette from bounce 0, the reference's policy "
+                        "(pt.cpp:53-57) and the reference arm's; the headline value uses the workload's "
+                        "roulette from bounce 3"},
             "roofline_config3": roof3,
             "gpu_launches": int(launches),
             "autotune": tuning,
@@ -443,11 +491,11 @@ def run_reference(args):
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(el / args.steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-            "config": {"workload": WORKLOAD, "sample": sample,
+            "config": {"workload": WORKLOAD, "sample": sample, "max_path_len": MAX_PATH_LEN, "rr_start_bounce": 0,
                        "reference": "PathTracer/TileScheduler/Scene/materials of the reference built in place "
                                     "(oracle/_ref); traversal = the oracle's CPU restatement"},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

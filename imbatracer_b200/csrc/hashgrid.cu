@@ -230,10 +230,21 @@ __global__ void query_kernel(const float4* __restrict__ sorted, const int* __res
     }
 }
 
+// Grid-stride launches over n items: at most 8 blocks per SM of the current device (SM
+// counts cached per device index).
 int grid_for(int n) {
-    static int sms = 0;
-    if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-    return std::max(1, std::min((n + kBlock - 1) / kBlock, sms * 8));
+    static std::mutex mu;
+    static int sms_of[64] = {};
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!sms_of[dev]) cudaDeviceGetAttribute(&sms_of[dev], cudaDevAttrMultiProcessorCount, dev);
+        sms = sms_of[dev];
+    } else {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return std::max(1, std::min((n + kBlock - 1) / kBlock, std::max(sms, 1) * 8));
 }
 
 // Grows geometrically: reallocation synchronizes the device, and a grid rebuilt every
@@ -414,6 +425,9 @@ extern "C" int imbart_hashgrid_build_noalloc(const float* positions, int stride,
                                     "(the size of its static scratch); use imbart_hashgrid_build for more");
         return IMBART_ERR_LIMIT;
     }
+    // A launch error left pending by earlier work on this thread is cleared here, so that
+    // the status returned below describes this call's own launches.
+    (void)cudaGetLastError();
     int device = 0;
     if (!ok(cudaGetDevice(&device), "cudaGetDevice")) return IMBART_ERR_CUDA;
     if (device < 0 || device >= 64) {

@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cmath>
 #include <cstdlib>
 #include <condition_variable>
 #include <cstring>
@@ -175,6 +176,17 @@ MemKind mem_kind(const void* p) {
 int env_lanes() {
     const char* e = std::getenv("IMBART_SERVE_VCM_LANES");
     return e && *e ? std::atoi(e) : 4;
+}
+
+// A share of the resident block slots from the environment: a finite number in (0, 1];
+// anything else (unset, text, NaN, out of range) gives `dflt`.
+float env_share(const char* name, float dflt) {
+    const char* e = std::getenv(name);
+    if (!e || !*e) return dflt;
+    char* end = nullptr;
+    const float v = std::strtof(e, &end);
+    if (end == e || *end != '\0' || !std::isfinite(v) || !(v > 0.0f) || v > 1.0f) return dflt;
+    return v;
 }
 
 double now_ms(std::chrono::steady_clock::time_point t0) {
@@ -711,10 +723,7 @@ void fail_all_active(imbart_server* S, int code) {
 }
 
 float serve_grid_share() {
-    static const float v = [] {
-        const char* e = std::getenv("IMBART_SERVE_GRID_SHARE");
-        return e && *e ? (float)std::atof(e) : 0.75f;
-    }();
+    static const float v = env_share("IMBART_SERVE_GRID_SHARE", 0.75f);
     return v;
 }
 
@@ -1202,10 +1211,7 @@ imbart_server* imbart_server_create(int device, int mode, long long hbm_budget_b
                    (lane.view = scene_pool_view(device, S->pool, S->pool_bytes)) != nullptr;
             // Share of the resident block slots a lane's persistent traversal launches take
             // (IMBART_SERVE_LANE_GRID_SHARE, default all).
-            if (good) {
-                const char* e = std::getenv("IMBART_SERVE_LANE_GRID_SHARE");
-                scene_set_grid_share(lane.view, e && *e ? (float)std::atof(e) : 1.0f);
-            }
+            if (good) scene_set_grid_share(lane.view, env_share("IMBART_SERVE_LANE_GRID_SHARE", 1.0f));
         }
         S->alloc.reset(S->pool_bytes);
         for (int i = kMaxReqSlots - 1; i >= 0; --i) S->free_req_slots.push_back(i);

@@ -510,7 +510,8 @@ int add_trace_node(cudaGraph_t graph, const cudaGraphNode_t* deps, int n_deps, c
 }
 
 void scene_set_grid_share(imbart_scene* s, float share) {
-    s->grid_share = std::min(std::max(share, 0.05f), 1.0f);
+    // Written so that NaN takes the lower bound too.
+    s->grid_share = !(share > 0.05f) ? 0.05f : (share < 1.0f ? share : 1.0f);
 }
 
 void scene_launch_key(const imbart_scene* s, unsigned long long out[12]) {

@@ -315,9 +315,14 @@ int imbart_hashgrid_get_arrays(const imbart_hashgrid* grid, const void** sorted,
  * until the process exits; it bounds n to 1,048,576 photons and table_size (<= 0: 2n) to
  * 2,097,152 buckets — larger requests return IMBART_ERR_LIMIT without launching anything.
  * The first call on a device looks the array's address up for that device
- * (cudaGetSymbolAddress with the device current); make that first call before any stream
- * capture. All calls share the one array: calls that overlap on the GPU (different streams,
- * no ordering between them) race and must be serialized by the caller. Stream-ordered. */
+ * (cudaGetSymbolAddress with the device current). With CUDA's lazy module loading (the
+ * default) that first call is also when the driver loads the module and reserves the array,
+ * which can synchronize the device: make one call per device at start-up (n = 0 is enough),
+ * before admitting work and before any stream capture. All calls share the one array: calls
+ * that overlap on the GPU (different streams, no ordering between them) race and must be
+ * serialized by the caller. A launch error pending on the calling thread is cleared on entry;
+ * when the call fails after its first launch (IMBART_ERR_CUDA), the outputs are undefined.
+ * Stream-ordered. */
 int imbart_hashgrid_build_noalloc(const float* positions, int stride, int n, float radius, float cell_factor,
                                   int table_size, void* sorted_out, int* cell_ends_out, float* params_out,
                                   void* stream);

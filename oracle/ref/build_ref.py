@@ -30,16 +30,24 @@ REF_SOURCES = [
     "src/imbatracer/loaders/load_hdr.cpp",
 ]
 OWN_SOURCES = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_vcm.cpp"),
-               os.path.join(HERE, "ref_scene_io.cpp")]
+               os.path.join(HERE, "ref_scene_io.cpp"), os.path.join(HERE, "ref_pt_rr.cpp")]
 ORACLE_C = [os.path.join(ORACLE, "traversal.c")]
 
 FLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-w"]
 
 
+def present() -> bool:
+    return os.path.isdir(os.path.join(REF, "src", "imbatracer"))
+
+
 def build(verbose: bool = False) -> str:
-    if not os.path.isdir(os.path.join(REF, "src", "imbatracer")):
+    if not present():
         raise SystemExit(f"reference tree not found at {REF}")
     os.makedirs(OUT, exist_ok=True)
+    # Where the sources were found, for the CPU tests that read the reference's scene files
+    # (oracle.refwrap.reference_root); they copy them elsewhere before loading them.
+    with open(os.path.join(OUT, "reference_root.txt"), "w") as f:
+        f.write(REF)
     objdir = os.path.join(OUT, "obj")
     os.makedirs(objdir, exist_ok=True)
     inc = ["-I", os.path.join(HERE, "shim"), "-I", os.path.join(REF, "src"), "-I", os.path.join(ROOT, "include"),
@@ -62,4 +70,7 @@ def build(verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    if "--if-present" in sys.argv and not present():
+        print(f"reference tree not found at {REF}: oracle/_ref not built")
+    else:
+        print(build(verbose="-v" in sys.argv))

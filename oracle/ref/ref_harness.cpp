@@ -510,6 +510,32 @@ int ref_render_pt(void* h, int w, int ht, const float* pos, const float* dir, co
     return 0;
 }
 
+extern "C" imba::Integrator* imbart_make_pt_rr(imba::Scene& scene, imba::PerspectiveCamera& cam,
+                                              imba::RayScheduler<imba::PTState, imba::ShadowState>& sched,
+                                              int max_path_len, int rr_start);
+
+// The reference path tracer with its Russian roulette deferred to bounce rr_start
+// (ref_pt_rr.cpp), otherwise as ref_render_pt.
+extern "C" int ref_render_pt_rr(void* h, int w, int ht, const float* pos, const float* dir, const float* up,
+                                float fov, int spp, int max_path_len, int rr_start, uint64_t seed_base,
+                                float* image_out) {
+    RefScene* rs = static_cast<RefScene*>(h);
+    use_scene_masks(rs->scene);
+    PerspectiveCamera cam((float)w, (float)ht, fov);
+    cam.move(f3(pos), f3(dir), f3(up));
+    const int tile = w > ht ? w : ht;
+    DefaultTileGen<PTState> gen(w, ht, spp, tile);
+    TileScheduler<PTState, ShadowState, false> sched(gen, rs->scene, 1, 1, tile * tile * spp, true);
+    std::unique_ptr<Integrator> pt(imbart_make_pt_rr(rs->scene, cam, sched, max_path_len, rr_start));
+    AtomicImage img(w, ht);
+    img.clear();
+    imbart_ref_set_seed(seed_base, 0);
+    pt->render(img);
+    for (int i = 0; i < w * ht; ++i)
+        for (int k = 0; k < 3; ++k) image_out[3 * i + k] = img.pixels()[i][k];
+    return 0;
+}
+
 // The reference path tracer as its CPU baseline runs it: `threads` TileScheduler threads on
 // tiles of `tile` pixels, traversal by the oracle on the calling thread of each tile. Ray
 // counts are the reference TileScheduler's own statistics (tile_scheduler.h:117-127), which

@@ -19,6 +19,38 @@ def available() -> bool:
     return os.path.exists(LIB)
 
 
+def reference_root() -> str | None:
+    """The reference tree libref.so was built from (IMBART_REFERENCE, else the path the build
+    recipe recorded), or None where it is absent (for example on a machine that only received
+    the built files). Tests read its scene files from copies, never in place, because loading
+    a scene with `accel` lines makes the reference write cache files beside it."""
+    root = os.environ.get("IMBART_REFERENCE")
+    if not root:
+        try:
+            with open(os.path.join(HERE, "_ref", "reference_root.txt")) as f:
+                root = f.read().strip()
+        except OSError:
+            return None
+    return root if root and os.path.isdir(root) else None
+
+
+def copy_reference_scenes(dst: str, sub: str = "cornell") -> str | None:
+    """Copies the reference's test/scenes/<sub> folder (scene, OBJ and MTL files, without cache
+    files) to dst/<sub> and returns that folder; None without the reference tree."""
+    import shutil
+    root = reference_root()
+    src = os.path.join(root, "test", "scenes", sub) if root else None
+    if not src or not os.path.isdir(src):
+        return None
+    out = os.path.join(dst, sub)
+    shutil.copytree(src, out, ignore=shutil.ignore_patterns("*.bvh"), dirs_exist_ok=True)
+    for dirpath, _, files in os.walk(out):      # the copies must be writable: caches go there
+        os.chmod(dirpath, 0o755)
+        for f in files:
+            os.chmod(os.path.join(dirpath, f), 0o644)
+    return out
+
+
 def load() -> C.CDLL:
     global _lib
     if _lib is None:
@@ -51,6 +83,7 @@ def load() -> C.CDLL:
             "ref_store_accel": (I, [I, C.c_char_p, P, I, I, P, I, I, I]),
             "ref_render_pt": (I, [P, I, I, P, P, P, F, I, I, U64, P]),
             "ref_render_pt_threads": (I, [P, I, I, P, P, P, F, I, I, U64, I, I, P, P]),
+            "ref_render_pt_rr": (I, [P, I, I, P, P, P, F, I, I, I, U64, P]),
             "ref_vcm_create": (P, [P, I, I, I, P, P, P, F, I, I, I, I, I, F, I, U64]),
             "ref_vcm_destroy": (None, [P]),
             "ref_vcm_info": (None, [P, P]),
@@ -285,6 +318,18 @@ class RefScene:
         p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
         rc = load().ref_render_pt(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, seed_base,
                                   _p(img))
+        assert rc == 0
+        return img
+
+    def render_pt_rr(self, w, h, spp, max_path_len, rr_start, seed_base, cam=None):
+        """render_pt with the reference PathTracer's Russian roulette deferred to bounce
+        rr_start (ref_pt_rr.cpp): no roulette draw and no kill before it; rr_start 0 is the
+        reference itself."""
+        cam = cam or self.desc.camera
+        img = np.zeros((h, w, 3), np.float32)
+        p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
+        rc = load().ref_render_pt_rr(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, rr_start,
+                                     seed_base, _p(img))
         assert rc == 0
         return img
 

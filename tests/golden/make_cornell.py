@@ -1,6 +1,7 @@
 """Regenerates the Cornell-box fixtures in this folder from the reference's own code and
 assets (oracle/_ref built from the reference sources, the reference's test scenes under
-test/scenes/cornell). Run from the repo root where the reference tree exists:
+test/scenes/cornell, loaded from a temporary copy). Run from the repo root where the
+reference tree exists:
 
     python tests/golden/make_cornell.py
 
@@ -27,7 +28,6 @@ sys.path.insert(0, ROOT)
 from imbatracer_b200 import assets as A  # noqa: E402
 from oracle import refwrap as R  # noqa: E402
 
-REF = os.environ.get("IMBART_REFERENCE", "/root/reference")
 SCENES = {"org": "ref_cornell_org.png", "indirect": "ref_cornell_indirect.png", "specular": "ref_cornell_specular.png",
           "specular_front": "ref_cornell_specular_front.png"}
 W = H = 64
@@ -51,14 +51,22 @@ def scene_to_arrays(desc) -> dict:
 
 
 def main():
+    import tempfile
+    ref = R.reference_root()
+    if ref is None:
+        raise SystemExit("the reference tree is needed (build oracle/_ref first, or set IMBART_REFERENCE)")
+    # The scenes are loaded from a copy: their `accel` lines make the reference write .bvh
+    # cache files beside the meshes.
+    tmp = tempfile.TemporaryDirectory()
+    cornell = R.copy_reference_scenes(tmp.name)
     for name, golden in SCENES.items():
-        path = os.path.join(REF, "test", "scenes", "cornell", f"cornell_{name}.scene")
+        path = os.path.join(cornell, f"cornell_{name}.scene")
         desc = A.load_scene_file(path, width=W, height=H)
         arrays = scene_to_arrays(desc)
         rs = R.RefScene.from_file(path, W, H)
         arrays["ref_pt"] = rs.render_pt(W, H, SPP, MAX_LEN, SEED)
         arrays["ref_settings"] = np.array([W, H, SPP, MAX_LEN, SEED], np.int64)
-        gpath = os.path.join(REF, "test", "references", golden)
+        gpath = os.path.join(ref, "test", "references", golden)
         if os.path.exists(gpath):
             img = A.load_png(gpath)[..., :3]
             lin = (img.astype(np.float64)) ** 2

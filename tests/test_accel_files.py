@@ -181,3 +181,33 @@ def test_malformed_files_are_errors(tmp_path):
     assert lib.imbart_store_accel_node2(os.fsencode(good), N.ptr(nodes), 0, 1, N.ptr(tris), 0, 3, 0) != 0
     lib.imbart_clear_error()
     assert S.accel_file_counts(good, N.ACCEL_CPU) is None
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("name", ["mixed", "config1"])
+def test_reference_written_files_trace_on_the_gpu(cuda, tmp_path, name):
+    """Bottom levels loaded from .bvh files the reference's Scene wrote while building
+    (store_accel_gpu, scene.cpp:62-68), converted to the 8-wide layout and traced by the GPU
+    kernels: closest hits (triangle, instance, t, u, v) bit-exact with the oracle's walk of the
+    same arrays, any-hit occlusion equal."""
+    from tests.test_traversal_gpu import run_gpu
+    desc = small_mixed_scene() if name == "mixed" else H.scene_desc(name)
+    files = [str(tmp_path / f"{name}{i}.bvh") for i in range(len(desc.meshes))]
+    R.RefScene(desc, accel_files=files)                  # the reference builds and stores
+    assert all(os.path.exists(f) for f in files)
+    td = S.build_traversal_data(desc.meshes, desc.instances, accel_files=files)
+    _, ref_nodes, _, _ = R.RefScene(desc, accel_files=files).gpu_layout()
+    n_bottom = td.layout[-1] + S.accel_file_counts(files[-1])[0]
+    assert td.nodes[:n_bottom].tobytes() == ref_nodes[:n_bottom].tobytes()   # loaded, not rebuilt
+    lo, hi = G.scene_box(desc)
+    rays = G.random_rays(np.random.default_rng(11), 50000, lo - 0.1 * (hi - lo), hi + 0.1 * (hi - lo))
+    ds = S.DeviceScene(td)
+    ref, ref_v = O.trace_node2(td, rays, with_v=True)
+    hits, v, _ = run_gpu(ds, rays)
+    assert (ref["tri_id"] >= 0).sum() > 1000
+    assert H.hits_equal(ref, hits).all()
+    assert np.array_equal(ref_v.view(np.int32), v.view(np.int32))
+    occ, _, _ = run_gpu(ds, rays, any_hit=True)
+    assert np.array_equal(occ["tri_id"] >= 0, O.trace_node2(td, rays, any_hit=True)["tri_id"] >= 0)
+    ds.close()

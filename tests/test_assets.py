@@ -24,11 +24,18 @@ from imbatracer_b200.scene import Instance, Mesh
 from oracle import refwrap as R
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("IMBART_REFERENCE", "/root/reference")
-CORNELL = os.path.join(REF, "test", "scenes", "cornell")
-needs_ref = pytest.mark.skipif(not (R.available() and os.path.isdir(CORNELL)),
+REF = R.reference_root()
+needs_ref = pytest.mark.skipif(not (R.available() and REF and os.path.isdir(os.path.join(REF, "test", "scenes",
+                                                                                         "cornell"))),
                                reason="oracle/_ref or the reference's scenes absent")
 RMSE_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def cornell(tmp_path_factory):
+    """A writable copy of the reference's Cornell-box scenes: loading a scene whose file has
+    `accel` lines makes the reference's Scene write .bvh cache files beside the meshes."""
+    return R.copy_reference_scenes(str(tmp_path_factory.mktemp("ref_scenes")))
 
 
 def rel_rmse(a, b):
@@ -120,8 +127,8 @@ def compare_with_reference(path):
 
 @needs_ref
 @pytest.mark.parametrize("name", ["org", "indirect", "specular", "specular_front", "water", "instances"])
-def test_cornell_scenes_load_as_the_reference_loads_them(name):
-    d, e = compare_with_reference(os.path.join(CORNELL, f"cornell_{name}.scene"))
+def test_cornell_scenes_load_as_the_reference_loads_them(cornell, name):
+    d, e = compare_with_reference(os.path.join(cornell, f"cornell_{name}.scene"))
     assert len(d.lights) > 0 and d.meshes[0].triangle_count > 0
 
 
@@ -366,10 +373,10 @@ def scene_from_fixture(z, width, height):
 
 
 @needs_ref
-def test_fixtures_hold_the_loaders_arrays():
+def test_fixtures_hold_the_loaders_arrays(cornell):
     from tests.golden.make_cornell import scene_to_arrays
     z = np.load(os.path.join(HERE, "golden", "cornell_specular.npz"))
-    cur = scene_to_arrays(A.load_scene_file(os.path.join(CORNELL, "cornell_specular.scene"), 64, 64))
+    cur = scene_to_arrays(A.load_scene_file(os.path.join(cornell, "cornell_specular.scene"), 64, 64))
     for k, v in cur.items():
         assert np.array_equal(np.asarray(v), z[k]), k
 

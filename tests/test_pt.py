@@ -116,6 +116,60 @@ def test_path_tracer_image_matches_reference(cuda, name, w, h, spp, max_len):
     assert pt.last_stats[0] >= w * h * spp and pt.last_stats[1] > 0
 
 
+@needs_ref
+def test_deferred_roulette_oracle_is_the_reference_at_bounce_0():
+    """The oracle for rr_start (the reference's pt.cpp with its roulette call deferred,
+    oracle/ref/ref_pt_rr.cpp) is the reference itself at rr_start 0, and changes the image
+    when the roulette starts later."""
+    rs = R.RefScene(small_mixed_scene())
+    a = rs.render_pt(48, 32, 2, 5, 1234)
+    assert np.array_equal(rs.render_pt_rr(48, 32, 2, 5, 0, 1234).view(np.int32), a.view(np.int32))
+    assert not np.array_equal(rs.render_pt_rr(48, 32, 2, 5, 3, 1234), a)
+
+
+@pytest.fixture(scope="module")
+def bench_scene():
+    """The benchmarked scene (200 instances of 8 meshes; Lambertian, Phong, Cook-Torrance,
+    glass and mirror materials; 16 triangle lights and a constant environment) in both
+    renderers."""
+    from imbatracer_b200.integrators import GpuScene
+    d = G.config2()
+    return d, R.RefScene(d), GpuScene(d)
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("rr_start", [0, 3])
+def test_benchmark_frame_matches_reference(cuda, bench_scene, rr_start):
+    """The benchmarked frame's settings (max_path_len 9, i.e. 8 bounces) on a 240x135 image
+    of the benchmarked scene at 4 spp against the reference's PathTracer on the same seeds:
+    rr_start 0 is the reference's own Russian roulette (pt.cpp:53-57), rr_start 3 the bench's
+    (the reference's pt.cpp with its roulette deferred to bounce 3)."""
+    from imbatracer_b200.integrators import PathTracer
+    d, rs, gs = bench_scene
+    w, h, spp, max_len, seed = 240, 135, 4, 9, 424242
+    ref = rs.render_pt(w, h, spp, max_len, seed) if rr_start == 0 else \
+        rs.render_pt_rr(w, h, spp, max_len, rr_start, seed)
+    pt = PathTracer(gs, max_path_len=max_len, rr_start=rr_start)
+    img = pt.render(spp, seed, w, h).cpu().numpy()
+    pt.close()
+    err = rel_rmse(img, ref)
+    assert ref.sum() > 0 and err <= RMSE_TOL, f"relative RMSE {err:.2e}"
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_deferred_roulette_matches_reference(cuda):
+    """rr_start 2 on the scene with every material kind against the deferred-roulette oracle."""
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    d = small_mixed_scene()
+    w, h, spp, max_len, seed = 96, 64, 8, 7, 99
+    ref = R.RefScene(d).render_pt_rr(w, h, spp, max_len, 2, seed)
+    img = PathTracer(GpuScene(d), max_path_len=max_len, rr_start=2).render(spp, seed, w, h).cpu().numpy()
+    err = rel_rmse(img, ref)
+    assert err <= RMSE_TOL, f"relative RMSE {err:.2e}"
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,max_paths,mode", [("mixed", 0, 1), ("mixed", 0, 2), ("mixed", 10000, 2),
                                                  ("config1", 7000, 1), ("config1", 7000, 2)])
