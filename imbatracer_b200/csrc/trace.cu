@@ -135,20 +135,25 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 // Three query classes keep their own variant and refill threshold: incoherent closest hit,
 // any hit, and closest hit over coherent rays (camera rays, flag IMBART_TRACE_COHERENT),
 // which traverse best in static batches (refill only when the whole warp is idle).
-constexpr int kTraceVariants = 10;   // persistent-kernel shapes 1..10 (0: one ray per thread)
+constexpr int kTraceVariants = 16;   // persistent-kernel shapes 1..16 (0: one ray per thread)
+constexpr int kFirstCoopVariant = 11; // 11..16: the shapes with the cooperative triangle phase
 
-// Each class also keeps its triangle batch: the triangles a lane tests per loop trip before
-// the lanes with node work take their next node step (0: the whole group at once). Two
-// measured best on the frame's ray sets (secondary rays +13 %, camera rays +7 % over 0).
+// Each class also keeps its triangle batch: in the per-lane shapes, the triangles a lane
+// tests per loop trip before the lanes with node work take their next node step (0: the
+// whole group at once; two measured best there: secondary rays +13 %, camera rays +7 % over
+// 0); in the cooperative shapes, 0 = lanes load their pairs' triangles, >= 1 = staged.
+// Defaults: the cooperative 256 x 3 shape with lane loads for every class (on the frame's
+// ray sets of the instanced scene: camera / secondary / shadow rays +2 / +9 / +10 % over
+// the best per-lane shapes; staging measured 5 % slower).
 struct TraceConfig {
     int variant, refill, postpone, variant_any;
     int refill_any, variant_coh, refill_coh;
-    int tri_batch = 2, tri_batch_any = 2, tri_batch_coh = 2;
+    int tri_batch = 0, tri_batch_any = 0, tri_batch_coh = 0;
 };
 
 std::mutex g_cfg_mutex;
 bool g_cfg_init = false;
-TraceConfig g_cfg{4, 12, 0, 6, 24, 4, 32};
+TraceConfig g_cfg{11, 24, 0, 11, 8, 11, 32};
 
 int env_int(const char* name, int dflt) {
     const char* v = getenv(name);
@@ -234,9 +239,9 @@ int max_grid(Kernel k, int block, int device) {
 }
 
 // One persistent block per resident slot (fewer for short queues).
-template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
+template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop = false>
 LaunchSpec persistent_spec(int count, int device, float share, TraceParams& p) {
-    auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh>;
+    auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh, kCoop>;
     const int slots = std::max(1, (int)(max_grid(k, kBlock, device) * share));
     const int grid = std::min(slots, (count + kBlock - 1) / kBlock);
     p.total_warps = grid * (kBlock / 32);
@@ -256,6 +261,13 @@ LaunchSpec variant_spec(int variant, int count, int device, float share, TracePa
         case 8: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12>(count, device, share, p);
         case 9: return persistent_spec<kAny, kMasked, kStats, 256, 4, 16>(count, device, share, p);
         case 10: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12>(count, device, share, p);
+        // Cooperative triangle phase (all lanes test the warp's pending ray/triangle pairs).
+        case 11: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12, true>(count, device, share, p);
+        case 12: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8, true>(count, device, share, p);
+        case 13: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12, true>(count, device, share, p);
+        case 14: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16, true>(count, device, share, p);
+        case 15: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12, true>(count, device, share, p);
+        case 16: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12, true>(count, device, share, p);
         default: return {};
     }
 }
@@ -309,6 +321,10 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
         p.refill_lanes = std::min(std::max(refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
         p.tri_batch = std::max(any ? cfg.tri_batch_any : coherent ? cfg.tri_batch_coh : cfg.tri_batch, 0);
+        // In the cooperative shapes the class's triangle-batch setting selects how triangles
+        // reach the lanes: 0 = each lane loads its pair's triangle, >= 1 = the warp stages
+        // the pass's triangles in shared memory.
+        p.tri_stage = variant >= kFirstCoopVariant && p.tri_batch > 0 ? 1 : 0;
         spec = stats ? persistent_kernel_spec<true>(variant, any, masked, count, s->device, s->grid_share, p)
                      : persistent_kernel_spec<false>(variant, any, masked, count, s->device, s->grid_share, p);
     }
@@ -799,6 +815,7 @@ int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imb
     static const int kTriBatches[] = {0, 1, 2, 3, 4};
     for (int b : kTriBatches) {
         if (rc || b == b0) continue;
+        if (best_v >= kFirstCoopVariant && b > 1) continue;   // cooperative shapes: 0 or 1 (staged)
         imbart_set_trace_tri_batch(flags, b);
         float ms = 0.0f;
         rc = time_config(best_v, best_r, &ms);

@@ -57,6 +57,7 @@ struct TraceParams {
     int refill_lanes;                       // refill a warp's idle lanes once this many are idle
     int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
     int tri_batch;                          // triangles a lane tests per loop trip (0: its whole group)
+    int tri_stage;                          // cooperative kernels: stage triangles in shared memory
 };
 
 constexpr uint32_t kEntryTri = 3u;      // triangle group (postponed): x = prim base, y = prim mask
@@ -232,6 +233,17 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
     }
 }
 
+// Position of the k-th (0-based) set bit of m by halving; always in [0, 31].
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, int k) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        const int c = __popc(m & ((1u << w) - 1u));
+        if (k >= c) { k -= c; m >>= w; pos += (uint32_t)w; }
+    }
+    return pos;
+}
+
 // Alpha-mask lookup for a candidate hit (mask.h:22-40): transparent texels reject the hit.
 __device__ __forceinline__ bool mask_opaque(const TraceParams& p, int tri, float u, float v) {
     const int m = __ldg(p.indices + 4 * tri + 3);
@@ -382,15 +394,33 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 // idle until the slowest ray of a static batch ends. The loop follows the node-group /
 // triangle-group scheme of Ylitie, Karras and Laine (HPG 2017): a node step pops the next hit
 // child of the current group and intersects its 8 boxes, producing a group of hit internal
-// children and a group of hit leaf primitives; triangle tests are postponed (the triangle
-// group goes onto the stack) while fewer than postpone_lanes/32 of the live lanes would test
-// triangles together. The stack lives in shared memory (kSh entries per thread, laid out so
-// that neighbouring threads touch neighbouring words) and spills to local memory.
-// Results are identical to the per-thread kernel: same tests, same tie rule.
+// children and a group of hit leaf primitives. The stack lives in shared memory (kSh entries
+// per thread, laid out so that neighbouring threads touch neighbouring words) and spills to
+// local memory. Results are identical to the per-thread kernel: same tests, same tie rule.
+//
+// Triangle groups are tested in one of two ways:
+//  * per lane (kCoop false): a lane tests up to `tri_batch` triangles of its group per loop
+//    trip (the rest wait for the next trip while lanes with node work take their node step);
+//    triangle tests are postponed (the group goes onto the stack) while fewer than
+//    postpone_lanes/32 of the live lanes would test triangles together;
+//  * cooperatively (kCoop true): after the node step, the warp lists every (ray, triangle)
+//    pair its lanes' triangle groups hold and all 32 lanes — idle and finished ones included —
+//    test 32 pairs per pass, reading the owning lane's ray through shuffles. With `tri_stage`
+//    the pass's triangle records are first staged in shared memory by coalesced 16-byte warp
+//    loads. Each owner's closest candidate is found by shared-memory atomic minima over
+//    (t, triangle id), any-hit queries take the first accepted pair in the group's test
+//    order, so hits and the work counters equal those of the per-lane tests.
 // ---------------------------------------------------------------------------------------
-template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh>
+template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TraceParams p) {
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int kCW = kCoop ? kBlock / 32 : 1;     // warps with cooperative-phase slots
     __shared__ uint2 sstack[kSh][kBlock];
+    __shared__ uint32_t s_key[kCW][32];              // per owner lane: smallest key of a pass
+    __shared__ int s_tri[kCW][32];                   // per owner lane: its winning triangle id
+    __shared__ float4 s_hit[kCW][32];                // per owner lane: the winner's t, u, v
+    __shared__ int s_idx[kCW][32];                   // staging: triangle index of each pair
+    __shared__ float4 s_tv[kCW][kCoop ? 96 : 1];     // staging: the pass's triangle records
     uint2 lstack[kStackSize - kSh];
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -406,6 +436,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     uint32_t g_base = 0, g_imask = 0, g_hits = 0, t_base = 0, t_mask = 0;
     int sp = 0;
     RayStats st;
+    r.ox = r.oy = r.oz = 0.0f;
+    r.Sx = r.Sy = r.Sz = 0.0f;
     r.kx = r.ky = r.kz = 0;
     const int count = p.count_ptr ? min(__ldg(p.count_ptr), p.count) : p.count;
 
@@ -429,13 +461,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
 
     for (;;) {
         // Refill idle lanes in warp-wide batches.
-        const unsigned idle = __ballot_sync(0xffffffffu, ray < 0);
-        unsigned live = __ballot_sync(0xffffffffu, ray >= 0 && ray < count);
+        const unsigned idle = __ballot_sync(kFull, ray < 0);
+        unsigned live = __ballot_sync(kFull, ray >= 0 && ray < count);
         if (idle != 0u && (live == 0u || __popc(idle) >= p.refill_lanes)) {
             const int leader = __ffs(idle) - 1;
             int base = 0;
             if ((int)lane == leader) base = atomicAdd(p.work, __popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
+            base = __shfl_sync(kFull, base, leader);
             if (ray < 0) {
                 const int idx = base + __popc(idle & lt_mask);
                 if (idx >= count) {
@@ -460,18 +492,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     }
                 }
             }
-            live = __ballot_sync(0xffffffffu, ray >= 0 && ray < count);
+            live = __ballot_sync(kFull, ray >= 0 && ray < count);
         }
         if (live == 0u) {
-            if (__ballot_sync(0xffffffffu, ray < 0) == 0u) break;   // every lane exhausted
+            if (__ballot_sync(kFull, ray < 0) == 0u) break;   // every lane exhausted
             continue;
         }
         const bool active = ray >= 0 && ray < count;
-        if (!active) continue;
+        // The per-lane form lets idle lanes skip the trip; the cooperative form keeps every
+        // lane for the triangle phase.
+        if (!kCoop && !active) continue;
         const int n_live = __popc(live);
+        bool next = !active;   // this lane's trip is over (finished, or entered an instance)
 
         // Node step.
-        if (t_mask == 0 && g_hits != 0) {
+        if (!next && t_mask == 0 && g_hits != 0) {
             const uint32_t bitpos = __ffs(g_hits) - 1;
             g_hits &= g_hits - 1;
             const uint32_t slot = bitpos ^ r.oct;
@@ -479,51 +514,54 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
             if (g_hits != 0 && !push(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask)) {
                 atomicAdd(p.error_flags, 1);
                 finish();
-                continue;
+                next = true;
+            } else {
+                intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+                if (kStats) st.nodes++;
             }
-            intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
-            if (kStats) st.nodes++;
         }
 
-        // Primitive step.
-        if (t_mask != 0) {
+        // Primitive step: instance entry, and per-lane triangle tests.
+        if (!next && t_mask != 0) {
             if (bottom) {
-                bool stop = false;
-                int tested = 0;
-                while (t_mask != 0) {
-                    // The rest of the group waits for the next trip (the lanes with node work
-                    // take their node step meanwhile).
-                    if (p.tri_batch > 0 && tested == p.tri_batch) break;
-                    ++tested;
-                    // Postpone only while node work remains, so that a ray with nothing
-                    // but triangles left always makes progress.
-                    if (g_hits != 0 && __popc(__activemask()) * 32 < n_live * p.postpone_lanes) {
-                        if (!push(t_base | (kEntryTri << kTypeShift), t_mask)) {
-                            atomicAdd(p.error_flags, 1);
-                            stop = true;
+                if (!kCoop) {
+                    bool stop = false;
+                    int tested = 0;
+                    while (t_mask != 0) {
+                        // The rest of the group waits for the next trip (the lanes with node
+                        // work take their node step meanwhile).
+                        if (p.tri_batch > 0 && tested == p.tri_batch) break;
+                        ++tested;
+                        // Postpone only while node work remains, so that a ray with nothing
+                        // but triangles left always makes progress.
+                        if (g_hits != 0 && __popc(__activemask()) * 32 < n_live * p.postpone_lanes) {
+                            if (!push(t_base | (kEntryTri << kTypeShift), t_mask)) {
+                                atomicAdd(p.error_flags, 1);
+                                stop = true;
+                            }
+                            t_mask = 0;
+                            break;
                         }
-                        t_mask = 0;
-                        break;
+                        const uint32_t i = __ffs(t_mask) - 1;
+                        t_mask &= t_mask - 1;
+                        const float4* tp = reinterpret_cast<const float4*>(p.tris + t_base + i);
+                        const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                        if (kStats) st.tris++;
+                        float t, u, v;
+                        if (!tri_test(r, a, b, c, t, u, v)) continue;
+                        if (!(t >= tmin)) continue;
+                        const int tri = __float_as_int(a.w);
+                        const bool closer = (t < best_t) ||
+                            (t == best_t && (best_tri < 0 || cur_inst < best_inst ||
+                                             (cur_inst == best_inst && tri < best_tri)));
+                        if (!closer) continue;
+                        if (kMasked && !mask_opaque(p, tri, u, v)) continue;
+                        best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
+                        tlimit = best_t * IMBART_SLACK;
+                        if (kAnyHit) { stop = true; break; }
                     }
-                    const uint32_t i = __ffs(t_mask) - 1;
-                    t_mask &= t_mask - 1;
-                    const float4* tp = reinterpret_cast<const float4*>(p.tris + t_base + i);
-                    const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                    if (kStats) st.tris++;
-                    float t, u, v;
-                    if (!tri_test(r, a, b, c, t, u, v)) continue;
-                    if (!(t >= tmin)) continue;
-                    const int tri = __float_as_int(a.w);
-                    const bool closer = (t < best_t) ||
-                        (t == best_t && (best_tri < 0 || cur_inst < best_inst ||
-                                         (cur_inst == best_inst && tri < best_tri)));
-                    if (!closer) continue;
-                    if (kMasked && !mask_opaque(p, tri, u, v)) continue;
-                    best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
-                    tlimit = best_t * IMBART_SLACK;
-                    if (kAnyHit) { stop = true; break; }
+                    if (stop) { finish(); next = true; }
                 }
-                if (stop) { finish(); continue; }
             } else {
                 // Enter the next instance of the group.
                 const uint32_t i = __ffs(t_mask) - 1;
@@ -532,28 +570,151 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                 if (g_hits != 0) ok = push(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask);
                 if (ok && t_mask != 0) ok = push(t_base | (kEntryInst << kTypeShift), t_mask);
                 if (ok) ok = push(kEntryMarker << kTypeShift, 0u);
-                if (!ok) { atomicAdd(p.error_flags, 1); finish(); continue; }
-                t_mask = 0;
-                const float4* ip = reinterpret_cast<const float4*>(p.insts + t_base + i);
-                const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
-                const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
-                if (kStats) st.insts++;
-                r.ox = xform_row(m0, wox, woy, woz, 1.0f);
-                r.oy = xform_row(m1, wox, woy, woz, 1.0f);
-                r.oz = xform_row(m2, wox, woy, woz, 1.0f);
-                r.dx = xform_row(m0, wdx, wdy, wdz, 0.0f);
-                r.dy = xform_row(m1, wdx, wdy, wdz, 0.0f);
-                r.dz = xform_row(m2, wdx, wdy, wdz, 0.0f);
-                setup_space(r);
-                cur_inst = meta.x;
-                bottom = true;
-                g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
-                continue;
+                if (!ok) {
+                    atomicAdd(p.error_flags, 1);
+                    finish();
+                } else {
+                    t_mask = 0;
+                    const float4* ip = reinterpret_cast<const float4*>(p.insts + t_base + i);
+                    const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
+                    const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
+                    if (kStats) st.insts++;
+                    r.ox = xform_row(m0, wox, woy, woz, 1.0f);
+                    r.oy = xform_row(m1, wox, woy, woz, 1.0f);
+                    r.oz = xform_row(m2, wox, woy, woz, 1.0f);
+                    r.dx = xform_row(m0, wdx, wdy, wdz, 0.0f);
+                    r.dy = xform_row(m1, wdx, wdy, wdz, 0.0f);
+                    r.dz = xform_row(m2, wdx, wdy, wdz, 0.0f);
+                    setup_space(r);
+                    cur_inst = meta.x;
+                    bottom = true;
+                    g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                }
+                next = true;
+            }
+        }
+
+        // Cooperative triangle phase (every lane of the warp takes part).
+        if (kCoop) {
+            const bool want = !next && bottom && t_mask != 0;
+            if (__ballot_sync(kFull, want) != 0u) {
+                const int w = tid >> 5;
+                const int cnt = want ? __popc(t_mask) : 0;
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(kFull, incl, o);
+                    if ((int)lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(kFull, incl, 31);
+                const int excl = incl - cnt;
+                const uint32_t kpack = (uint32_t)r.kx | ((uint32_t)r.ky << 2) | ((uint32_t)r.kz << 4);
+                int found_k = -1;    // any hit: position of the group's first accepted triangle
+                for (int pass = 0; pass < total; pass += 32) {
+                    const int j = pass + (int)lane;
+                    // Owner of pair j: the first lane whose inclusive count exceeds j.
+                    int o = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int c = __shfl_sync(kFull, incl, o + step - 1);
+                        if (c <= j) o += step;
+                    }
+                    const int o_excl = __shfl_sync(kFull, excl, o);
+                    const uint32_t o_mask = __shfl_sync(kFull, t_mask, o);
+                    const uint32_t o_base = __shfl_sync(kFull, t_base, o);
+                    SpaceRay q;
+                    q.ox = __shfl_sync(kFull, r.ox, o);
+                    q.oy = __shfl_sync(kFull, r.oy, o);
+                    q.oz = __shfl_sync(kFull, r.oz, o);
+                    q.Sx = __shfl_sync(kFull, r.Sx, o);
+                    q.Sy = __shfl_sync(kFull, r.Sy, o);
+                    q.Sz = __shfl_sync(kFull, r.Sz, o);
+                    const uint32_t qk = __shfl_sync(kFull, kpack, o);
+                    q.kx = (int)(qk & 3u); q.ky = (int)((qk >> 2) & 3u); q.kz = (int)((qk >> 4) & 3u);
+                    const float o_tmin = __shfl_sync(kFull, tmin, o);
+                    const float o_best = __shfl_sync(kFull, best_t, o);
+                    const bool has = j < total;
+                    const int k = j - o_excl;
+                    const int ti = has ? (int)(o_base + nth_set_bit(o_mask, k)) : -1;
+                    float4 a, b, c;
+                    if (p.tri_stage) {
+                        // Stage the pass's triangles: lane f loads 16-byte word f, f+32, f+64
+                        // of the 32 records, so neighbouring lanes read neighbouring words.
+                        s_idx[w][lane] = ti;
+                        __syncwarp();
+#pragma unroll
+                        for (int f = (int)lane; f < 96; f += 32) {
+                            const int pr = f / 3;
+                            const int tj = s_idx[w][pr];
+                            if (tj >= 0) s_tv[w][f] = __ldg(reinterpret_cast<const float4*>(p.tris + tj) + (f - 3 * pr));
+                        }
+                        __syncwarp();
+                        a = s_tv[w][3 * lane]; b = s_tv[w][3 * lane + 1]; c = s_tv[w][3 * lane + 2];
+                    } else if (has) {
+                        const float4* tp = reinterpret_cast<const float4*>(p.tris + ti);
+                        a = __ldg(tp + 0); b = __ldg(tp + 1); c = __ldg(tp + 2);
+                    }
+                    bool cand = false;
+                    float t = 0.0f, u = 0.0f, v = 0.0f;
+                    int tri = 0;
+                    if (has && tri_test(q, a, b, c, t, u, v) && t >= o_tmin && t <= o_best) {
+                        tri = __float_as_int(a.w);
+                        cand = !kMasked || mask_opaque(p, tri, u, v);
+                    }
+                    const bool in_pass = want && excl < pass + 32 && incl > pass;
+                    if (in_pass) { s_key[w][lane] = 0xffffffffu; s_tri[w][lane] = 0x7fffffff; }
+                    __syncwarp();
+                    uint32_t key;
+                    if (kAnyHit) {
+                        key = (uint32_t)k;            // the group's test order
+                    } else {
+                        // t as an ordered unsigned key (+0 and -0 equal, as the tie rule has it)
+                        const uint32_t tb = __float_as_uint(__fadd_rn(t, 0.0f));
+                        key = (tb & 0x80000000u) ? ~tb : (tb | 0x80000000u);
+                    }
+                    if (cand) atomicMin(&s_key[w][o], key);
+                    __syncwarp();
+                    bool win = cand && s_key[w][o] == key;
+                    if (!kAnyHit) {
+                        if (win) atomicMin(&s_tri[w][o], tri);
+                        __syncwarp();
+                        win = win && s_tri[w][o] == tri;
+                    }
+                    if (win) {
+                        if (kAnyHit) s_tri[w][o] = tri;
+                        s_hit[w][o] = make_float4(t, u, v, 0.0f);
+                    }
+                    __syncwarp();
+                    if (in_pass && s_key[w][lane] != 0xffffffffu) {
+                        const int tc = s_tri[w][lane];
+                        const float4 hv = s_hit[w][lane];
+                        if (kAnyHit) {
+                            if (found_k < 0) {
+                                found_k = (int)s_key[w][lane];
+                                best_t = hv.x; best_u = hv.y; best_v = hv.z; best_tri = tc; best_inst = cur_inst;
+                            }
+                        } else {
+                            const bool closer = (hv.x < best_t) ||
+                                (hv.x == best_t && (best_tri < 0 || cur_inst < best_inst ||
+                                                    (cur_inst == best_inst && tc < best_tri)));
+                            if (closer) {
+                                best_t = hv.x; best_u = hv.y; best_v = hv.z; best_tri = tc; best_inst = cur_inst;
+                                tlimit = best_t * IMBART_SLACK;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+                if (want) {
+                    if (kStats) st.tris += (kAnyHit && found_k >= 0) ? (uint32_t)(found_k + 1) : (uint32_t)cnt;
+                    t_mask = 0;
+                    if (kAnyHit && found_k >= 0) { finish(); next = true; }
+                }
             }
         }
 
         // Pop the next group when the current ones are exhausted.
-        if (g_hits == 0 && t_mask == 0) {
+        if (!next && ray >= 0 && g_hits == 0 && t_mask == 0) {
             for (;;) {
                 if (sp == 0) { finish(); break; }
                 --sp;
@@ -573,9 +734,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     }
 
     if (kStats) {
-        const unsigned n = __reduce_add_sync(0xffffffffu, st.nodes);
-        const unsigned t = __reduce_add_sync(0xffffffffu, st.tris);
-        const unsigned k = __reduce_add_sync(0xffffffffu, st.insts);
+        const unsigned n = __reduce_add_sync(kFull, st.nodes);
+        const unsigned t = __reduce_add_sync(kFull, st.tris);
+        const unsigned k = __reduce_add_sync(kFull, st.insts);
         if (lane == 0) {
             atomicAdd(p.stats + 0, (unsigned long long)n);
             atomicAdd(p.stats + 1, (unsigned long long)t);

@@ -67,15 +67,64 @@ def vertex_normals(v: np.ndarray, idx: np.ndarray, fn: np.ndarray) -> np.ndarray
     return (acc / ln).astype(np.float32)
 
 
+def _cofactor_terms():
+    """For each entry (i, j) of the adjugate of a 4x4 matrix: its sign and six products of
+    three entries, in the order the reference's invert (float4x4.h:144-197) sums them. With
+    the rows R = (r0, r1, r2) other than j and the columns C = (c0, c1, c2) other than i, the
+    products are (r0,c0)(r1,c1)(r2,c2), (r0,c0)(r1,c2)(r2,c1), (r1,c0)(r0,c1)(r2,c2),
+    (r1,c0)(r0,c2)(r2,c1), (r2,c0)(r0,c1)(r1,c2), (r2,c0)(r0,c2)(r1,c1) with the signs
+    + - - + + -, all negated when i + j is odd."""
+    pattern = [((0, 0), (1, 1), (2, 2), 1), ((0, 0), (1, 2), (2, 1), -1), ((1, 0), (0, 1), (2, 2), -1),
+               ((1, 0), (0, 2), (2, 1), 1), ((2, 0), (0, 1), (1, 2), 1), ((2, 0), (0, 2), (1, 1), -1)]
+    table = {}
+    for i in range(4):
+        for j in range(4):
+            rows = [r for r in range(4) if r != j]
+            cols = [c for c in range(4) if c != i]
+            sgn = 1 if (i + j) % 2 == 0 else -1
+            table[i, j] = [(sgn * s, (rows[a[0]], cols[a[1]]), (rows[b[0]], cols[b[1]]), (rows[c[0]], cols[c[1]]))
+                           for a, b, c, s in pattern]
+    return table
+
+
+_COFACTORS = _cofactor_terms()
+
+
+def invert_f32(m: np.ndarray) -> np.ndarray:
+    """Inverse of a 4x4 matrix in single precision with the reference's operation order
+    (float4x4.h:144-197: adjugate by cofactors summed left to right, each product formed left
+    to right, det = a[0] . column 0 of the adjugate, then every entry times the rounded 1/det;
+    a singular matrix gives zeros), so instance transforms, hits and shading normals agree
+    with the reference's bit for bit."""
+    a = np.asarray(m, np.float32).reshape(4, 4)
+    f = np.float32
+    res = np.zeros((4, 4), np.float32)
+    with np.errstate(over="ignore", invalid="ignore"):
+        for (i, j), terms in _COFACTORS.items():
+            acc = None
+            for s, (r0, c0), (r1, c1), (r2, c2) in terms:
+                prod = f(f(a[r0, c0] * a[r1, c1]) * a[r2, c2])
+                if acc is None:
+                    acc = prod if s > 0 else f(-prod)
+                else:
+                    acc = f(acc + prod) if s > 0 else f(acc - prod)
+            res[i, j] = acc
+        det = f(f(f(f(a[0, 0] * res[0, 0]) + f(a[0, 1] * res[1, 0])) + f(a[0, 2] * res[2, 0])) + f(a[0, 3] * res[3, 0]))
+        if det == 0:
+            return np.zeros((4, 4), np.float32)
+        return (res * f(f(1.0) / det)).astype(np.float32)
+
+
 @dataclass
 class Instance:
-    """A mesh instance with its object-to-world matrix (mesh.h:19-27)."""
+    """A mesh instance with its object-to-world matrix and the world-to-object inverse the
+    reference stores beside it (mesh.h:19-27, computed as float4x4.h's invert does)."""
     mesh_id: int
     mat: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
 
     def __post_init__(self):
         self.mat = np.asarray(self.mat, np.float32).reshape(4, 4)
-        self.inv_mat = np.linalg.inv(self.mat.astype(np.float64)).astype(np.float32)[:3].copy()
+        self.inv_mat = invert_f32(self.mat)[:3].copy()
 
 
 class TraversalData:

@@ -115,3 +115,27 @@ def test_reference_sbvh_layout_gives_identical_hits(name):
     wn, wt, wi, root = H.wide_arrays(td_ref)
     c, _, _ = O.wide_walk(wn, wt, wi, root, rays)
     assert H.hits_equal(a, c).all()
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["config1", "config2"])
+def test_instance_inverses_are_the_references(name):
+    """The world-to-object matrices equal the ones the reference's Scene computes (its
+    single-precision cofactor inverse, float4x4.h:144-197) bit for bit: the traversal then
+    transforms rays, and the shading code normals, exactly as the reference does."""
+    from imbatracer_b200 import scenegen as G
+    d = G.config1() if name == "config1" else G.config2()
+    _, _, insts, _ = R.RefScene(d).gpu_layout()
+    assert len(insts) == len(d.instances)
+    for r in insts:
+        ours = d.instances[int(r["id"])].inv_mat
+        assert np.array_equal(np.asarray(r["transf"], np.float32).reshape(3, 4).view(np.int32), ours.view(np.int32))
+
+
+def test_inverse_handles_singular_and_general_matrices():
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        m = rng.normal(size=(4, 4)).astype(np.float32)
+        inv = S.invert_f32(m)
+        assert np.allclose(inv @ m, np.eye(4), atol=1e-3)
+    assert not S.invert_f32(np.zeros((4, 4), np.float32)).any()
