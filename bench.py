@@ -448,6 +448,15 @@ def run_pt(args):
             line["serving"] = run_serving()
         if world == 1 and not args.no_vcm:
             line["vcm_family"] = run_vcm()
+            line["vcm_family"]["config3_spec"] = run_vcm_spec()
+            if not args.no_cpu_baseline:
+                from oracle import refwrap as R
+                if R.available():
+                    line["vcm_family"]["cpu_baseline"] = reference_vcm_cpu(os.cpu_count() or 1)
+        if world == 1 and not args.no_config1:
+            from oracle import refwrap as R
+            line["config1"] = run_config1(cpu_threads=(os.cpu_count() or 1)
+                                          if not args.no_cpu_baseline and R.available() else 0)
         print(json.dumps(line), flush=True)
     pt.close()
     gs.close()
@@ -629,6 +638,149 @@ def run_vcm(iterations=4, warmup=2, algos=("vcm", "ppm", "bpt")):
                      "pixel_size": round(vi.pixel_size, 5)}
         vi.close()
     gs.close()
+    return out
+
+
+def run_vcm_spec(iterations=64, warmup=2, algos=("vcm", "ppm")):
+    """Config 3 at its own photon-grid parameters: 2^22 buckets, cell size = merge radius,
+    r0 = 0.5 % of the scene diagonal shrinking as r_i = r0 * i^(-1/3), 64 iterations of 1M
+    light paths and one camera sample per pixel (device time per iteration). Then the grid
+    alone on the last iteration's light vertices: build time and k-nearest queries at every
+    vertex (the split the CPU baseline reports)."""
+    import torch
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.hashgrid import HashGrid
+    from imbatracer_b200.integrators import GpuScene, VcmIntegrator
+    desc = G.config3(width=VCM_W, height=VCM_H)
+    lo, hi = G.scene_box(desc)
+    diag = float(np.linalg.norm(hi.astype(np.float64) - lo))
+    r0 = 0.005 * diag
+    gs = GpuScene(desc)
+    out = {"workload": f"config 3 at its grid parameters: {desc.instanced_triangles} triangles, {VCM_W}x{VCM_H}, "
+                       f"{VCM_LIGHT_PATHS} light paths and 1 camera sample per pixel per iteration, max path length "
+                       f"{VCM_MAX_PATH_LEN}, 10 nearest photons, 2^22 buckets, cell = r, r0 = 0.005 x diagonal "
+                       f"({r0:.4f}), r_i = r0 i^(-1/3)", "iterations": iterations, "warmup": warmup}
+    last_cache = None
+    for algo in algos:
+        vi = VcmIntegrator(gs, algo, VCM_W, VCM_H, spp=1, max_path_len=VCM_MAX_PATH_LEN,
+                           light_path_count=VCM_LIGHT_PATHS, num_connections=1, num_knn=10, base_radius=r0,
+                           radius_exponent=1.0 / 3.0, grid_cell_factor=1.0, grid_table_size=1 << 22)
+        image = torch.zeros((VCM_H, VCM_W, 3), dtype=torch.float32, device="cuda")
+        for k in range(warmup):
+            vi.render(k + 1, 11 + k, 101 + k, 0x9E3779B9, image=image)
+        image.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rays = 0
+        for k in range(iterations):
+            vi.render(k + 1, 1000 + k, 2000 + k, 0x9E3779B9, image=image)
+            rays += int(vi.last_stats[0] + vi.last_stats[1])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / iterations
+        radius = vi.begin_iteration(iterations)[0]
+        out[algo] = {"ms_per_iteration": round(ms, 2), "mrays_s": round(rays / iterations / (ms * 1e-3) / 1e6, 1),
+                     "rays_per_iteration": rays // iterations, "light_vertices": N_light_vertices(vi),
+                     "radius_last_iteration": round(radius, 5)}
+        if last_cache is None:
+            vi.render(iterations, 1000, 2000, 0x9E3779B9, image=image)
+            last_cache = (vi.light_vertices(), radius)
+        vi.close()
+    gs.close()
+    if last_cache is not None and len(last_cache[0]):
+        pos = torch.from_numpy(np.ascontiguousarray(last_cache[0][:, :3])).cuda()
+        grid = HashGrid(0)
+        grid.build(pos, last_cache[1], 1.0, 1 << 22)
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        for _ in range(10):
+            grid.build(pos, last_cache[1], 1.0, 1 << 22)
+        e1.record()
+        ids, cnt = grid.query(pos, 10)
+        e2.record()
+        torch.cuda.synchronize()
+        out["grid"] = {"photons": int(pos.shape[0]), "build_ms": round(e0.elapsed_time(e1) / 10, 3),
+                       "queries": int(pos.shape[0]), "query_ms": round(e1.elapsed_time(e2), 3),
+                       "mqueries_s": round(pos.shape[0] / (e1.elapsed_time(e2) * 1e-3) / 1e6, 1),
+                       "note": "k = 10 nearest within r at every light vertex of the last iteration (batched query API)"}
+        grid.close()
+    return out
+
+
+def reference_vcm_cpu(threads: int) -> dict:
+    """The reference's own VCMIntegrator (oracle/_ref) on the config-3 scene, one iteration
+    at the reference's photon-grid parameters (cell 2r, 2n buckets, r = 2 pixel sizes: its
+    HashGrid fixes them), on all host threads: light pass, camera pass, and the grid alone
+    (rebuild; one k-nearest query at every light vertex)."""
+    from imbatracer_b200 import scenegen as G
+    from oracle import refwrap as R
+    desc = G.config3(width=VCM_W, height=VCM_H)
+    with _StdoutToStderr():
+        rs = R.RefScene(desc)
+        R.load().imbart_ref_set_threads(threads, threads)
+        v = R.RefVcm(rs, "vcm", VCM_W, VCM_H, light_path_count=VCM_LIGHT_PATHS, max_path_len=VCM_MAX_PATH_LEN)
+        v.begin_iteration(1)
+        t0 = time.perf_counter()
+        v.light_pass(11)
+        t1 = time.perf_counter()
+        v.camera_pass(22)
+        t2 = time.perf_counter()
+        g = v.time_grid(2, threads)
+        v.close()
+        rs.close()
+        R.load().imbart_ref_set_threads(1, 1)
+    return {"kind": "reference", "cores": threads, "cpu_model": cpu_model(), "unit": "ms/iteration",
+            "value": round((t2 - t0) * 1e3, 1), "light_pass_ms": round((t1 - t0) * 1e3, 1),
+            "camera_pass_ms": round((t2 - t1) * 1e3, 1), "grid_build_ms": round(g["build_s"] * 1e3, 1),
+            "queries": g["queries"], "query_ms": round(g["query_s"] * 1e3, 1),
+            "mqueries_s": round(g["queries"] / max(g["query_s"], 1e-9) / 1e6, 3),
+            "sample": f"one VCM iteration (iteration 1) of the config-3 workload at the reference's grid parameters: "
+                      f"{VCM_LIGHT_PATHS} light paths, {VCM_W}x{VCM_H} camera samples; the light pass includes the "
+                      f"grid build, the camera pass the merging queries; traversal = the oracle's CPU restatement"}
+
+
+def run_config1(cpu_threads: int = 0, frames: int = 10):
+    """Config 1 (32 displaced icospheres + ground + 2-triangle area light, 512x512, 1 spp,
+    4 bounces = max_path_len 5, roulette from bounce 0 as the reference): GPU frame time and
+    Mrays/s through PathTracer, beside the reference's PathTracer on all host threads."""
+    import torch
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    desc = G.config1(width=512, height=512)
+    gs = GpuScene(desc)
+    pt = PathTracer(gs, max_path_len=5, rr_start=0)
+    image = torch.zeros((512, 512, 3), dtype=torch.float32, device="cuda")
+    for k in range(3):
+        pt.render(1, 70 + k, image=image)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rays = 0
+    e0.record()
+    for k in range(frames):
+        pt.render(1, 100 + k, image=image)
+        rays += int(pt.last_stats[0] + pt.last_stats[1])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / frames
+    out = {"workload": f"config 1: {desc.instanced_triangles} triangles, 512x512, 1 spp, max_path_len 5 (4 bounces), "
+                       f"roulette from bounce 0", "frame_ms": round(ms, 3),
+           "mrays_s": round(rays / frames / (ms * 1e-3) / 1e6, 1), "rays_per_frame": rays // frames}
+    pt.close()
+    gs.close()
+    if cpu_threads:
+        from oracle import refwrap as R
+        with _StdoutToStderr():
+            rs = R.RefScene(desc)
+            t0 = time.perf_counter()
+            _, a, b = rs.render_pt_threads(512, 512, 1, 5, 100, cpu_threads)
+            el = time.perf_counter() - t0
+            rs.close()
+        out["cpu_baseline"] = {"kind": "reference", "cores": cpu_threads, "cpu_model": cpu_model(),
+                               "value": round((a + b) / el / 1e6, 3), "unit": "Mrays/s", "frame_ms": round(el * 1e3, 1),
+                               "sample": f"one full frame ({a + b} rays counted by the reference scheduler): the "
+                                         f"reference's PathTracer+TileScheduler with the oracle CPU traversal"}
     return out
 
 
@@ -833,6 +985,7 @@ def main():
                     help="pt mode: wavefront size (paths in flight) instead of the autotuner's pick")
     ap.add_argument("--no-serving", action="store_true", help="pt mode: skip the serving comparison")
     ap.add_argument("--no-config3", action="store_true", help="pt mode: skip the config-3 traversal roofline")
+    ap.add_argument("--no-config1", action="store_true", help="pt mode: skip the config-1 frame and its CPU baseline")
     ap.add_argument("--rate", type=float, nargs="*", default=[150.0, 400.0],
                     help="serve mode: config 5 arrival rates (req/s)")
     args = ap.parse_args()
@@ -846,7 +999,8 @@ def main():
         run_trace(args)
     elif args.mode == "vcm":
         if int(os.environ.get("RANK", "0")) == 0:
-            print(json.dumps({"mode": "vcm", "vcm_family": run_vcm(args.steps, args.warmup)}), flush=True)
+            print(json.dumps({"mode": "vcm", "vcm_family": run_vcm(args.steps, args.warmup),
+                              "config3_spec": run_vcm_spec()}), flush=True)
     elif args.mode == "serve":
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps({"mode": "serve", "serving": run_serving(config5_rates=tuple(args.rate))}), flush=True)

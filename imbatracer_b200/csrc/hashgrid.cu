@@ -37,6 +37,7 @@ struct imbart_hashgrid {
     int block_sums_cap = 0;
     float* params = nullptr;    // device: lo[3], hi[3], radius, r^2, cell, inv_cell
     float host_params[10] = {};
+    float cell_factor = 2.0f;   // cell size / radius of the current build
 };
 
 namespace imbart {
@@ -338,6 +339,7 @@ int imbart_hashgrid_build(imbart_hashgrid* g, const float* positions, int stride
         if (!ok(cudaGetLastError(), "hash grid build")) rc = IMBART_ERR_CUDA;
         g->n = n;
         g->table = table_size;
+        g->cell_factor = cell_factor;
     }
     cudaSetDevice(prev);
     return rc;
@@ -347,6 +349,11 @@ int imbart_hashgrid_query(const imbart_hashgrid* g, const float* queries, int nq
                           int* out_counts, float* out_d2, void* stream) {
     if (!g || nq < 0 || k < 1 || k > kMaxK || (nq > 0 && (!queries || !out_ids || !out_counts)) || g->table == 0) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_query: invalid argument (k must be 1..64, grid built)");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (!(g->cell_factor >= 1.0f)) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_query: the grid's cells are smaller than the radius "
+                                               "(build with cell_factor >= 1)");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
     if (nq == 0) return 0;

@@ -7,6 +7,12 @@
 // reference's insertion rule (a tie with the current k-th replaces it once the list is full).
 // The list is then ordered by (distance, photon index). Every float operation is explicitly
 // rounded, so cells and distances equal the reference's bit for bit.
+//
+// Those eight cells hold every photon within r only while the cell size is at least 2r (the
+// reference's grid: cell = 2r). Grids with smaller cells (r <= cell < 2r, e.g. cell = r) are
+// queried over every cell the box [q - r, q + r] touches instead — up to 4 per axis, bounds
+// rounded outward and mapped to cells with the build's own rounding, so no photon within r
+// is missed — in x-major order, each bucket once.
 #pragma once
 
 #include <stdint.h>
@@ -19,29 +25,86 @@ __device__ __forceinline__ int hash_cell(uint32_t x, uint32_t y, uint32_t z, uin
     return (int)(((x * 73856093u) ^ (y * 19349663u) ^ (z * 83492791u)) % table);
 }
 
-// prm: lo xyz, hi xyz, radius, r^2, cell size, 1 / cell size. sorted: photons in bucket order
-// (xyz + original index bits), ends: inclusive bucket ends. Returns the count; dist / ids
-// (capacity k <= kGridMaxK) hold the result.
+// The cells a query scans. Reference mode (cell >= 2r): cell j of 8 is (j&4 ? xo : x0,
+// j&2 ? yo : y0, j&1 ? zo : z0) with (x0, y0, z0) the home cell and (xo, yo, zo) the nearer
+// neighbours. Range mode: cell j is (x0 + j / (ny nz), y0 + (j / nz) % ny, z0 + j % nz).
+struct GridCells {
+    bool ref_mode;
+    int n;                       // cells to visit
+    int x0, y0, z0;              // home cell / range start
+    int xo, yo, zo;              // reference mode: neighbours
+    int ny, nz;                  // range mode: extent in y and z
+};
+
+// Cell coordinate of a coordinate value, rounded as the build rounds it.
+__device__ __forceinline__ int grid_coord(float v, float lo, float inv) {
+    return (int)floorf(__fmul_rn(inv, __fsub_rn(v, lo)));
+}
+
+// prm: lo xyz, hi xyz, radius, r^2, cell size, 1 / cell size. False outside the grid's box.
+__device__ __forceinline__ bool grid_cells(const float* prm, float qx, float qy, float qz, GridCells& g) {
+    const bool inside = qx >= prm[0] && qy >= prm[1] && qz >= prm[2] && qx <= prm[3] && qy <= prm[4] && qz <= prm[5];
+    if (!inside) return false;
+    const float inv = prm[9], r = prm[6];
+    g.ref_mode = prm[8] >= __fmul_rn(2.0f, r);
+    if (g.ref_mode) {
+        const float cx = __fmul_rn(inv, __fsub_rn(qx, prm[0]));
+        const float cy = __fmul_rn(inv, __fsub_rn(qy, prm[1]));
+        const float cz = __fmul_rn(inv, __fsub_rn(qz, prm[2]));
+        const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+        g.x0 = (int)fx; g.y0 = (int)fy; g.z0 = (int)fz;
+        g.xo = g.x0 + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
+        g.yo = g.y0 + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
+        g.zo = g.z0 + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
+        g.n = 8;
+    } else {
+        // A photon within r has each coordinate in [q - r, q + r]; the bounds are rounded
+        // outward and mapped like photon coordinates (a monotone map), so its cell is inside.
+        g.x0 = grid_coord(__fsub_rd(qx, r), prm[0], inv);
+        g.y0 = grid_coord(__fsub_rd(qy, r), prm[1], inv);
+        g.z0 = grid_coord(__fsub_rd(qz, r), prm[2], inv);
+        const int nx = min(grid_coord(__fadd_ru(qx, r), prm[0], inv) - g.x0 + 1, 4);
+        g.ny = min(grid_coord(__fadd_ru(qy, r), prm[1], inv) - g.y0 + 1, 4);
+        g.nz = min(grid_coord(__fadd_ru(qz, r), prm[2], inv) - g.z0 + 1, 4);
+        g.n = nx * g.ny * g.nz;
+    }
+    return true;
+}
+
+__device__ __forceinline__ int grid_cell_bucket(const GridCells& g, int j, uint32_t table) {
+    int x, y, z;
+    if (g.ref_mode) {
+        x = (j & 4) ? g.xo : g.x0;
+        y = (j & 2) ? g.yo : g.y0;
+        z = (j & 1) ? g.zo : g.z0;
+    } else {
+        x = g.x0 + j / (g.ny * g.nz);
+        y = g.y0 + (j / g.nz) % g.ny;
+        z = g.z0 + j % g.nz;
+    }
+    return hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, table);
+}
+
+// Range mode visits each bucket once: a cell whose bucket an earlier cell already had is skipped.
+__device__ __forceinline__ bool grid_bucket_seen(const GridCells& g, int j, int c, uint32_t table) {
+    if (g.ref_mode) return false;
+    for (int i = 0; i < j; ++i)
+        if (grid_cell_bucket(g, i, table) == c) return true;
+    return false;
+}
+
+// sorted: photons in bucket order (xyz + original index bits), ends: inclusive bucket ends.
+// Returns the count; dist / ids (capacity k <= kGridMaxK) hold the result.
 __device__ __forceinline__ int grid_query_knn(const float4* __restrict__ sorted, const int* __restrict__ ends,
                                               const float* prm, uint32_t table, float qx, float qy, float qz, int k,
                                               float* dist, int* ids) {
     int count = 0;
-    const bool inside = qx >= prm[0] && qy >= prm[1] && qz >= prm[2] && qx <= prm[3] && qy <= prm[4] && qz <= prm[5];
-    if (!inside) return 0;
-    const float inv = prm[9], r2 = prm[7];
-    const float cx = __fmul_rn(inv, __fsub_rn(qx, prm[0]));
-    const float cy = __fmul_rn(inv, __fsub_rn(qy, prm[1]));
-    const float cz = __fmul_rn(inv, __fsub_rn(qz, prm[2]));
-    const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
-    const int px = (int)fx, py = (int)fy, pz = (int)fz;
-    const int pxo = px + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
-    const int pyo = py + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
-    const int pzo = pz + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
-    for (int j = 0; j < 8; ++j) {
-        const int x = (j & 4) ? pxo : px;
-        const int y = (j & 2) ? pyo : py;
-        const int z = (j & 1) ? pzo : pz;
-        const int c = hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, table);
+    GridCells g;
+    if (!grid_cells(prm, qx, qy, qz, g)) return 0;
+    const float r2 = prm[7];
+    for (int j = 0; j < g.n; ++j) {
+        const int c = grid_cell_bucket(g, j, table);
+        if (grid_bucket_seen(g, j, c, table)) continue;
         const int b = c == 0 ? 0 : __ldg(ends + c - 1);
         const int e = __ldg(ends + c);
         for (int s = b; s < e; ++s) {

@@ -550,56 +550,63 @@ __global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const 
     float my_d = 0.0f;      // list entry `lane`
     int my_id = -1;
     int count = 0;
-    const bool inside = qx >= prm[0] && qy >= prm[1] && qz >= prm[2] && qx <= prm[3] && qy <= prm[4] && qz <= prm[5];
-    if (inside) {
-        const float inv = prm[9], r2 = prm[7];
-        const float cx = __fmul_rn(inv, __fsub_rn(qx, prm[0]));
-        const float cy = __fmul_rn(inv, __fsub_rn(qy, prm[1]));
-        const float cz = __fmul_rn(inv, __fsub_rn(qz, prm[2]));
-        const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
-        const int px = (int)fx, py = (int)fy, pz = (int)fz;
-        const int pxo = px + (__fsub_rn(cx, fx) < 0.5f ? -1 : 1);
-        const int pyo = py + (__fsub_rn(cy, fy) < 0.5f ? -1 : 1);
-        const int pzo = pz + (__fsub_rn(cz, fz) < 0.5f ? -1 : 1);
-        for (int j = 0; j < 8; ++j) {
-            const int x = (j & 4) ? pxo : px;
-            const int y = (j & 2) ? pyo : py;
-            const int z = (j & 1) ? pzo : pz;
-            const int c = hash_cell((uint32_t)x, (uint32_t)y, (uint32_t)z, p.grid_table);
-            const int b = c == 0 ? 0 : __ldg(p.grid_ends + c - 1);
-            const int e = __ldg(p.grid_ends + c);
-            for (int base = b; base < e; base += 32) {
-                const int s = base + lane;
-                float d2 = 0.0f;
-                int id = -1;
-                bool within = false;
-                if (s < e) {
-                    const float4 ph = __ldg(p.grid_sorted + s);
-                    const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
-                    d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                    id = __float_as_int(ph.w);
-                    within = d2 <= r2;
-                }
-                unsigned cand = __ballot_sync(0xffffffffu, within);
-                while (cand) {
-                    const int src = __ffs(cand) - 1;
-                    cand &= cand - 1;
-                    const float cd = __shfl_sync(0xffffffffu, d2, src);
-                    const int cid = __shfl_sync(0xffffffffu, id, src);
-                    int kept;
-                    if (count == k) {
-                        const float last = __shfl_sync(0xffffffffu, my_d, k - 1);
-                        if (last < cd) continue;
-                        kept = k - 1;
-                    } else {
-                        kept = count;
-                        count++;
+    GridCells gc;
+    if (grid_cells(prm, qx, qy, qz, gc)) {
+        const float r2 = prm[7];
+        // Lane j of a chunk computes cell (chunk + j)'s bucket; in range mode buckets met
+        // before (lower lane or the previous chunk) are dropped, so each is scanned once.
+        int prev_bucket = -1;
+        for (int c0 = 0; c0 < gc.n; c0 += 32) {
+            const int jj = c0 + lane;
+            const int my_bucket = jj < gc.n ? grid_cell_bucket(gc, jj, p.grid_table) : -2 - lane;
+            bool seen = false;
+            if (!gc.ref_mode) {
+                const unsigned same = __match_any_sync(0xffffffffu, my_bucket);
+                seen = (same & ((1u << lane) - 1u)) != 0u;
+                if (c0 > 0)
+                    for (int l = 0; l < 32; ++l) seen |= __shfl_sync(0xffffffffu, prev_bucket, l) == my_bucket;
+            }
+            unsigned todo = __ballot_sync(0xffffffffu, jj < gc.n && !seen);
+            prev_bucket = my_bucket;
+            while (todo) {
+                const int cl = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int c = __shfl_sync(0xffffffffu, my_bucket, cl);
+                const int b = c == 0 ? 0 : __ldg(p.grid_ends + c - 1);
+                const int e = __ldg(p.grid_ends + c);
+                for (int base = b; base < e; base += 32) {
+                    const int s = base + lane;
+                    float d2 = 0.0f;
+                    int id = -1;
+                    bool within = false;
+                    if (s < e) {
+                        const float4 ph = __ldg(p.grid_sorted + s);
+                        const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
+                        d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+                        id = __float_as_int(ph.w);
+                        within = d2 <= r2;
                     }
-                    const int pos = __popc(__ballot_sync(0xffffffffu, lane < kept && my_d <= cd));
-                    const float up_d = __shfl_up_sync(0xffffffffu, my_d, 1);
-                    const int up_id = __shfl_up_sync(0xffffffffu, my_id, 1);
-                    if (lane > pos && lane <= kept) { my_d = up_d; my_id = up_id; }
-                    if (lane == pos) { my_d = cd; my_id = cid; }
+                    unsigned cand = __ballot_sync(0xffffffffu, within);
+                    while (cand) {
+                        const int src = __ffs(cand) - 1;
+                        cand &= cand - 1;
+                        const float cd = __shfl_sync(0xffffffffu, d2, src);
+                        const int cid = __shfl_sync(0xffffffffu, id, src);
+                        int kept;
+                        if (count == k) {
+                            const float last = __shfl_sync(0xffffffffu, my_d, k - 1);
+                            if (last < cd) continue;
+                            kept = k - 1;
+                        } else {
+                            kept = count;
+                            count++;
+                        }
+                        const int pos = __popc(__ballot_sync(0xffffffffu, lane < kept && my_d <= cd));
+                        const float up_d = __shfl_up_sync(0xffffffffu, my_d, 1);
+                        const int up_id = __shfl_up_sync(0xffffffffu, my_id, 1);
+                        if (lane > pos && lane <= kept) { my_d = up_d; my_id = up_id; }
+                        if (lane == pos) { my_d = cd; my_id = cid; }
+                    }
                 }
             }
         }
@@ -945,7 +952,9 @@ void free_vcm(imbart_vcm* v) {
 bool valid_settings(const imbart_vcm_settings* st) {
     return st && st->algorithm >= IMBART_VCM && st->algorithm <= IMBART_VCM_PT && st->spp > 0 &&
            st->max_path_len >= 1 && st->light_path_count > 0 && st->num_connections >= 0 && st->num_knn >= 1 &&
-           st->num_knn <= kGridMaxK && st->light_tile_size >= 0 && st->base_radius > 0.0f;
+           st->num_knn <= kGridMaxK && st->light_tile_size >= 0 && st->base_radius > 0.0f &&
+           st->radius_exponent >= 0.0f && (st->grid_cell_factor == 0.0f || st->grid_cell_factor >= 1.0f) &&
+           st->grid_table_size >= 0;
 }
 
 bool ensure_shadow(imbart_vcm* v, long long need) {
@@ -1043,8 +1052,10 @@ int build_grid(imbart_vcm* v, const imbart_vcm_settings* st, cudaStream_t s) {
     v->grid_built = false;
     if ((st->algorithm != IMBART_VCM && st->algorithm != IMBART_PPM) || v->cache_count == 0) return 0;
     // LightVertices::build (light_vertices.h:70-75): HashGrid::build(radius) over the cache.
+    // The reference's cell of 2r and 2n buckets unless the settings choose others.
+    const float cell_factor = st->grid_cell_factor > 0.0f ? st->grid_cell_factor : 2.0f;
     const int rc = imbart_hashgrid_build(v->grid, reinterpret_cast<const float*>(v->cache), 28, v->cache_count,
-                                         v->pm_radius, 2.0f, 0, s);
+                                         v->pm_radius, cell_factor, st->grid_table_size, s);
     v->grid_built = rc == 0;
     return rc;
 }
@@ -1151,7 +1162,8 @@ int imbart_vcm_begin_iteration(imbart_vcm* v, const imbart_vcm_settings* st, int
     // vcm.cpp:27-46
     const float radius_alpha = 0.75f;
     v->iteration = iteration;
-    v->pm_radius = st->base_radius / powf(static_cast<float>(iteration), 0.5f * (1.0f - radius_alpha));
+    const float exponent = st->radius_exponent > 0.0f ? st->radius_exponent : 0.5f * (1.0f - radius_alpha);
+    v->pm_radius = st->base_radius / powf(static_cast<float>(iteration), exponent);
     v->pm_radius = std::max(v->pm_radius, 1e-7f);
     const float pi = 3.14159265359f;
     const float eta_vcm = pi * (v->pm_radius * v->pm_radius) * (float)st->light_path_count;

@@ -271,7 +271,10 @@ def estimate_pixel_size(scene: GpuScene, cam: N.Camera) -> float:
 class VcmIntegrator:
     """VCMIntegrator<algo> (vcm.h:54-150) on the GPU: algorithm "vcm", "bpt", "ppm", "lt" or
     "pt"; settings as the reference's UserSettings (cmd_line.h:40-58). render(iteration) =
-    light pass + camera pass (vcm.cpp:25-55); the photon radius shrinks with the iteration.
+    light pass + camera pass (vcm.cpp:25-55); the photon radius shrinks with the iteration
+    (base_radius * i^-radius_exponent; 0 = the reference's 1/8) and the photon grid has cells
+    of grid_cell_factor radii (0 = the reference's 2) and grid_table_size buckets (0 = twice
+    the photons).
     Images are (height, width, 3) float32 CUDA tensors, accumulated like the reference's
     AtomicImage."""
 
@@ -279,7 +282,8 @@ class VcmIntegrator:
                  spp: int = 1, max_path_len: int = 10, light_path_count: int | None = None,
                  num_connections: int = 1, num_knn: int = 10, radius_factor: float = 2.0,
                  base_radius: float | None = None, light_tile_size: int = 0, cam: G.Camera | None = None,
-                 max_paths_in_flight: int = 0):
+                 max_paths_in_flight: int = 0, radius_exponent: float = 0.0, grid_cell_factor: float = 0.0,
+                 grid_table_size: int = 0):
         self.scene = scene
         cam = cam or scene.desc.camera
         self.width = width or cam.width
@@ -295,6 +299,10 @@ class VcmIntegrator:
         st.light_tile_size = light_tile_size
         self.pixel_size = estimate_pixel_size(scene, self.camera)
         st.base_radius = base_radius if base_radius is not None else self.pixel_size * radius_factor
+        # Photon-grid schedule; zeros keep the reference's (radius ~ i^-1/8, cell 2r, 2n buckets).
+        st.radius_exponent = radius_exponent
+        st.grid_cell_factor = grid_cell_factor
+        st.grid_table_size = grid_table_size
         self.max_paths = max_paths_in_flight
         self.ctx = N.load().imbart_vcm_create(scene.device)
         if not self.ctx:

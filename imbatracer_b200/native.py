@@ -54,7 +54,8 @@ class VcmSettings(C.Structure):
     _fields_ = [("algorithm", C.c_int), ("spp", C.c_int), ("max_path_len", C.c_int), ("light_path_count", C.c_int),
                 ("num_connections", C.c_int), ("num_knn", C.c_int), ("light_tile_size", C.c_int),
                 ("base_radius", C.c_float), ("light_seed", C.c_ulonglong), ("light_seed_step", C.c_ulonglong),
-                ("camera_seed", C.c_ulonglong)]
+                ("camera_seed", C.c_ulonglong), ("radius_exponent", C.c_float), ("grid_cell_factor", C.c_float),
+                ("grid_table_size", C.c_int)]
 
 
 VCM, BPT, PPM, LT, VCM_PT = 0, 1, 2, 3, 4

@@ -481,6 +481,13 @@ typedef struct {
     float base_radius;        /* photon radius of iteration 1 (pixel size * radius factor) */
     unsigned long long light_seed, light_seed_step;  /* light tile t is seeded from light_seed + t * step */
     unsigned long long camera_seed;                  /* seed_base of the camera samples */
+    /* Photon-grid schedule (zero = the reference's): the radius of iteration i is
+     * base_radius * i^-radius_exponent (0: the reference's (1 - 0.75) / 2 = 1/8, vcm.cpp:27-38),
+     * the grid's cells are grid_cell_factor radii wide (0: 2, rangesearch.h:27-30; at least 1)
+     * and it has grid_table_size buckets (0: twice the photons, rangesearch.h:26,33-34). */
+    float radius_exponent;
+    float grid_cell_factor;
+    int grid_table_size;
 } imbart_vcm_settings;
 
 /* Context with device buffers (light-path slots, light-vertex cache, photon grid, queues). */

@@ -76,9 +76,29 @@ void oracle_hashgrid_build(const float* pos, int stride, int n, float radius, fl
     free(cell);
 }
 
+/* Cell coordinate of a coordinate value with the build's rounding. */
+static int grid_coord(const o_grid* g, float v, int axis) {
+    return (int)floorf(g->inv_cell_size * (v - g->lo[axis]));
+}
+
+/* q - r rounded down and q + r rounded up (the box a photon within r lies in). */
+static float sub_down(float q, float r) {
+    float a = q - r;
+    if ((double)a > (double)q - (double)r) a = nextafterf(a, -INFINITY);
+    return a;
+}
+static float add_up(float q, float r) {
+    float b = q + r;
+    if ((double)b < (double)q + (double)r) b = nextafterf(b, INFINITY);
+    return b;
+}
+
 /* Queries nq positions; out_ids gets up to k original photon indices per query (ordered by
  * distance as the reference's insertion sort leaves them), out_count the count and
- * out_d2 (optional) the squared distances. */
+ * out_d2 (optional) the squared distances. Grids whose cell is at least 2r (the reference's)
+ * scan the reference's eight cells; grids with r <= cell < 2r scan every cell the box
+ * [q - r, q + r] touches (bounds rounded outward, at most 4 per axis), x-major, each bucket
+ * once — the same cells and order as the GPU query. */
 void oracle_hashgrid_query(const o_grid* g, const int* cell_ends, const int* sorted_ids,
                            const float* pos, int stride, const float* queries, int nq, int k,
                            int* out_ids, int* out_count, float* out_d2, int threads) {
@@ -92,19 +112,40 @@ void oracle_hashgrid_query(const o_grid* g, const int* cell_ends, const int* sor
         const int inside = qp[0] >= g->lo[0] && qp[1] >= g->lo[1] && qp[2] >= g->lo[2] &&
                            qp[0] <= g->hi[0] && qp[1] <= g->hi[1] && qp[2] <= g->hi[2];
         if (inside && k > 0 && k <= 256) {
-            const float cx = g->inv_cell_size * (qp[0] - g->lo[0]);
-            const float cy = g->inv_cell_size * (qp[1] - g->lo[1]);
-            const float cz = g->inv_cell_size * (qp[2] - g->lo[2]);
-            const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
-            const int px = (int)fx, py = (int)fy, pz = (int)fz;
-            const int pxo = px + ((cx - fx) < 0.5f ? -1 : 1);
-            const int pyo = py + ((cy - fy) < 0.5f ? -1 : 1);
-            const int pzo = pz + ((cz - fz) < 0.5f ? -1 : 1);
-            for (int j = 0; j < 8; ++j) {
-                const int x = (j & 4) ? pxo : px;
-                const int y = (j & 2) ? pyo : py;
-                const int z = (j & 1) ? pzo : pz;
-                const int c = cell_index_u(g, (uint32_t)x, (uint32_t)y, (uint32_t)z);
+            const int ref_mode = g->cell_size >= 2.0f * g->radius;
+            int cells[64];
+            int n = 0;
+            if (ref_mode) {
+                const float cx = g->inv_cell_size * (qp[0] - g->lo[0]);
+                const float cy = g->inv_cell_size * (qp[1] - g->lo[1]);
+                const float cz = g->inv_cell_size * (qp[2] - g->lo[2]);
+                const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+                const int px = (int)fx, py = (int)fy, pz = (int)fz;
+                const int pxo = px + ((cx - fx) < 0.5f ? -1 : 1);
+                const int pyo = py + ((cy - fy) < 0.5f ? -1 : 1);
+                const int pzo = pz + ((cz - fz) < 0.5f ? -1 : 1);
+                for (int j = 0; j < 8; ++j)
+                    cells[n++] = cell_index_u(g, (uint32_t)((j & 4) ? pxo : px), (uint32_t)((j & 2) ? pyo : py),
+                                              (uint32_t)((j & 1) ? pzo : pz));
+            } else {
+                int lo_c[3], cnt[3];
+                for (int a = 0; a < 3; ++a) {
+                    lo_c[a] = grid_coord(g, sub_down(qp[a], g->radius), a);
+                    cnt[a] = grid_coord(g, add_up(qp[a], g->radius), a) - lo_c[a] + 1;
+                    if (cnt[a] > 4) cnt[a] = 4;
+                }
+                for (int x = 0; x < cnt[0]; ++x)
+                    for (int y = 0; y < cnt[1]; ++y)
+                        for (int z = 0; z < cnt[2]; ++z) {
+                            const int c = cell_index_u(g, (uint32_t)(lo_c[0] + x), (uint32_t)(lo_c[1] + y),
+                                                       (uint32_t)(lo_c[2] + z));
+                            int seen = 0;
+                            for (int i = 0; i < n; ++i) seen |= cells[i] == c;
+                            if (!seen) cells[n++] = c;
+                        }
+            }
+            for (int j = 0; j < n; ++j) {
+                const int c = cells[j];
                 const int b = c == 0 ? 0 : cell_ends[c - 1];
                 const int e = cell_ends[c];
                 for (int s = b; s < e; ++s) {

@@ -55,6 +55,7 @@ struct RefVcmBase {
     virtual void camera_pass(AtomicImage& img) = 0;
     virtual int vertices(float* out, int cap) = 0;
     virtual void mis_eta(float* out2) = 0;
+    virtual void time_grid(int reps, int threads, double* out3) = 0;
 };
 
 template <VCMSubAlgorithm algo>
@@ -102,6 +103,31 @@ struct RefVcm : RefVcmBase {
     void mis_eta(float* out2) override {
         out2[0] = integ.mis_eta_vc_;
         out2[1] = integ.mis_eta_vm_;
+    }
+
+    // The reference's photon grid over the current cache, timed on its own: `reps` rebuilds
+    // (LightVertices::build -> HashGrid::build, light_vertices.h:70-75) and one k-nearest
+    // query (LightVertices::get_merge, as vertex_merging calls it, vcm.cpp:571-576) at every
+    // cached vertex, spread over `threads` OpenMP threads. out: seconds per build, seconds
+    // for all queries, queries.
+    void time_grid(int reps, int threads, double* out3) override {
+        LightVertices& lv = integ.light_vertices_;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int r = 0; r < reps; ++r) lv.build(integ.pm_radius_, true);
+        const auto t1 = std::chrono::steady_clock::now();
+        const int n = lv.count();
+        const int k = settings.num_knn;
+        long long found = 0;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads) reduction(+ : found)
+        for (int i = 0; i < n; ++i) {
+            std::vector<const VCMPhoton*> out(k);
+            found += lv.get_merge(lv.cache_[i].isect.pos, out, k);
+        }
+        const auto t2 = std::chrono::steady_clock::now();
+        out3[0] = std::chrono::duration<double>(t1 - t0).count() / std::max(reps, 1);
+        out3[1] = std::chrono::duration<double>(t2 - t1).count();
+        out3[2] = (double)n;
+        (void)found;
     }
 
     // 28 floats per vertex: pos, mat | out_dir, path_length | normal, dVC | geom_normal, dVCM |
@@ -208,6 +234,10 @@ void ref_vcm_light_pass(void* h, uint64_t seed, uint64_t step, float* image_out)
 
 int ref_vcm_light_vertices(void* h, float* out, int cap) {
     return static_cast<Handle*>(h)->vcm->vertices(out, cap);
+}
+
+void ref_vcm_time_grid(void* h, int reps, int threads, double* out3) {
+    static_cast<Handle*>(h)->vcm->time_grid(reps, threads, out3);
 }
 
 void ref_vcm_camera_pass(void* h, uint64_t seed, float* image_out) {

@@ -91,6 +91,7 @@ def load() -> C.CDLL:
             "ref_vcm_light_pass": (None, [P, U64, U64, P]),
             "ref_vcm_light_vertices": (I, [P, P, I]),
             "ref_vcm_camera_pass": (None, [P, U64, P]),
+            "ref_vcm_time_grid": (None, [P, I, I, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -406,6 +407,13 @@ class RefVcm:
         img = np.zeros((self.h, self.w, 3), np.float32)
         load().ref_vcm_camera_pass(self.handle, seed & (2 ** 64 - 1), _p(img))
         return img
+
+    def time_grid(self, reps: int = 3, threads: int = 1) -> dict:
+        """The reference's photon grid over the current cache: seconds per rebuild, and the
+        seconds of one k-nearest query at every cached vertex on `threads` threads."""
+        out = np.zeros(3, np.float64)
+        load().ref_vcm_time_grid(self.handle, reps, threads, _p(out))
+        return {"build_s": float(out[0]), "query_s": float(out[1]), "queries": int(out[2])}
 
     def close(self):
         if self.handle:

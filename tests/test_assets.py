@@ -428,11 +428,14 @@ needs_ref_lib = pytest.mark.skipif(not R.available(), reason="oracle/_ref not bu
 
 @pytest.mark.gpu
 @needs_ref_lib
-@pytest.mark.parametrize("w,h,spp,max_len,seed", [(64, 48, 8, 6, 31), (40, 30, 4, 3, 32)])
+@pytest.mark.parametrize("w,h,spp,max_len,seed", [(64, 48, 8, 6, 31), (40, 30, 16, 3, 32)])
 def test_feature_scene_path_traced_like_the_reference(cuda, tmp_path, w, h, spp, max_len, seed):
     """Every feature the asset path carries (environment image, all light kinds, raw / RLE
     TGA textures, bump maps, opacity masks, glass / mirror / glossy / emissive materials,
-    rotated and scaled instances) rendered by the reference from the same files."""
+    rotated and scaled instances) rendered by the reference from the same files. About one
+    path in 5,000 takes a different turn after float-level differences (ulps of sinf / powf
+    in the shading code), so each image holds enough samples (>= 19,200) that one such path
+    stays below the tolerance; at 40x30 x 4 spp one diverged path alone measured 4.3e-3."""
     from imbatracer_b200.integrators import GpuScene, PathTracer
     path = feature_scene(str(tmp_path))
     ref = R.RefScene.from_file(path, w, h).render_pt(w, h, spp, max_len, seed)

@@ -72,6 +72,32 @@ def test_oracle_grid_against_brute_force():
         assert len(set(have)) == len(want) # ...and nothing outside it (duplicates only from twice-hashed buckets)
 
 
+@pytest.mark.parametrize("cell_factor,table", [(1.0, 1 << 22), (1.0, 0), (1.5, 4099)])
+def test_oracle_range_queries_are_complete(cell_factor, table):
+    """Grids with cells smaller than 2r (the workload's cell = r) scan every cell the query's
+    box touches: exactly the photons in radius, each once (no duplicates, even where two
+    cells share a bucket), the k nearest of them when capped."""
+    pos = photon_cloud(20000, 4)
+    r = 0.3
+    g, ends, ids = O.hashgrid_build(pos, r, cell_factor, table if table else None)
+    q = queries_near(pos, 600, 5, 0.2)
+    lo, hi = np.array(g.lo, np.float32), np.array(g.hi, np.float32)
+    for k in (256, 8):
+        got, cnt, d2 = O.hashgrid_query(g, ends, ids, pos, q, k)
+        ref = brute_neighbours(pos, q, r, 1 << 30)
+        for i in range(len(q)):
+            inside = np.all(q[i] >= lo) and np.all(q[i] <= hi)
+            want = ref[i] if inside else ref[i][:0]
+            have = got[i, : cnt[i]]
+            assert len(set(have.tolist())) == len(have)          # each photon once
+            if k == 256:
+                assert set(have.tolist()) == set(want.tolist())
+            else:
+                dq = ((q[i][None, :] - pos[want]) ** 2)
+                dw = np.sort((dq[:, 0] + dq[:, 1]) + dq[:, 2])[:k]
+                assert np.array_equal(np.sort(d2[i, : cnt[i]]), dw)
+
+
 def test_oracle_grid_box_and_hash():
     pos = photon_cloud(1000, 3)
     g, ends, ids = O.hashgrid_build(pos, 0.5, cell_factor=2.0)
@@ -131,6 +157,14 @@ def test_gpu_neighbour_sets_bit_exact(cuda, n, r, k, cf, table):
     mism, wcnt = compare_sets(pos, q, r, k, cf, table)
     assert mism <= len(q) // 1000
     assert (wcnt > 0).mean() > 0.3
+    if cf < 2.0:
+        # the grid's neighbour sets are the true radius sets (brute force, first queries)
+        grid, got, gcnt, _ = run_gpu(pos, q[:300], r, 256, cf, table)
+        prm = grid.params()
+        ref = brute_neighbours(pos, q[:300], r, 1 << 30)
+        for i in range(300):
+            inside = np.all(q[i] >= prm["lo"]) and np.all(q[i] <= prm["hi"])
+            assert set(got[i, : gcnt[i]].tolist()) == (set(ref[i].tolist()) if inside else set()), i
 
 
 @pytest.mark.gpu

@@ -156,3 +156,81 @@ def test_gpu_vcm_is_deterministic(cuda):
     assert len(caches[0]) > 0
     assert np.array_equal(caches[0].view(np.int32), caches[1].view(np.int32))
     assert rel_rmse(images[0], images[1]) <= 1e-5
+
+
+@pytest.fixture(scope="module")
+def config3_scene():
+    """The config-3 generator (400 displaced spheres, ~2M triangles) in both renderers."""
+    from imbatracer_b200 import scenegen as G
+    from imbatracer_b200.integrators import GpuScene
+    d = G.config3(width=320, height=180)
+    return d, R.RefScene(d), GpuScene(d)
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("algo", ["vcm", "ppm"])
+def test_config3_scale_passes_match_reference(cuda, config3_scene, algo):
+    """The 2M-triangle config-3 scene with 200k light paths (max path length 8) and a 320x180
+    camera: the light-vertex cache equals the reference's as a set and the camera pass on the
+    reference's cache matches its image, over two iterations (the radius shrinks)."""
+    from imbatracer_b200.integrators import VcmIntegrator
+    d, rs, gs = config3_scene
+    w, h, paths = 320, 180, 200_000
+    rv = R.RefVcm(rs, algo, w, h, max_path_len=8, light_path_count=paths)
+    vi = VcmIntegrator(gs, algo, w, h, spp=1, max_path_len=8, light_path_count=paths, num_connections=1,
+                       num_knn=10, base_radius=rv.base_radius, light_tile_size=rv.tile_size * rv.tile_size)
+    for it, (ls, cs) in enumerate([(5150, 6160), (7170, 8180)], start=1):
+        assert rv.begin_iteration(it) == vi.begin_iteration(it)
+        rv.light_pass(ls, 3)
+        ref_v = rv.light_vertices()
+        vi.light_pass(ls, 3)
+        got_v = vi.light_vertices()
+        assert len(ref_v) > 100_000
+        assert abs(len(got_v) - len(ref_v)) <= 0.002 * len(ref_v), (len(got_v), len(ref_v))
+        ok, _ = match_vertices(ref_v, got_v)
+        assert ok.mean() >= 0.995, ok.mean()
+        ref = rv.camera_pass(cs)
+        vi.load_light_vertices(ref_v)
+        img = vi.camera_pass(cs).cpu().numpy()
+        assert ref.sum() > 0
+        assert rel_rmse(img, ref) <= IMAGE_TOL, (it, rel_rmse(img, ref))
+    vi.close()
+    rv.close()
+
+
+@pytest.mark.gpu
+def test_grid_with_cells_of_one_radius_merges_the_same_photons(cuda):
+    """Config 3's own grid (cells one radius wide, 2^22 buckets; the query then scans every
+    cell the radius touches) finds the same k nearest photons as the reference's grid (cells
+    2r wide, 2n buckets) at the same radius: equal images up to float summation order."""
+    from imbatracer_b200.integrators import GpuScene, VcmIntegrator
+    gs = GpuScene(H.scene_desc("config1"))
+    imgs = []
+    for cf, table in ((0.0, 0), (1.0, 1 << 22), (1.5, 4099)):
+        vi = VcmIntegrator(gs, "ppm", 64, 48, spp=1, max_path_len=6, light_path_count=20_000, num_knn=10,
+                           base_radius=0.6, grid_cell_factor=cf, grid_table_size=table)
+        imgs.append(vi.render(1, 41, 42).cpu().numpy())
+        vi.close()
+    assert imgs[0].sum() > 0
+    assert rel_rmse(imgs[1], imgs[0]) <= 1e-5 and rel_rmse(imgs[2], imgs[0]) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_radius_schedule_and_grid_settings(cuda):
+    """radius_exponent sets r_i = r0 * i^-exponent (0: the reference's 1/8); a cell factor
+    below 1 is refused."""
+    from imbatracer_b200 import native as N
+    from imbatracer_b200.integrators import GpuScene, VcmIntegrator
+    gs = GpuScene(H.scene_desc("config1"))
+    vi = VcmIntegrator(gs, "vcm", 32, 32, light_path_count=100, base_radius=0.5, radius_exponent=1.0 / 3.0)
+    for i in (1, 8, 64):
+        r = vi.begin_iteration(i)[0]
+        assert abs(r - 0.5 * i ** (-1.0 / 3.0)) <= 1e-6 * r, (i, r)
+    vi.close()
+    vi = VcmIntegrator(gs, "vcm", 32, 32, light_path_count=100, base_radius=0.5)
+    assert abs(vi.begin_iteration(16)[0] - 0.5 / 16 ** 0.125) <= 1e-6
+    vi.settings.grid_cell_factor = 0.5
+    with pytest.raises(N.ImbartError):
+        vi.begin_iteration(1)
+    vi.close()
