@@ -679,9 +679,10 @@ def run_vcm_spec(iterations=64, warmup=2, algos=("vcm", "ppm")):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / iterations
+        vertices = N_light_vertices(vi)
         radius = vi.begin_iteration(iterations)[0]
         out[algo] = {"ms_per_iteration": round(ms, 2), "mrays_s": round(rays / iterations / (ms * 1e-3) / 1e6, 1),
-                     "rays_per_iteration": rays // iterations, "light_vertices": N_light_vertices(vi),
+                     "rays_per_iteration": rays // iterations, "light_vertices": vertices,
                      "radius_last_iteration": round(radius, 5)}
         if last_cache is None:
             vi.render(iterations, 1000, 2000, 0x9E3779B9, image=image)
@@ -704,7 +705,8 @@ def run_vcm_spec(iterations=64, warmup=2, algos=("vcm", "ppm")):
         out["grid"] = {"photons": int(pos.shape[0]), "build_ms": round(e0.elapsed_time(e1) / 10, 3),
                        "queries": int(pos.shape[0]), "query_ms": round(e1.elapsed_time(e2), 3),
                        "mqueries_s": round(pos.shape[0] / (e1.elapsed_time(e2) * 1e-3) / 1e6, 1),
-                       "note": "k = 10 nearest within r at every light vertex of the last iteration (batched query API)"}
+                       "note": "cell = r, 2^22 buckets, r of the last iteration; k = 10 nearest within r at "
+                               "every light vertex (batched query API, one thread per query)"}
         grid.close()
     return out
 

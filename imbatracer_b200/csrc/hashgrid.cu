@@ -369,6 +369,119 @@ int imbart_hashgrid_query(const imbart_hashgrid* g, const float* queries, int nq
     return good ? 0 : IMBART_ERR_CUDA;
 }
 
+}  // extern "C"
+
+namespace imbart {
+namespace {
+// Staging buffers and a stream of one host thread for the host-array entry points (on one
+// device at a time; they move to another device when the grid does).
+struct HostStaging {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    float* in = nullptr;
+    size_t in_cap = 0;
+    int* ids = nullptr;
+    size_t out_cap = 0;
+    float* d2 = nullptr;
+    size_t d2_cap = 0;
+    int* counts = nullptr;
+    size_t count_cap = 0;
+
+    void release() {
+        cudaFree(in); cudaFree(ids); cudaFree(d2); cudaFree(counts);
+        if (stream) cudaStreamDestroy(stream);
+        in = nullptr; ids = nullptr; d2 = nullptr; counts = nullptr; stream = nullptr;
+        in_cap = out_cap = d2_cap = count_cap = 0;
+    }
+    ~HostStaging() { if (device >= 0) release(); }
+
+    bool on(int dev) {
+        if (device == dev) return true;
+        if (device >= 0) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(device);
+            release();
+            cudaSetDevice(prev);
+        }
+        device = dev;
+        return ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+};
+
+template <typename T>
+bool stage(T** p, size_t* cap, size_t need) {
+    if (*cap >= need) return true;
+    const size_t n = std::max(need, *cap * 3 / 2);
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (!ok(cudaMalloc((void**)p, sizeof(T) * n), "cudaMalloc")) return false;
+    *cap = n;
+    return true;
+}
+
+thread_local HostStaging t_staging;
+}  // namespace
+}  // namespace imbart
+
+extern "C" {
+
+int imbart_hashgrid_build_host(imbart_hashgrid* g, const float* positions, int stride, int n, float radius,
+                               float cell_factor, int table_size) {
+    if (!g || n < 0 || (n > 0 && !positions) || stride < 3) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_build_host: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    HostStaging& h = t_staging;
+    const size_t floats = (size_t)std::max(n, 1) * (size_t)stride;
+    int rc = 0;
+    if (!h.on(g->device) || !stage(&h.in, &h.in_cap, floats)) rc = IMBART_ERR_CUDA;
+    if (!rc && n > 0 &&
+        !ok(cudaMemcpyAsync(h.in, positions, sizeof(float) * (size_t)n * stride, cudaMemcpyHostToDevice, h.stream),
+            "cudaMemcpyAsync"))
+        rc = IMBART_ERR_CUDA;
+    if (!rc) rc = imbart_hashgrid_build(g, h.in, stride, n, radius, cell_factor, table_size, h.stream);
+    if (!rc && !ok(cudaStreamSynchronize(h.stream), "imbart_hashgrid_build_host")) rc = IMBART_ERR_CUDA;
+    cudaSetDevice(prev);
+    return rc;
+}
+
+int imbart_hashgrid_query_host(const imbart_hashgrid* g, const float* queries, int nq, int k, int* out_ids,
+                               int* out_counts, float* out_d2) {
+    if (!g || nq < 0 || k < 1 || k > kMaxK || (nq > 0 && (!queries || !out_ids || !out_counts))) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_query_host: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    if (nq == 0) return 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->device);
+    HostStaging& h = t_staging;
+    const size_t nk = (size_t)nq * (size_t)k;
+    int rc = 0;
+    if (!h.on(g->device) || !stage(&h.in, &h.in_cap, (size_t)nq * 3) || !stage(&h.ids, &h.out_cap, nk) ||
+        !stage(&h.counts, &h.count_cap, (size_t)nq))
+        rc = IMBART_ERR_CUDA;
+    if (!rc && out_d2 && !stage(&h.d2, &h.d2_cap, nk)) rc = IMBART_ERR_CUDA;
+    if (!rc && !ok(cudaMemcpyAsync(h.in, queries, sizeof(float) * 3 * (size_t)nq, cudaMemcpyHostToDevice, h.stream),
+                   "cudaMemcpyAsync"))
+        rc = IMBART_ERR_CUDA;
+    if (!rc) rc = imbart_hashgrid_query(g, h.in, nq, k, h.ids, h.counts, out_d2 ? h.d2 : nullptr, h.stream);
+    if (!rc && !(ok(cudaMemcpyAsync(out_ids, h.ids, sizeof(int) * nk, cudaMemcpyDeviceToHost, h.stream), "D2H") &&
+                 ok(cudaMemcpyAsync(out_counts, h.counts, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost, h.stream),
+                    "D2H") &&
+                 (!out_d2 || ok(cudaMemcpyAsync(out_d2, h.d2, sizeof(float) * nk, cudaMemcpyDeviceToHost, h.stream),
+                                "D2H")) &&
+                 ok(cudaStreamSynchronize(h.stream), "imbart_hashgrid_query_host")))
+        rc = IMBART_ERR_CUDA;
+    cudaSetDevice(prev);
+    return rc;
+}
+
 int imbart_hashgrid_get_params(const imbart_hashgrid* g, float* params10, int* n, int* table_size) {
     if (!g) { set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_hashgrid_get_params"); return IMBART_ERR_INVALID_ARGUMENT; }
     int prev = 0;

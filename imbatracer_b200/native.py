@@ -149,6 +149,8 @@ _SIGNATURES = {
     "imbart_hashgrid_destroy": (None, [P]),
     "imbart_hashgrid_build": (I, [P, P, I, I, C.c_float, C.c_float, I, P]),
     "imbart_hashgrid_query": (I, [P, P, I, I, P, P, P, P]),
+    "imbart_hashgrid_build_host": (I, [P, P, I, I, C.c_float, C.c_float, I]),
+    "imbart_hashgrid_query_host": (I, [P, P, I, I, P, P, P]),
     "imbart_hashgrid_get_params": (I, [P, P, P, P]),
     "imbart_hashgrid_get_arrays": (I, [P, C.POINTER(P), C.POINTER(P)]),
     "imbart_hashgrid_build_noalloc": (I, [P, I, I, C.c_float, C.c_float, I, P, P, P, P]),

@@ -292,9 +292,22 @@ int imbart_hashgrid_build(imbart_hashgrid* grid, const float* positions, int str
  * out_ids (nq*k) receives the indices (build order) of the photons within the radius, at most
  * the k nearest, ordered by (squared distance, index) and padded with -1; out_counts (nq) the
  * count; out_d2 (nq*k, may be NULL) the squared distances. A bucket reached twice through the
- * 8 neighbour cells is scanned twice, as in the reference (rangesearch.h:94-104). */
+ * 8 neighbour cells is scanned twice, as in the reference (rangesearch.h:94-104). Grids built
+ * with 1 <= cell_factor < 2 are queried over every cell within the radius instead (each
+ * bucket once); cell_factor < 1 is refused. */
 int imbart_hashgrid_query(const imbart_hashgrid* grid, const float* queries, int nq, int k, int* out_ids,
                           int* out_counts, float* out_d2, void* stream);
+
+/* The same build and queries on HOST arrays, for HashGrid::build / HashGrid::query callers
+ * that hold their photons in host memory (as the reference's LightVertices does,
+ * light_vertices.h:70-100): the library copies positions in and results out through its own
+ * staging buffers and returns when done. Queries may run concurrently from several host
+ * threads (each thread has its own staging buffers and stream); a build must not overlap
+ * queries of the same grid. */
+int imbart_hashgrid_build_host(imbart_hashgrid* grid, const float* positions, int stride, int n, float radius,
+                               float cell_factor, int table_size);
+int imbart_hashgrid_query_host(const imbart_hashgrid* grid, const float* queries, int nq, int k, int* out_ids,
+                               int* out_counts, float* out_d2);
 
 /* Grid parameters after a build (synchronous): params10 = {lo xyz, hi xyz, radius, radius^2,
  * cell size, 1 / cell size}, photon count and table size. */

@@ -7,6 +7,7 @@ TEST INFRASTRUCTURE ONLY (the product never loads libref.so).
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
@@ -52,21 +53,74 @@ def build(verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     inc = ["-I", os.path.join(HERE, "shim"), "-I", os.path.join(REF, "src"), "-I", os.path.join(ROOT, "include"),
            "-include", os.path.join(HERE, "shim", "ref_prelude.h")]
-    objs = []
+    objs = compile_all(objdir, inc, [], verbose)
+    lib = os.path.join(OUT, "libref.so")
+    subprocess.run(["g++", "-shared", "-fopenmp", "-Wl,-Bsymbolic", "-o", lib, *objs, "-lm"], check=True)
+    build_gpu_grid(verbose)
+    build_imbart_linked(verbose)
+    return lib
+
+
+def compile_all(objdir, inc, defines, verbose):
+    """The reference sources, the harness and the oracle's traversal into objdir (in parallel)."""
+    cmds, objs = [], []
     for src in [os.path.join(REF, s) for s in REF_SOURCES] + OWN_SOURCES:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = ["g++", "-std=c++14", *FLAGS, *inc, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(["g++", "-std=c++14", *FLAGS, *defines, *inc, "-c", src, "-o", obj])
         objs.append(obj)
     for src in ORACLE_C:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        subprocess.run(["gcc", "-std=c11", *FLAGS, "-c", src, "-o", obj], check=True)
+        cmds.append(["gcc", "-std=c11", *FLAGS, "-c", src, "-o", obj])
         objs.append(obj)
-    lib = os.path.join(OUT, "libref.so")
-    subprocess.run(["g++", "-shared", "-fopenmp", "-Wl,-Bsymbolic", "-o", lib, *objs, "-lm"], check=True)
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(run, cmds))
+    return objs
+
+
+def build_imbart_linked(verbose: bool = False) -> str | None:
+    """The same harness with the reference's traversal entry points taken from libimbart (the
+    drop-in boundary) instead of the oracle, and its AnyDSL Platform::Cuda arrays in GPU memory
+    (shim_cuda ahead of shim): oracle/_ref/libref_imbart.so. Skipped when libimbart is not
+    built yet."""
+    imbart_lib = os.path.join(ROOT, "imbatracer_b200", "_lib")
+    if not os.path.exists(os.path.join(imbart_lib, "libimbart.so")):
+        return None
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    objdir = os.path.join(OUT, "obj_imbart")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(HERE, "shim_cuda"), "-I", os.path.join(HERE, "shim"), "-I", os.path.join(REF, "src"),
+           "-I", os.path.join(ROOT, "include"), "-include", os.path.join(HERE, "shim", "ref_prelude.h")]
+    objs = compile_all(objdir, inc, ["-DIMBART_REF_TRAVERSAL_FROM_IMBART"], verbose)
+    lib = os.path.join(OUT, "libref_imbart.so")
+    subprocess.run(["g++", "-shared", "-fopenmp", "-Wl,-Bsymbolic", "-o", lib, *objs, "-L", imbart_lib, "-limbart",
+                    "-Wl,-rpath,$ORIGIN/../../imbatracer_b200/_lib", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+                    "-Wl,-rpath," + os.path.join(cuda, "lib64"), "-lm"], check=True)
     return lib
+
+
+def build_gpu_grid(verbose: bool = False) -> str | None:
+    """The reference's LightVertices against libimbart's GPU photon grid: compiled with
+    include/shadow ahead of the reference's src/ (its rangesearch.h replaced by the adapter)
+    and linked to the in-tree libimbart; skipped when libimbart is not built yet."""
+    imbart_lib = os.path.join(ROOT, "imbatracer_b200", "_lib")
+    if not os.path.exists(os.path.join(imbart_lib, "libimbart.so")):
+        return None
+    inc = ["-I", os.path.join(ROOT, "include", "shadow"), "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(HERE, "shim"), "-I", os.path.join(REF, "src"),
+           "-include", os.path.join(HERE, "shim", "ref_prelude.h")]
+    out = os.path.join(OUT, "libref_gpu_grid.so")
+    cmd = ["g++", "-std=c++14", *FLAGS, *inc, "-shared", "-o", out, os.path.join(HERE, "ref_gpu_grid.cpp"),
+           "-L", imbart_lib, "-limbart", "-Wl,-rpath,$ORIGIN/../../imbatracer_b200/_lib"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return out
 
 
 if __name__ == "__main__":

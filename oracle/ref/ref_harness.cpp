@@ -50,14 +50,20 @@ void use_scene_masks(const imba::Scene& scene) {
     const auto& td = scene.traversal_data_gpu();
     g_masks_active = 0;
     g_n_masks = (int)td.masks.size();
-    for (size_t i = 0; i < td.masks.size(); ++i) {
-        const auto& m = td.masks.data()[i];
+    // A host copy: under the device-memory shim (libref_imbart.so) the arrays are on the GPU.
+    using Mask = typename std::decay<decltype(td.masks.data()[0])>::type;
+    anydsl::Array<Mask> host(anydsl::Platform::Host, anydsl::Device(0), td.masks.size());
+    anydsl::copy(td.masks, host, td.masks.size());
+    for (int64_t i = 0; i < host.size(); ++i) {
+        const auto& m = host.data()[i];
         if (m.width * m.height > 1) g_masks_active = 1;
     }
 }
 }
 
-// The reference's GPU entry points, served on the CPU by the oracle.
+#ifndef IMBART_REF_TRAVERSAL_FROM_IMBART
+// The reference's GPU entry points, served on the CPU by the oracle. (The build that links
+// libimbart instead, libref_imbart.so, leaves them to libimbart.)
 extern "C" void intersect_gpu_masked_instanced(int root, traversal_gpu::Node* nodes, traversal_gpu::InstanceNode* insts,
                                                traversal_gpu::Vec4* tris, traversal_gpu::Ray* rays,
                                                traversal_gpu::Hit* hits, int* indices, traversal_gpu::Vec2* texcoords,
@@ -88,6 +94,7 @@ extern "C" void occluded_cpu_masked_instanced(int, traversal_cpu::Node*, travers
                                               int count) {
     for (int i = 0; i < count; ++i) hits[i].tri_id = -1;
 }
+#endif
 
 using namespace imba;
 

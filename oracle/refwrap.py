@@ -12,11 +12,37 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libref.so")
 
-_lib = None
+# The same harness built a second time with the reference's traversal entry points taken from
+# libimbart instead of the oracle and its AnyDSL device arrays in GPU memory
+# (oracle/ref/build_ref.py: libref_imbart.so), for the drop-in test of the traversal boundary.
+LIB_IMBART = os.path.join(HERE, "_ref", "libref_imbart.so")
+
+_libs: dict = {}
+_active = LIB
 
 
 def available() -> bool:
     return os.path.exists(LIB)
+
+
+def imbart_linked_available() -> bool:
+    return os.path.exists(LIB_IMBART)
+
+
+class imbart_linked:
+    """Within this context, RefScene objects are created by libref_imbart.so: the reference's
+    RayQueue::traverse_gpu / traverse_occluded_gpu (ray_queue.h:269-343) call libimbart's
+    intersect_gpu_masked_instanced / occluded_gpu_masked_instanced on device buffers."""
+
+    def __enter__(self):
+        global _active
+        self.saved, _active = _active, LIB_IMBART
+        return self
+
+    def __exit__(self, *exc):
+        global _active
+        _active = self.saved
+        return False
 
 
 def reference_root() -> str | None:
@@ -52,9 +78,9 @@ def copy_reference_scenes(dst: str, sub: str = "cornell") -> str | None:
 
 
 def load() -> C.CDLL:
-    global _lib
+    _lib = _libs.get(_active)
     if _lib is None:
-        lib = C.CDLL(LIB)
+        lib = C.CDLL(_active)
         P, I, U64, F = C.c_void_p, C.c_int, C.c_uint64, C.c_float
         sig = {
             "imbart_ref_set_seed": (None, [U64, U64]),
@@ -96,7 +122,7 @@ def load() -> C.CDLL:
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
             fn.restype, fn.argtypes = res, args
-        _lib = lib
+        _lib = _libs[_active] = lib
     return _lib
 
 
@@ -139,6 +165,29 @@ def hashgrid_query(pos, radius, queries, k):
     ids = np.zeros((len(q), k), np.int32)
     cnt = np.zeros(len(q), np.int32)
     load().ref_hashgrid_query(_p(pos), len(pos), radius, _p(q), len(q), k, _p(ids), _p(cnt))
+    return ids, cnt
+
+
+GPU_GRID_LIB = os.path.join(HERE, "_ref", "libref_gpu_grid.so")
+
+
+def gpu_grid_available() -> bool:
+    return os.path.exists(GPU_GRID_LIB)
+
+
+def light_vertices_merge_gpu(pos, radius, queries, k):
+    """The reference's LightVertices with its HashGrid replaced, by include path, by the C++
+    adapter over libimbart's GPU grid (oracle/ref/ref_gpu_grid.cpp): cache indices and counts
+    of get_merge at each query."""
+    lib = C.CDLL(GPU_GRID_LIB)
+    fn = lib.refgpu_light_vertices_merge
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    pos = np.ascontiguousarray(pos, np.float32)
+    q = np.ascontiguousarray(queries, np.float32)
+    ids = np.zeros((len(q), k), np.int32)
+    cnt = np.zeros(len(q), np.int32)
+    assert fn(_p(pos), len(pos), radius, _p(q), len(q), k, _p(ids), _p(cnt)) == 0
     return ids, cnt
 
 
@@ -191,11 +240,12 @@ class RefScene:
 
     def __init__(self, desc, cpu_buffers: bool = False, accel_files=None):
         self.desc = desc
+        self.lib = load()
         names = None
         if accel_files is not None:
             enc = [os.fsencode(f) if f else None for f in accel_files]
             names = (C.c_char_p * len(enc))(*enc)
-        load().ref_set_next_scene_options(1 if cpu_buffers else 0, len(accel_files or []), names)
+        self.lib.ref_set_next_scene_options(1 if cpu_buffers else 0, len(accel_files or []), names)
         meshes = desc.meshes
         nv = np.array([len(m.vertices) for m in meshes], np.int32)
         nt = np.array([m.triangle_count for m in meshes], np.int32)
@@ -212,7 +262,7 @@ class RefScene:
             lights[i] = np.concatenate([p0, p1, p2, e])
         env = None if desc.env_intensity is None else np.array(desc.env_intensity, np.float32)
         self._keep = (nv, nt, verts, idx, nrm, tc, gn, im, mats, kinds, prm, lights, env)
-        self.handle = load().ref_scene_create(len(meshes), _p(nv), _p(nt), _p(verts), _p(idx), _p(nrm), _p(tc),
+        self.handle = self.lib.ref_scene_create(len(meshes), _p(nv), _p(nt), _p(verts), _p(idx), _p(nrm), _p(tc),
                                               _p(gn), len(im), _p(im), _p(mats), len(kinds), _p(kinds), _p(prm),
                                               len(desc.lights), _p(lights), _p(env))
         assert self.handle
@@ -226,7 +276,7 @@ class RefScene:
             px = (np.ascontiguousarray(np.concatenate([np.asarray(t, np.float32).reshape(-1) for t in tex]))
                   if tex else np.zeros(4, np.float32))
             self._keep2 = (kinds, lp, dims, px, mtex, mbump)
-            rc = load().ref_scene_extend(self.handle, len(delta), _p(kinds), _p(lp), len(tex), _p(dims), _p(px),
+            rc = self.lib.ref_scene_extend(self.handle, len(delta), _p(kinds), _p(lp), len(tex), _p(dims), _p(px),
                                          _p(mtex), _p(mbump))
             assert rc == 0, rc
 
@@ -236,7 +286,7 @@ class RefScene:
         root = C.c_int(0)
         pn, pi, pt = C.c_void_p(), C.c_void_p(), C.c_void_p()
         sizes = np.zeros(3, np.int64)
-        load().ref_scene_gpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt), _p(sizes))
+        self.lib.ref_scene_gpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt), _p(sizes))
 
         def grab(ptr, n, dtype):
             buf = (C.c_char * (int(n) * dtype.itemsize)).from_address(ptr)
@@ -255,8 +305,9 @@ class RefScene:
 
         from imbatracer_b200 import scenegen as G
         self = cls.__new__(cls)
+        self.lib = load()
         cam9 = np.zeros(9, np.float32)
-        self.handle = load().ref_scene_load(os.fsencode(path), _p(cam9))
+        self.handle = self.lib.ref_scene_load(os.fsencode(path), _p(cam9))
         if not self.handle:
             raise RuntimeError(f"the reference could not load {path}")
         cam = G.Camera(tuple(map(float, cam9[0:3])), tuple(map(float, cam9[3:6])), tuple(map(float, cam9[6:9])),
@@ -268,7 +319,7 @@ class RefScene:
         """The arrays of the reference's scene (ref_scene_io.cpp): meshes, instances,
         materials, lights, textures, masks."""
         cnt = np.zeros(10, np.int64)
-        lib = load()
+        lib = self.lib
         lib.ref_scene_counts(self.handle, _p(cnt))
         n_mesh, nv, nt, ni, nm, nl, ntex, texels, nmask, nbuf = (int(c) for c in cnt)
         out = {"mesh_counts": np.zeros((n_mesh, 2), np.int32), "vertices": np.zeros((nv, 3), np.float32),
@@ -303,7 +354,7 @@ class RefScene:
         root = C.c_int(0)
         pn, pi, pt = C.c_void_p(), C.c_void_p(), C.c_void_p()
         sizes = np.zeros(3, np.int64)
-        assert load().ref_scene_cpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt),
+        assert self.lib.ref_scene_cpu_layout(self.handle, C.byref(root), C.byref(pn), C.byref(pi), C.byref(pt),
                                            _p(sizes)) == 0
 
         def grab(ptr, n, dtype):
@@ -317,7 +368,7 @@ class RefScene:
         cam = cam or self.desc.camera
         img = np.zeros((h, w, 3), np.float32)
         p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
-        rc = load().ref_render_pt(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, seed_base,
+        rc = self.lib.ref_render_pt(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, seed_base,
                                   _p(img))
         assert rc == 0
         return img
@@ -329,7 +380,7 @@ class RefScene:
         cam = cam or self.desc.camera
         img = np.zeros((h, w, 3), np.float32)
         p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
-        rc = load().ref_render_pt_rr(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, rr_start,
+        rc = self.lib.ref_render_pt_rr(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len, rr_start,
                                      seed_base, _p(img))
         assert rc == 0
         return img
@@ -341,15 +392,15 @@ class RefScene:
         img = np.zeros((h, w, 3), np.float32)
         counts = np.zeros(2, np.int64)
         p3, d3, u3 = (np.ascontiguousarray(np.asarray(v, np.float32)) for v in (cam.pos, cam.dir, cam.up))
-        load().imbart_ref_set_threads(1, 1)
-        rc = load().ref_render_pt_threads(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len,
+        self.lib.imbart_ref_set_threads(1, 1)
+        rc = self.lib.ref_render_pt_threads(self.handle, w, h, _p(p3), _p(d3), _p(u3), cam.fov, spp, max_path_len,
                                           seed_base, tile, threads, _p(img), _p(counts))
         assert rc == 0
         return img, int(counts[0]), int(counts[1])
 
     def close(self):
         if self.handle:
-            load().ref_scene_destroy(self.handle)
+            self.lib.ref_scene_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

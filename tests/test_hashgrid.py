@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from oracle import refwrap as R
 
 
 def photon_cloud(n, seed, clustered=True):
@@ -159,7 +160,7 @@ def test_gpu_neighbour_sets_bit_exact(cuda, n, r, k, cf, table):
     assert (wcnt > 0).mean() > 0.3
     if cf < 2.0:
         # the grid's neighbour sets are the true radius sets (brute force, first queries)
-        grid, got, gcnt, _ = run_gpu(pos, q[:300], r, 256, cf, table)
+        grid, got, gcnt, _ = run_gpu(pos, q[:300], r, 64, cf, table)
         prm = grid.params()
         ref = brute_neighbours(pos, q[:300], r, 1 << 30)
         for i in range(300):
@@ -201,3 +202,29 @@ def test_gpu_empty_and_rebuild(cuda):
         g, ends, oid = O.hashgrid_build(pos[:n], 0.2)
         want, wcnt, _ = O.hashgrid_query(g, ends, oid, pos[:n], q, 8)
         assert np.array_equal(wcnt, cnt.cpu().numpy())
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (R.available() and R.gpu_grid_available()),
+                    reason="oracle/_ref (the reference built against include/shadow) not built")
+@pytest.mark.parametrize("n,r,k", [(100000, 0.15, 10), (20000, 0.5, 32)])
+def test_reference_light_vertices_merge_through_the_gpu_grid(cuda, n, r, k):
+    """The drop-in for the photon grid: the reference's LightVertices compiled with
+    include/shadow ahead of its sources, so that its HashGrid is the C++ adapter over
+    libimbart's GPU grid (include/imbart_hashgrid.hpp), finds exactly the photons the
+    reference's own HashGrid finds (compared as multisets; queries whose k-th distance ties
+    with a photon left out may differ)."""
+    pos = photon_cloud(n, 31)
+    q = queries_near(pos, 20000, 32, r)
+    got, gcnt = R.light_vertices_merge_gpu(pos, r, q, k)
+    want, wcnt = R.hashgrid_query(pos, r, q, k)
+    assert np.array_equal(gcnt, wcnt)
+    assert (wcnt > 0).mean() > 0.3
+    differ = 0
+    for i in range(len(q)):
+        a, b = np.sort(got[i, : gcnt[i]]), np.sort(want[i, : wcnt[i]])
+        if not np.array_equal(a, b):
+            d = ((pos[want[i, : wcnt[i]]] - q[i]) ** 2).sum(1)
+            assert wcnt[i] == k and np.sum(d == d.max()) >= 1, i
+            differ += 1
+    assert differ <= len(q) // 500

@@ -287,3 +287,28 @@ def test_every_kernel_variant_is_exact(cuda):
         for flags, (v, r, b) in saved.items():
             lib.imbart_set_trace_class(flags, v, r)
             lib.imbart_set_trace_tri_batch(flags, b)
+
+
+@pytest.mark.skipif(not __import__("oracle.refwrap", fromlist=["x"]).imbart_linked_available(),
+                    reason="oracle/_ref/libref_imbart.so not built (reference tree absent)")
+@pytest.mark.parametrize("name,w,h,spp,max_len", [("mixed", 96, 64, 4, 6), ("config1", 64, 64, 2, 5)])
+def test_reference_path_tracer_on_libimbart_traversal(cuda, name, w, h, spp, max_len):
+    """The traversal boundary end to end: the reference's own Scene, PathTracer, TileScheduler
+    and RayQueue — whose traverse_gpu / traverse_occluded_gpu copy the rays into device
+    arrays, call intersect_gpu_masked_instanced / occluded_gpu_masked_instanced and copy the
+    hits back (ray_queue.h:269-293, 319-343) — compiled against include/traversal_gpu.h and
+    linked to libimbart (oracle/_ref/libref_imbart.so, AnyDSL device arrays in GPU memory)
+    render the same image, bit for bit, as the same code over the oracle's traversal."""
+    from oracle import refwrap as R
+    from tests.test_pt import small_mixed_scene
+    d = small_mixed_scene() if name == "mixed" else H.scene_desc(name)
+    seed = 4242
+    oracle_img = R.RefScene(d).render_pt(w, h, spp, max_len, seed)
+    N.load().imbart_invalidate_scenes()       # device arrays of earlier scenes may be reused
+    with R.imbart_linked():
+        rs = R.RefScene(d)
+    img = rs.render_pt(w, h, spp, max_len, seed)
+    rs.close()
+    N.load().imbart_invalidate_scenes()
+    assert oracle_img.sum() > 0
+    assert np.array_equal(img.view(np.int32), oracle_img.view(np.int32))

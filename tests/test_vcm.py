@@ -163,7 +163,7 @@ def config3_scene():
     """The config-3 generator (400 displaced spheres, ~2M triangles) in both renderers."""
     from imbatracer_b200 import scenegen as G
     from imbatracer_b200.integrators import GpuScene
-    d = G.config3(width=320, height=180)
+    d = G.config3(width=320, height=176)
     return d, R.RefScene(d), GpuScene(d)
 
 
@@ -171,12 +171,14 @@ def config3_scene():
 @needs_ref
 @pytest.mark.parametrize("algo", ["vcm", "ppm"])
 def test_config3_scale_passes_match_reference(cuda, config3_scene, algo):
-    """The 2M-triangle config-3 scene with 200k light paths (max path length 8) and a 320x180
-    camera: the light-vertex cache equals the reference's as a set and the camera pass on the
-    reference's cache matches its image, over two iterations (the radius shrinks)."""
+    """The 2M-triangle config-3 scene with 200k light paths (max path length 8) and a 320x176
+    camera (sides multiples of 8: the reference's pixel-size probe overflows its queue
+    otherwise, integrator.cpp:18-27): the light-vertex cache equals the reference's as a set
+    and the camera pass on the reference's cache matches its image, over two iterations (the
+    radius shrinks)."""
     from imbatracer_b200.integrators import VcmIntegrator
     d, rs, gs = config3_scene
-    w, h, paths = 320, 180, 200_000
+    w, h, paths = 320, 176, 200_000
     rv = R.RefVcm(rs, algo, w, h, max_path_len=8, light_path_count=paths)
     vi = VcmIntegrator(gs, algo, w, h, spp=1, max_path_len=8, light_path_count=paths, num_connections=1,
                        num_knn=10, base_radius=rv.base_radius, light_tile_size=rv.tile_size * rv.tile_size)
