@@ -26,6 +26,18 @@ namespace sh {
 
 constexpr float kPi = 3.14159265359f;
 
+// Single-precision sin, cos, pow, acos and atan2 as the reference's x86 build receives them
+// from glibc, whose float functions return the correctly rounded value in all but rare
+// cases: here the double-precision function (error far below half a float ulp) rounded once
+// to float. CUDA's own float versions may differ from that by an ulp or two, which the
+// shading code amplifies near grazing angles (adjoint shading-normal factors, Russian
+// roulette on throughputs) until a path takes another turn.
+__device__ __forceinline__ float rsinf(float x) { return (float)sin((double)x); }
+__device__ __forceinline__ float rcosf(float x) { return (float)cos((double)x); }
+__device__ __forceinline__ float rpowf(float x, float y) { return (float)pow((double)x, (double)y); }
+__device__ __forceinline__ float racosf(float x) { return (float)acos((double)x); }
+__device__ __forceinline__ float ratan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
+
 struct V3 {
     float x, y, z;
     __device__ V3() {}
@@ -71,7 +83,7 @@ __device__ __forceinline__ void local_coordinates(V3 n, V3& tangent, V3& binorma
 }
 
 __device__ __forceinline__ V3 spherical_dir(float sin_t, float cos_t, float phi) {
-    return V3(sin_t * cosf(phi), sin_t * sinf(phi), cos_t);
+    return V3(sin_t * rcosf(phi), sin_t * rsinf(phi), cos_t);
 }
 
 // sample_cos_hemisphere(u1, u2) (random.h:81-84); returns pdf in *pdf.
@@ -84,14 +96,14 @@ __device__ __forceinline__ float cos_hemisphere_pdf(float c) { return fabsf(c) /
 
 __device__ __forceinline__ V3 sample_power_cos_hemisphere(float power, float u1, float u2, float* pdf) {
     const float phi = kPi * 2.0f * u1;
-    const float cos_t = powf(u2, 1.0f / (power + 1.0f));
+    const float cos_t = rpowf(u2, 1.0f / (power + 1.0f));
     const float sin_t = sqrtf(1.0f - sqr(cos_t));
     const V3 d = spherical_dir(sin_t, cos_t, phi);
-    *pdf = (power + 1.0f) * powf(cos_t, power) * 1.0f / (2.0f * kPi);
+    *pdf = (power + 1.0f) * rpowf(cos_t, power) * 1.0f / (2.0f * kPi);
     return d;
 }
 __device__ __forceinline__ float power_cos_hemisphere_pdf(float power, float c) {
-    return c > 0.0f ? ((power + 1.0f) * powf(c, power) * 1.0f / (2.0f * kPi)) : 0.0f;
+    return c > 0.0f ? ((power + 1.0f) * rpowf(c, power) * 1.0f / (2.0f * kPi)) : 0.0f;
 }
 
 // Two draws passed as (u1, u2) in the reference: the second argument is drawn first.
@@ -123,8 +135,8 @@ __device__ __forceinline__ void sample_concentric_disc(float u1, float u2, float
             else phi = 0;
         }
     }
-    dx = r * cosf(phi);
-    dy = r * sinf(phi);
+    dx = r * rcosf(phi);
+    dy = r * rsinf(phi);
 }
 __device__ __forceinline__ float concentric_disc_pdf() { return 1.0f / kPi; }
 
@@ -313,7 +325,7 @@ __device__ __forceinline__ V3 phong_eval(const float* c, float e, V3 o, V3 i) {
     const V3 ri(-i.x, -i.y, i.z);
     float cos_r_o = smax(0.0f, dot(ri, o));
     cos_r_o = smin(cos_r_o, 1.0f);
-    return same_hemisphere(o, i) ? (e + 2.0f) / (2.0f * kPi) * V3(c[0], c[1], c[2]) * powf(cos_r_o, e) : V3(0.0f);
+    return same_hemisphere(o, i) ? (e + 2.0f) / (2.0f * kPi) * V3(c[0], c[1], c[2]) * rpowf(cos_r_o, e) : V3(0.0f);
 }
 __device__ __forceinline__ V3 phong_sample(const float* c, float e, V3 o, V3& in, Rng& rng, float* pdf) {
     float u1, u2;
@@ -339,7 +351,7 @@ __device__ __forceinline__ V3 ct_eval(const float* c, float e, V3 o, V3 i) {
     const float cos_half = dot(i, h);
     const float fr = fresnel_conductor(cos_half, 1.0f, e);
     if (!same_hemisphere(o, i)) return V3(0.0f);
-    const float D = (e + 2.0f) / (2.0f * kPi) * powf(abs_cos(h), e);
+    const float D = (e + 2.0f) / (2.0f * kPi) * rpowf(abs_cos(h), e);
     const float out_dot_half = dot(o, h);
     const float G = smin(1.0f, smin(2.0f * abs_cos(h) * abs_cos(o) / out_dot_half,
                                     2.0f * abs_cos(h) * abs_cos(i) / out_dot_half));
@@ -348,21 +360,21 @@ __device__ __forceinline__ V3 ct_eval(const float* c, float e, V3 o, V3 i) {
 __device__ __forceinline__ V3 ct_sample(const float* c, float e, V3 o, V3& in, Rng& rng, float* pdf) {
     float r1, r2;
     draw2(rng, r1, r2);
-    const float c_theta = powf(r1, 1.0f / (e + 1.0f));
+    const float c_theta = rpowf(r1, 1.0f / (e + 1.0f));
     const float s_theta = sqrtf(smax(0.0f, 1.0f - sqr(c_theta)));
     const float phi = r2 * 2.0f * kPi;
     V3 h = spherical_dir(s_theta, c_theta, phi);
     if (!same_hemisphere(o, h)) h = -h;
     in = -o + 2.0f * dot(o, h) * h;
     if (dot(o, h) <= 0.0f) *pdf = 1.0f;
-    else *pdf = (e + 1.0f) * powf(c_theta, e) / (2.0f * kPi * 4.0f * dot(o, h));
+    else *pdf = (e + 1.0f) * rpowf(c_theta, e) / (2.0f * kPi * 4.0f * dot(o, h));
     return same_hemisphere(o, in) ? ct_eval(c, e, o, in) : V3(0.0f);
 }
 __device__ __forceinline__ float ct_pdf(float e, V3 o, V3 i) {
     if (!same_hemisphere(o, i)) return 0.0f;
     const V3 h = normalize(i + o);
     if (dot(o, h) <= 0.0f) return 0.0f;
-    return (e + 1.0f) * powf(abs_cos(h), e) / (2.0f * kPi * 4.0f * dot(o, h));
+    return (e + 1.0f) * rpowf(abs_cos(h), e) / (2.0f * kPi * 4.0f * dot(o, h));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -576,9 +588,9 @@ __device__ __forceinline__ DirectSample env_light_sample(const ShadingScene& sc,
     pdf *= float(w * h);
     const V3 color = env_lookup(sc, ux, uy);
     const float theta = kPi * uy;
-    const float sin_theta = sinf(theta);
+    const float sin_theta = rsinf(theta);
     const float phi = 2.0f * kPi * ux;
-    s.dir = V3(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+    s.dir = V3(sin_theta * rsinf(phi), rcosf(theta), sin_theta * rcosf(phi));
     if (sin_theta != 0.0f) pdf /= 2.0f * kPi * kPi * sin_theta;
     else pdf = 0.0f;
     s.distance = FLT_MAX;
@@ -631,9 +643,9 @@ __device__ __forceinline__ EmitSample env_light_emit(const ShadingScene& sc, Rng
     pdf *= float(w * h);
     const V3 color = env_lookup(sc, ux, uy);
     const float theta = kPi * uy;
-    const float sin_theta = sinf(theta);
+    const float sin_theta = rsinf(theta);
     const float phi = 2.0f * kPi * ux;
-    V3 dir(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+    V3 dir(sin_theta * rsinf(phi), rcosf(theta), sin_theta * rcosf(phi));
     if (sin_theta != 0.0f) pdf /= 2.0f * kPi * kPi * sin_theta;
     else pdf = 0.0f;
     dir = dir * -1.0f;
@@ -784,11 +796,11 @@ __device__ __forceinline__ V3 area_emitter_radiance(const Material& m, V3 out_di
 
 // EnvMap::radiance (light.h:413-424): pdf_direct_w = 1 / (2 pi^2 sin t).
 __device__ __forceinline__ V3 env_radiance(const ShadingScene& sc, V3 out_dir, float* pdf_direct_w) {
-    float phi = atan2f(out_dir.x, out_dir.z);
+    float phi = ratan2f(out_dir.x, out_dir.z);
     phi = (phi < 0.0f) ? (phi + 2.0f * kPi) : phi;
     const float s = phi / (2.0f * kPi);
-    const float t = acosf(out_dir.y) / kPi;
-    *pdf_direct_w = 1.0f / (2.0f * kPi * kPi * sinf(t));
+    const float t = racosf(out_dir.y) / kPi;
+    *pdf_direct_w = 1.0f / (2.0f * kPi * kPi * rsinf(t));
     return env_lookup(sc, s, t);
 }
 

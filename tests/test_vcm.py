@@ -24,7 +24,7 @@ LIGHT_PATHS = 3000
 MAX_LEN = 6
 IMAGE_TOL = 1e-4          # camera pass on the reference's cache (measured: <= 1.6e-6)
 LIGHT_IMAGE_TOL = 1e-3    # light tracing: a diverging light path moves whole splats (measured: <= 9e-6)
-MATCH_MIN = 0.98          # fraction of the reference's light vertices found in the GPU cache
+MATCH_MIN = 0.995         # fraction of the reference's light vertices found in the GPU cache
 
 
 def rel_rmse(a, b):
@@ -100,7 +100,7 @@ def test_light_pass_matches_reference(cuda, name, algo):
         assert len(ref_v) == 0 and len(got_v) == 0
     else:
         assert len(ref_v) > 100
-        assert abs(len(got_v) - len(ref_v)) <= max(2, 0.01 * len(ref_v))
+        assert abs(len(got_v) - len(ref_v)) <= max(2, 0.002 * len(ref_v))
         ok, j = match_vertices(ref_v, got_v)
         assert ok.mean() >= MATCH_MIN, ok.mean()
         r, g = ref_v[ok], got_v[j[ok]]
@@ -179,19 +179,27 @@ def test_config3_scale_passes_match_reference(cuda, config3_scene, algo):
     from imbatracer_b200.integrators import VcmIntegrator
     d, rs, gs = config3_scene
     w, h, paths = 320, 176, 200_000
-    rv = R.RefVcm(rs, algo, w, h, max_path_len=8, light_path_count=paths)
+    # Camera tiles as wide as the image (the reference's camera pass renders nothing when its
+    # tile is much larger than the image); light tiles of 320^2 paths hold each light's paths.
+    rv = R.RefVcm(rs, algo, w, h, max_path_len=8, light_path_count=paths, tile_size=max(w, h))
     vi = VcmIntegrator(gs, algo, w, h, spp=1, max_path_len=8, light_path_count=paths, num_connections=1,
                        num_knn=10, base_radius=rv.base_radius, light_tile_size=rv.tile_size * rv.tile_size)
     for it, (ls, cs) in enumerate([(5150, 6160), (7170, 8180)], start=1):
         assert rv.begin_iteration(it) == vi.begin_iteration(it)
-        rv.light_pass(ls, 3)
+        ref_light = rv.light_pass(ls, 3)
         ref_v = rv.light_vertices()
-        vi.light_pass(ls, 3)
+        light = vi.light_pass(ls, 3).cpu().numpy()
         got_v = vi.light_vertices()
         assert len(ref_v) > 100_000
         assert abs(len(got_v) - len(ref_v)) <= 0.002 * len(ref_v), (len(got_v), len(ref_v))
         ok, _ = match_vertices(ref_v, got_v)
-        assert ok.mean() >= 0.995, ok.mean()
+        # Long light paths (up to ~30 vertices here) let float-level differences accumulate:
+        # measured 99.5 % matched overall, 100 % of the first two bounces' vertices.
+        assert ok.mean() >= 0.99, ok.mean()
+        first = ref_v[:, 7].view(np.int32) <= 3
+        assert ok[first].mean() >= 0.999, ok[first].mean()
+        if algo == "vcm":
+            assert rel_rmse(light, ref_light) <= LIGHT_IMAGE_TOL, rel_rmse(light, ref_light)
         ref = rv.camera_pass(cs)
         vi.load_light_vertices(ref_v)
         img = vi.camera_pass(cs).cpu().numpy()
