@@ -514,7 +514,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------
 SERVE_MAX_PATH_LEN = 5        # 4 bounces, as the sphere-field renders
 SERVE_PATHS = int(os.environ.get("IMBART_SERVE_PATHS", 4 << 20))   # paths per merged (and single-request) wavefront
-SERVE_BUDGET = 16 << 30       # device pool of the batched server
+SERVE_BUDGET = 120 << 30      # device pool of the batched server (config 5's HBM budget)
 
 
 def serve_scenes():
@@ -791,7 +791,7 @@ def N_light_vertices(vi):
     return max(int(N.load().imbart_vcm_copy_light_vertices(vi.ctx, None, 0)), 0)
 
 
-def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0):
+def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0, saturation=True):
     """Config 4 (closed batch of 256 renders) and config 5 (Poisson arrivals) in both arms."""
     import torch
     from imbatracer_b200 import scenegen as G
@@ -826,6 +826,36 @@ def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0):
                 c5[mode] = serve_arm(mode, scenes, jobs5, open_loop=True, ray_buf=ray_buf, hit_buf=hit_buf)
             c5["p99_ratio"] = round(c5["plain"]["p99_ms"] / c5["batched"]["p99_ms"], 3)
             out["config5"].append(c5)
+        if saturation:
+            out["config5_saturation"] = config5_saturation(scenes, ray_buf, hit_buf)
+    return out
+
+
+def config5_saturation(scenes, ray_buf, hit_buf, p99_bound_ms=100.0, duration_s=1.5, start=200.0, step=1.5,
+                       top=4000.0):
+    """The highest Poisson arrival rate of the config-5 mix each arm sustains: rates grow by
+    `step` from `start` while the arm serves at least 95 % of the offered rate with p99
+    latency within the bound; the last rate that passed is the arm's sustained rate."""
+    from imbatracer_b200 import scenegen as G
+    out = {"p99_bound_ms": p99_bound_ms, "seconds_per_rate": duration_s,
+           "rule": "sustained = served >= 0.95 x offered and p99 <= bound"}
+    for mode in ("plain", "batched"):
+        rate, best, tried = start, None, []
+        while rate <= top:
+            jobs = G.config5_requests(seed=int(rate), rate=rate, duration_s=duration_s)
+            r = serve_arm(mode, scenes, jobs, open_loop=True, ray_buf=ray_buf, hit_buf=hit_buf)
+            ok = r["requests_per_s"] >= 0.95 * rate and r["p99_ms"] <= p99_bound_ms
+            tried.append({"rate": round(rate, 1), "served": r["requests_per_s"], "p99_ms": r["p99_ms"],
+                          "p50_ms": r["p50_ms"], "sustained": ok})
+            if not ok:
+                break
+            best = r | {"rate": round(rate, 1)}
+            rate *= step
+        out[mode] = {"sustained_rate_per_s": best["rate"] if best else None,
+                     "requests_per_s": best["requests_per_s"] if best else None,
+                     "p99_ms": best["p99_ms"] if best else None, "sweep": tried}
+    if out["plain"]["requests_per_s"] and out["batched"]["requests_per_s"]:
+        out["requests_per_s_ratio"] = round(out["batched"]["requests_per_s"] / out["plain"]["requests_per_s"], 3)
     return out
 
 

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -807,8 +808,244 @@ int build_scene_gpu(const imbart_mesh_desc* meshes, int n_meshes, const imbart_i
     return rc;
 }
 
+// ---------------------------------------------------------------------------------------
+// Refit: the vertices moved, the topology did not. Triangle records take their triangle's
+// new vertices; node boxes are recomputed bottom-up (bottom levels, then the instances'
+// world boxes, then the top level) and requantized with the build's conservative
+// arithmetic. Each leaf-only node starts a thread that refits it and climbs: the last child
+// of a parent to finish refits the parent (a counter per node).
+// ---------------------------------------------------------------------------------------
+__global__ void refit_tris_kernel(WideTri* tris, long long n, const float* __restrict__ verts,
+                                  const int4* __restrict__ tri_verts, int n_tri_ids, long long n_verts, int* error) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    WideTri t = tris[i];
+    if (t.id < 0 || t.id >= n_tri_ids) { atomicExch(error, 1); return; }
+    const int4 v = tri_verts[t.id];
+    if (v.x < 0 || v.y < 0 || v.z < 0 || v.x >= n_verts || v.y >= n_verts || v.z >= n_verts) {
+        atomicExch(error, 2);
+        return;
+    }
+    for (int k = 0; k < 3; ++k) {
+        t.v0[k] = verts[3 * (long long)v.x + k];
+        t.v1[k] = verts[3 * (long long)v.y + k];
+        t.v2[k] = verts[3 * (long long)v.z + k];
+    }
+    tris[i] = t;
+}
+
+// Parent of every internal child and the count of internal children of nodes [first, last).
+__global__ void refit_links_kernel(const WideNode* __restrict__ nodes, int first, int last, int* parent, int* pending) {
+    const int n = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= last) return;
+    const WideNode nd = nodes[n];
+    pending[n] = __popc(nd.imask);
+    int rank = 0;
+    for (int s = 0; s < 8; ++s)
+        if (nd.imask & (1u << s)) parent[nd.child_base + rank++] = n;
+}
+
+__device__ __forceinline__ Box6 empty_box() {
+    Box6 b;
+    for (int a = 0; a < 3; ++a) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; }
+    return b;
+}
+
+// Another thread's finished box, read past the L1 cache.
+__device__ __forceinline__ Box6 load_box_cg(const Box6* p) {
+    const float* f = reinterpret_cast<const float*>(p);
+    Box6 b;
+    for (int a = 0; a < 3; ++a) { b.lo[a] = __ldcg(f + a); b.hi[a] = __ldcg(f + 3 + a); }
+    return b;
+}
+
+// Requantizes node n from its children (leaf slots: their triangles or instances; internal
+// slots: the boxes their refits stored) and stores its own box.
+__device__ void refit_node(WideNode* nodes, int n, const WideTri* __restrict__ tris, const Box6* inst_boxes, bool top,
+                           Box6* exact) {
+    WideNode nd = nodes[n];
+    float blo[3][8], bhi[3][8];
+    bool valid[8];
+    float mag = 0.0f;
+    Box6 all = empty_box();
+    int rank = 0;
+    for (int s = 0; s < 8; ++s) {
+        Box6 b = empty_box();
+        if (nd.imask & (1u << s)) {
+            b = load_box_cg(exact + nd.child_base + rank++);
+            valid[s] = true;
+        } else {
+            const int count = nd.meta[s] >> 5, off = nd.meta[s] & 31;
+            valid[s] = count > 0;
+            for (int k = 0; k < count; ++k) {
+                const long long r = (long long)nd.prim_base + off + k;
+                if (top) {
+                    b = merge(b, inst_boxes[r]);
+                } else {
+                    const WideTri t = tris[r];
+                    for (int a = 0; a < 3; ++a) {
+                        b.lo[a] = fminf(b.lo[a], fminf(t.v0[a], fminf(t.v1[a], t.v2[a])));
+                        b.hi[a] = fmaxf(b.hi[a], fmaxf(t.v0[a], fmaxf(t.v1[a], t.v2[a])));
+                    }
+                }
+            }
+        }
+        for (int a = 0; a < 3; ++a) { blo[a][s] = valid[s] ? b.lo[a] : 0.0f; bhi[a][s] = valid[s] ? b.hi[a] : 0.0f; }
+        if (!valid[s]) continue;
+        all = merge(all, b);
+        for (int a = 0; a < 3; ++a) {
+            mag = fmaxf(mag, fmaxf(fabsf(b.lo[a]), fabsf(b.hi[a])));
+            mag = fmaxf(mag, b.hi[a] - b.lo[a]);
+        }
+    }
+    const float pad = mag * 9.5367431640625e-07f + 1e-30f;
+    float p[3];
+    uint8_t bexp[3];
+    quantize_axis_dev(blo[0], bhi[0], valid, pad, &p[0], &bexp[0], nd.qlo_x, nd.qhi_x);
+    quantize_axis_dev(blo[1], bhi[1], valid, pad, &p[1], &bexp[1], nd.qlo_y, nd.qhi_y);
+    quantize_axis_dev(blo[2], bhi[2], valid, pad, &p[2], &bexp[2], nd.qlo_z, nd.qhi_z);
+    nd.px = p[0]; nd.py = p[1]; nd.pz = p[2];
+    nd.ex = bexp[0]; nd.ey = bexp[1]; nd.ez = bexp[2];
+    nodes[n] = nd;
+    exact[n] = all;
+}
+
+__global__ void refit_up_kernel(WideNode* nodes, int first, int last, const int* __restrict__ parent, int* pending,
+                                const WideTri* __restrict__ tris, const Box6* inst_boxes, bool top, Box6* exact) {
+    int n = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= last || nodes[n].imask != 0) return;
+    for (;;) {
+        refit_node(nodes, n, tris, inst_boxes, top, exact);
+        __threadfence();
+        const int p = parent[n];
+        if (p < 0) return;
+        if (atomicSub(pending + p, 1) != 1) return;   // the parent's last child to finish goes on
+        __threadfence();
+        n = p;
+    }
+}
+
+// World box of each instance record: its mesh root's box through the object-to-world
+// transform (the inverse of the stored world-to-object rows, in double precision), corners
+// rounded outward and widened by 2^-20 of their magnitude.
+__global__ void refit_inst_boxes_kernel(const WideInst* __restrict__ insts, int n, const Box6* exact, Box6* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const WideInst w = insts[i];
+    const Box6 b = load_box_cg(exact + w.root);
+    double a[3][3], t[3];
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) a[r][c] = w.m[4 * r + c];
+        t[r] = w.m[4 * r + 3];
+    }
+    const double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+                       a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                       a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int c = 0; c < 8; ++c) {
+        const double x = (c & 1) ? b.hi[0] : b.lo[0], y = (c & 2) ? b.hi[1] : b.lo[1], z = (c & 4) ? b.hi[2] : b.lo[2];
+        const double px = x - t[0], py = y - t[1], pz = z - t[2];   // object = A world + t  =>  world = A^-1 (object - t)
+        for (int r = 0; r < 3; ++r) {
+            const double v = inv[r][0] * px + inv[r][1] * py + inv[r][2] * pz;
+            lo[r] = fmin(lo[r], v);
+            hi[r] = fmax(hi[r], v);
+        }
+    }
+    Box6 o;
+    double m = 0.0;
+    for (int r = 0; r < 3; ++r) m = fmax(m, fmax(fabs(lo[r]), fabs(hi[r])));
+    const double pad = m * 9.5367431640625e-07 + 1e-30;
+    for (int r = 0; r < 3; ++r) {
+        o.lo[r] = __double2float_rd(lo[r] - pad);
+        o.hi[r] = __double2float_ru(hi[r] + pad);
+    }
+    out[i] = o;
+}
+
+int refit_scene(imbart_scene* scene, const float* verts, long long n_verts, const int* tri_verts, int n_tri_ids,
+                cudaStream_t st) {
+    imbart_scene_info info;
+    const void *vn = nullptr, *vt = nullptr, *vi = nullptr;
+    if (imbart_scene_get_info(scene, &info) != 0 || imbart_scene_get_device_arrays(scene, &vn, &vt, &vi) != 0)
+        return imbart_last_error() ? imbart_last_error() : IMBART_ERR_INVALID_ARGUMENT;
+    if (!vn || info.wide_nodes <= 0 || info.wide_nodes > INT_MAX || info.top_nodes <= 0 ||
+        info.top_nodes > info.wide_nodes) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_scene_refit: scene without its own node array");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    WideNode* nodes = static_cast<WideNode*>(const_cast<void*>(vn));
+    WideTri* tris = static_cast<WideTri*>(const_cast<void*>(vt));
+    const WideInst* insts = static_cast<const WideInst*>(vi);
+    const int n_nodes = (int)info.wide_nodes, first_top = (int)(info.wide_nodes - info.top_nodes);
+    Box6 *exact = nullptr, *inst_boxes = nullptr;
+    int *parent = nullptr, *pending = nullptr, *error = nullptr;
+    bool good = dmalloc(&exact, n_nodes) && dmalloc(&inst_boxes, info.instances) && dmalloc(&parent, n_nodes) &&
+                dmalloc(&pending, n_nodes) && dmalloc(&error, 1) &&
+                ck(cudaMemsetAsync(parent, 0xff, sizeof(int) * (size_t)n_nodes, st), "cudaMemsetAsync") &&
+                ck(cudaMemsetAsync(error, 0, sizeof(int), st), "cudaMemsetAsync");
+    if (good) {
+        refit_tris_kernel<<<grid(info.triangles), kBlock, 0, st>>>(tris, info.triangles, verts,
+                                                                    reinterpret_cast<const int4*>(tri_verts), n_tri_ids,
+                                                                    n_verts, error);
+        refit_links_kernel<<<grid(n_nodes), kBlock, 0, st>>>(nodes, 0, n_nodes, parent, pending);
+        if (first_top > 0)
+            refit_up_kernel<<<grid(first_top), kBlock, 0, st>>>(nodes, 0, first_top, parent, pending, tris, nullptr,
+                                                               false, exact);
+        refit_inst_boxes_kernel<<<grid(info.instances), kBlock, 0, st>>>(insts, (int)info.instances, exact,
+                                                                        inst_boxes);
+        refit_up_kernel<<<grid(info.top_nodes), kBlock, 0, st>>>(nodes, first_top, n_nodes, parent, pending, tris,
+                                                                inst_boxes, true, exact);
+        note_launches(first_top > 0 ? 5 : 4);
+        int h_error = 0;
+        good = ck(cudaGetLastError(), "refit launch") &&
+               ck(cudaMemcpyAsync(&h_error, error, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync") &&
+               ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (good && h_error) {
+            set_error(IMBART_ERR_INVALID_ARGUMENT, h_error == 1 ? "imbart_scene_refit: a triangle id beyond n_tri_ids"
+                                                                : "imbart_scene_refit: a vertex index out of range");
+            good = false;
+        }
+    }
+    cudaFree(exact); cudaFree(inst_boxes); cudaFree(parent); cudaFree(pending); cudaFree(error);
+    return good ? 0 : (imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA);
+}
+
 }  // namespace
 }  // namespace imbart
+
+extern "C" int imbart_scene_refit(imbart_scene* scene, const float* vertices, long long n_vertices,
+                                  const int* tri_vertices, int n_tri_ids, void* stream) {
+    if (!scene || !vertices || !tri_vertices || n_vertices <= 0 || n_tri_ids <= 0) {
+        imbart::set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_scene_refit: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    imbart_scene_info info;
+    if (imbart_scene_get_info(scene, &info) != 0) return imbart_last_error();
+    int prev = 0;
+    cudaGetDevice(&prev);
+    int dev = prev;
+    // The scene's device: the one its arrays live on (pointer attributes).
+    const void* vn = nullptr;
+    const void* vt = nullptr;
+    const void* vi = nullptr;
+    imbart_scene_get_device_arrays(scene, &vn, &vt, &vi);
+    cudaPointerAttributes attr;
+    if (vn && cudaPointerGetAttributes(&attr, vn) == cudaSuccess && attr.type == cudaMemoryTypeDevice) dev = attr.device;
+    cudaSetDevice(dev);
+    const int rc = imbart::refit_scene(scene, vertices, n_vertices, tri_vertices, n_tri_ids, (cudaStream_t)stream);
+    cudaSetDevice(prev);
+    return rc;
+}
 
 extern "C" imbart_scene* imbart_scene_build_gpu(const imbart_mesh_desc* meshes, int n_meshes,
                                                 const imbart_instance_desc* instances, int n_instances, int device,

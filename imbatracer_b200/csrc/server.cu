@@ -90,10 +90,12 @@ public:
         size_ = size;
         used_ = 0;
     }
-    // Returns the offset of `bytes` aligned to `align`, or SIZE_MAX.
-    size_t alloc(size_t bytes, size_t align) {
+    // Returns the offset of `bytes` aligned to `align` and ending at or below `limit`, or
+    // SIZE_MAX.
+    size_t alloc(size_t bytes, size_t align, size_t limit = SIZE_MAX) {
         for (auto it = free_.begin(); it != free_.end(); ++it) {
             const size_t start = align_up(it->first, align), end = it->first + it->second;
+            if (start + bytes > limit) break;
             if (start + bytes > end) continue;
             const size_t off = it->first;
             free_.erase(it);
@@ -428,10 +430,16 @@ bool evict_one_locked(imbart_server* S) {
     return true;
 }
 
-// Allocates pool bytes, evicting unused scenes as needed. SIZE_MAX when it cannot.
-size_t pool_alloc_locked(imbart_server* S, size_t bytes, size_t align) {
+// Scene blocks must end below this pool offset: the traversal kernels keep node, triangle
+// and instance indices in 30 bits (the stack's entry type takes the top two), and the
+// 48-byte triangles reach 2^30 records first.
+constexpr size_t kSceneIndexLimit = (size_t(1) << 30) * sizeof(WideTri);
+
+// Allocates pool bytes below `limit`, evicting unused scenes as needed. SIZE_MAX when it
+// cannot.
+size_t pool_alloc_locked(imbart_server* S, size_t bytes, size_t align, size_t limit = SIZE_MAX) {
     for (;;) {
-        const size_t off = S->alloc.alloc(bytes, align);
+        const size_t off = S->alloc.alloc(bytes, align, limit);
         if (off != SIZE_MAX) return off;
         if (!evict_one_locked(S)) return SIZE_MAX;
     }
@@ -442,7 +450,7 @@ size_t pool_alloc_locked(imbart_server* S, size_t bytes, size_t align) {
 int make_resident_locked(imbart_server* S, SceneRec& s) {
     if (s.resident) return 0;
     if (S->free_scene_slots.empty()) return evict_one_locked(S) ? make_resident_locked(S, s) : 1;
-    const size_t block = pool_alloc_locked(S, s.bytes, kBlockAlign);
+    const size_t block = pool_alloc_locked(S, s.bytes, kBlockAlign, kSceneIndexLimit);
     if (block == SIZE_MAX) return 1;
     uint8_t* b = S->pool + block;
     cudaStream_t st = S->stream;
@@ -1323,8 +1331,8 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
     }
     layout_scene(*s);
     std::lock_guard<std::mutex> lk(S->mu);
-    if (S->mode == IMBART_SERVE_BATCHED && s->bytes > S->pool_bytes) {
-        set_error(IMBART_ERR_LIMIT, "imbart_server_add_scene: scene larger than the pool");
+    if (S->mode == IMBART_SERVE_BATCHED && s->bytes > std::min(S->pool_bytes, kSceneIndexLimit)) {
+        set_error(IMBART_ERR_LIMIT, "imbart_server_add_scene: scene larger than the pool (or its scene region)");
         return -IMBART_ERR_LIMIT;
     }
     if (S->scenes.size() >= kMaxScenes) {

@@ -179,6 +179,7 @@ _SIGNATURES = {
     "imbart_get_trace_tri_batch": (I, [I]),
     "imbart_shading_set_env_map": (I, [P, I, C.c_float]),
     "imbart_scene_build_gpu": (P, [C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, I, P, C.POINTER(C.c_float)]),
+    "imbart_scene_refit": (I, [P, P, C.c_longlong, P, I, P]),
     "imbart_load_accel_node2": (I, [C.c_char_p, I, P, I, P, P, I, P]),
     "imbart_load_accel_node4": (I, [C.c_char_p, I, P, I, P, P, I, P]),
     "imbart_store_accel_node2": (I, [C.c_char_p, P, I, I, P, I, I, I]),

@@ -308,6 +308,25 @@ class DeviceScene:
             rc = lib.imbart_trace_uv(self.handle, N.ptr(rays), N.ptr(hits), N.ptr(v_out), n, flags, st)
         N.check(rc, "imbart_trace")
 
+    def refit(self, meshes: list[Mesh], stream=None) -> None:
+        """imbart_scene_refit with the meshes' new vertex positions (same topology, triangles
+        numbered mesh after mesh as the scene was built)."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        verts = np.ascontiguousarray(np.concatenate([m.vertices for m in meshes]).astype(np.float32))
+        tv, off = [], 0
+        for m in meshes:
+            t = np.zeros((m.triangle_count, 4), np.int32)
+            t[:, :3] = m.indices[:, :3] + off
+            tv.append(t)
+            off += len(m.vertices)
+        tv = np.concatenate(tv)
+        d_v = torch.from_numpy(verts).to(dev)
+        d_t = torch.from_numpy(tv).to(dev)
+        st = None if stream is None else stream.cuda_stream
+        N.check(N.load().imbart_scene_refit(self.handle, N.ptr(d_v), len(verts), N.ptr(d_t), len(tv), st),
+                "imbart_scene_refit")
+
     def trace_host(self, rays: np.ndarray, hits: np.ndarray, any_hit: bool = False, stream=None):
         lib = N.load()
         st = None if stream is None else stream.cuda_stream

@@ -760,6 +760,19 @@ imbart_scene* imbart_scene_build_gpu(const imbart_mesh_desc* meshes, int n_meshe
                                      const imbart_instance_desc* instances, int n_instances, int device,
                                      void* stream, float* build_ms);
 
+/* Refit (no counterpart in the reference, which rebuilds on the CPU): after a scene's mesh
+ * vertices moved with the topology unchanged, rewrites its triangle records from the new
+ * positions and recomputes every node box bottom-up — the meshes' BVHs, the instances' world
+ * boxes, the top level — with the build's conservative quantization, so traversal finds the
+ * closest hits of the moved triangles exactly (the tree may fit them less tightly than a
+ * rebuild). vertices: DEVICE xyz floats (object space) of every mesh's vertices, n_vertices
+ * of them; tri_vertices: DEVICE {v0, v1, v2, unused} per global triangle id, indexing
+ * `vertices` (the layout of the shading data's triangles). For scenes with their own arrays
+ * (imbart_scene_from_node2/4, imbart_scene_build_gpu), not views of a server's pool.
+ * Synchronizes `stream`. */
+int imbart_scene_refit(imbart_scene* scene, const float* vertices, long long n_vertices, const int* tri_vertices,
+                       int n_tri_ids, void* stream);
+
 /* ------------------------------------------------------------------------------------ */
 /* Acceleration-structure cache files (.bvh), as the reference reads and writes them      */
 /* (load_accel_gpu / load_accel_cpu / store_accel_gpu / store_accel_cpu,                   */

@@ -11,6 +11,7 @@ import pytest
 
 from imbatracer_b200 import native as N
 from imbatracer_b200 import scene as S
+from imbatracer_b200 import scenegen as G
 from oracle import oracle as O
 from tests import helpers as H
 from tests.test_pt import small_mixed_scene
@@ -104,3 +105,59 @@ def test_gpu_build_rejects_bad_input(cuda):
     with pytest.raises(N.ImbartError):
         S.DeviceScene.build_gpu([m2], [Instance(1)])
     N.load().imbart_clear_error()
+
+
+def _moved(desc, seed):
+    """The scene's meshes with every vertex moved: scaled about its mesh's centre by 1.2 and
+    jittered (the triangles keep their vertex indices)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in desc.meshes:
+        c = m.vertices.mean(0)
+        v = (c + (m.vertices - c) * 1.2 + rng.normal(scale=0.01, size=m.vertices.shape)).astype(np.float32)
+        out.append(S.Mesh(v, m.indices, m.normals, m.texcoords, m.geom_normals))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,gpu_built", [("mixed", False), ("mixed", True), ("config1", False),
+                                            ("config2", True)])
+def test_refit_traces_the_moved_triangles_exactly(cuda, name, gpu_built):
+    """imbart_scene_refit after every vertex moved (scaled by 1.2 about each mesh's centre and
+    jittered): closest hits equal brute force over the moved triangles bit for bit and
+    occlusion equals it, on trees built by the host (SBVH) and on the GPU."""
+    from tests.test_pt import small_mixed_scene
+    desc = small_mixed_scene() if name == "mixed" else H.scene_desc(name)
+    td = S.build_traversal_data(desc.meshes, desc.instances)
+    ds = S.DeviceScene.build_gpu(desc.meshes, desc.instances) if gpu_built else S.DeviceScene(td)
+    moved = _moved(desc, 7)
+    ds.refit(moved)
+    lo, hi = G.scene_box(desc)
+    ext = hi - lo
+    rays = G.random_rays(np.random.default_rng(8), 30000, lo - 0.2 * ext, hi + 0.2 * ext)
+    ref = O.trace_brute(moved, desc.instances, td.tri_layout, rays)
+    assert (ref["tri_id"] >= 0).sum() > 2000
+    from tests.test_traversal_gpu import run_gpu
+    hits, _, _ = run_gpu(ds, rays)
+    assert H.hits_equal(ref, hits).all(), int((~H.hits_equal(ref, hits)).sum())
+    occ, _, _ = run_gpu(ds, rays, any_hit=True)
+    assert np.array_equal(occ["tri_id"] >= 0, ref["tri_id"] >= 0)
+    # Refitting back to the original positions restores the original hits.
+    ds.refit(desc.meshes)
+    hits, _, _ = run_gpu(ds, rays)
+    assert H.hits_equal(O.trace_node2(td, rays), hits).all()
+    ds.close()
+
+
+@pytest.mark.gpu
+def test_refit_rejects_bad_input(cuda):
+    import torch
+    desc = H.scene_desc("tiny")
+    ds = S.DeviceScene(H.traversal_data("tiny"))
+    lib = N.load()
+    v = torch.zeros((10, 3), dtype=torch.float32, device="cuda")
+    t = torch.full((3, 4), 99, dtype=torch.int32, device="cuda")       # vertex 99 of 10
+    assert lib.imbart_scene_refit(ds.handle, N.ptr(v), 10, N.ptr(t), 3, None) != 0
+    assert lib.imbart_scene_refit(ds.handle, N.ptr(v), 10, N.ptr(t), 0, None) != 0
+    lib.imbart_clear_error()
+    ds.close()
