@@ -517,11 +517,45 @@ SERVE_PATHS = int(os.environ.get("IMBART_SERVE_PATHS", 4 << 20))   # paths per m
 SERVE_BUDGET = 120 << 30      # device pool of the batched server (config 5's HBM budget)
 
 
+HOST_BUILD_S: list = []      # host SBVH build + layout time of each serving scene
+
+
 def serve_scenes():
     from imbatracer_b200 import scene as S
     from imbatracer_b200 import scenegen as G
     descs = G.config4_scenes()
-    return [(d, S.build_traversal_data(d.meshes, d.instances)) for d in descs]
+    out = []
+    HOST_BUILD_S.clear()
+    for d in descs:
+        t0 = time.perf_counter()
+        out.append((d, S.build_traversal_data(d.meshes, d.instances)))
+        HOST_BUILD_S.append(time.perf_counter() - t0)
+    return out
+
+
+def admission_times(scenes):
+    """Scene admission: registering each serving scene with its traversal arrays built on the
+    GPU (imbart_server_add_scene_gpu_build) and serving a first 64x64 frame on it (upload into
+    the pool), beside the host SBVH build that the other registration path needs."""
+    from imbatracer_b200.serving import Server
+    srv = Server(mode="batched", hbm_budget=SERVE_BUDGET, max_paths=SERVE_PATHS)
+    gpu_ms, first_ms = [], []
+    for d, _ in scenes:
+        sid = srv.add_scene(d, gpu_build=True)
+        gpu_ms.append(srv.last_build_ms)
+        t0 = time.perf_counter()
+        t, _ = srv.submit_render(sid, d.camera, 64, 64, 1, SERVE_MAX_PATH_LEN, 1)
+        srv.wait(t)
+        first_ms.append((time.perf_counter() - t0) * 1e3)
+    srv.close()
+    tris = [d.instanced_triangles for d, _ in scenes]
+    out = {"scene_triangles": tris, "gpu_build_ms": [round(v, 1) for v in gpu_ms],
+           "first_frame_ms": [round(v, 1) for v in first_ms],
+           "gpu_build_total_ms": round(sum(gpu_ms), 1)}
+    if len(HOST_BUILD_S) == len(scenes):
+        out["host_build_s"] = [round(v, 2) for v in HOST_BUILD_S]
+        out["host_build_total_s"] = round(sum(HOST_BUILD_S), 2)
+    return out
 
 
 def _percentile(v, q):
@@ -809,6 +843,7 @@ def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0, satura
     c4["requests_per_s_ratio"] = round(c4["batched"]["requests_per_s"] / c4["plain"]["requests_per_s"], 3)
     c4["p99_ratio"] = round(c4["plain"]["p99_ms"] / c4["batched"]["p99_ms"], 3)
     out["config4"] = c4
+    out["admission"] = admission_times(scenes)
     if config5_rates:
         n_rays = 4 << 20
         ray_buf = torch.empty((n_rays, 8), dtype=torch.float32).pin_memory().numpy()

@@ -1258,14 +1258,29 @@ void imbart_server_destroy(imbart_server* S) {
     cudaSetDevice(prev);
 }
 
+}  // extern "C"
+
+namespace imbart {
+namespace {
+bool valid_shading_source(const imbart_scene_source* src) {
+    return src && src->vertices && src->n_vertices > 0 && src->normals && src->texcoords && src->mesh_tris &&
+           src->geom_normals && src->n_mesh_tris > 0 && src->inst_inv && src->n_inst_inv > 0 && src->mat_kind &&
+           src->mat_params && src->n_mats > 0 && src->n_tri_lights >= 0 &&
+           !(src->n_tri_lights > 0 && !src->tri_lights) &&
+           !(src->n_tri_lights == 0 && !src->env_color && src->env_map <= 0) &&
+           valid_light_kinds(src->light_kinds, src->n_tri_lights) && src->n_textures >= 0 &&
+           !(src->n_textures > 0 && (!src->tex_dims || !src->tex_pixels));
+}
+
+int register_scene(imbart_server* S, const imbart_scene_source* src, std::unique_ptr<SceneRec> s);
+}  // namespace
+}  // namespace imbart
+
+extern "C" {
+
 int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
-    if (!S || !src || !src->nodes || src->n_nodes <= 0 || !src->instances || src->n_instances <= 0 || !src->tris ||
-        src->n_tri_vec4 <= 0 || !src->vertices || src->n_vertices <= 0 || !src->normals || !src->texcoords ||
-        !src->mesh_tris || !src->geom_normals || src->n_mesh_tris <= 0 || !src->inst_inv || src->n_inst_inv <= 0 ||
-        !src->mat_kind || !src->mat_params || src->n_mats <= 0 || src->n_tri_lights < 0 ||
-        (src->n_tri_lights > 0 && !src->tri_lights) || (src->n_tri_lights == 0 && !src->env_color && src->env_map <= 0) ||
-        !valid_light_kinds(src->light_kinds, src->n_tri_lights) || src->n_textures < 0 ||
-        (src->n_textures > 0 && (!src->tex_dims || !src->tex_pixels))) {
+    if (!S || !valid_shading_source(src) || !src->nodes || src->n_nodes <= 0 || !src->instances ||
+        src->n_instances <= 0 || !src->tris || src->n_tri_vec4 <= 0) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene: invalid argument");
         return -IMBART_ERR_INVALID_ARGUMENT;
     }
@@ -1276,6 +1291,59 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         set_error(IMBART_ERR_BAD_SCENE, "imbart_server_add_scene: " + err);
         return -IMBART_ERR_BAD_SCENE;
     }
+    return register_scene(S, src, std::move(s));
+}
+
+int imbart_server_add_scene_gpu_build(imbart_server* S, const imbart_scene_source* src, const imbart_mesh_desc* meshes,
+                                      int n_meshes, const imbart_instance_desc* instances, int n_instances,
+                                      float* build_ms) {
+    if (!S || !valid_shading_source(src) || !meshes || n_meshes <= 0 || !instances || n_instances <= 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_server_add_scene_gpu_build: invalid argument");
+        return -IMBART_ERR_INVALID_ARGUMENT;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(S->device);
+    cudaStream_t st = nullptr;
+    auto s = std::make_unique<SceneRec>();
+    imbart_scene* g = nullptr;
+    bool good = cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate") &&
+                (g = imbart_scene_build_gpu(meshes, n_meshes, instances, n_instances, S->device, st, nullptr)) != nullptr;
+    if (good) {
+        // The built arrays come to the host like a converted scene's: the pool uploads and
+        // evicts scenes from their host copies.
+        imbart_scene_info info;
+        const void *vn = nullptr, *vt = nullptr, *vi = nullptr;
+        good = imbart_scene_get_info(g, &info) == 0 && imbart_scene_get_device_arrays(g, &vn, &vt, &vi) == 0;
+        if (good) {
+            s->wide.nodes.resize((size_t)info.wide_nodes);
+            s->wide.tris.resize((size_t)info.triangles);
+            s->wide.insts.resize((size_t)info.instances);
+            s->wide.root = info.root;
+            s->wide.top_nodes = (int)info.top_nodes;
+            good = cuda_check(cudaMemcpyAsync(s->wide.nodes.data(), vn, sizeof(WideNode) * s->wide.nodes.size(),
+                                              cudaMemcpyDeviceToHost, st), "D2H") &&
+                   cuda_check(cudaMemcpyAsync(s->wide.tris.data(), vt, sizeof(WideTri) * s->wide.tris.size(),
+                                              cudaMemcpyDeviceToHost, st), "D2H") &&
+                   cuda_check(cudaMemcpyAsync(s->wide.insts.data(), vi, sizeof(WideInst) * s->wide.insts.size(),
+                                              cudaMemcpyDeviceToHost, st), "D2H") &&
+                   cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        }
+    }
+    if (g) imbart_scene_destroy(g);
+    if (st) cudaStreamDestroy(st);
+    cudaSetDevice(prev);
+    if (!good) return -(imbart_last_error() ? imbart_last_error() : IMBART_ERR_CUDA);
+    if (build_ms) *build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return register_scene(S, src, std::move(s));
+}
+
+}  // extern "C"
+
+namespace imbart {
+namespace {
+int register_scene(imbart_server* S, const imbart_scene_source* src, std::unique_ptr<SceneRec> s) {
     auto vec = [](const auto* p, size_t n) { return std::vector<std::remove_const_t<std::remove_pointer_t<decltype(p)>>>(p, p + n); };
     s->vertices = vec(src->vertices, 3 * (size_t)src->n_vertices);
     s->normals = vec(src->normals, 3 * (size_t)src->n_vertices);
@@ -1342,6 +1410,10 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
     S->scenes.push_back(std::move(s));
     return (int)S->scenes.size() - 1;
 }
+}  // namespace
+}  // namespace imbart
+
+extern "C" {
 
 static long long submit(imbart_server* S, std::unique_ptr<Request> r) {
     std::lock_guard<std::mutex> lk(S->mu);

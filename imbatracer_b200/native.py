@@ -202,6 +202,7 @@ _SIGNATURES = {
     "imbart_server_create": (P, [I, I, C.c_longlong, C.c_longlong]),
     "imbart_server_destroy": (None, [P]),
     "imbart_server_add_scene": (I, [P, C.POINTER(SceneSource)]),
+    "imbart_server_add_scene_gpu_build": (I, [P, P, C.POINTER(MeshDesc), I, C.POINTER(InstanceDesc), I, C.POINTER(C.c_float)]),
     "imbart_server_submit_render": (C.c_longlong, [P, C.POINTER(RenderRequest)]),
     "imbart_server_submit_rays": (C.c_longlong, [P, I, P, P, I, I]),
     "imbart_server_submit_vcm": (C.c_longlong, [P, C.POINTER(VcmRequest)]),

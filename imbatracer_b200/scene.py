@@ -241,6 +241,28 @@ def build_traversal_data(meshes: list[Mesh], instances: list[Instance], leaf_siz
                          np.ascontiguousarray(mask_buffer, dtype=np.uint8), layout, tri_layout)
 
 
+def build_descs(meshes: list[Mesh], instances: list[Instance]):
+    """Mesh and instance descriptors of imbart_scene_build_gpu (triangles numbered mesh after
+    mesh); returns (meshes, instances, arrays to keep alive during the call)."""
+    md = (N.MeshDesc * len(meshes))()
+    keep, off = [], 0
+    for k, m in enumerate(meshes):
+        v = np.ascontiguousarray(m.vertices, np.float32)
+        ix = np.ascontiguousarray(m.indices, np.int32)
+        keep += [v, ix]
+        md[k].vertices, md[k].n_vertices = N.ptr(v), len(v)
+        md[k].indices, md[k].n_tris = N.ptr(ix), len(ix)
+        md[k].tri_offset = off
+        off += m.triangle_count
+    idesc = (N.InstanceDesc * len(instances))()
+    for i, inst in enumerate(instances):
+        idesc[i].obj_to_world[:] = [float(x) for x in inst.mat[:3].reshape(-1)]
+        idesc[i].world_to_obj[:] = [float(x) for x in inst.inv_mat.reshape(-1)]
+        idesc[i].mesh = inst.mesh_id
+        idesc[i].id = i
+    return md, idesc, keep
+
+
 class DeviceScene:
     """A prepared scene resident on one GPU (imbart_scene)."""
 
@@ -250,22 +272,7 @@ class DeviceScene:
         triangle ids are numbered mesh after mesh as build_traversal_data numbers them.
         `build_ms` holds the build's wall time."""
         lib = N.load()
-        md = (N.MeshDesc * len(meshes))()
-        keep, off = [], 0
-        for k, m in enumerate(meshes):
-            v = np.ascontiguousarray(m.vertices, np.float32)
-            ix = np.ascontiguousarray(m.indices, np.int32)
-            keep += [v, ix]
-            md[k].vertices, md[k].n_vertices = N.ptr(v), len(v)
-            md[k].indices, md[k].n_tris = N.ptr(ix), len(ix)
-            md[k].tri_offset = off
-            off += m.triangle_count
-        idesc = (N.InstanceDesc * len(instances))()
-        for i, inst in enumerate(instances):
-            idesc[i].obj_to_world[:] = [float(x) for x in inst.mat[:3].reshape(-1)]
-            idesc[i].world_to_obj[:] = [float(x) for x in inst.inv_mat.reshape(-1)]
-            idesc[i].mesh = inst.mesh_id
-            idesc[i].id = i
+        md, idesc, keep = build_descs(meshes, instances)
         ms = C.c_float(0.0)
         st = None if stream is None else stream.cuda_stream
         h = lib.imbart_scene_build_gpu(md, len(meshes), idesc, len(instances), device, st, C.byref(ms))

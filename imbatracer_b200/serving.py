@@ -35,18 +35,23 @@ class Server:
         self._scenes = []          # host arrays of registered scenes (the server copies them; kept for reuse)
         self._lock = threading.Lock()
 
-    def add_scene(self, desc: G.SceneDesc, td: S.TraversalData | None = None) -> int:
+    def add_scene(self, desc: G.SceneDesc, td: S.TraversalData | None = None, gpu_build: bool = False) -> int:
+        """Registers a scene: its traversal arrays from `td` (built on the host when None) or,
+        with gpu_build, built on the server's GPU (imbart_server_add_scene_gpu_build; the
+        build's wall time is then in last_build_ms)."""
         masks = getattr(desc, "masks", None)
         if masks is not None and (np.asarray(masks["width"]) * np.asarray(masks["height"]) > 1).any():
             raise N.ImbartError("imbart_server_add_scene: opacity masks are not supported by the server")
-        td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances,
-                                                              accel_files=getattr(desc, "accel_files", None))
+        if not gpu_build:
+            td = td if td is not None else S.build_traversal_data(desc.meshes, desc.instances,
+                                                                  accel_files=getattr(desc, "accel_files", None))
         sd = ShadingData(desc)
         src = N.SceneSource()
-        src.root = td.root
-        src.nodes, src.n_nodes = N.ptr(td.nodes), len(td.nodes)
-        src.instances, src.n_instances = N.ptr(td.instances), len(td.instances)
-        src.tris, src.n_tri_vec4 = N.ptr(td.tris), len(td.tris)
+        if not gpu_build:
+            src.root = td.root
+            src.nodes, src.n_nodes = N.ptr(td.nodes), len(td.nodes)
+            src.instances, src.n_instances = N.ptr(td.instances), len(td.instances)
+            src.tris, src.n_tri_vec4 = N.ptr(td.tris), len(td.tris)
         src.vertices, src.n_vertices = N.ptr(sd.vertices), len(sd.vertices)
         src.normals, src.texcoords = N.ptr(sd.normals), N.ptr(sd.texcoords)
         src.mesh_tris, src.geom_normals, src.n_mesh_tris = N.ptr(sd.tris), N.ptr(sd.geom_normals), len(sd.tris)
@@ -58,7 +63,14 @@ class Server:
         src.tex_dims, src.tex_pixels, src.n_textures = N.ptr(sd.tex_dims), N.ptr(sd.tex_pixels), sd.n_textures
         src.env_map, src.env_intensity = sd.env_map + 1, sd.env_map_intensity
         self._scenes.append((td, sd))   # the arrays the source points to stay alive during the call
-        sid = self.lib.imbart_server_add_scene(self.h, C.byref(src))
+        if gpu_build:
+            md, idesc, keep = S.build_descs(desc.meshes, desc.instances)
+            ms = C.c_float(0.0)
+            sid = self.lib.imbart_server_add_scene_gpu_build(self.h, C.byref(src), md, len(desc.meshes), idesc,
+                                                             len(desc.instances), C.byref(ms))
+            self.last_build_ms = ms.value
+        else:
+            sid = self.lib.imbart_server_add_scene(self.h, C.byref(src))
         if sid < 0:
             raise N.ImbartError("imbart_server_add_scene: " + N.last_error()[1])
         return sid

@@ -678,6 +678,19 @@ void imbart_server_destroy(imbart_server* server);
 /* Registers a scene; returns its id (>= 0) or -(error code). Scenes are not uploaded until
  * a request needs them. */
 int imbart_server_add_scene(imbart_server* server, const imbart_scene_source* source);
+
+/* Registers a scene whose traversal arrays are built on the server's GPU from its meshes
+ * and instances (imbart_scene_build_gpu: a fraction of a second where the host SBVH build
+ * and conversion take seconds for millions of triangles) instead of taken from `source`,
+ * whose traversal fields are then ignored (the shading fields are as for
+ * imbart_server_add_scene). The built arrays are kept on the host like a converted scene's,
+ * so the pool uploads and evicts the scene the same way. build_ms (may be NULL): wall time
+ * of the build and its download. */
+typedef struct imbart_mesh_desc imbart_mesh_desc;
+typedef struct imbart_instance_desc imbart_instance_desc;
+int imbart_server_add_scene_gpu_build(imbart_server* server, const imbart_scene_source* source,
+                                      const imbart_mesh_desc* meshes, int n_meshes,
+                                      const imbart_instance_desc* instances, int n_instances, float* build_ms);
 /* Submits a request; returns a ticket (> 0) or -(error code). */
 long long imbart_server_submit_render(imbart_server* server, const imbart_render_request* request);
 long long imbart_server_submit_vcm(imbart_server* server, const imbart_vcm_request* request);
@@ -736,20 +749,20 @@ int imbart_build_top_node2(const float* boxes, const float* inv_mats, const int*
 /* A triangle mesh: HOST arrays of n_vertices xyz floats and n_tris {v0, v1, v2, material}
  * ints; tri_offset is the global id of its first triangle (hits report tri_offset + local
  * index, as Scene::build_mesh_accels numbers triangles, scene.cpp:75-97). */
-typedef struct {
+struct imbart_mesh_desc {
     const float* vertices; int n_vertices;
     const int* indices; int n_tris;
     int tri_offset;
-} imbart_mesh_desc;
+};
 
 /* An instance: row-major 3x4 object-to-world and world-to-object matrices, the mesh it
  * instances and the id its hits report. */
-typedef struct {
+struct imbart_instance_desc {
     float obj_to_world[12];
     float world_to_obj[12];
     int mesh;
     int id;
-} imbart_instance_desc;
+};
 
 /* Builds a scene entirely on the GPU (PLOC clustering over Morton-sorted primitives, a
  * surface-area leaf pass, a collapse into the compressed 8-wide layout) and returns it ready

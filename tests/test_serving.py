@@ -275,3 +275,38 @@ def test_scene_larger_than_pool_is_refused(cuda, scenes):
     with pytest.raises(N.ImbartError):
         srv.add_scene(d, td)
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_scenes_registered_through_the_gpu_builder(cuda, scenes, mode):
+    """imbart_server_add_scene_gpu_build (traversal arrays built on the GPU, kept on the host
+    like a converted scene's): renders equal the single-request path's on the host-built
+    scene (hits do not depend on the tree) and ray batches equal imbart_trace's hits."""
+    from imbatracer_b200 import scene as S
+    from imbatracer_b200.serving import Server
+    srv = Server(mode=mode, hbm_budget=64 << 20, max_paths=1 << 16)
+    ids = []
+    for d, _ in scenes:
+        ids.append(srv.add_scene(d, gpu_build=True))
+        assert srv.last_build_ms > 0
+    tickets = []
+    for k, (si, w, h, spp, ml, seed, rr) in enumerate(REQS):
+        d, td = scenes[si]
+        t, img = srv.submit_render(ids[si], d.camera, w, h, spp, ml, seed, rr_start=rr)
+        tickets.append((t, img, plain_image(d, td, w, h, spp, ml, seed, rr), k))
+    d, td = scenes[2]
+    lo, hi = G.scene_box(d)
+    rays = G.random_rays(np.random.default_rng(3), 5000, lo - 0.1 * (hi - lo), hi + 0.1 * (hi - lo))
+    hits = np.zeros(len(rays), N.HIT_DTYPE)
+    tb = srv.submit_rays(ids[2], rays, hits)
+    for t, img, want, k in tickets:
+        assert srv.wait(t)["status"] == 0
+        assert rel_rmse(img, want) <= MIX_TOL, (k, rel_rmse(img, want))
+    assert srv.wait(tb)["status"] == 0
+    ds = S.DeviceScene(td)
+    ref = np.zeros_like(hits)
+    ds.trace_host(rays, ref)
+    assert (ref["tri_id"] >= 0).sum() > 500
+    assert np.array_equal(hits.view(np.int32), ref.view(np.int32))
+    srv.close()
