@@ -160,19 +160,6 @@ __device__ __forceinline__ float xform_row(const float4 m, float x, float y, flo
     return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
 }
 
-// Three-input minimum and maximum (PTX min.f32 / max.f32 with three operands, sm_100):
-// exact, like the two-input forms they replace.
-__device__ __forceinline__ float fmax3f(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-__device__ __forceinline__ float fmin3f(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-
 // 32768 + (byte k of w) as an exact float, with one byte permute: the byte lands in bits
 // 8..15 of the float 2^15 (0x47000000), whose mantissa step there is 1. The node's origin
 // is stored 32768 quanta low, so this value feeds the slab FMA directly.
@@ -225,8 +212,8 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
         const float tfy = fmaf(byte_plane(wf_y, k), ay, bfy);
         const float tnz = fmaf(byte_plane(wn_z, k), az, bnz);
         const float tfz = fmaf(byte_plane(wf_z, k), az, bfz);
-        const float tn = fmax3f(tnx, tny, fmaxf(tnz, tmin));
-        const float tf = fmin3f(tfx, tfy, tfz) * IMBART_SLACK;
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+        const float tf = fminf(fminf(tfx, tfy), tfz) * IMBART_SLACK;
         hitbits |= (tn <= fminf(tf, tlimit) ? 1u : 0u) << s;
     }
     // Internal children, with bit s moved to s ^ oct (three conditional bit-group swaps).
@@ -648,11 +635,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     const float o_best = __shfl_sync(kFull, best_t, o);
                     const bool has = j < total;
                     const int k = j - o_excl;
-                    // k-th set bit of the owner's mask (fns; checked, with the halving search
-                    // as the fallback, so the index always stays inside the owner's group).
-                    uint32_t bit = __fns(o_mask, 0u, k + 1);
-                    if (bit > 31u || !((o_mask >> bit) & 1u)) bit = nth_set_bit(o_mask, k);
-                    const int ti = has ? (int)(o_base + bit) : -1;
+                    const int ti = has ? (int)(o_base + nth_set_bit(o_mask, k)) : -1;
                     float4 a, b, c;
                     if (p.tri_stage) {
                         // Stage the pass's triangles: lane f loads 16-byte word f, f+32, f+64
