@@ -135,8 +135,8 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
 // Three query classes keep their own variant and refill threshold: incoherent closest hit,
 // any hit, and closest hit over coherent rays (camera rays, flag IMBART_TRACE_COHERENT),
 // which traverse best in static batches (refill only when the whole warp is idle).
-constexpr int kTraceVariants = 16;   // persistent-kernel shapes 1..16 (0: one ray per thread)
-constexpr int kFirstCoopVariant = 11; // 11..16: the shapes with the cooperative triangle phase
+constexpr int kTraceVariants = 17;   // persistent-kernel shapes 1..17 (0: one ray per thread)
+constexpr int kFirstCoopVariant = 11; // 11..17: the shapes with the cooperative triangle phase
 
 // Each class also keeps its triangle batch: in the per-lane shapes, the triangles a lane
 // tests per loop trip before the lanes with node work take their next node step (0: the
@@ -268,6 +268,7 @@ LaunchSpec variant_spec(int variant, int count, int device, float share, TracePa
         case 14: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16, true>(count, device, share, p);
         case 15: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12, true>(count, device, share, p);
         case 16: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12, true>(count, device, share, p);
+        case 17: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10, true>(count, device, share, p);
         default: return {};
     }
 }

@@ -226,7 +226,7 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
             t = N.TraceTuning()
             N.check(lib.imbart_trace_autotune(ds.handle, N.ptr(d_rays), N.ptr(d_hits), len(rays), flags, None,
                                               C.byref(t)), "autotune")
-            assert 1 <= t.variant <= 16 and t.refill in (4, 8, 16, 24, 32) and 0 < t.ms <= t.default_ms * 1.0001
+            assert 1 <= t.variant <= 17 and t.refill in (4, 8, 16, 24, 32) and 0 < t.ms <= t.default_ms * 1.0001
             v, r = C.c_int(0), C.c_int(0)
             lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r))
             assert (v.value, r.value) == (t.variant, t.refill)
@@ -248,7 +248,7 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
 @pytest.mark.gpu
 def test_every_kernel_variant_is_exact(cuda):
     """Each traversal kernel shape the autotuner may pick (0: one ray per thread, 1..10:
-    persistent warps at different block sizes, blocks per SM and shared stack depths, 11..16:
+    persistent warps at different block sizes, blocks per SM and shared stack depths, 11..17:
     the same with the cooperative triangle phase; with triangle batches 0, 1 and 2, which in
     the cooperative shapes select loads by each lane or staging in shared memory) gives the
     oracle's closest hits bit for bit, its occlusion answers, and the restated walk's node,
@@ -268,7 +268,7 @@ def test_every_kernel_variant_is_exact(cuda):
         refa = O.trace_node2(td, rays, any_hit=True)
         wn, wt, wi, root = H.wide_arrays(td)
         counts = {a: O.wide_walk(wn, wt, wi, root, rays, any_hit=a)[2] for a in (False, True)}
-        for variant in range(17):
+        for variant in range(18):
             for tri_batch in (0, 1, 2):
                 for flags in saved:
                     N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
@@ -280,7 +280,7 @@ def test_every_kernel_variant_is_exact(cuda):
                 for a in (False, True):
                     _, _, st = run_gpu(ds, rays, any_hit=a, stats=True)
                     assert np.array_equal(st, counts[a]), (variant, tri_batch, a, st, counts[a])
-        assert lib.imbart_set_trace_class(N.TRACE_CLOSEST, 17, 16) != 0
+        assert lib.imbart_set_trace_class(N.TRACE_CLOSEST, 18, 16) != 0
         assert lib.imbart_set_trace_tri_batch(N.TRACE_CLOSEST, -1) != 0
         lib.imbart_clear_error()
     finally:
