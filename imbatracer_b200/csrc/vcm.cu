@@ -283,6 +283,15 @@ __global__ void __launch_bounds__(128) light_shade_kernel(VcmParams p, int n, fl
     }
 }
 
+// Stable compaction of the live light-path slots (path length >= 0): flags, then the same
+// block-count / scan as the vertex append, then a scatter of the path states to the second
+// buffers in slot order, so paths keep their relative order and the vertex cache its
+// (wavefront, path) order.
+__global__ void live_flags_kernel(const float4* __restrict__ thrs, int n, int* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = __float_as_int(thrs[i].w) >= 0 ? 1 : 0;
+}
+
 // Deterministic append of the staged vertices: exclusive scan of the per-slot flags in slot
 // order (block counts, one scan of the block counts, per-block ranks).
 constexpr int kScanBlock = 256;
@@ -353,6 +362,41 @@ __global__ void vertex_scatter_kernel(const int* flags, int n, const int* block_
         if (f) {
             const int dst = cache_base + carry + before + __popc(m & ((1u << lane) - 1u));
             for (int q = 0; q < 7; ++q) cache[7 * (size_t)dst + q] = stage[7 * (size_t)i + q];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < kScanBlock / 32; ++w) t += warp_sums[w];
+            carry += t;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void compact_paths_kernel(const int* flags, int n, const int* block_offsets, const float4* rays,
+                                     const unsigned long long* rngs, const float4* thrs, const float4* ws,
+                                     float4* rays2, unsigned long long* rngs2, float4* thrs2, float4* ws2) {
+    __shared__ int warp_sums[kScanBlock / 32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = block_offsets[blockIdx.x];
+    __syncthreads();
+    const int base = blockIdx.x * kScanTile;
+    for (int k = 0; k < kScanPer; ++k) {
+        const int i = base + k * kScanBlock + threadIdx.x;
+        const int f = i < n ? flags[i] : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        const int lane = threadIdx.x & 31;
+        if (lane == 0) warp_sums[threadIdx.x >> 5] = __popc(m);
+        __syncthreads();
+        int before = 0;
+        for (int w = 0; w < (int)(threadIdx.x >> 5); ++w) before += warp_sums[w];
+        if (f) {
+            const int dst = carry + before + __popc(m & ((1u << lane) - 1u));
+            rays2[2 * (size_t)dst] = rays[2 * (size_t)i];
+            rays2[2 * (size_t)dst + 1] = rays[2 * (size_t)i + 1];
+            rngs2[dst] = rngs[i];
+            thrs2[dst] = thrs[i];
+            ws2[dst] = ws[i];
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -893,6 +937,11 @@ struct imbart_vcm {
     unsigned long long* l_rng = nullptr;
     float4* l_thr = nullptr;
     float4* l_w = nullptr;
+    // second set of path states, for the stable compaction of the live slots
+    float4* l_rays2 = nullptr;
+    unsigned long long* l_rng2 = nullptr;
+    float4* l_thr2 = nullptr;
+    float4* l_w2 = nullptr;
     float4* stage = nullptr;
     int* vflags = nullptr;
     int* bsums = nullptr;
@@ -937,7 +986,8 @@ namespace {
 
 void free_vcm(imbart_vcm* v) {
     void* ptrs[] = {v->keys, v->perm, v->tile_counts,
-                    v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage, v->vflags, v->bsums, v->d_tiles,
+                    v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->l_rays2, v->l_rng2, v->l_thr2, v->l_w2,
+                    v->stage, v->vflags, v->bsums, v->d_tiles,
                     v->cache, v->c_hits, v->c_merge, v->s_rays, v->s_hits, v->s_pixel, v->s_contrib, v->counts};
     for (void* p : ptrs) cudaFree(p);
     for (int k = 0; k < 2; ++k) {
@@ -1205,14 +1255,15 @@ int imbart_vcm_light_pass_range(imbart_vcm* v, const imbart_scene* scene, const 
     const int desired = st->light_tile_size > 0 ? st->light_tile_size : P_total;
     const std::vector<LightTile> tiles =
         light_tiles(sh->s.light_count, P_total, desired, st->light_seed, st->light_seed_step);
-    const int n_blocks = (P + kScanTile - 1) / kScanTile;
     bool good = true;
     if (v->l_cap < P) {
         const long long c = std::max<long long>(P, v->l_cap * 3 / 2);
         const long long cb = (c + kScanTile - 1) / kScanTile;
         good = realloc_exact(&v->l_rays, 2 * (size_t)c) && realloc_exact(&v->l_hits, (size_t)c) &&
                realloc_exact(&v->l_rng, (size_t)c) && realloc_exact(&v->l_thr, (size_t)c) &&
-               realloc_exact(&v->l_w, (size_t)c) && realloc_exact(&v->stage, 7 * (size_t)c) &&
+               realloc_exact(&v->l_w, (size_t)c) && realloc_exact(&v->l_rays2, 2 * (size_t)c) &&
+               realloc_exact(&v->l_rng2, (size_t)c) && realloc_exact(&v->l_thr2, (size_t)c) &&
+               realloc_exact(&v->l_w2, (size_t)c) && realloc_exact(&v->stage, 7 * (size_t)c) &&
                realloc_exact(&v->vflags, (size_t)c) && realloc_exact(&v->bsums, (size_t)cb + 1);
         v->l_cap = good ? c : 0;
     }
@@ -1235,40 +1286,60 @@ int imbart_vcm_light_pass_range(imbart_vcm* v, const imbart_scene* scene, const 
     int rc = 0;
     long long n_closest = 0, n_shadow = 0, n_waves = 0;
     int live = P;
+    int n = P;   // slots in use: the live paths after the last compaction, in path order
     while (live > 0 && !rc) {
-        rc = launch_trace_internal(scene, v->l_rays, v->l_hits, nullptr, P, IMBART_TRACE_CLOSEST, s, nullptr);
+        if (live <= n / 2) {
+            // At most half the slots are live: compact them (stable) so that this and later
+            // wavefronts launch over the live paths only.
+            const int nb = (n + kScanTile - 1) / kScanTile;
+            live_flags_kernel<<<(n + 255) / 256, 256, 0, s>>>(v->l_thr, n, v->vflags);
+            flag_count_kernel<<<nb, kScanBlock, 0, s>>>(v->vflags, n, v->bsums);
+            block_scan_kernel<<<1, kScanBlock, 0, s>>>(v->bsums, nb);
+            compact_paths_kernel<<<nb, kScanBlock, 0, s>>>(v->vflags, n, v->bsums, v->l_rays, v->l_rng, v->l_thr,
+                                                           v->l_w, v->l_rays2, v->l_rng2, v->l_thr2, v->l_w2);
+            note_launches(4);
+            std::swap(v->l_rays, v->l_rays2);
+            std::swap(v->l_rng, v->l_rng2);
+            std::swap(v->l_thr, v->l_thr2);
+            std::swap(v->l_w, v->l_w2);
+            n = live;
+        }
+        const int grid_n = (n + 127) / 128;
+        const int n_blocks_n = (n + kScanTile - 1) / kScanTile;
+        rc = launch_trace_internal(scene, v->l_rays, v->l_hits, nullptr, n, IMBART_TRACE_CLOSEST, s, nullptr);
         if (rc) break;
         n_closest += live;
         ++n_waves;
-        // Room for up to P new vertices before the wavefront appends.
-        if (!grow(&v->cache, &v->cache_cap, 7ll * (v->cache_count + (long long)P), 7ll * v->cache_count)) {
+        // Room for up to n new vertices before the wavefront appends.
+        if (!grow(&v->cache, &v->cache_cap, 7ll * (v->cache_count + (long long)n), 7ll * v->cache_count)) {
             rc = IMBART_ERR_OUT_OF_MEMORY;
             break;
         }
         p.cache = v->cache;
         if (!ok(cudaMemsetAsync(v->counts, 0, sizeof(int) * 4, s), "cudaMemsetAsync")) { rc = IMBART_ERR_CUDA; break; }
-        if (!group_paths(v, sh, P, s, [&](uint8_t* keys) {
-                light_key_kernel<<<(P + 255) / 256, 256, 0, s>>>(p.s, v->l_hits, v->l_thr, P, keys);
+        if (!group_paths(v, sh, n, s, [&](uint8_t* keys) {
+                light_key_kernel<<<(n + 255) / 256, 256, 0, s>>>(p.s, v->l_hits, v->l_thr, n, keys);
             })) {
             rc = IMBART_ERR_CUDA;
             break;
         }
-        light_shade_kernel<<<grid, 128, 0, s>>>(p, P, v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage,
-                                                v->vflags, v->s_rays, v->s_pixel, v->s_contrib, v->use_perm ? v->perm : nullptr);
-        flag_count_kernel<<<n_blocks, kScanBlock, 0, s>>>(v->vflags, P, v->bsums);
-        block_scan_kernel<<<1, kScanBlock, 0, s>>>(v->bsums, n_blocks);
-        vertex_scatter_kernel<<<n_blocks, kScanBlock, 0, s>>>(v->vflags, P, v->bsums, v->stage, v->cache,
-                                                              v->cache_count);
+        light_shade_kernel<<<grid_n, 128, 0, s>>>(p, n, v->l_rays, v->l_hits, v->l_rng, v->l_thr, v->l_w, v->stage,
+                                                  v->vflags, v->s_rays, v->s_pixel, v->s_contrib,
+                                                  v->use_perm ? v->perm : nullptr);
+        flag_count_kernel<<<n_blocks_n, kScanBlock, 0, s>>>(v->vflags, n, v->bsums);
+        block_scan_kernel<<<1, kScanBlock, 0, s>>>(v->bsums, n_blocks_n);
+        vertex_scatter_kernel<<<n_blocks_n, kScanBlock, 0, s>>>(v->vflags, n, v->bsums, v->stage, v->cache,
+                                                                v->cache_count);
         note_launches(4);
-        rc = launch_trace_internal(scene, v->s_rays, v->s_hits, nullptr, P, IMBART_TRACE_ANY, s, nullptr, nullptr,
+        rc = launch_trace_internal(scene, v->s_rays, v->s_hits, nullptr, n, IMBART_TRACE_ANY, s, nullptr, nullptr,
                                    v->counts + 1);
         if (rc) break;
-        vcm_shadow_kernel<<<grid, 128, 0, s>>>(v->counts + 1, v->s_hits, v->s_pixel, v->s_contrib, image);
+        vcm_shadow_kernel<<<grid_n, 128, 0, s>>>(v->counts + 1, v->s_hits, v->s_pixel, v->s_contrib, image);
         note_launches(1);
         if (!ok(cudaGetLastError(), "light pass kernels") ||
             !ok(cudaMemcpyAsync(v->host_counts, v->counts, sizeof(int) * 3, cudaMemcpyDeviceToHost, s),
                 "cudaMemcpyAsync") ||
-            !ok(cudaMemcpyAsync(v->host_counts + 3, v->bsums + n_blocks, sizeof(int), cudaMemcpyDeviceToHost, s),
+            !ok(cudaMemcpyAsync(v->host_counts + 3, v->bsums + n_blocks_n, sizeof(int), cudaMemcpyDeviceToHost, s),
                 "cudaMemcpyAsync") ||
             !ok(cudaStreamSynchronize(s), "cudaStreamSynchronize")) {
             rc = IMBART_ERR_CUDA;
