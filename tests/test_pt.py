@@ -159,6 +159,19 @@ def test_benchmark_frame_matches_reference(cuda, bench_scene, rr_start):
 
 @pytest.mark.gpu
 @needs_ref
+def test_config1_full_frame_matches_reference(cuda):
+    """Config 1 as specified (512x512, 1 spp, 4 bounces = max_path_len 5) against the
+    reference's PathTracer on the same seeds: the frame the CPU baseline renders."""
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    d = G.config1(width=512, height=512)
+    ref = R.RefScene(d).render_pt(512, 512, 1, 5, 31337)
+    img = PathTracer(GpuScene(d), max_path_len=5).render(1, 31337, 512, 512).cpu().numpy()
+    assert ref.sum() > 0
+    assert rel_rmse(img, ref) <= RMSE_TOL, rel_rmse(img, ref)
+
+
+@pytest.mark.gpu
+@needs_ref
 def test_deferred_roulette_matches_reference(cuda):
     """rr_start 2 on the scene with every material kind against the deferred-roulette oracle."""
     from imbatracer_b200.integrators import GpuScene, PathTracer

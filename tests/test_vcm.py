@@ -244,3 +244,19 @@ def test_radius_schedule_and_grid_settings(cuda):
     with pytest.raises(N.ImbartError):
         vi.begin_iteration(1)
     vi.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_config3_scale_path_tracing_matches_reference(cuda, config3_scene):
+    """The path tracer on the 2M-triangle config-3 scene (320x176, 2 spp, 8 bounces) against
+    the reference's PathTracer on the same seeds."""
+    from imbatracer_b200.integrators import PathTracer
+    d, rs, gs = config3_scene
+    w, h, spp, max_len, seed = 320, 176, 2, 9, 777
+    ref = rs.render_pt(w, h, spp, max_len, seed)
+    pt = PathTracer(gs, max_path_len=max_len)
+    img = pt.render(spp, seed, w, h).cpu().numpy()
+    pt.close()
+    assert ref.sum() > 0
+    assert rel_rmse(img, ref) <= 1e-3, rel_rmse(img, ref)
