@@ -191,10 +191,10 @@ def config3_roofline(torch, dev, stream, peak):
     desc = G.config3()
     gs = GpuScene(desc, device=dev.index or 0)
     sets = make_wavefront(desc, gs.trace_scene, torch, dev, 99, shadow_from_bounce=True)
-    for (rays, _), flags in zip(sets, classes):
-        hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
-        gs.trace_scene.autotune(rays, hits, flags, stream=stream)
-    del sets
+    ray_sets = [(rays, torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev), flags)
+                for (rays, _), flags in zip(sets, classes)]
+    nw = gs.autotune_node_width(ray_sets, stream=stream)
+    del sets, ray_sets
     pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
     image = torch.zeros((desc.camera.height, desc.camera.width, 3), dtype=torch.float32, device=dev)
     for k in range(2):
@@ -205,7 +205,8 @@ def config3_roofline(torch, dev, stream, peak):
            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
            "closest_mrays_s": round(work.closest_rays / max(prof.closest_ms, 1e-9) / 1e3, 1),
            "bytes_per_ray": round(trace_bytes(work.closest_rays, work.closest_work) / max(work.closest_rays, 1), 1),
-           "launches": int(prof.closest_launches)}
+           "launches": int(prof.closest_launches), "node_width": nw["node_width"],
+           "node_width_tuned_ms": {str(k): v for k, v in nw["ms"].items()}}
     pt.close()
     for flags, v, r, b in saved:   # the main frame's tuning again for what follows
         lib.imbart_set_trace_class(flags, v, r)
@@ -278,21 +279,27 @@ def run_pt(args):
 
     desc = G.config2()
     gs = GpuScene(desc, device=local)
-    pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
     W, H = desc.camera.width, desc.camera.height
     stream = torch.cuda.current_stream(dev)
-    # Autotuner (untimed): the kernel configuration of each query class on this scene's rays.
+    # Autotuner (untimed): the node width of the scene, then the kernel configuration of each
+    # query class on this scene's rays at that width.
     tuning = {}
     if not args.no_autotune:
         sets = make_wavefront(desc, gs.trace_scene, torch, dev, 4321, shadow_from_bounce=True)
-        for (rays, any_hit), name, flags in zip(sets, ("camera", "bounce", "shadow"),
-                                                (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)):
-            hits = torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev)
-            t = gs.trace_scene.autotune(rays, hits, flags, stream=stream)
+        classes = (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)
+        ray_sets = [(rays, torch.zeros((rays.shape[0], 4), dtype=torch.int32, device=dev), flags)
+                    for (rays, _), flags in zip(sets, classes)]
+        nw = gs.autotune_node_width(ray_sets, stream=stream)
+        tuning["node_width"] = {"chosen": nw["node_width"],
+                                "tuned_ms_all_classes": {str(k): v for k, v in nw["ms"].items()}}
+        for name, flags in zip(("camera", "bounce", "shadow"), classes):
+            t = nw["classes"][flags]
             tuning[name] = {"variant": t["variant"], "refill": t["refill"], "tri_batch": t["tri_batch"],
                             "speedup": round(t["default_ms"] / max(t["ms"], 1e-9), 3)}
-        del sets
+        del sets, ray_sets
         torch.cuda.synchronize()
+    pt = PathTracer(gs, max_path_len=MAX_PATH_LEN, rr_start=RR_START)
+    if not args.no_autotune:
         # Wavefront size (paths in flight) for this frame shape, with the tuned kernels.
         if not args.paths_in_flight:
             wf = pt.autotune_wavefront(SPP, seed_base=777, stream=stream)
@@ -897,10 +904,10 @@ def config5_saturation(scenes, ray_buf, hit_buf, p99_bound_ms=100.0, duration_s=
 # ---------------------------------------------------------------------------------------
 # --mode trace: traversal kernels alone on fixed ray sets of the frame (kernel tuning)
 # ---------------------------------------------------------------------------------------
-def make_scene():
+def make_scene(name: str = "config2"):
     from imbatracer_b200 import scene as S
     from imbatracer_b200 import scenegen as G
-    desc = G.config2()
+    desc = {"config1": G.config1, "config2": G.config2, "config3": G.config3}[name]()
     td = S.build_traversal_data(desc.meshes, desc.instances)
     return desc, td
 
@@ -1018,7 +1025,7 @@ def run_trace(args):
     from imbatracer_b200 import native as N
     from imbatracer_b200 import scene as S
     dev = torch.device("cuda", 0)
-    desc, td = make_scene()
+    desc, td = make_scene(args.scene)
     ds = S.DeviceScene(td)
     sets = make_wavefront(desc, ds, torch, dev, 1234)
     hits = [torch.zeros((r.shape[0], 4), dtype=torch.int32, device=dev) for r, _ in sets]
@@ -1035,7 +1042,8 @@ def run_trace(args):
         e1.record()
         torch.cuda.synchronize()
         out[name] = round(r.shape[0] * args.steps / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)
-    print(json.dumps({"mode": "trace", "Mrays_s": out, "rays": [r.shape[0] for r, _ in sets]}), flush=True)
+    print(json.dumps({"mode": "trace", "scene": args.scene, "Mrays_s": out, "rays": [r.shape[0] for r, _ in sets]}),
+          flush=True)
 
 
 def main():
@@ -1045,6 +1053,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="pt", choices=["pt", "trace", "serve", "vcm"])
+    ap.add_argument("--scene", default="config2", choices=["config1", "config2", "config3"],
+                    help="trace mode: the scene whose frame's ray sets are traced")
     ap.add_argument("--no-vcm", action="store_true", help="pt mode: skip the VCM-family iterations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="pt mode: keep the default kernel configurations")

@@ -11,7 +11,11 @@
 // leaves into runs of at most three primitives, collapses the tree into 8-wide nodes
 // (repeatedly opening the child with the largest surface area), assigns child slots by
 // direction octant and quantizes child boxes conservatively to 8 bits per plane.
+// The node width is 8 or 4 (imbart_set_node_width): a 4-wide tree uses slots 0..3 of the
+// same 80-byte record, ordered by the x/y quadrant, and leaves slots 4..7 empty.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -22,6 +26,24 @@
 #include "imbart_internal.h"
 
 namespace imbart {
+
+// Node width of the scenes converted from now on (IMBART_NODE_WIDTH, imbart_set_node_width).
+namespace {
+std::atomic<int> g_node_width{0};
+}  // namespace
+
+int current_node_width() {
+    int w = g_node_width.load(std::memory_order_relaxed);
+    if (w == 0) {
+        const char* e = std::getenv("IMBART_NODE_WIDTH");
+        const int v = e ? std::atoi(e) : 8;
+        int expected = 0;
+        g_node_width.compare_exchange_strong(expected, v == 4 ? 4 : 8);
+        w = g_node_width.load(std::memory_order_relaxed);
+    }
+    return w;
+}
+
 namespace {
 
 constexpr int kMaxLeafPrims = 3;
@@ -126,19 +148,20 @@ int add_leaf(ITree& tree, int first, int n, const IBox& leaf_box, PrimBox prim_b
 
 struct WideBuilder {
     std::vector<WideNode>& out;
-    explicit WideBuilder(std::vector<WideNode>& o) : out(o) {}
+    int width;   // children per node: 8, or 4 (slots 0..3)
+    WideBuilder(std::vector<WideNode>& o, int w) : out(o), width(w == 4 ? 4 : 8) {}
 
-    // Children of a wide node: open the internal child with the largest area until 8.
-    static std::vector<int> gather(const ITree& t, int n) {
+    // Children of a wide node: open the internal child with the largest area until `width`.
+    static std::vector<int> gather(const ITree& t, int n, int width) {
         std::vector<int> kids;
         if (t.nodes[n].leaf()) { kids.push_back(n); return kids; }
         kids = t.nodes[n].kids;
-        while ((int)kids.size() < 8) {
+        while ((int)kids.size() < width) {
             int best = -1; float best_area = -1.0f;
             for (int i = 0; i < (int)kids.size(); ++i) {
                 const INode& k = t.nodes[kids[i]];
                 if (k.leaf()) continue;
-                if ((int)(kids.size() - 1 + k.kids.size()) > 8) continue;
+                if ((int)(kids.size() - 1 + k.kids.size()) > width) continue;
                 const float a = k.box.half_area();
                 if (a > best_area) { best_area = a; best = i; }
             }
@@ -150,8 +173,9 @@ struct WideBuilder {
         return kids;
     }
 
-    // Greedy slot assignment: slot s prefers children towards (s&1?+x:-x, s&2?+y:-y, s&4?+z:-z).
-    static void assign_slots(const ITree& t, const std::vector<int>& kids, int slot_of[8]) {
+    // Greedy slot assignment: slot s prefers children towards (s&1?+x:-x, s&2?+y:-y, s&4?+z:-z);
+    // a 4-wide node uses slots 0..3, ordered by x and y alone.
+    static void assign_slots(const ITree& t, const std::vector<int>& kids, int width, int slot_of[8]) {
         const int n = (int)kids.size();
         IBox all = IBox::empty();
         for (int k : kids) all.grow(t.nodes[k].box);
@@ -163,8 +187,9 @@ struct WideBuilder {
             const IBox& b = t.nodes[kids[i]].box;
             float d[3];
             for (int a = 0; a < 3; ++a) d[a] = 0.5f * (b.lo[a] + b.hi[a]) - pc[a];
-            for (int s = 0; s < 8; ++s) {
-                const float score = (s & 1 ? d[0] : -d[0]) + (s & 2 ? d[1] : -d[1]) + (s & 4 ? d[2] : -d[2]);
+            for (int s = 0; s < width; ++s) {
+                const float score = (s & 1 ? d[0] : -d[0]) + (s & 2 ? d[1] : -d[1]) +
+                                    (width == 4 ? 0.0f : (s & 4 ? d[2] : -d[2]));
                 cands.push_back({score, i, s});
             }
         }
@@ -237,9 +262,9 @@ struct WideBuilder {
         while (!work.empty()) {
             auto [w, n] = work.front();
             work.pop_front();
-            std::vector<int> kids = gather(t, n);
+            std::vector<int> kids = gather(t, n, width);
             int slot_of[8];
-            assign_slots(t, kids, slot_of);
+            assign_slots(t, kids, width, slot_of);
             int kid_in_slot[8];
             for (int s = 0; s < 8; ++s) kid_in_slot[s] = -1;
             for (int i = 0; i < (int)kids.size(); ++i) kid_in_slot[slot_of[i]] = kids[i];
@@ -396,8 +421,11 @@ struct Parser {
 // Shared driver: parses the top level, converts each distinct mesh BVH once, then the top level.
 template <typename Kids, typename BottomRun>
 std::string convert_common(int root, int n_nodes, const imbart_instance_node* insts, int n_insts,
-                           HostWideScene& out, Kids kids, BottomRun bottom_run) {
+                           HostWideScene& out, Kids kids, BottomRun bottom_run, int node_width) {
+    if (node_width < 0) node_width = current_node_width();
+    if (node_width != 4 && node_width != 8) return "node width must be 4 or 8";
     out.nodes.clear(); out.tris.clear(); out.insts.clear();
+    out.node_width = node_width;
     Parser ps(out);
     if (root < 0 || root >= n_nodes) return "root out of bounds";
 
@@ -425,7 +453,7 @@ std::string convert_common(int root, int n_nodes, const imbart_instance_node* in
 
     // Bottom level: one wide tree per distinct mesh root.
     std::unordered_map<int, int> wide_root_of;
-    WideBuilder wb(out.nodes);
+    WideBuilder wb(out.nodes, node_width);
     for (int src : inst_src) {
         const int mroot = insts[src].next;
         if (wide_root_of.count(mroot)) continue;
@@ -475,7 +503,7 @@ std::string convert_common(int root, int n_nodes, const imbart_instance_node* in
 
 std::string convert_node2(int root, const imbart_node2* nodes, int n_nodes,
                           const imbart_instance_node* insts, int n_insts,
-                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out) {
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out, int node_width) {
     auto kids = [&](int n, std::vector<std::pair<int, IBox>>& ch) {
         const imbart_node2& nd = nodes[n];
         ch.push_back({nd.left, box_from(nd.left_bb)});
@@ -484,12 +512,12 @@ std::string convert_node2(int root, const imbart_node2* nodes, int n_nodes,
     auto bottom_run = [&](Parser& ps, int at, std::vector<int>& recs) {
         return ps.tri_run2(tris, n_tri_vec4, at, recs);
     };
-    return convert_common(root, n_nodes, insts, n_insts, out, kids, bottom_run);
+    return convert_common(root, n_nodes, insts, n_insts, out, kids, bottom_run, node_width);
 }
 
 std::string convert_node4(int root, const imbart_node4* nodes, int n_nodes,
                           const imbart_instance_node* insts, int n_insts,
-                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out) {
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out, int node_width) {
     auto kids = [&](int n, std::vector<std::pair<int, IBox>>& ch) {
         const imbart_node4& nd = nodes[n];
         for (int j = 0; j < 4; ++j) {
@@ -503,10 +531,22 @@ std::string convert_node4(int root, const imbart_node4* nodes, int n_nodes,
     auto bottom_run = [&](Parser& ps, int at, std::vector<int>& recs) {
         return ps.tri_run4(tris, n_tri_vec4, at, recs);
     };
-    return convert_common(root, n_nodes, insts, n_insts, out, kids, bottom_run);
+    return convert_common(root, n_nodes, insts, n_insts, out, kids, bottom_run, node_width);
 }
 
 }  // namespace imbart
+
+extern "C" int imbart_set_node_width(int width) {
+    if (width != 4 && width != 8) {
+        imbart::set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_set_node_width: width must be 4 or 8");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    imbart::current_node_width();   // settle the environment default first
+    imbart::g_node_width.store(width, std::memory_order_relaxed);
+    return 0;
+}
+
+extern "C" int imbart_get_node_width(void) { return imbart::current_node_width(); }
 
 extern "C" int imbart_wide_from_node2(int root, const imbart_node2* nodes, int n_nodes,
                                       const imbart_instance_node* instances, int n_instances,

@@ -67,6 +67,7 @@ struct HostWideScene {
     std::vector<WideInst> insts;
     int root = 0;          // wide index of the top-level root
     int top_nodes = 0;     // number of top-level wide nodes
+    int node_width = 8;    // children per node: 8, or 4 (slots 0..3 of the same record)
     bool masked = false;
     std::vector<int> indices;
     std::vector<imbart_vec2> texcoords;
@@ -75,12 +76,15 @@ struct HostWideScene {
 };
 
 // Converters (convert.cpp). Return empty string on success, else an error message.
+// node_width: 8 or 4; -1 takes the process setting (current_node_width).
 std::string convert_node2(int root, const imbart_node2* nodes, int n_nodes,
                           const imbart_instance_node* insts, int n_insts,
-                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out);
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out, int node_width = -1);
 std::string convert_node4(int root, const imbart_node4* nodes, int n_nodes,
                           const imbart_instance_node* insts, int n_insts,
-                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out);
+                          const imbart_vec4* tris, int n_tri_vec4, HostWideScene& out, int node_width = -1);
+// Node width of the scenes converted from now on: IMBART_NODE_WIDTH or imbart_set_node_width.
+int current_node_width();
 // Decides whether the masks are all opaque and copies them when they are not.
 void attach_masks(HostWideScene& out, const int* indices, int n_indices,
                   const imbart_vec2* texcoords, int n_texcoords,

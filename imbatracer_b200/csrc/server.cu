@@ -1285,8 +1285,9 @@ int imbart_server_add_scene(imbart_server* S, const imbart_scene_source* src) {
         return -IMBART_ERR_INVALID_ARGUMENT;
     }
     auto s = std::make_unique<SceneRec>();
+    // The pool's scenes share one traversal view, so they are all 8-wide.
     const std::string err = convert_node2(src->root, src->nodes, src->n_nodes, src->instances, src->n_instances,
-                                          src->tris, src->n_tri_vec4, s->wide);
+                                          src->tris, src->n_tri_vec4, s->wide, 8);
     if (!err.empty()) {
         set_error(IMBART_ERR_BAD_SCENE, "imbart_server_add_scene: " + err);
         return -IMBART_ERR_BAD_SCENE;

@@ -17,6 +17,7 @@
 
 #include "imbart_internal.h"
 #include "trace_kernel.cuh"
+#include "trace_launch.cuh"
 
 struct imbart_scene {
     int device = 0;
@@ -32,6 +33,9 @@ struct imbart_scene {
     imbart_scene_info info{};
     bool owns_arrays = true;   // false for views into a node pool shared by several scenes
     float grid_share = 1.0f;   // persistent launches use this share of the resident block slots
+    // Top level = one identity instance: its wide root and id (TraceParams::direct_root).
+    int direct_root = -1, direct_inst = -1;
+    imbart_scene() { info.node_width = 8; }   // converted scenes overwrite it
 };
 
 namespace imbart {
@@ -68,6 +72,14 @@ void free_scene(imbart_scene* s) {
     delete s;
 }
 
+// World-to-object rows exactly (1 0 0 0 / 0 1 0 0 / 0 0 1 0).
+bool identity_instance(const WideInst& in) {
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 4; ++c)
+            if (in.m[4 * a + c] != (a == c ? 1.0f : 0.0f)) return false;
+    return true;
+}
+
 imbart_scene* upload_scene(const HostWideScene& h, int device) {
     int prev = 0;
     cudaGetDevice(&prev);
@@ -100,6 +112,11 @@ imbart_scene* upload_scene(const HostWideScene& h, int device) {
     s->info.device_bytes = bytes;
     s->info.root = h.root;
     s->info.masked = h.masked ? 1 : 0;
+    s->info.node_width = h.node_width;
+    if (h.insts.size() == 1 && identity_instance(h.insts[0])) {
+        s->direct_root = h.insts[0].root;
+        s->direct_inst = h.insts[0].id;
+    }
     return s.release();
 }
 
@@ -114,7 +131,7 @@ imbart_scene* prepare(Convert convert, int root, const Node* nodes, int n_nodes,
         return nullptr;
     }
     HostWideScene h;
-    const std::string err = convert(root, nodes, n_nodes, insts, n_insts, tris, n_tri_vec4, h);
+    const std::string err = convert(root, nodes, n_nodes, insts, n_insts, tris, n_tri_vec4, h, -1);
     if (!err.empty()) {
         set_error(IMBART_ERR_BAD_SCENE, "scene preparation: " + err);
         return nullptr;
@@ -208,78 +225,12 @@ int* work_slot(int device) {
     return pool + 2 * slot;
 }
 
-// A traversal launch: kernel, grid, block (the parameters are the TraceParams beside it).
-struct LaunchSpec {
-    const void* func = nullptr;
-    dim3 grid, block;
-};
-
 template <bool kStats>
 const void* simple_kernel(bool any, bool masked) {
     if (any && masked) return (const void*)trace_kernel<true, true, kStats>;
     if (any) return (const void*)trace_kernel<true, false, kStats>;
     if (masked) return (const void*)trace_kernel<false, true, kStats>;
     return (const void*)trace_kernel<false, false, kStats>;
-}
-
-template <typename Kernel>
-int max_grid(Kernel k, int block, int device) {
-    static std::mutex m;
-    static std::map<std::pair<const void*, int>, int> cache;
-    std::lock_guard<std::mutex> lk(m);
-    const auto key = std::make_pair((const void*)k, device);
-    auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
-    int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, 0);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int g = std::max(1, per_sm) * std::max(1, sms);
-    cache[key] = g;
-    return g;
-}
-
-// One persistent block per resident slot (fewer for short queues).
-template <bool kAny, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop = false>
-LaunchSpec persistent_spec(int count, int device, float share, TraceParams& p) {
-    auto k = trace_persistent<kAny, kMasked, kStats, kBlock, kMinBlocks, kSh, kCoop>;
-    const int slots = std::max(1, (int)(max_grid(k, kBlock, device) * share));
-    const int grid = std::min(slots, (count + kBlock - 1) / kBlock);
-    p.total_warps = grid * (kBlock / 32);
-    return {(const void*)k, dim3(grid), dim3(kBlock)};
-}
-
-template <bool kAny, bool kMasked, bool kStats>
-LaunchSpec variant_spec(int variant, int count, int device, float share, TraceParams& p) {
-    switch (variant) {
-        case 1: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16>(count, device, share, p);
-        case 2: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12>(count, device, share, p);
-        case 3: return persistent_spec<kAny, kMasked, kStats, 256, 2, 16>(count, device, share, p);
-        case 4: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12>(count, device, share, p);
-        case 5: return persistent_spec<kAny, kMasked, kStats, 64, 8, 16>(count, device, share, p);
-        case 6: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8>(count, device, share, p);
-        case 7: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10>(count, device, share, p);
-        case 8: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12>(count, device, share, p);
-        case 9: return persistent_spec<kAny, kMasked, kStats, 256, 4, 16>(count, device, share, p);
-        case 10: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12>(count, device, share, p);
-        // Cooperative triangle phase (all lanes test the warp's pending ray/triangle pairs).
-        case 11: return persistent_spec<kAny, kMasked, kStats, 256, 3, 12, true>(count, device, share, p);
-        case 12: return persistent_spec<kAny, kMasked, kStats, 256, 4, 8, true>(count, device, share, p);
-        case 13: return persistent_spec<kAny, kMasked, kStats, 128, 6, 12, true>(count, device, share, p);
-        case 14: return persistent_spec<kAny, kMasked, kStats, 128, 4, 16, true>(count, device, share, p);
-        case 15: return persistent_spec<kAny, kMasked, kStats, 128, 8, 12, true>(count, device, share, p);
-        case 16: return persistent_spec<kAny, kMasked, kStats, 256, 4, 12, true>(count, device, share, p);
-        case 17: return persistent_spec<kAny, kMasked, kStats, 128, 7, 10, true>(count, device, share, p);
-        default: return {};
-    }
-}
-
-template <bool kStats>
-LaunchSpec persistent_kernel_spec(int variant, bool any, bool masked, int count, int device, float share,
-                                  TraceParams& p) {
-    if (any && masked) return variant_spec<true, true, kStats>(variant, count, device, share, p);
-    if (any) return variant_spec<true, false, kStats>(variant, count, device, share, p);
-    if (masked) return variant_spec<false, true, kStats>(variant, count, device, share, p);
-    return variant_spec<false, false, kStats>(variant, count, device, share, p);
 }
 
 // The launch of one traversal query (kernel, grid, block and parameters) under the current
@@ -302,6 +253,8 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
     p.count = count;
     p.roots = roots;
     p.count_ptr = count_ptr;
+    p.direct_root = roots ? -1 : s->direct_root;
+    p.direct_inst = s->direct_inst;
     p.error_flags = s->error_flags;
     p.stats = stats;
     const bool any = (flags & IMBART_TRACE_ANY) != 0;
@@ -326,8 +279,14 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
         // reach the lanes: 0 = each lane loads its pair's triangle, >= 1 = the warp stages
         // the pass's triangles in shared memory.
         p.tri_stage = variant >= kFirstCoopVariant && p.tri_batch > 0 ? 1 : 0;
-        spec = stats ? persistent_kernel_spec<true>(variant, any, masked, count, s->device, s->grid_share, p)
-                     : persistent_kernel_spec<false>(variant, any, masked, count, s->device, s->grid_share, p);
+        // 4-wide scenes take the 4-slot kernels (trace_w4.cu); the 8-slot kernels also trace
+        // them correctly (empty slots never hit), only with twice the box tests.
+        if (s->info.node_width == 4)
+            spec = persistent_kernel_spec_w4(stats != nullptr, variant, any, masked, count, s->device,
+                                             s->grid_share, p);
+        else
+            spec = stats ? persistent_kernel_spec<true, 8>(variant, any, masked, count, s->device, s->grid_share, p)
+                         : persistent_kernel_spec<false, 8>(variant, any, masked, count, s->device, s->grid_share, p);
     }
     if (!spec.func) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_trace: unknown kernel variant");

@@ -58,7 +58,21 @@ struct TraceParams {
     int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
     int tri_batch;                          // triangles a lane tests per loop trip (0: its whole group)
     int tri_stage;                          // cooperative kernels: stage triangles in shared memory
+    // A scene whose top level is one instance with the identity transform: rays with finite
+    // components start in that instance's tree (wide root direct_root, instance id
+    // direct_inst), -1 otherwise. The object-space ray the instance entry would compute,
+    // ((1*x + 0*y) + 0*z) + 0*w per component, is x + 0 for finite inputs (the world ray with
+    // -0 turned into +0), so hits are those of the full walk; the top-level node step, the
+    // instance fetch and the second ray set-up are skipped. Never with per-ray roots.
+    int direct_root;
+    int direct_inst;
 };
+
+// Whether a ray starts in the identity instance's tree (TraceParams::direct_root).
+__device__ __forceinline__ bool direct_start(const TraceParams& p, const float4 ro, const float4 rd) {
+    return p.direct_root >= 0 && isfinite(ro.x) && isfinite(ro.y) && isfinite(ro.z) && isfinite(rd.x) &&
+           isfinite(rd.y) && isfinite(rd.z);
+}
 
 constexpr uint32_t kEntryTri = 3u;      // triangle group (postponed): x = prim base, y = prim mask
 
@@ -160,6 +174,19 @@ __device__ __forceinline__ float xform_row(const float4 m, float x, float y, flo
     return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
 }
 
+// Three-input maximum / minimum (PTX ISA 8.8, sm_100): the values of fmaxf(fmaxf(a, b), c)
+// and fminf(fminf(a, b), c), NaN inputs ignored as fmaxf / fminf ignore them.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // 32768 + (byte k of w) as an exact float, with one byte permute: the byte lands in bits
 // 8..15 of the float 2^15 (0x47000000), whose mantissa step there is 1. The node's origin
 // is stored 32768 quanta low, so this value feeds the slab FMA directly.
@@ -167,8 +194,11 @@ __device__ __forceinline__ float byte_plane(uint32_t w, int k) {
     return __int_as_float(__byte_perm(w, 0x47000000u, 0x7604u | ((uint32_t)k << 4)));
 }
 
-// Intersects the 8 child boxes of a node. Returns internal-child hits in octant order
-// (bit slot^oct) and the triangle/instance hit mask relative to prim_base.
+// Intersects the child boxes of a node: all 8 slots, or slots 0..3 of a 4-wide node
+// (kSlots = 4, whose slots are ordered by the x/y quadrant). Returns internal-child hits in
+// octant order (bit slot ^ (oct & (kSlots - 1))) and the triangle/instance hit mask relative
+// to prim_base.
+template <int kSlots = 8>
 __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node, const SpaceRay& r,
                                                float tmin, float tlimit,
                                                uint32_t& child_base, uint32_t& imask, uint32_t& hits8,
@@ -200,27 +230,29 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
     if (r.iy < 0.0f) { uint32_t t0 = qy.x, t1 = qy.y; qy.x = qy.z; qy.y = qy.w; qy.z = t0; qy.w = t1; }
     if (r.iz < 0.0f) { uint32_t t0 = qz.x, t1 = qz.y; qz.x = qz.z; qz.y = qz.w; qz.z = t0; qz.w = t1; }
     uint32_t hitbits = 0;
+    // Near and far planes of an axis in one packed FMA (the same correctly rounded fmaf per
+    // half), and the slab intervals' ends in three-input min / max: the values of
+    // fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin)) and fminf(fminf(tfx, tfy), tfz).
+    const float2 a2x = make_float2(ax, ax), a2y = make_float2(ay, ay), a2z = make_float2(az, az);
+    const float2 b2x = make_float2(bnx, bfx), b2y = make_float2(bny, bfy), b2z = make_float2(bnz, bfz);
 #pragma unroll
-    for (int s = 0; s < 8; ++s) {
+    for (int s = 0; s < kSlots; ++s) {
         const uint32_t wn_x = s < 4 ? qx.x : qx.y, wf_x = s < 4 ? qx.z : qx.w;
         const uint32_t wn_y = s < 4 ? qy.x : qy.y, wf_y = s < 4 ? qy.z : qy.w;
         const uint32_t wn_z = s < 4 ? qz.x : qz.y, wf_z = s < 4 ? qz.z : qz.w;
         const int k = s & 3;
-        const float tnx = fmaf(byte_plane(wn_x, k), ax, bnx);
-        const float tfx = fmaf(byte_plane(wf_x, k), ax, bfx);
-        const float tny = fmaf(byte_plane(wn_y, k), ay, bny);
-        const float tfy = fmaf(byte_plane(wf_y, k), ay, bfy);
-        const float tnz = fmaf(byte_plane(wn_z, k), az, bnz);
-        const float tfz = fmaf(byte_plane(wf_z, k), az, bfz);
-        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-        const float tf = fminf(fminf(tfx, tfy), tfz) * IMBART_SLACK;
+        const float2 tx = __ffma2_rn(make_float2(byte_plane(wn_x, k), byte_plane(wf_x, k)), a2x, b2x);
+        const float2 ty = __ffma2_rn(make_float2(byte_plane(wn_y, k), byte_plane(wf_y, k)), a2y, b2y);
+        const float2 tz = __ffma2_rn(make_float2(byte_plane(wn_z, k), byte_plane(wf_z, k)), a2z, b2z);
+        const float tn = fmax3(tx.x, ty.x, fmaxf(tz.x, tmin));
+        const float tf = fmin3(tx.y, ty.y, tz.y) * IMBART_SLACK;
         hitbits |= (tn <= fminf(tf, tlimit) ? 1u : 0u) << s;
     }
-    // Internal children, with bit s moved to s ^ oct (three conditional bit-group swaps).
+    // Internal children, with bit s moved to s ^ oct (conditional bit-group swaps).
     uint32_t ib = hitbits & imask;
     if (r.oct & 1u) ib = ((ib & 0x55u) << 1) | ((ib & 0xAAu) >> 1);
     if (r.oct & 2u) ib = ((ib & 0x33u) << 2) | ((ib & 0xCCu) >> 2);
-    if (r.oct & 4u) ib = ((ib & 0x0Fu) << 4) | ((ib & 0xF0u) >> 4);
+    if (kSlots == 8 && (r.oct & 4u)) ib = ((ib & 0x0Fu) << 4) | ((ib & 0xF0u) >> 4);
     hits8 = ib;
     // Leaf children: their primitive runs (count << 5 | offset in the meta byte).
     uint32_t lb = hitbits & ~imask;
@@ -277,20 +309,25 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 
     const bool valid = (tmin <= tmax) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f);
     if (valid) {
+        const bool direct = direct_start(p, ro, rd);
         SpaceRay world;
         world.ox = ro.x; world.oy = ro.y; world.oz = ro.z;
         world.dx = rd.x; world.dy = rd.y; world.dz = rd.z;
+        if (direct) {
+            world.ox = __fadd_rn(ro.x, 0.0f); world.oy = __fadd_rn(ro.y, 0.0f); world.oz = __fadd_rn(ro.z, 0.0f);
+            world.dx = __fadd_rn(rd.x, 0.0f); world.dy = __fadd_rn(rd.y, 0.0f); world.dz = __fadd_rn(rd.z, 0.0f);
+        }
         setup_space(world);
         SpaceRay r = world;
-        bool bottom = false;
-        int cur_inst = -1;
+        bool bottom = direct;
+        int cur_inst = direct ? p.direct_inst : -1;
         float tlimit = best_t * IMBART_SLACK;
 
         uint2 stack[kStackSize];
         int sp = 0;
         // Root group: one internal child in slot 0.
-        uint32_t g_base = (uint32_t)(p.roots ? __ldg(p.roots + ray_index) : p.root), g_imask = 1u,
-                 g_hits = 1u << (0u ^ r.oct);
+        uint32_t g_base = (uint32_t)(direct ? p.direct_root : p.roots ? __ldg(p.roots + ray_index) : p.root),
+                 g_imask = 1u, g_hits = 1u << (0u ^ r.oct);
         uint32_t t_base = 0, t_mask = 0;
         bool done = false;
 
@@ -411,9 +448,10 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 //    (t, triangle id), any-hit queries take the first accepted pair in the group's test
 //    order, so hits and the work counters equal those of the per-lane tests.
 // ---------------------------------------------------------------------------------------
-template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop>
+template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop, int kSlots = 8>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TraceParams p) {
     constexpr unsigned kFull = 0xffffffffu;
+    constexpr uint32_t kOct = kSlots - 1;             // octant bits that order a node's slots
     constexpr int kCW = kCoop ? kBlock / 32 : 1;     // warps with cooperative-phase slots
     __shared__ uint2 sstack[kSh][kBlock];
     __shared__ uint32_t s_key[kCW][32];              // per owner lane: smallest key of a pass
@@ -481,13 +519,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     if (!((tmin <= best_t) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f))) {
                         finish();
                     } else {
+                        const bool direct = direct_start(p, ro, rd);
                         r.ox = ro.x; r.oy = ro.y; r.oz = ro.z;
                         r.dx = rd.x; r.dy = rd.y; r.dz = rd.z;
+                        if (direct) {
+                            r.ox = __fadd_rn(ro.x, 0.0f); r.oy = __fadd_rn(ro.y, 0.0f); r.oz = __fadd_rn(ro.z, 0.0f);
+                            r.dx = __fadd_rn(rd.x, 0.0f); r.dy = __fadd_rn(rd.y, 0.0f); r.dz = __fadd_rn(rd.z, 0.0f);
+                            bottom = true;
+                            cur_inst = p.direct_inst;
+                        }
                         setup_space(r);
                         wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
                         wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
                         tlimit = best_t * IMBART_SLACK;
-                        g_base = (uint32_t)(p.roots ? __ldg(p.roots + ray) : p.root); g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                        g_base = (uint32_t)(direct ? p.direct_root : p.roots ? __ldg(p.roots + ray) : p.root);
+                        g_imask = 1u; g_hits = 1u << (0u ^ (r.oct & kOct));
                         t_mask = 0;
                     }
                 }
@@ -509,14 +555,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
         if (!next && t_mask == 0 && g_hits != 0) {
             const uint32_t bitpos = __ffs(g_hits) - 1;
             g_hits &= g_hits - 1;
-            const uint32_t slot = bitpos ^ r.oct;
+            const uint32_t slot = bitpos ^ (r.oct & kOct);
             const uint32_t idx = g_base + __popc(g_imask & ((1u << slot) - 1u));
             if (g_hits != 0 && !push(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask)) {
                 atomicAdd(p.error_flags, 1);
                 finish();
                 next = true;
             } else {
-                intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+                intersect_node<kSlots>(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
                 if (kStats) st.nodes++;
             }
         }
@@ -588,7 +634,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     setup_space(r);
                     cur_inst = meta.x;
                     bottom = true;
-                    g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ r.oct);
+                    g_base = (uint32_t)meta.y; g_imask = 1u; g_hits = 1u << (0u ^ (r.oct & kOct));
                 }
                 next = true;
             }

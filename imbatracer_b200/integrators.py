@@ -138,6 +138,40 @@ class GpuScene:
         if sd.env_map >= 0:
             N.check(lib.imbart_shading_set_env_map(h, sd.env_map, sd.env_map_intensity), "imbart_shading_set_env_map")
 
+    def autotune_node_width(self, ray_sets, stream=None, widths=(8, 4)) -> dict:
+        """Chooses the node width with the autotuner: the scene is prepared at each width from
+        the same reference-layout arrays, each query class in `ray_sets` ((rays, hits, flags)
+        device tensors) is tuned on it (imbart_trace_autotune, from the same starting
+        configuration), and the width whose tuned kernels trace all classes fastest is kept
+        with its configuration. Call before creating integrators on this scene (they hold
+        its traversal handle). Host-built scenes only."""
+        if self.td is None:
+            raise N.ImbartError("autotune_node_width: the scene was built on the GPU (8-wide only)")
+        start = S.trace_config_snapshot()
+        results, best = {}, None
+        for w in widths:
+            scene = self.trace_scene if self.trace_scene.node_width == w else S.DeviceScene(self.td, self.device,
+                                                                                            node_width=w)
+            S.trace_config_restore(start)
+            classes = {}
+            for rays, hits, flags in ray_sets:
+                classes[flags] = scene.autotune(rays, hits, flags, stream=stream)
+            total = sum(c["ms"] for c in classes.values())
+            results[w] = {"ms": total, "classes": classes, "config": S.trace_config_snapshot()}
+            if best is None or total < results[best[0]]["ms"]:
+                if best is not None and best[1] is not self.trace_scene:
+                    best[1].close()
+                best = (w, scene)
+            elif scene is not self.trace_scene:
+                scene.close()
+        w, scene = best
+        if scene is not self.trace_scene:
+            self.trace_scene.close()
+            self.trace_scene = scene
+        S.trace_config_restore(results[w]["config"])
+        return {"node_width": w, "ms": {k: round(v["ms"], 4) for k, v in results.items()},
+                "classes": results[w]["classes"]}
+
     def close(self):
         if getattr(self, "shading", None):
             N.load().imbart_shading_destroy(self.shading)

@@ -35,7 +35,7 @@ TRACE_COHERENT = 2
 class SceneInfo(C.Structure):
     _fields_ = [("wide_nodes", C.c_int64), ("top_nodes", C.c_int64), ("triangles", C.c_int64),
                 ("instances", C.c_int64), ("device_bytes", C.c_int64), ("root", C.c_int32),
-                ("masked", C.c_int32)]
+                ("masked", C.c_int32), ("node_width", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PtProfile(C.Structure):
@@ -137,6 +137,8 @@ _SIGNATURES = {
     "imbart_scene_from_node4": (P, [I, P, I, P, I, P, I, P, I, P, I, P, I, P, I, I]),
     "imbart_scene_destroy": (None, [P]),
     "imbart_wide_from_node2": (I, [I, P, I, P, I, P, I, P, I, P, I, P, I, P]),
+    "imbart_set_node_width": (I, [I]),
+    "imbart_get_node_width": (I, []),
     "imbart_scene_get_info": (I, [P, C.POINTER(SceneInfo)]),
     "imbart_scene_get_device_arrays": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "imbart_trace": (I, [P, P, P, I, I, P]),

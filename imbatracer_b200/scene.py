@@ -263,6 +263,39 @@ def build_descs(meshes: list[Mesh], instances: list[Instance]):
     return md, idesc, keep
 
 
+def _nbytes(t) -> int:
+    return int(t.numel() * t.element_size()) if hasattr(t, "element_size") else int(t.nbytes)
+
+
+def _check_ray_buffers(rays, hits, n: int, what: str) -> None:
+    """Rays are 32 B and hits 16 B records: the buffers must hold n of each."""
+    if n < 0 or _nbytes(rays) < 32 * n or _nbytes(hits) < 16 * n:
+        raise N.ImbartError(f"{what}: {n} rays need {32 * n} B of rays and {16 * n} B of hits "
+                            f"(have {_nbytes(rays)} and {_nbytes(hits)})")
+
+
+TRACE_CLASSES = (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)
+
+
+def trace_config_snapshot() -> list[tuple[int, int, int, int]]:
+    """The process-wide kernel configuration of the three query classes:
+    (flags, variant, refill lanes, triangle batch) each."""
+    lib = N.load()
+    out = []
+    for flags in TRACE_CLASSES:
+        v, r = C.c_int(0), C.c_int(0)
+        N.check(lib.imbart_get_trace_class(flags, C.byref(v), C.byref(r)), "imbart_get_trace_class")
+        out.append((flags, v.value, r.value, lib.imbart_get_trace_tri_batch(flags)))
+    return out
+
+
+def trace_config_restore(snapshot) -> None:
+    lib = N.load()
+    for flags, v, r, b in snapshot:
+        N.check(lib.imbart_set_trace_class(flags, v, r), "imbart_set_trace_class")
+        N.check(lib.imbart_set_trace_tri_batch(flags, b), "imbart_set_trace_tri_batch")
+
+
 class DeviceScene:
     """A prepared scene resident on one GPU (imbart_scene)."""
 
@@ -287,12 +320,20 @@ class DeviceScene:
         self.build_ms = ms.value
         return self
 
-    def __init__(self, td: TraversalData, device: int = 0):
+    def __init__(self, td: TraversalData, device: int = 0, node_width: int | None = None):
+        """node_width: 8 or 4 for this scene (imbart_set_node_width around the conversion);
+        None keeps the process setting."""
         lib = N.load()
-        h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),
-                                        len(td.instances), N.ptr(td.tris), len(td.tris), N.ptr(td.indices),
-                                        len(td.indices), N.ptr(td.texcoords), len(td.texcoords), N.ptr(td.masks),
-                                        len(td.masks), N.ptr(td.mask_buffer), len(td.mask_buffer), device)
+        prev_width = lib.imbart_get_node_width()
+        if node_width is not None:
+            N.check(lib.imbart_set_node_width(node_width), "imbart_set_node_width")
+        try:
+            h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),
+                                            len(td.instances), N.ptr(td.tris), len(td.tris), N.ptr(td.indices),
+                                            len(td.indices), N.ptr(td.texcoords), len(td.texcoords), N.ptr(td.masks),
+                                            len(td.masks), N.ptr(td.mask_buffer), len(td.mask_buffer), device)
+        finally:
+            lib.imbart_set_node_width(prev_width)
         if not h:
             code, msg = N.last_error()
             raise N.ImbartError(f"imbart_scene_from_node2 failed ({code}): {msg}")
@@ -307,6 +348,7 @@ class DeviceScene:
         """Traces device tensors: rays (N,8) float32, hits (N,4) int32; stream-ordered."""
         lib = N.load()
         n = rays.shape[0] if count is None else count
+        _check_ray_buffers(rays, hits, n, "trace")
         st = None if stream is None else stream.cuda_stream
         flags = N.TRACE_ANY if any_hit else N.TRACE_CLOSEST
         if v_out is None:
@@ -346,10 +388,15 @@ class DeviceScene:
         class `flags` (TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST | TRACE_COHERENT) for these rays."""
         t = N.TraceTuning()
         st = None if stream is None else stream.cuda_stream
+        _check_ray_buffers(rays, hits, rays.shape[0], "autotune")
         N.check(N.load().imbart_trace_autotune(self.handle, N.ptr(rays), N.ptr(hits), rays.shape[0], flags, st,
                                                C.byref(t)), "imbart_trace_autotune")
         return {"variant": t.variant, "refill": t.refill, "tri_batch": t.tri_batch, "ms": t.ms,
                 "default_ms": t.default_ms}
+
+    @property
+    def node_width(self) -> int:
+        return int(self.info.node_width)
 
     def device_arrays(self):
         lib = N.load()

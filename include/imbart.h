@@ -167,10 +167,20 @@ imbart_scene* imbart_scene_from_node4(int root, const imbart_node4* nodes, int n
 
 void imbart_scene_destroy(imbart_scene* scene);
 
-/* Host-only conversion of the two-wide layout into the 8-wide layout, without a GPU (for
- * inspection, byte accounting and tests). Writes up to the given capacities and returns the
- * required sizes in counts[0..3] = {wide nodes, triangles, instances, root}. Call with zero
- * capacities to query the sizes. Returns 0 or an error code. */
+/* Node width of the scenes converted from the reference layouts from now on (process-wide):
+ * 8 (the default), or 4, which fills slots 0..3 of the same 80 B record in x/y-quadrant order
+ * and traverses with a 4-slot kernel. IMBART_NODE_WIDTH in the environment sets the initial
+ * value. Hits never depend on the width; speed does (imbart_trace_autotune measures the
+ * kernel shapes of one prepared scene, so comparing widths means preparing the scene once per
+ * width). Scenes built on the device (imbart_scene_build_gpu) and loaded from .bvh files are
+ * always 8-wide. Returns 0 or IMBART_ERR_INVALID_ARGUMENT. */
+int imbart_set_node_width(int width);
+int imbart_get_node_width(void);
+
+/* Host-only conversion of the two-wide layout into the wide layout, without a GPU (for
+ * inspection, byte accounting and tests), at the current node width. Writes up to the given
+ * capacities and returns the required sizes in counts[0..3] = {wide nodes, triangles,
+ * instances, root}. Call with zero capacities to query the sizes. Returns 0 or an error code. */
 int imbart_wide_from_node2(int root, const imbart_node2* nodes, int n_nodes,
                            const imbart_instance_node* instances, int n_instances,
                            const imbart_vec4* tris, int n_tri_vec4,
@@ -186,6 +196,8 @@ typedef struct {
     int64_t device_bytes;      /* total device memory held */
     int32_t root;              /* wide index of the top-level root */
     int32_t masked;            /* 1 when the alpha-mask test is active */
+    int32_t node_width;        /* children per node: 8, or 4 */
+    int32_t reserved;
 } imbart_scene_info;
 int imbart_scene_get_info(const imbart_scene* scene, imbart_scene_info* out);
 

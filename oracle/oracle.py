@@ -48,7 +48,7 @@ def load() -> C.CDLL:
         sig = {
             "oracle_trace_node2": (None, [I, P, P, P, P, P, P, I, P, P, P, P, I, I, I]),
             "oracle_trace_brute": (None, [P, P, P, P, P, P, I, P, P, P, I, I, I]),
-            "oracle_wide_walk": (None, [P, P, P, I, P, P, P, P, I, I, I]),
+            "oracle_wide_walk": (None, [P, P, P, I, P, P, P, P, I, I, I, I]),
             "oracle_hashgrid_build": (None, [P, I, I, C.c_float, C.c_float, I, C.POINTER(Grid), P, P]),
             "oracle_hashgrid_query": (None, [C.POINTER(Grid), P, P, P, I, P, I, I, P, P, P, I]),
             "oracle_mwc64x": (C.c_uint32, [P]),
@@ -124,7 +124,7 @@ def wide_walk(wnodes, wtris, winsts, root, rays: np.ndarray, any_hit: bool = Fal
     nbytes = np.zeros(len(rays), np.int64)
     counts = np.zeros(3, np.int64)
     load().oracle_wide_walk(_p(wnodes), _p(wtris), _p(winsts), root, _p(rays), _p(hits), _p(nbytes), _p(counts),
-                            len(rays), 1 if any_hit else 0, nthreads or threads())
+                            len(rays), 1 if any_hit else 0, nthreads or threads(), len(winsts))
     return hits, nbytes, counts
 
 

@@ -390,8 +390,25 @@ static void wnode_hit(const o_wnode* n, const wspace_t* r, float tmin, float tli
 }
 
 /* Returns bytes fetched by the GPU kernel for one ray; writes the hit. */
+/* A scene whose top level is a single instance with the identity transform (all 12 matrix
+ * entries exactly 1 or 0): the kernel starts rays with finite components in that instance's
+ * tree directly. The object-space ray it would compute is the world ray with -0 components
+ * turned into +0 (((1*x + 0*y) + 0*z) + 0*w equals x + 0 for finite inputs), so hits are
+ * unchanged; the top-level node step and the instance entry are skipped (counts). */
+static int identity_inst(const o_winst* in) {
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 4; ++c)
+            if (in->m[4 * a + c] != (a == c ? 1.0f : 0.0f)) return 0;
+    return 1;
+}
+
+static int finite6(const o_ray* ray) {
+    return isfinite(ray->org.x) && isfinite(ray->org.y) && isfinite(ray->org.z) && isfinite(ray->dir.x) &&
+           isfinite(ray->dir.y) && isfinite(ray->dir.z);
+}
+
 static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst* insts, int root,
-                        const o_ray* ray, int any, o_hit* hit, int64_t* counts) {
+                        const o_ray* ray, int any, o_hit* hit, int64_t* counts, const o_winst* direct) {
     int64_t bytes = 32 + 16;
     best_t b;
     b.t = ray->dir.w; b.u = 0.0f; b.v = 0.0f; b.tri = -1; b.inst = -1;
@@ -401,6 +418,9 @@ static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst*
         wspace_t world, r;
         world.o[0] = ray->org.x; world.o[1] = ray->org.y; world.o[2] = ray->org.z;
         world.d[0] = ray->dir.x; world.d[1] = ray->dir.y; world.d[2] = ray->dir.z;
+        const int start_direct = direct && finite6(ray);
+        if (start_direct)
+            for (int a = 0; a < 3; ++a) { world.o[a] = world.o[a] + 0.0f; world.d[a] = world.d[a] + 0.0f; }
         wsetup(&world);
         r = world;
         int bottom = 0, cur_inst = -1;
@@ -408,6 +428,7 @@ static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst*
         unsigned stack_x[64], stack_y[64];
         int sp = 0;
         unsigned g_base = (unsigned)root, g_imask = 1u, g_hits = 1u << (0u ^ r.oct);
+        if (start_direct) { bottom = 1; cur_inst = direct->id; g_base = (unsigned)direct->root; }
         unsigned t_base = 0, t_mask = 0;
         int done = 0;
         while (!done) {
@@ -485,13 +506,14 @@ static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst*
  * counts_out (3 int64) accumulates visited nodes, tested triangles and entered instances. */
 void oracle_wide_walk(const o_wnode* nodes, const o_wtri* tris, const o_winst* insts, int root,
                       const o_ray* rays, o_hit* hits, int64_t* bytes_out, int64_t* counts_out,
-                      int count, int any, int threads) {
+                      int count, int any, int threads, int n_insts) {
     if (threads < 1) threads = 1;
+    const o_winst* direct = (n_insts == 1 && identity_inst(insts)) ? insts : 0;
     int64_t c0 = 0, c1 = 0, c2 = 0;
 #pragma omp parallel for schedule(dynamic, 256) num_threads(threads) reduction(+ : c0, c1, c2)
     for (int i = 0; i < count; ++i) {
         int64_t c[3] = {0, 0, 0};
-        bytes_out[i] = wide_one(nodes, tris, insts, root, rays + i, any, hits + i, c);
+        bytes_out[i] = wide_one(nodes, tris, insts, root, rays + i, any, hits + i, c, direct);
         c0 += c[0]; c1 += c[1]; c2 += c[2];
     }
     counts_out[0] += c0; counts_out[1] += c1; counts_out[2] += c2;

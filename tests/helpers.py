@@ -104,17 +104,24 @@ def hits_equal(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return (a.view(np.int32).reshape(-1, 4) == b.view(np.int32).reshape(-1, 4)).all(1)
 
 
-def wide_arrays(td):
-    """Host-side 8-wide conversion of a traversal data set (no GPU)."""
+def wide_arrays(td, node_width=None):
+    """Host-side wide conversion of a traversal data set (no GPU), 8-wide unless node_width
+    says 4."""
     from oracle import oracle as O
     lib = N.load()
-    cnt = np.zeros(4, np.int32)
-    args = (td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances), len(td.instances), N.ptr(td.tris),
-            len(td.tris))
-    N.check(lib.imbart_wide_from_node2(*args, None, 0, None, 0, None, 0, N.ptr(cnt)), "wide")
-    wn = np.zeros(cnt[0], O.WNODE_DTYPE)
-    wt = np.zeros(cnt[1], O.WTRI_DTYPE)
-    wi = np.zeros(cnt[2], O.WINST_DTYPE)
-    N.check(lib.imbart_wide_from_node2(*args, N.ptr(wn), len(wn), N.ptr(wt), len(wt), N.ptr(wi), len(wi),
-                                       N.ptr(cnt)), "wide")
+    prev = lib.imbart_get_node_width()
+    if node_width is not None:
+        N.check(lib.imbart_set_node_width(node_width), "imbart_set_node_width")
+    try:
+        cnt = np.zeros(4, np.int32)
+        args = (td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances), len(td.instances), N.ptr(td.tris),
+                len(td.tris))
+        N.check(lib.imbart_wide_from_node2(*args, None, 0, None, 0, None, 0, N.ptr(cnt)), "wide")
+        wn = np.zeros(cnt[0], O.WNODE_DTYPE)
+        wt = np.zeros(cnt[1], O.WTRI_DTYPE)
+        wi = np.zeros(cnt[2], O.WINST_DTYPE)
+        N.check(lib.imbart_wide_from_node2(*args, N.ptr(wn), len(wn), N.ptr(wt), len(wt), N.ptr(wi), len(wi),
+                                           N.ptr(cnt)), "wide")
+    finally:
+        lib.imbart_set_node_width(prev)
     return wn, wt, wi, int(cnt[3])

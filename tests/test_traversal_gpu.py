@@ -289,6 +289,73 @@ def test_every_kernel_variant_is_exact(cuda):
             lib.imbart_set_trace_tri_batch(flags, b)
 
 
+@pytest.mark.gpu
+def test_four_wide_scene_every_variant_is_exact(cuda):
+    """A scene converted 4-wide runs the 4-slot kernels (every shape, triangle batches 0 and 1)
+    and gives the oracle's closest hits bit for bit, its occlusion answers, and the restated
+    walk's counts over the 4-wide tree."""
+    import ctypes as C
+    lib = N.load()
+    saved = S.trace_config_snapshot()
+    try:
+        td = H.traversal_data("config2")
+        ds = S.DeviceScene(td, node_width=4)
+        assert ds.node_width == 4 and lib.imbart_get_node_width() == 8
+        rays = H.ray_set("config2", 20000, seed=23)
+        ref = O.trace_node2(td, rays)
+        refa = O.trace_node2(td, rays, any_hit=True)
+        wn, wt, wi, root = H.wide_arrays(td, node_width=4)
+        assert ds.info.wide_nodes == len(wn)
+        counts = {a: O.wide_walk(wn, wt, wi, root, rays, any_hit=a)[2] for a in (False, True)}
+        for variant in range(18):
+            for tri_batch in (0, 1):
+                for flags in (N.TRACE_CLOSEST, N.TRACE_ANY):
+                    N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
+                    N.check(lib.imbart_set_trace_tri_batch(flags, tri_batch), "imbart_set_trace_tri_batch")
+                hits, v, _ = run_gpu(ds, rays)
+                assert H.hits_equal(ref, hits).all(), (variant, tri_batch)
+                hitsa, _, _ = run_gpu(ds, rays, any_hit=True)
+                assert np.array_equal(refa["tri_id"] >= 0, hitsa["tri_id"] >= 0), (variant, tri_batch)
+                for a in (False, True):
+                    _, _, st = run_gpu(ds, rays, any_hit=a, stats=True)
+                    assert np.array_equal(st, counts[a]), (variant, tri_batch, a, st, counts[a])
+        assert lib.imbart_scene_error_count(ds.handle) == 0
+        ds.close()
+    finally:
+        S.trace_config_restore(saved)
+
+
+@pytest.mark.gpu
+def test_autotuner_chooses_node_width(cuda):
+    """GpuScene.autotune_node_width prepares the scene at widths 8 and 4, tunes each query class
+    at each, keeps the faster width with its tuned kernels, and the kept scene's hits are the
+    oracle's."""
+    import torch
+    from imbatracer_b200.integrators import GpuScene
+    saved = S.trace_config_snapshot()
+    try:
+        desc = H.scene_desc("config1")
+        gs = GpuScene(desc, td=H.traversal_data("config1"))
+        dev = torch.device("cuda:0")
+        rays = H.ray_set("config1", 50000, seed=31)
+        d_rays = torch.from_numpy(np.ascontiguousarray(rays).view(np.float32).reshape(-1, 8)).to(dev)
+        assert d_rays.shape[0] == len(rays)
+        ray_sets = [(d_rays, torch.zeros((len(rays), 4), dtype=torch.int32, device=dev), f)
+                    for f in (N.TRACE_CLOSEST, N.TRACE_ANY)]
+        # A byte view of the rays is refused on the host (its first dimension is not the count).
+        with pytest.raises(N.ImbartError):
+            gs.trace_scene.autotune(to_dev(rays, torch, dev), ray_sets[0][1], N.TRACE_CLOSEST)
+        out = gs.autotune_node_width(ray_sets)
+        assert out["node_width"] in (4, 8) and set(out["ms"]) == {4, 8}
+        assert out["ms"][out["node_width"]] == min(out["ms"].values())
+        assert gs.trace_scene.node_width == out["node_width"]
+        hits, _, _ = run_gpu(gs.trace_scene, rays)
+        assert H.hits_equal(O.trace_node2(H.traversal_data("config1"), rays), hits).all()
+        gs.close()
+    finally:
+        S.trace_config_restore(saved)
+
+
 @pytest.mark.skipif(not __import__("oracle.refwrap", fromlist=["x"]).imbart_linked_available(),
                     reason="oracle/_ref/libref_imbart.so not built (reference tree absent)")
 @pytest.mark.parametrize("name,w,h,spp,max_len", [("mixed", 96, 64, 4, 6), ("config1", 64, 64, 2, 5)])
