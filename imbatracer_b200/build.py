@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
-SOURCES_CU = ["trace.cu", "trace_w4.cu", "hashgrid.cu", "wavefront.cu", "server.cu", "vcm.cu", "gpu_build.cu"]
+SOURCES_CU = ["trace.cu", "trace_w4.cu", "trace_flat.cu", "hashgrid.cu", "wavefront.cu", "server.cu", "vcm.cu", "gpu_build.cu"]
 SOURCES_CPP = ["builder.cpp", "convert.cpp", "error.cpp", "camera.cpp", "accel_file.cpp"]
 # Shading and sample generation mirror the reference's separately rounded single-precision
 # arithmetic: no fused multiply-add in device code, no contraction in the host camera set-up.

@@ -280,10 +280,14 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
         // the pass's triangles in shared memory.
         p.tri_stage = variant >= kFirstCoopVariant && p.tri_batch > 0 ? 1 : 0;
         // 4-wide scenes take the 4-slot kernels (trace_w4.cu); the 8-slot kernels also trace
-        // them correctly (empty slots never hit), only with twice the box tests.
+        // them correctly (empty slots never hit), only with twice the box tests. Single
+        // identity-instance scenes take the flat kernels (trace_flat.cu).
         if (s->info.node_width == 4)
             spec = persistent_kernel_spec_w4(stats != nullptr, variant, any, masked, count, s->device,
                                              s->grid_share, p);
+        else if (p.direct_root >= 0)
+            spec = persistent_kernel_spec_flat(stats != nullptr, variant, any, masked, count, s->device,
+                                               s->grid_share, p);
         else
             spec = stats ? persistent_kernel_spec<true, 8>(variant, any, masked, count, s->device, s->grid_share, p)
                          : persistent_kernel_spec<false, 8>(variant, any, masked, count, s->device, s->grid_share, p);

@@ -58,21 +58,14 @@ struct TraceParams {
     int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
     int tri_batch;                          // triangles a lane tests per loop trip (0: its whole group)
     int tri_stage;                          // cooperative kernels: stage triangles in shared memory
-    // A scene whose top level is one instance with the identity transform: rays with finite
-    // components start in that instance's tree (wide root direct_root, instance id
-    // direct_inst), -1 otherwise. The object-space ray the instance entry would compute,
-    // ((1*x + 0*y) + 0*z) + 0*w per component, is x + 0 for finite inputs (the world ray with
-    // -0 turned into +0), so hits are those of the full walk; the top-level node step, the
-    // instance fetch and the second ray set-up are skipped. Never with per-ray roots.
+    // A scene whose top level is one instance with the identity transform: rays start in that
+    // instance's tree (wide root direct_root, instance id direct_inst), -1 otherwise. The ray
+    // is transformed by the identity rows with the instance entry's arithmetic, so it is the
+    // object-space ray of the full walk bit for bit and hits are unchanged; the top-level node
+    // step, the instance fetch and the second ray set-up are skipped. Never with per-ray roots.
     int direct_root;
     int direct_inst;
 };
-
-// Whether a ray starts in the identity instance's tree (TraceParams::direct_root).
-__device__ __forceinline__ bool direct_start(const TraceParams& p, const float4 ro, const float4 rd) {
-    return p.direct_root >= 0 && isfinite(ro.x) && isfinite(ro.y) && isfinite(ro.z) && isfinite(rd.x) &&
-           isfinite(rd.y) && isfinite(rd.z);
-}
 
 constexpr uint32_t kEntryTri = 3u;      // triangle group (postponed): x = prim base, y = prim mask
 
@@ -174,6 +167,20 @@ __device__ __forceinline__ float xform_row(const float4 m, float x, float y, flo
     return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m.x, x), __fmul_rn(m.y, y)), __fmul_rn(m.z, z)), __fmul_rn(m.w, w));
 }
 
+// The object-space ray of the identity instance (TraceParams::direct_root): the instance
+// entry's transform with the identity rows (for finite components it is the world ray with
+// -0 turned into +0).
+__device__ __forceinline__ void identity_space(SpaceRay& r, const float4 ro, const float4 rd) {
+    const float4 e0 = make_float4(1.0f, 0.0f, 0.0f, 0.0f), e1 = make_float4(0.0f, 1.0f, 0.0f, 0.0f),
+                 e2 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    r.ox = xform_row(e0, ro.x, ro.y, ro.z, 1.0f);
+    r.oy = xform_row(e1, ro.x, ro.y, ro.z, 1.0f);
+    r.oz = xform_row(e2, ro.x, ro.y, ro.z, 1.0f);
+    r.dx = xform_row(e0, rd.x, rd.y, rd.z, 0.0f);
+    r.dy = xform_row(e1, rd.x, rd.y, rd.z, 0.0f);
+    r.dz = xform_row(e2, rd.x, rd.y, rd.z, 0.0f);
+}
+
 // Three-input maximum / minimum (PTX ISA 8.8, sm_100): the values of fmaxf(fmaxf(a, b), c)
 // and fminf(fminf(a, b), c), NaN inputs ignored as fmaxf / fminf ignore them.
 __device__ __forceinline__ float fmax3(float a, float b, float c) {
@@ -198,7 +205,7 @@ __device__ __forceinline__ float byte_plane(uint32_t w, int k) {
 // (kSlots = 4, whose slots are ordered by the x/y quadrant). Returns internal-child hits in
 // octant order (bit slot ^ (oct & (kSlots - 1))) and the triangle/instance hit mask relative
 // to prim_base.
-template <int kSlots = 8>
+template <int kSlots = 8, bool kPacked = true>
 __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node, const SpaceRay& r,
                                                float tmin, float tlimit,
                                                uint32_t& child_base, uint32_t& imask, uint32_t& hits8,
@@ -230,9 +237,10 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
     if (r.iy < 0.0f) { uint32_t t0 = qy.x, t1 = qy.y; qy.x = qy.z; qy.y = qy.w; qy.z = t0; qy.w = t1; }
     if (r.iz < 0.0f) { uint32_t t0 = qz.x, t1 = qz.y; qz.x = qz.z; qz.y = qz.w; qz.z = t0; qz.w = t1; }
     uint32_t hitbits = 0;
-    // Near and far planes of an axis in one packed FMA (the same correctly rounded fmaf per
-    // half), and the slab intervals' ends in three-input min / max: the values of
-    // fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin)) and fminf(fminf(tfx, tfy), tfz).
+    // kPacked: near and far planes of an axis in one packed FMA (the same correctly rounded
+    // fmaf per half). Either way the slab intervals' ends come from three-input min / max:
+    // the values of fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin)) and fminf(fminf(tfx, tfy), tfz).
+    // (Measured: packed is 2-4 % faster for closest hits, scalar 1-2 % for any hit.)
     const float2 a2x = make_float2(ax, ax), a2y = make_float2(ay, ay), a2z = make_float2(az, az);
     const float2 b2x = make_float2(bnx, bfx), b2y = make_float2(bny, bfy), b2z = make_float2(bnz, bfz);
 #pragma unroll
@@ -241,9 +249,16 @@ __device__ __forceinline__ void intersect_node(const WideNode* __restrict__ node
         const uint32_t wn_y = s < 4 ? qy.x : qy.y, wf_y = s < 4 ? qy.z : qy.w;
         const uint32_t wn_z = s < 4 ? qz.x : qz.y, wf_z = s < 4 ? qz.z : qz.w;
         const int k = s & 3;
-        const float2 tx = __ffma2_rn(make_float2(byte_plane(wn_x, k), byte_plane(wf_x, k)), a2x, b2x);
-        const float2 ty = __ffma2_rn(make_float2(byte_plane(wn_y, k), byte_plane(wf_y, k)), a2y, b2y);
-        const float2 tz = __ffma2_rn(make_float2(byte_plane(wn_z, k), byte_plane(wf_z, k)), a2z, b2z);
+        float2 tx, ty, tz;
+        if (kPacked) {
+            tx = __ffma2_rn(make_float2(byte_plane(wn_x, k), byte_plane(wf_x, k)), a2x, b2x);
+            ty = __ffma2_rn(make_float2(byte_plane(wn_y, k), byte_plane(wf_y, k)), a2y, b2y);
+            tz = __ffma2_rn(make_float2(byte_plane(wn_z, k), byte_plane(wf_z, k)), a2z, b2z);
+        } else {
+            tx = make_float2(fmaf(byte_plane(wn_x, k), ax, bnx), fmaf(byte_plane(wf_x, k), ax, bfx));
+            ty = make_float2(fmaf(byte_plane(wn_y, k), ay, bny), fmaf(byte_plane(wf_y, k), ay, bfy));
+            tz = make_float2(fmaf(byte_plane(wn_z, k), az, bnz), fmaf(byte_plane(wf_z, k), az, bfz));
+        }
         const float tn = fmax3(tx.x, ty.x, fmaxf(tz.x, tmin));
         const float tf = fmin3(tx.y, ty.y, tz.y) * IMBART_SLACK;
         hitbits |= (tn <= fminf(tf, tlimit) ? 1u : 0u) << s;
@@ -309,14 +324,11 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 
     const bool valid = (tmin <= tmax) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f);
     if (valid) {
-        const bool direct = direct_start(p, ro, rd);
+        const bool direct = p.direct_root >= 0;
         SpaceRay world;
         world.ox = ro.x; world.oy = ro.y; world.oz = ro.z;
         world.dx = rd.x; world.dy = rd.y; world.dz = rd.z;
-        if (direct) {
-            world.ox = __fadd_rn(ro.x, 0.0f); world.oy = __fadd_rn(ro.y, 0.0f); world.oz = __fadd_rn(ro.z, 0.0f);
-            world.dx = __fadd_rn(rd.x, 0.0f); world.dy = __fadd_rn(rd.y, 0.0f); world.dz = __fadd_rn(rd.z, 0.0f);
-        }
+        if (direct) identity_space(world, ro, rd);
         setup_space(world);
         SpaceRay r = world;
         bool bottom = direct;
@@ -341,7 +353,7 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
                     if (sp == kStackSize) { atomicAdd(p.error_flags, 1); break; }
                     stack[sp++] = make_uint2(g_base | (kEntryNode << kTypeShift), (g_hits << 8) | g_imask);
                 }
-                intersect_node(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+                intersect_node<8, !kAnyHit>(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
                 if (kStats) st.nodes++;
             }
 
@@ -448,17 +460,24 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 //    (t, triangle id), any-hit queries take the first accepted pair in the group's test
 //    order, so hits and the work counters equal those of the per-lane tests.
 // ---------------------------------------------------------------------------------------
-template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop, int kSlots = 8>
+template <bool kAnyHit, bool kMasked, bool kStats, int kBlock, int kMinBlocks, int kSh, bool kCoop, int kSlots = 8,
+          bool kFlat = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TraceParams p) {
     constexpr unsigned kFull = 0xffffffffu;
     constexpr uint32_t kOct = kSlots - 1;             // octant bits that order a node's slots
+    // kFlat: the launch's scene is one identity instance (p.direct_root >= 0, no per-ray
+    // roots); every ray starts in its tree and never leaves it, so the instance entry and
+    // exit, the saved world ray and the current-instance register are compiled out.
     constexpr int kCW = kCoop ? kBlock / 32 : 1;     // warps with cooperative-phase slots
     __shared__ uint2 sstack[kSh][kBlock];
     __shared__ uint32_t s_key[kCW][32];              // per owner lane: smallest key of a pass
     __shared__ int s_tri[kCW][32];                   // per owner lane: its winning triangle id
     __shared__ float4 s_hit[kCW][32];                // per owner lane: the winner's t, u, v
-    __shared__ int s_idx[kCW][32];                   // staging: triangle index of each pair
-    __shared__ float4 s_tv[kCW][kCoop ? 96 : 1];     // staging: the pass's triangle records
+    // Triangle staging (p.tri_stage) exists in the closest-hit cooperative kernels only: in
+    // the any-hit ones the buffer's shared memory measured worth more as L1 (+3 % shadow rays).
+    constexpr bool kStage = kCoop && !kAnyHit;
+    __shared__ int s_idx[kStage ? kCW : 1][32];      // staging: triangle index of each pair
+    __shared__ float4 s_tv[kStage ? kCW : 1][kStage ? 96 : 1];   // staging: the pass's triangle records
     uint2 lstack[kStackSize - kSh];
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -489,7 +508,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     auto finish = [&]() {
         int4 h;
         h.x = best_tri;
-        h.y = best_tri >= 0 ? best_inst : -1;
+        h.y = best_tri >= 0 ? (kFlat ? p.direct_inst : best_inst) : -1;
         h.z = __float_as_int(best_t);
         h.w = __float_as_int(best_tri >= 0 ? best_u : 0.0f);
         p.hits[ray] = h;
@@ -519,18 +538,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     if (!((tmin <= best_t) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f))) {
                         finish();
                     } else {
-                        const bool direct = direct_start(p, ro, rd);
+                        const bool direct = kFlat || p.direct_root >= 0;
                         r.ox = ro.x; r.oy = ro.y; r.oz = ro.z;
                         r.dx = rd.x; r.dy = rd.y; r.dz = rd.z;
                         if (direct) {
-                            r.ox = __fadd_rn(ro.x, 0.0f); r.oy = __fadd_rn(ro.y, 0.0f); r.oz = __fadd_rn(ro.z, 0.0f);
-                            r.dx = __fadd_rn(rd.x, 0.0f); r.dy = __fadd_rn(rd.y, 0.0f); r.dz = __fadd_rn(rd.z, 0.0f);
+                            identity_space(r, ro, rd);
                             bottom = true;
                             cur_inst = p.direct_inst;
                         }
                         setup_space(r);
-                        wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
-                        wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
+                        if (!kFlat) {
+                            wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
+                            wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
+                        }
                         tlimit = best_t * IMBART_SLACK;
                         g_base = (uint32_t)(direct ? p.direct_root : p.roots ? __ldg(p.roots + ray) : p.root);
                         g_imask = 1u; g_hits = 1u << (0u ^ (r.oct & kOct));
@@ -562,14 +582,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                 finish();
                 next = true;
             } else {
-                intersect_node<kSlots>(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
+                intersect_node<kSlots, !kAnyHit>(p.nodes + idx, r, tmin, tlimit, g_base, g_imask, g_hits, t_base, t_mask);
                 if (kStats) st.nodes++;
             }
         }
 
         // Primitive step: instance entry, and per-lane triangle tests.
         if (!next && t_mask != 0) {
-            if (bottom) {
+            if (kFlat || bottom) {
                 if (!kCoop) {
                     bool stop = false;
                     int tested = 0;
@@ -598,8 +618,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                         if (!(t >= tmin)) continue;
                         const int tri = __float_as_int(a.w);
                         const bool closer = (t < best_t) ||
-                            (t == best_t && (best_tri < 0 || cur_inst < best_inst ||
-                                             (cur_inst == best_inst && tri < best_tri)));
+                            (t == best_t && (kFlat ? (best_tri < 0 || tri < best_tri)
+                                                   : (best_tri < 0 || cur_inst < best_inst ||
+                                                      (cur_inst == best_inst && tri < best_tri))));
                         if (!closer) continue;
                         if (kMasked && !mask_opaque(p, tri, u, v)) continue;
                         best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
@@ -642,7 +663,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
 
         // Cooperative triangle phase (every lane of the warp takes part).
         if (kCoop) {
-            const bool want = !next && bottom && t_mask != 0;
+            const bool want = !next && (kFlat || bottom) && t_mask != 0;
             if (__ballot_sync(kFull, want) != 0u) {
                 const int w = tid >> 5;
                 const int cnt = want ? __popc(t_mask) : 0;
@@ -683,7 +704,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     const int k = j - o_excl;
                     const int ti = has ? (int)(o_base + nth_set_bit(o_mask, k)) : -1;
                     float4 a, b, c;
-                    if (p.tri_stage) {
+                    if (kStage && p.tri_stage) {
                         // Stage the pass's triangles: lane f loads 16-byte word f, f+32, f+64
                         // of the 32 records, so neighbouring lanes read neighbouring words.
                         s_idx[w][lane] = ti;
@@ -741,8 +762,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                             }
                         } else {
                             const bool closer = (hv.x < best_t) ||
-                                (hv.x == best_t && (best_tri < 0 || cur_inst < best_inst ||
-                                                    (cur_inst == best_inst && tc < best_tri)));
+                                (hv.x == best_t && (kFlat ? (best_tri < 0 || tc < best_tri)
+                                                          : (best_tri < 0 || cur_inst < best_inst ||
+                                                             (cur_inst == best_inst && tc < best_tri))));
                             if (closer) {
                                 best_t = hv.x; best_u = hv.y; best_v = hv.z; best_tri = tc; best_inst = cur_inst;
                                 tlimit = best_t * IMBART_SLACK;
@@ -766,7 +788,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                 --sp;
                 const uint2 e = sp < kSh ? sstack[sp][tid] : lstack[sp - kSh];
                 const uint32_t type = e.x >> kTypeShift;
-                if (type == kEntryMarker) {
+                if (!kFlat && type == kEntryMarker) {
                     r.ox = wox; r.oy = woy; r.oz = woz; r.dx = wdx; r.dy = wdy; r.dz = wdz;
                     r.ix = wix; r.iy = wiy; r.iz = wiz; r.pad = wpad; r.oct = woct;
                     bottom = false; cur_inst = -1;

@@ -391,20 +391,14 @@ static void wnode_hit(const o_wnode* n, const wspace_t* r, float tmin, float tli
 
 /* Returns bytes fetched by the GPU kernel for one ray; writes the hit. */
 /* A scene whose top level is a single instance with the identity transform (all 12 matrix
- * entries exactly 1 or 0): the kernel starts rays with finite components in that instance's
- * tree directly. The object-space ray it would compute is the world ray with -0 components
- * turned into +0 (((1*x + 0*y) + 0*z) + 0*w equals x + 0 for finite inputs), so hits are
- * unchanged; the top-level node step and the instance entry are skipped (counts). */
+ * entries exactly 1 or 0): the kernel starts every ray in that instance's tree directly, with
+ * the object-space ray the instance entry computes, so hits are unchanged; the top-level node
+ * step and the instance entry are skipped (counts). */
 static int identity_inst(const o_winst* in) {
     for (int a = 0; a < 3; ++a)
         for (int c = 0; c < 4; ++c)
             if (in->m[4 * a + c] != (a == c ? 1.0f : 0.0f)) return 0;
     return 1;
-}
-
-static int finite6(const o_ray* ray) {
-    return isfinite(ray->org.x) && isfinite(ray->org.y) && isfinite(ray->org.z) && isfinite(ray->dir.x) &&
-           isfinite(ray->dir.y) && isfinite(ray->dir.z);
 }
 
 static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst* insts, int root,
@@ -418,9 +412,15 @@ static int64_t wide_one(const o_wnode* nodes, const o_wtri* tris, const o_winst*
         wspace_t world, r;
         world.o[0] = ray->org.x; world.o[1] = ray->org.y; world.o[2] = ray->org.z;
         world.d[0] = ray->dir.x; world.d[1] = ray->dir.y; world.d[2] = ray->dir.z;
-        const int start_direct = direct && finite6(ray);
-        if (start_direct)
-            for (int a = 0; a < 3; ++a) { world.o[a] = world.o[a] + 0.0f; world.d[a] = world.d[a] + 0.0f; }
+        const int start_direct = direct != 0;
+        if (start_direct) {
+            const float o0 = world.o[0], o1 = world.o[1], o2 = world.o[2];
+            const float d0 = world.d[0], d1 = world.d[1], d2 = world.d[2];
+            for (int a = 0; a < 3; ++a) {
+                world.o[a] = xform_row(direct->m + 4 * a, o0, o1, o2, 1.0f);
+                world.d[a] = xform_row(direct->m + 4 * a, d0, d1, d2, 0.0f);
+            }
+        }
         wsetup(&world);
         r = world;
         int bottom = 0, cur_inst = -1;
