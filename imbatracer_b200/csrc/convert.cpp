@@ -32,6 +32,13 @@ namespace {
 std::atomic<int> g_node_width{0};
 }  // namespace
 
+bool identity_instance(const WideInst& in) {
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 4; ++c)
+            if (in.m[4 * a + c] != (a == c ? 1.0f : 0.0f)) return false;
+    return true;
+}
+
 int current_node_width() {
     int w = g_node_width.load(std::memory_order_relaxed);
     if (w == 0) {

@@ -231,6 +231,29 @@ __global__ void query_kernel(const float4* __restrict__ sorted, const int* __res
     }
 }
 
+// One warp per query (k <= 32; the search is grid_query_knn_warp): lane i writes entry i.
+__global__ void __launch_bounds__(128) query_warp_kernel(const float4* __restrict__ sorted,
+                                                         const int* __restrict__ ends, const float* __restrict__ prm,
+                                                         uint32_t table, const float* __restrict__ queries, int nq,
+                                                         int k, int* __restrict__ out_ids, int* __restrict__ out_count,
+                                                         float* __restrict__ out_d2) {
+    __shared__ float sp[10];
+    if (threadIdx.x < 10) sp[threadIdx.x] = prm[threadIdx.x];
+    __syncthreads();
+    const long long q = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (q >= nq) return;   // uniform across the warp
+    const int lane = threadIdx.x & 31;
+    const float qx = queries[3 * q + 0], qy = queries[3 * q + 1], qz = queries[3 * q + 2];
+    float my_d;
+    int my_id;
+    const int count = grid_query_knn_warp(sorted, ends, sp, table, qx, qy, qz, k, my_d, my_id);
+    if (lane == 0) out_count[q] = count;
+    if (lane < k) {
+        out_ids[q * k + lane] = lane < count ? my_id : -1;
+        if (out_d2) out_d2[q * k + lane] = lane < count ? my_d : 0.0f;
+    }
+}
+
 // Grid-stride launches over n items: at most 8 blocks per SM of the current device (SM
 // counts cached per device index).
 int grid_for(int n) {
@@ -360,9 +383,16 @@ int imbart_hashgrid_query(const imbart_hashgrid* g, const float* queries, int nq
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(g->device);
-    const int grid = (nq + 127) / 128;
-    query_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(g->sorted, g->cell_ends, g->params, (uint32_t)g->table,
-                                                         queries, nq, k, out_ids, out_counts, out_d2);
+    if (k <= 32) {
+        // One warp per query: coalesced photon loads and the list in registers.
+        const long long grid = ((long long)nq * 32 + 127) / 128;
+        query_warp_kernel<<<(unsigned)grid, 128, 0, (cudaStream_t)stream>>>(
+            g->sorted, g->cell_ends, g->params, (uint32_t)g->table, queries, nq, k, out_ids, out_counts, out_d2);
+    } else {
+        const int grid = (nq + 127) / 128;
+        query_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(g->sorted, g->cell_ends, g->params, (uint32_t)g->table,
+                                                             queries, nq, k, out_ids, out_counts, out_d2);
+    }
     note_launches(1);
     const bool good = ok(cudaGetLastError(), "hash grid query");
     cudaSetDevice(prev);

@@ -60,6 +60,14 @@ struct alignas(16) WideInst {
 };
 static_assert(sizeof(WideInst) == 64, "WideInst must be 64 bytes");
 
+// Per-ray root words (the traversal's per-ray roots) with this bit set name the mesh tree of a
+// scene whose top level is one identity instance of id 0: the ray starts in that tree with the
+// instance entry's transform by the identity. Node indices stay below 2^30.
+constexpr int kDirectRootBit = 1 << 30;
+
+// World-to-object rows exactly (1 0 0 0 / 0 1 0 0 / 0 0 1 0) (convert.cpp).
+bool identity_instance(const WideInst& in);
+
 // Host-side result of converting a reference layout.
 struct HostWideScene {
     std::vector<WideNode> nodes;
@@ -139,7 +147,9 @@ imbart_scene* upload_wide_scene(const HostWideScene& h, int device);
 imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes);
 void scene_pool_view_destroy(imbart_scene* s);
 // Root used by launches without a per-ray root array (single-scene work on the pool).
-void scene_pool_view_set_root(imbart_scene* s, int root);
+// The view's top-level root, and the mesh root and instance id of a top level that is one
+// identity instance (direct_root -1: none).
+void scene_pool_view_set_root(imbart_scene* s, int root, int direct_root = -1, int direct_inst = -1);
 
 // A scene over device arrays built on the GPU; the scene takes ownership (cudaFree on
 // destroy). NULL on error (the arrays are then still the caller's).

@@ -217,7 +217,9 @@ struct SceneRec {
     bool resident = false;
     size_t block = 0;
     int slot = -1;
-    int root = 0;
+    int root = 0;                 // top-level root in the pool
+    int start_root = 0;           // per-ray root word: root, or the mesh root | kDirectRootBit
+    int direct_root = -1;         // mesh root of a top level that is one identity instance of id 0
     long long last_used = 0;
     int refs = 0;
     // Plain mode.
@@ -528,6 +530,10 @@ int make_resident_locked(imbart_server* S, SceneRec& s) {
     s.block = block;
     s.slot = slot;
     s.root = s.wide.root + (int)node_off;
+    // A top level that is one identity instance of id 0: rays start in the mesh tree.
+    const bool direct = s.wide.insts.size() == 1 && s.wide.insts[0].id == 0 && identity_instance(s.wide.insts[0]);
+    s.direct_root = direct ? s.wide.insts[0].root + (int)node_off : -1;
+    s.start_root = direct ? (s.direct_root | kDirectRootBit) : s.root;
     S->stats.scene_uploads += 1;
     return 0;
 }
@@ -611,7 +617,7 @@ void admit(imbart_server* S) {
             std::memcpy(d.pos, r->rr.cam_pos, sizeof(d.pos));
             d.width = r->rr.width; d.height = r->rr.height; d.spp = r->rr.spp;
             d.max_path_len = r->rr.max_path_len; d.rr_start = r->rr.rr_start;
-            d.scene_slot = s.slot; d.root = s.root;
+            d.scene_slot = s.slot; d.root = s.start_root;
             d.seed_base = r->rr.seed_base;
             d.image = reinterpret_cast<float*>(S->pool + off);
             if (!cuda_check(cudaMemsetAsync(d.image, 0, bytes, S->stream), "cudaMemsetAsync") ||
@@ -820,7 +826,7 @@ bool batched_wave(imbart_server* S) {
         int n_runs = 0;
         for (const BatchPiece& p : pieces) {
             good = good && copy_rays_in(S, p);
-            S->h_runs[n_runs++] = RootRun{p.dst, S->scenes[p.r->scene]->root};
+            S->h_runs[n_runs++] = RootRun{p.dst, S->scenes[p.r->scene]->start_root};
         }
         const int nb = n_bc + n_ba;
         good = good &&
@@ -956,7 +962,7 @@ void vcm_lane_main(imbart_server* S, int index) {
         SceneRec& s = *S->scenes[r->scene];
         // The lane's stream waits for the upload and the image clear on the worker stream.
         if (r->ready) cudaStreamWaitEvent(lane.stream, r->ready, 0);
-        scene_pool_view_set_root(lane.view, s.root);
+        scene_pool_view_set_root(lane.view, s.root, s.direct_root, s.direct_root >= 0 ? 0 : -1);
         imbart_shading sh;
         sh.device = S->device;
         sh.s = S->h_scenes[s.slot];

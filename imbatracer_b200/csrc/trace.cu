@@ -72,14 +72,6 @@ void free_scene(imbart_scene* s) {
     delete s;
 }
 
-// World-to-object rows exactly (1 0 0 0 / 0 1 0 0 / 0 0 1 0).
-bool identity_instance(const WideInst& in) {
-    for (int a = 0; a < 3; ++a)
-        for (int c = 0; c < 4; ++c)
-            if (in.m[4 * a + c] != (a == c ? 1.0f : 0.0f)) return false;
-    return true;
-}
-
 imbart_scene* upload_scene(const HostWideScene& h, int device) {
     int prev = 0;
     cudaGetDevice(&prev);
@@ -535,7 +527,11 @@ imbart_scene* scene_pool_view(int device, const void* pool, size_t pool_bytes) {
 
 void scene_pool_view_destroy(imbart_scene* s) { free_scene(s); }
 
-void scene_pool_view_set_root(imbart_scene* s, int root) { s->info.root = root; }
+void scene_pool_view_set_root(imbart_scene* s, int root, int direct_root, int direct_inst) {
+    s->info.root = root;
+    s->direct_root = direct_root;
+    s->direct_inst = direct_inst;
+}
 
 imbart_scene* scene_adopt_device_arrays(int device, WideNode* nodes, int64_t n_nodes, int64_t top_nodes,
                                         WideTri* tris, int64_t n_tris, WideInst* insts, int64_t n_insts, int root) {

@@ -45,7 +45,7 @@ struct TraceParams {
     float* __restrict__ v_out;              // optional
     int count;
     // Batches over several scenes of one node pool: ray i starts at node roots[i] instead of
-    // `root`. With count_ptr set, the ray count is read from device memory at kernel start
+    // `root` (with kDirectRootBit: in that mesh tree, as instance 0). With count_ptr set, the ray count is read from device memory at kernel start
     // (`count` is then an upper bound the launch was sized for).
     const int* __restrict__ roots;
     const int* __restrict__ count_ptr;
@@ -324,7 +324,8 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 
     const bool valid = (tmin <= tmax) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f);
     if (valid) {
-        const bool direct = p.direct_root >= 0;
+        const int root_word = p.roots ? __ldg(p.roots + ray_index) : p.root;
+        const bool direct = p.roots ? (root_word & kDirectRootBit) != 0 : p.direct_root >= 0;
         SpaceRay world;
         world.ox = ro.x; world.oy = ro.y; world.oz = ro.z;
         world.dx = rd.x; world.dy = rd.y; world.dz = rd.z;
@@ -332,13 +333,13 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
         setup_space(world);
         SpaceRay r = world;
         bool bottom = direct;
-        int cur_inst = direct ? p.direct_inst : -1;
+        int cur_inst = direct ? (p.roots ? 0 : p.direct_inst) : -1;
         float tlimit = best_t * IMBART_SLACK;
 
         uint2 stack[kStackSize];
         int sp = 0;
         // Root group: one internal child in slot 0.
-        uint32_t g_base = (uint32_t)(direct ? p.direct_root : p.roots ? __ldg(p.roots + ray_index) : p.root),
+        uint32_t g_base = (uint32_t)(p.roots ? (root_word & ~kDirectRootBit) : direct ? p.direct_root : p.root),
                  g_imask = 1u, g_hits = 1u << (0u ^ r.oct);
         uint32_t t_base = 0, t_mask = 0;
         bool done = false;
@@ -538,13 +539,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     if (!((tmin <= best_t) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f))) {
                         finish();
                     } else {
-                        const bool direct = kFlat || p.direct_root >= 0;
+                        const int root_word = (!kFlat && p.roots) ? __ldg(p.roots + ray) : p.root;
+                        const bool direct = kFlat || (p.roots ? (root_word & kDirectRootBit) != 0 : p.direct_root >= 0);
                         r.ox = ro.x; r.oy = ro.y; r.oz = ro.z;
                         r.dx = rd.x; r.dy = rd.y; r.dz = rd.z;
                         if (direct) {
                             identity_space(r, ro, rd);
                             bottom = true;
-                            cur_inst = p.direct_inst;
+                            cur_inst = (!kFlat && p.roots) ? 0 : p.direct_inst;
                         }
                         setup_space(r);
                         if (!kFlat) {
@@ -552,7 +554,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                             wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
                         }
                         tlimit = best_t * IMBART_SLACK;
-                        g_base = (uint32_t)(direct ? p.direct_root : p.roots ? __ldg(p.roots + ray) : p.root);
+                        g_base = (uint32_t)((!kFlat && p.roots) ? (root_word & ~kDirectRootBit)
+                                                                : direct ? p.direct_root : p.root);
                         g_imask = 1u; g_hits = 1u << (0u ^ (r.oct & kOct));
                         t_mask = 0;
                     }

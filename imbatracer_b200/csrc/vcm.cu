@@ -573,13 +573,10 @@ __global__ void __launch_bounds__(128) vcm_merge_kernel(VcmParams p, const int* 
     add_image(p.image, __float_as_int(m0.w), vcm_merge(p, v3(m6), m2.w, m3.w, is, bsdf));
 }
 
-// Vertex merging with one warp per queued camera vertex (k <= 32). The 32 lanes scan each of
-// the 8 buckets together, in the reference's order; photons inside the radius are inserted in
-// scan order into a k-nearest list held one entry per lane, with the reference's insertion
-// rule (after every kept photon at distance <= d2; when the list is full the last entry
-// leaves first). Equal distances are then ordered by photon index, the found photons are
-// evaluated one per lane, and their contributions are summed in list order, so the result
-// equals the per-thread query's.
+// Vertex merging with one warp per queued camera vertex (k <= 32): the warp's k-nearest
+// search (grid_query_knn_warp, one list entry per lane), the found photons evaluated one per
+// lane, and their contributions summed in list order, so the result equals the per-thread
+// query's.
 __global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const int* count_ptr, const float4* recs) {
     const int lane = threadIdx.x & 31;
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -591,87 +588,9 @@ __global__ void __launch_bounds__(128) vcm_merge_warp_kernel(VcmParams p, const 
 #pragma unroll
     for (int k = 0; k < 10; ++k) prm[k] = __ldg(p.grid_params + k);
     const int k = p.num_knn;
-    float my_d = 0.0f;      // list entry `lane`
-    int my_id = -1;
-    int count = 0;
-    GridCells gc;
-    if (grid_cells(prm, qx, qy, qz, gc)) {
-        const float r2 = prm[7];
-        // Lane j of a chunk computes cell (chunk + j)'s bucket; in range mode buckets met
-        // before (lower lane or the previous chunk) are dropped, so each is scanned once.
-        int prev_bucket = -1;
-        for (int c0 = 0; c0 < gc.n; c0 += 32) {
-            const int jj = c0 + lane;
-            const int my_bucket = jj < gc.n ? grid_cell_bucket(gc, jj, p.grid_table) : -2 - lane;
-            bool seen = false;
-            if (!gc.ref_mode) {
-                const unsigned same = __match_any_sync(0xffffffffu, my_bucket);
-                seen = (same & ((1u << lane) - 1u)) != 0u;
-                if (c0 > 0)
-                    for (int l = 0; l < 32; ++l) seen |= __shfl_sync(0xffffffffu, prev_bucket, l) == my_bucket;
-            }
-            unsigned todo = __ballot_sync(0xffffffffu, jj < gc.n && !seen);
-            prev_bucket = my_bucket;
-            while (todo) {
-                const int cl = __ffs(todo) - 1;
-                todo &= todo - 1;
-                const int c = __shfl_sync(0xffffffffu, my_bucket, cl);
-                const int b = c == 0 ? 0 : __ldg(p.grid_ends + c - 1);
-                const int e = __ldg(p.grid_ends + c);
-                for (int base = b; base < e; base += 32) {
-                    const int s = base + lane;
-                    float d2 = 0.0f;
-                    int id = -1;
-                    bool within = false;
-                    if (s < e) {
-                        const float4 ph = __ldg(p.grid_sorted + s);
-                        const float dx = __fsub_rn(qx, ph.x), dy = __fsub_rn(qy, ph.y), dz = __fsub_rn(qz, ph.z);
-                        d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                        id = __float_as_int(ph.w);
-                        within = d2 <= r2;
-                    }
-                    unsigned cand = __ballot_sync(0xffffffffu, within);
-                    while (cand) {
-                        const int src = __ffs(cand) - 1;
-                        cand &= cand - 1;
-                        const float cd = __shfl_sync(0xffffffffu, d2, src);
-                        const int cid = __shfl_sync(0xffffffffu, id, src);
-                        int kept;
-                        if (count == k) {
-                            const float last = __shfl_sync(0xffffffffu, my_d, k - 1);
-                            if (last < cd) continue;
-                            kept = k - 1;
-                        } else {
-                            kept = count;
-                            count++;
-                        }
-                        const int pos = __popc(__ballot_sync(0xffffffffu, lane < kept && my_d <= cd));
-                        const float up_d = __shfl_up_sync(0xffffffffu, my_d, 1);
-                        const int up_id = __shfl_up_sync(0xffffffffu, my_id, 1);
-                        if (lane > pos && lane <= kept) { my_d = up_d; my_id = up_id; }
-                        if (lane == pos) { my_d = cd; my_id = cid; }
-                    }
-                }
-            }
-        }
-        // Equal distances by photon index (odd-even transposition over adjacent equal pairs).
-        const float next_d = __shfl_down_sync(0xffffffffu, my_d, 1);
-        const unsigned ties = __ballot_sync(0xffffffffu, lane + 1 < count && my_d == next_d);
-        if (ties) {
-            for (int pass = 0; pass < count; ++pass) {
-                const float nd = __shfl_down_sync(0xffffffffu, my_d, 1);
-                const int nid = __shfl_down_sync(0xffffffffu, my_id, 1);
-                const float pd = __shfl_up_sync(0xffffffffu, my_d, 1);
-                const int pid = __shfl_up_sync(0xffffffffu, my_id, 1);
-                const bool left = ((lane & 1) == (pass & 1));   // this lane is the left of its pair
-                if (left) {
-                    if (lane + 1 < count && my_d == nd && my_id > nid) my_id = nid;
-                } else if (lane >= 1 && lane < count) {
-                    if (pd == my_d && pid > my_id) my_id = pid;
-                }
-            }
-        }
-    }
+    float my_d;               // list entry `lane`
+    int my_id;
+    const int count = grid_query_knn_warp(p.grid_sorted, p.grid_ends, prm, p.grid_table, qx, qy, qz, k, my_d, my_id);
     if (count == 0) return;
     // Evaluate the found photons, one per lane.
     const V3 pos(qx, qy, qz), out_dir = v3(m1), thr = v3(m6);
