@@ -206,7 +206,9 @@ def config3_roofline(torch, dev, stream, peak):
            "closest_mrays_s": round(work.closest_rays / max(prof.closest_ms, 1e-9) / 1e3, 1),
            "bytes_per_ray": round(trace_bytes(work.closest_rays, work.closest_work) / max(work.closest_rays, 1), 1),
            "launches": int(prof.closest_launches), "node_width": nw["node_width"],
-           "node_width_tuned_ms": {str(k): v for k, v in nw["ms"].items()}}
+           "node_width_tuned_ms": {str(k): v for k, v in nw["ms"].items()},
+           "tuned": {name: {"variant": t["variant"], "refill": t["refill"]}
+                     for name, t in zip(("camera", "bounce", "shadow"), (nw["classes"][f] for f in classes))}}
     pt.close()
     for flags, v, r, b in saved:   # the main frame's tuning again for what follows
         lib.imbart_set_trace_class(flags, v, r)
@@ -747,7 +749,7 @@ def run_vcm_spec(iterations=64, warmup=2, algos=("vcm", "ppm")):
                        "queries": int(pos.shape[0]), "query_ms": round(e1.elapsed_time(e2), 3),
                        "mqueries_s": round(pos.shape[0] / (e1.elapsed_time(e2) * 1e-3) / 1e6, 1),
                        "note": "cell = r, 2^22 buckets, r of the last iteration; k = 10 nearest within r at "
-                               "every light vertex (batched query API, one thread per query)"}
+                               "every light vertex (batched query API, one warp per query)"}
         grid.close()
     return out
 
@@ -874,25 +876,41 @@ def run_serving(scenes=None, config5_rates=(150.0, 400.0), config5_s=3.0, satura
 
 
 def config5_saturation(scenes, ray_buf, hit_buf, p99_bound_ms=100.0, duration_s=1.5, start=200.0, step=1.5,
-                       top=4000.0):
+                       top=4000.0, bisections=3):
     """The highest Poisson arrival rate of the config-5 mix each arm sustains: rates grow by
     `step` from `start` while the arm serves at least 95 % of the offered rate with p99
-    latency within the bound; the last rate that passed is the arm's sustained rate."""
+    latency within the bound; then `bisections` geometric midpoints between the last rate that
+    passed and the first that failed narrow the bracket. The highest rate that passed is the
+    arm's sustained rate."""
     from imbatracer_b200 import scenegen as G
     out = {"p99_bound_ms": p99_bound_ms, "seconds_per_rate": duration_s,
            "rule": "sustained = served >= 0.95 x offered and p99 <= bound"}
     for mode in ("plain", "batched"):
-        rate, best, tried = start, None, []
-        while rate <= top:
+        rate, best, tried, failed = start, None, [], None
+
+        def attempt(rate):
             jobs = G.config5_requests(seed=int(rate), rate=rate, duration_s=duration_s)
             r = serve_arm(mode, scenes, jobs, open_loop=True, ray_buf=ray_buf, hit_buf=hit_buf)
             ok = r["requests_per_s"] >= 0.95 * rate and r["p99_ms"] <= p99_bound_ms
             tried.append({"rate": round(rate, 1), "served": r["requests_per_s"], "p99_ms": r["p99_ms"],
                           "p50_ms": r["p50_ms"], "sustained": ok})
+            return r, ok
+
+        while rate <= top:
+            r, ok = attempt(rate)
             if not ok:
+                failed = rate
                 break
             best = r | {"rate": round(rate, 1)}
             rate *= step
+        lo = best["rate"] if best else None
+        for _ in range(bisections if (lo and failed) else 0):
+            mid = (lo * failed) ** 0.5
+            r, ok = attempt(mid)
+            if ok:
+                best, lo = r | {"rate": round(mid, 1)}, mid
+            else:
+                failed = mid
         out[mode] = {"sustained_rate_per_s": best["rate"] if best else None,
                      "requests_per_s": best["requests_per_s"] if best else None,
                      "p99_ms": best["p99_ms"] if best else None, "sweep": tried}
