@@ -150,10 +150,9 @@ constexpr int kFirstCoopVariant = 11; // 11..17: the shapes with the cooperative
 // Each class also keeps its triangle batch: in the per-lane shapes, the triangles a lane
 // tests per loop trip before the lanes with node work take their next node step (0: the
 // whole group at once; two measured best there: secondary rays +13 %, camera rays +7 % over
-// 0); in the cooperative shapes, 0 = lanes load their pairs' triangles, >= 1 = staged.
-// Defaults: the cooperative 256 x 3 shape with lane loads for every class (on the frame's
-// ray sets of the instanced scene: camera / secondary / shadow rays +2 / +9 / +10 % over
-// the best per-lane shapes; staging measured 5 % slower).
+// 0); the cooperative shapes ignore it. Defaults: the cooperative 256 x 3 shape for every
+// class (on the frame's ray sets of the instanced scene: camera / secondary / shadow rays
+// +2 / +9 / +10 % over the best per-lane shapes).
 struct TraceConfig {
     int variant, refill, postpone, variant_any;
     int refill_any, variant_coh, refill_coh;
@@ -267,10 +266,6 @@ bool trace_spec(const imbart_scene* s, const imbart_ray* rays, imbart_hit* hits,
         p.refill_lanes = std::min(std::max(refill, 1), 32);
         p.postpone_lanes = std::min(std::max(cfg.postpone, 0), 32);
         p.tri_batch = std::max(any ? cfg.tri_batch_any : coherent ? cfg.tri_batch_coh : cfg.tri_batch, 0);
-        // In the cooperative shapes the class's triangle-batch setting selects how triangles
-        // reach the lanes: 0 = each lane loads its pair's triangle, >= 1 = the warp stages
-        // the pass's triangles in shared memory.
-        p.tri_stage = variant >= kFirstCoopVariant && p.tri_batch > 0 ? 1 : 0;
         // 4-wide scenes take the 4-slot kernels (trace_w4.cu); the 8-slot kernels also trace
         // them correctly (empty slots never hit), only with twice the box tests. Single
         // identity-instance scenes take the flat kernels (trace_flat.cu).
@@ -775,7 +770,7 @@ int imbart_trace_autotune(const imbart_scene* scene, const imbart_ray* rays, imb
     static const int kTriBatches[] = {0, 1, 2, 3, 4};
     for (int b : kTriBatches) {
         if (rc || b == b0) continue;
-        if (best_v >= kFirstCoopVariant && b > 1) continue;   // cooperative shapes: 0 or 1 (staged)
+        if (best_v >= kFirstCoopVariant && b > 0) continue;   // the cooperative shapes ignore it
         imbart_set_trace_tri_batch(flags, b);
         float ms = 0.0f;
         rc = time_config(best_v, best_r, &ms);

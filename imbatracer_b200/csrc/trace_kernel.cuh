@@ -56,8 +56,8 @@ struct TraceParams {
     int total_warps;                        // warps in the launch
     int refill_lanes;                       // refill a warp's idle lanes once this many are idle
     int postpone_lanes;                     // postpone triangle tests while fewer lanes would test
-    int tri_batch;                          // triangles a lane tests per loop trip (0: its whole group)
-    int tri_stage;                          // cooperative kernels: stage triangles in shared memory
+    int tri_batch;                          // per-lane kernels: triangles a lane tests per loop trip
+                                            // (0: its whole group); the cooperative ones ignore it
     // A scene whose top level is one instance with the identity transform: rays start in that
     // instance's tree (wide root direct_root, instance id direct_inst), -1 otherwise. The ray
     // is transformed by the identity rows with the instance entry's arithmetic, so it is the
@@ -455,9 +455,10 @@ __device__ __forceinline__ void trace_one(const TraceParams& p, int ray_index, R
 //    postpone_lanes/32 of the live lanes would test triangles together;
 //  * cooperatively (kCoop true): after the node step, the warp lists every (ray, triangle)
 //    pair its lanes' triangle groups hold and all 32 lanes — idle and finished ones included —
-//    test 32 pairs per pass, reading the owning lane's ray through shuffles. With `tri_stage`
-//    the pass's triangle records are first staged in shared memory by coalesced 16-byte warp
-//    loads. Each owner's closest candidate is found by shared-memory atomic minima over
+//    test 32 pairs per pass, reading the owning lane's ray through shuffles and loading the
+//    pair's triangle itself (staging a pass's triangles in shared memory with coalesced warp
+//    loads measured slower: the records hit in L1/L2, and the buffer's shared memory is worth
+//    more as L1). Each owner's closest candidate is found by shared-memory atomic minima over
 //    (t, triangle id), any-hit queries take the first accepted pair in the group's test
 //    order, so hits and the work counters equal those of the per-lane tests.
 // ---------------------------------------------------------------------------------------
@@ -474,11 +475,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     __shared__ uint32_t s_key[kCW][32];              // per owner lane: smallest key of a pass
     __shared__ int s_tri[kCW][32];                   // per owner lane: its winning triangle id
     __shared__ float4 s_hit[kCW][32];                // per owner lane: the winner's t, u, v
-    // Triangle staging (p.tri_stage) exists in the closest-hit cooperative kernels only: in
-    // the any-hit ones the buffer's shared memory measured worth more as L1 (+3 % shadow rays).
-    constexpr bool kStage = kCoop && !kAnyHit;
-    __shared__ int s_idx[kStage ? kCW : 1][32];      // staging: triangle index of each pair
-    __shared__ float4 s_tv[kStage ? kCW : 1][kStage ? 96 : 1];   // staging: the pass's triangle records
+    // The world ray (origin, direction, inverse direction, pad, octant), restored when a ray
+    // leaves an instance: kept in shared memory rather than registers (11 registers fewer;
+    // measured +4-6 % on the instanced scene's ray sets). Flat kernels never leave the tree.
+    __shared__ float s_world[kFlat ? 1 : 11][kFlat ? 1 : kBlock];
     uint2 lstack[kStackSize - kSh];
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -486,8 +486,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
 
     int ray = -1;                       // -1: idle (wants a ray), >= count: queue exhausted
     SpaceRay r;                         // current space (world or instance)
-    float wox = 0, woy = 0, woz = 0, wdx = 0, wdy = 0, wdz = 0, wix = 0, wiy = 0, wiz = 0, wpad = 0;
-    uint32_t woct = 0;
     float tmin = 0.0f, best_t = 0.0f, best_u = 0.0f, best_v = 0.0f, tlimit = 0.0f;
     int best_tri = -1, best_inst = -1, cur_inst = -1;
     bool bottom = false;
@@ -550,8 +548,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                         }
                         setup_space(r);
                         if (!kFlat) {
-                            wox = r.ox; woy = r.oy; woz = r.oz; wdx = r.dx; wdy = r.dy; wdz = r.dz;
-                            wix = r.ix; wiy = r.iy; wiz = r.iz; wpad = r.pad; woct = r.oct;
+                            s_world[0][tid] = r.ox; s_world[1][tid] = r.oy; s_world[2][tid] = r.oz;
+                            s_world[3][tid] = r.dx; s_world[4][tid] = r.dy; s_world[5][tid] = r.dz;
+                            s_world[6][tid] = r.ix; s_world[7][tid] = r.iy; s_world[8][tid] = r.iz;
+                            s_world[9][tid] = r.pad; s_world[10][tid] = __uint_as_float(r.oct);
                         }
                         tlimit = best_t * IMBART_SLACK;
                         g_base = (uint32_t)((!kFlat && p.roots) ? (root_word & ~kDirectRootBit)
@@ -649,12 +649,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
                     const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
                     if (kStats) st.insts++;
-                    r.ox = xform_row(m0, wox, woy, woz, 1.0f);
-                    r.oy = xform_row(m1, wox, woy, woz, 1.0f);
-                    r.oz = xform_row(m2, wox, woy, woz, 1.0f);
-                    r.dx = xform_row(m0, wdx, wdy, wdz, 0.0f);
-                    r.dy = xform_row(m1, wdx, wdy, wdz, 0.0f);
-                    r.dz = xform_row(m2, wdx, wdy, wdz, 0.0f);
+                    const float wx = r.ox, wy = r.oy, wz = r.oz, vx = r.dx, vy = r.dy, vz = r.dz;
+                    r.ox = xform_row(m0, wx, wy, wz, 1.0f);
+                    r.oy = xform_row(m1, wx, wy, wz, 1.0f);
+                    r.oz = xform_row(m2, wx, wy, wz, 1.0f);
+                    r.dx = xform_row(m0, vx, vy, vz, 0.0f);
+                    r.dy = xform_row(m1, vx, vy, vz, 0.0f);
+                    r.dz = xform_row(m2, vx, vy, vz, 0.0f);
                     setup_space(r);
                     cur_inst = meta.x;
                     bottom = true;
@@ -707,20 +708,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     const int k = j - o_excl;
                     const int ti = has ? (int)(o_base + nth_set_bit(o_mask, k)) : -1;
                     float4 a, b, c;
-                    if (kStage && p.tri_stage) {
-                        // Stage the pass's triangles: lane f loads 16-byte word f, f+32, f+64
-                        // of the 32 records, so neighbouring lanes read neighbouring words.
-                        s_idx[w][lane] = ti;
-                        __syncwarp();
-#pragma unroll
-                        for (int f = (int)lane; f < 96; f += 32) {
-                            const int pr = f / 3;
-                            const int tj = s_idx[w][pr];
-                            if (tj >= 0) s_tv[w][f] = __ldg(reinterpret_cast<const float4*>(p.tris + tj) + (f - 3 * pr));
-                        }
-                        __syncwarp();
-                        a = s_tv[w][3 * lane]; b = s_tv[w][3 * lane + 1]; c = s_tv[w][3 * lane + 2];
-                    } else if (has) {
+                    if (has) {
                         const float4* tp = reinterpret_cast<const float4*>(p.tris + ti);
                         a = __ldg(tp + 0); b = __ldg(tp + 1); c = __ldg(tp + 2);
                     }
@@ -792,8 +780,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                 const uint2 e = sp < kSh ? sstack[sp][tid] : lstack[sp - kSh];
                 const uint32_t type = e.x >> kTypeShift;
                 if (!kFlat && type == kEntryMarker) {
-                    r.ox = wox; r.oy = woy; r.oz = woz; r.dx = wdx; r.dy = wdy; r.dz = wdz;
-                    r.ix = wix; r.iy = wiy; r.iz = wiz; r.pad = wpad; r.oct = woct;
+                    r.ox = s_world[0][tid]; r.oy = s_world[1][tid]; r.oz = s_world[2][tid];
+                    r.dx = s_world[3][tid]; r.dy = s_world[4][tid]; r.dz = s_world[5][tid];
+                    r.ix = s_world[6][tid]; r.iy = s_world[7][tid]; r.iz = s_world[8][tid];
+                    r.pad = s_world[9][tid]; r.oct = __float_as_uint(s_world[10][tid]);
                     bottom = false; cur_inst = -1;
                     continue;
                 }

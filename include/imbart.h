@@ -254,20 +254,22 @@ int imbart_get_trace_config(int* variant, int* refill_lanes, int* postpone_lanes
 int imbart_get_trace_variant_any(void);
 
 /* The configuration of one query class: flags IMBART_TRACE_CLOSEST (incoherent closest hit),
- * IMBART_TRACE_ANY, or IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT. variant 1..10 (threads
- * per block x blocks per SM x shared stack entries of the persistent kernel, 0: one ray per
- * thread), refill_lanes: idle lanes a warp waits for before it fetches new rays. */
+ * IMBART_TRACE_ANY, or IMBART_TRACE_CLOSEST | IMBART_TRACE_COHERENT. variant 1..17 (threads
+ * per block x blocks per SM x shared stack entries of the persistent kernel; 1..10 test
+ * triangles per lane, 11..17 with the cooperative triangle phase; 0: one ray per thread),
+ * refill_lanes: idle lanes a warp waits for before it fetches new rays. */
 int imbart_set_trace_class(int flags, int variant, int refill_lanes);
 int imbart_get_trace_class(int flags, int* variant, int* refill_lanes);
 
-/* Triangle batch of a query class (persistent kernels): the triangles a lane tests per loop
- * trip before the warp's lanes with node work take their next node step; 0 = the whole leaf
- * group at once. 0..24, default 2 (IMBART_TRACE_TRI_BATCH). Hits do not depend on it. */
+/* Triangle batch of a query class (per-lane persistent shapes 1..10): the triangles a lane
+ * tests per loop trip before the warp's lanes with node work take their next node step; 0 =
+ * the whole leaf group at once. 0..24, default 0 (IMBART_TRACE_TRI_BATCH). The cooperative
+ * shapes ignore it. Hits do not depend on it. */
 int imbart_set_trace_tri_batch(int flags, int tri_batch);
 int imbart_get_trace_tri_batch(int flags);
 
 /* Autotuner: times every persistent-kernel configuration of the query class of `flags`
- * (variants 1..10 x refill 4, 8, 16, 24, 32, then triangle batches 0..4 of the best; one
+ * (variants 1..17 x refill 4, 8, 16, 24, 32, then triangle batches 0..4 of a per-lane best; one
  * warm-up and three timed launches each, CUDA events on `stream`) on `count` DEVICE rays,
  * keeps the fastest as the class's configuration and reports it with the time of the
  * configuration it replaced. Hits are written to `hits`.

@@ -249,8 +249,8 @@ def test_autotuner_picks_a_configuration_and_hits_stay_exact(cuda):
 def test_every_kernel_variant_is_exact(cuda):
     """Each traversal kernel shape the autotuner may pick (0: one ray per thread, 1..10:
     persistent warps at different block sizes, blocks per SM and shared stack depths, 11..17:
-    the same with the cooperative triangle phase; with triangle batches 0, 1 and 2, which in
-    the cooperative shapes select loads by each lane or staging in shared memory) gives the
+    the same with the cooperative triangle phase; with triangle batches 0, 1 and 2, which the
+    cooperative shapes ignore) gives the
     oracle's closest hits bit for bit, its occlusion answers, and the restated walk's node,
     triangle and instance counts."""
     import ctypes as C
