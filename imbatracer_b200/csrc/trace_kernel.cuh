@@ -475,10 +475,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
     __shared__ uint32_t s_key[kCW][32];              // per owner lane: smallest key of a pass
     __shared__ int s_tri[kCW][32];                   // per owner lane: its winning triangle id
     __shared__ float4 s_hit[kCW][32];                // per owner lane: the winner's t, u, v
-    // The world ray (origin, direction, inverse direction, pad, octant), restored when a ray
-    // leaves an instance: kept in shared memory rather than registers (11 registers fewer;
-    // measured +4-6 % on the instanced scene's ray sets). Flat kernels never leave the tree.
+    // The world ray (origin, direction, inverse direction, pad, octant): instance entries read
+    // the world direction from here, exits restore the rest. Shared memory rather than
+    // registers (11 registers fewer; measured +4-6 % on the instanced scene's ray sets); the
+    // direction is not needed in registers after the ray's set-up. Flat kernels never leave
+    // the tree.
     __shared__ float s_world[kFlat ? 1 : 11][kFlat ? 1 : kBlock];
+    // The best hit's u and v (read once, when the ray finishes): shared memory, not registers
+    // (+0.5-1 % on both scenes' ray sets; the 64-register shapes then spill 8 bytes, not 60-130).
+    __shared__ float s_uv[2][kBlock];
     uint2 lstack[kStackSize - kSh];
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -486,7 +491,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
 
     int ray = -1;                       // -1: idle (wants a ray), >= count: queue exhausted
     SpaceRay r;                         // current space (world or instance)
-    float tmin = 0.0f, best_t = 0.0f, best_u = 0.0f, best_v = 0.0f, tlimit = 0.0f;
+    float tmin = 0.0f, best_t = 0.0f, tlimit = 0.0f;
     int best_tri = -1, best_inst = -1, cur_inst = -1;
     bool bottom = false;
     uint32_t g_base = 0, g_imask = 0, g_hits = 0, t_base = 0, t_mask = 0;
@@ -509,9 +514,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
         h.x = best_tri;
         h.y = best_tri >= 0 ? (kFlat ? p.direct_inst : best_inst) : -1;
         h.z = __float_as_int(best_t);
-        h.w = __float_as_int(best_tri >= 0 ? best_u : 0.0f);
+        h.w = __float_as_int(best_tri >= 0 ? s_uv[0][tid] : 0.0f);
         p.hits[ray] = h;
-        if (p.v_out) p.v_out[ray] = best_tri >= 0 ? best_v : 0.0f;
+        if (p.v_out) p.v_out[ray] = best_tri >= 0 ? s_uv[1][tid] : 0.0f;
         ray = -1;
     };
 
@@ -532,7 +537,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     ray = idx;
                     const float4 ro = __ldg(p.rays + 2 * ray + 0);
                     const float4 rd = __ldg(p.rays + 2 * ray + 1);
-                    tmin = ro.w; best_t = rd.w; best_u = 0.0f; best_v = 0.0f;
+                    tmin = ro.w; best_t = rd.w;
                     best_tri = -1; best_inst = -1; cur_inst = -1; bottom = false; sp = 0;
                     if (!((tmin <= best_t) && (rd.x != 0.0f || rd.y != 0.0f || rd.z != 0.0f))) {
                         finish();
@@ -626,7 +631,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                                                       (cur_inst == best_inst && tri < best_tri))));
                         if (!closer) continue;
                         if (kMasked && !mask_opaque(p, tri, u, v)) continue;
-                        best_t = t; best_u = u; best_v = v; best_tri = tri; best_inst = cur_inst;
+                        best_t = t; s_uv[0][tid] = u; s_uv[1][tid] = v; best_tri = tri; best_inst = cur_inst;
                         tlimit = best_t * IMBART_SLACK;
                         if (kAnyHit) { stop = true; break; }
                     }
@@ -649,7 +654,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                     const float4 m0 = __ldg(ip + 0), m1 = __ldg(ip + 1), m2 = __ldg(ip + 2);
                     const int4 meta = __ldg(reinterpret_cast<const int4*>(ip + 3));
                     if (kStats) st.insts++;
-                    const float wx = r.ox, wy = r.oy, wz = r.oz, vx = r.dx, vy = r.dy, vz = r.dz;
+                    const float wx = r.ox, wy = r.oy, wz = r.oz;
+                    const float vx = s_world[3][tid], vy = s_world[4][tid], vz = s_world[5][tid];
                     r.ox = xform_row(m0, wx, wy, wz, 1.0f);
                     r.oy = xform_row(m1, wx, wy, wz, 1.0f);
                     r.oz = xform_row(m2, wx, wy, wz, 1.0f);
@@ -749,7 +755,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                         if (kAnyHit) {
                             if (found_k < 0) {
                                 found_k = (int)s_key[w][lane];
-                                best_t = hv.x; best_u = hv.y; best_v = hv.z; best_tri = tc; best_inst = cur_inst;
+                                best_t = hv.x; s_uv[0][tid] = hv.y; s_uv[1][tid] = hv.z; best_tri = tc; best_inst = cur_inst;
                             }
                         } else {
                             const bool closer = (hv.x < best_t) ||
@@ -757,7 +763,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                                                           : (best_tri < 0 || cur_inst < best_inst ||
                                                              (cur_inst == best_inst && tc < best_tri))));
                             if (closer) {
-                                best_t = hv.x; best_u = hv.y; best_v = hv.z; best_tri = tc; best_inst = cur_inst;
+                                best_t = hv.x; s_uv[0][tid] = hv.y; s_uv[1][tid] = hv.z; best_tri = tc; best_inst = cur_inst;
                                 tlimit = best_t * IMBART_SLACK;
                             }
                         }
@@ -781,7 +787,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) trace_persistent(TracePara
                 const uint32_t type = e.x >> kTypeShift;
                 if (!kFlat && type == kEntryMarker) {
                     r.ox = s_world[0][tid]; r.oy = s_world[1][tid]; r.oz = s_world[2][tid];
-                    r.dx = s_world[3][tid]; r.dy = s_world[4][tid]; r.dz = s_world[5][tid];
                     r.ix = s_world[6][tid]; r.iy = s_world[7][tid]; r.iz = s_world[8][tid];
                     r.pad = s_world[9][tid]; r.oct = __float_as_uint(s_world[10][tid]);
                     bottom = false; cur_inst = -1;
