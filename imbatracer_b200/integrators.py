@@ -154,8 +154,15 @@ class GpuScene:
                                                                                             node_width=w)
             S.trace_config_restore(start)
             classes = {}
-            for rays, hits, flags in ray_sets:
-                classes[flags] = scene.autotune(rays, hits, flags, stream=stream)
+            try:
+                for rays, hits, flags in ray_sets:
+                    classes[flags] = scene.autotune(rays, hits, flags, stream=stream)
+            except Exception:
+                S.trace_config_restore(start)
+                for sc in (scene, best[1] if best else None):
+                    if sc is not None and sc is not self.trace_scene:
+                        sc.close()
+                raise
             total = sum(c["ms"] for c in classes.values())
             results[w] = {"ms": total, "classes": classes, "config": S.trace_config_snapshot()}
             if best is None or total < results[best[0]]["ms"]:

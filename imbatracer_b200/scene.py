@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -274,6 +275,10 @@ def _check_ray_buffers(rays, hits, n: int, what: str) -> None:
                             f"(have {_nbytes(rays)} and {_nbytes(hits)})")
 
 
+# The node width is a process setting of the library; DeviceScene(node_width=...) changes it
+# only for its own conversion, under this lock.
+_NODE_WIDTH_LOCK = threading.Lock()
+
 TRACE_CLASSES = (N.TRACE_CLOSEST | N.TRACE_COHERENT, N.TRACE_CLOSEST, N.TRACE_ANY)
 
 
@@ -321,19 +326,21 @@ class DeviceScene:
         return self
 
     def __init__(self, td: TraversalData, device: int = 0, node_width: int | None = None):
-        """node_width: 8 or 4 for this scene (imbart_set_node_width around the conversion);
-        None keeps the process setting."""
+        """node_width: 8 or 4 for this scene (imbart_set_node_width around the conversion, under
+        a lock that Python callers share); None keeps the process setting."""
         lib = N.load()
-        prev_width = lib.imbart_get_node_width()
-        if node_width is not None:
-            N.check(lib.imbart_set_node_width(node_width), "imbart_set_node_width")
-        try:
-            h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),
-                                            len(td.instances), N.ptr(td.tris), len(td.tris), N.ptr(td.indices),
-                                            len(td.indices), N.ptr(td.texcoords), len(td.texcoords), N.ptr(td.masks),
-                                            len(td.masks), N.ptr(td.mask_buffer), len(td.mask_buffer), device)
-        finally:
-            lib.imbart_set_node_width(prev_width)
+        with _NODE_WIDTH_LOCK:
+            prev_width = lib.imbart_get_node_width()
+            if node_width is not None:
+                N.check(lib.imbart_set_node_width(node_width), "imbart_set_node_width")
+            try:
+                h = lib.imbart_scene_from_node2(td.root, N.ptr(td.nodes), len(td.nodes), N.ptr(td.instances),
+                                                len(td.instances), N.ptr(td.tris), len(td.tris), N.ptr(td.indices),
+                                                len(td.indices), N.ptr(td.texcoords), len(td.texcoords),
+                                                N.ptr(td.masks), len(td.masks), N.ptr(td.mask_buffer),
+                                                len(td.mask_buffer), device)
+            finally:
+                lib.imbart_set_node_width(prev_width)
         if not h:
             code, msg = N.last_error()
             raise N.ImbartError(f"imbart_scene_from_node2 failed ({code}): {msg}")
