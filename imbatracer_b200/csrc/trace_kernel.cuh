@@ -45,8 +45,9 @@ struct TraceParams {
     float* __restrict__ v_out;              // optional
     int count;
     // Batches over several scenes of one node pool: ray i starts at node roots[i] instead of
-    // `root` (with kDirectRootBit: in that mesh tree, as instance 0). With count_ptr set, the ray count is read from device memory at kernel start
-    // (`count` is then an upper bound the launch was sized for).
+    // `root` (with kDirectRootBit set: in that mesh tree, as instance 0). With count_ptr set,
+    // the ray count is read from device memory at kernel start (`count` is then an upper
+    // bound the launch was sized for).
     const int* __restrict__ roots;
     const int* __restrict__ count_ptr;
     int* __restrict__ error_flags;          // [0]: stack overflow count
