@@ -162,9 +162,10 @@ def test_host_buffer_trace(cuda):
     assert H.hits_equal(O.trace_node2(td, rays), hits).all()
 
 
-def test_alpha_masks(cuda):
-    """Checkerboard opacity masks on config1's sphere materials: transparent texels let rays
-    through; GPU and oracle agree bit for bit."""
+def masked_config1(two_level: bool = False):
+    """config1's spheres with checkerboard opacity masks on every other sphere material and a
+    single transparent texel on the ground; two_level adds a second, translated instance of
+    the mesh (a two-level scene instead of one identity instance)."""
     d = H.scene_desc("config1")
     mesh = d.meshes[0]
     rng = np.random.default_rng(8)
@@ -181,7 +182,18 @@ def test_alpha_masks(cuda):
         buf += checker.tolist()
     masks[n_mats - 3] = (1, 1, len(buf))    # the ground: a single transparent texel
     buf.append(0)
-    td = S.build_traversal_data([m2], d.instances, masks=masks, mask_buffer=np.array(buf, np.uint8))
+    insts = list(d.instances)
+    if two_level:
+        t = np.eye(4, dtype=np.float32)
+        t[:3, 3] = [3.0, 0.5, -2.0]
+        insts.append(S.Instance(0, t))
+    return S.build_traversal_data([m2], insts, masks=masks, mask_buffer=np.array(buf, np.uint8))
+
+
+def test_alpha_masks(cuda):
+    """Checkerboard opacity masks on config1's sphere materials: transparent texels let rays
+    through; GPU and oracle agree bit for bit."""
+    td = masked_config1()
     ds = S.DeviceScene(td)
     assert ds.info.masked == 1
     rays = H.ray_set("config1", 100000, seed=9)
@@ -193,6 +205,33 @@ def test_alpha_masks(cuda):
     refa = O.trace_node2(td, rays, any_hit=True)
     occ, _, _ = run_gpu(ds, rays, any_hit=True)
     assert np.array_equal(refa["tri_id"] >= 0, occ["tri_id"] >= 0)
+
+
+@pytest.mark.parametrize("two_level,width", [(False, 8), (True, 8), (False, 4), (True, 4)])
+def test_alpha_masks_every_kernel_variant(cuda, two_level, width):
+    """The masked kernels of every shape (flat kernels for the single identity instance,
+    two-level ones with a second instance; 8- and 4-wide trees) give the oracle's closest hits
+    bit for bit and its occlusion answers."""
+    lib = N.load()
+    saved = S.trace_config_snapshot()
+    try:
+        td = masked_config1(two_level)
+        ds = S.DeviceScene(td, node_width=width)
+        assert ds.info.masked == 1 and ds.node_width == width
+        rays = H.ray_set("config1", 20000, seed=29)
+        ref = O.trace_node2(td, rays)
+        refa = O.trace_node2(td, rays, any_hit=True)
+        for variant in range(18):
+            for flags in (N.TRACE_CLOSEST, N.TRACE_ANY):
+                N.check(lib.imbart_set_trace_class(flags, variant, 16), "imbart_set_trace_class")
+            hits, _, _ = run_gpu(ds, rays)
+            assert H.hits_equal(ref, hits).all(), variant
+            occ, _, _ = run_gpu(ds, rays, any_hit=True)
+            assert np.array_equal(refa["tri_id"] >= 0, occ["tri_id"] >= 0), variant
+        assert lib.imbart_scene_error_count(ds.handle) == 0
+        ds.close()
+    finally:
+        S.trace_config_restore(saved)
 
 
 def test_empty_and_zero_count(cuda):
