@@ -381,8 +381,8 @@ int build_range_graph(imbart_pt_context* ctx, const imbart_scene* scene, const i
 // A frame through the bounce-loop graph: the graph is (re)built when a launch parameter
 // changed, then replayed once per sample range.
 int render_graph(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh, const CameraParams& c,
-                 int max_path_len, int rr_start, float* image, long long total, long long chunk, bool group,
-                 bool fork, long long* stats, cudaStream_t st) {
+                 int max_path_len, int rr_start, float* image, long long first, long long total, long long chunk,
+                 bool group, bool fork, long long* stats, cudaStream_t st) {
     if (!ensure_range_state(ctx, max_path_len, st)) return IMBART_ERR_OUT_OF_MEMORY;
     std::vector<unsigned char> key = frame_key(scene, sh, image, total, chunk, max_path_len, rr_start, group, fork);
     if (!ctx->exec || key != ctx->graph_key) {
@@ -393,10 +393,14 @@ int render_graph(imbart_pt_context* ctx, const imbart_scene* scene, const imbart
     }
     const int n_slots = 2 * max_path_len + 2;
     // A copy from pageable memory is staged before the call returns: `c` may go out of scope.
+    // The ranges cover samples [first, total): state[0] is the first sample of the next range.
     if (!ok(cudaMemcpyAsync(ctx->camera, &c, sizeof(CameraParams), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync") ||
-        !ok(cudaMemsetAsync(ctx->range_state, 0, sizeof(long long) * (n_slots + 2), st), "cudaMemsetAsync"))
+        !ok(cudaMemsetAsync(ctx->range_state, 0, sizeof(long long) * (n_slots + 2), st), "cudaMemsetAsync") ||
+        (first != 0 &&
+         !ok(cudaMemcpyAsync(ctx->range_state, &first, sizeof(long long), cudaMemcpyHostToDevice, st),
+             "cudaMemcpyAsync")))
         return IMBART_ERR_CUDA;
-    const long long ranges = (total + chunk - 1) / chunk;
+    const long long ranges = (total - first + chunk - 1) / chunk;
     for (long long r = 0; r < ranges; ++r)
         if (!ok(cudaGraphLaunch(ctx->exec, st), "cudaGraphLaunch")) return IMBART_ERR_CUDA;
     note_launches((int)(ctx->graph_kernels * ranges));
@@ -586,19 +590,22 @@ int imbart_camera_rays(const float* raster_to_world, const float* cam_pos, int w
     return ok(cudaGetLastError(), "camera kernel") ? 0 : IMBART_ERR_CUDA;
 }
 
-int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh,
-                     const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
-                     int max_path_len, int rr_start, unsigned long long seed_base, float* image,
-                     long long max_paths_in_flight, long long* stats, void* stream) {
+int imbart_pt_render_range(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh,
+                           const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
+                           int max_path_len, int rr_start, unsigned long long seed_base, float* image,
+                           long long max_paths_in_flight, long long first_sample, long long n_samples,
+                           long long* stats, void* stream) {
     if (!ctx || !scene || !sh || !raster_to_world || !cam_pos || !image || width <= 0 || height <= 0 || spp <= 0 ||
-        max_path_len < 1) {
+        max_path_len < 1 || first_sample < 0 || n_samples <= 0 ||
+        first_sample > (long long)width * height * spp - n_samples) {
         set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_pt_render: invalid argument");
         return IMBART_ERR_INVALID_ARGUMENT;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    const long long total = (long long)width * height * spp;
+    // Samples [first_sample, total) of the frame's width * height * spp sample indices.
+    const long long total = first_sample + n_samples;
     long long chunk = max_paths_in_flight > 0 ? max_paths_in_flight : (16ll << 20);
-    chunk = std::min(chunk, total);
+    chunk = std::min(chunk, n_samples);
     chunk = std::min(chunk, (long long)(1 << 30));
     int prev = 0;
     cudaGetDevice(&prev);
@@ -618,7 +625,8 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     const int mode = graph_mode(ctx);
     if (!prof && mode > 0) {
         // Measurement (per-launch events, host-side ray counts) keeps the host-driven loop.
-        rc = render_graph(ctx, scene, sh, c, max_path_len, rr_start, image, total, chunk, group, mode == 2, stats, st);
+        rc = render_graph(ctx, scene, sh, c, max_path_len, rr_start, image, first_sample, total, chunk, group, mode == 2,
+                          stats, st);
         cudaSetDevice(prev);
         return rc;
     }
@@ -649,7 +657,7 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
         }
         return r;
     };
-    for (long long first = 0; first < total && !rc; first += chunk) {
+    for (long long first = first_sample; first < total && !rc; first += chunk) {
         int n = (int)std::min(chunk, total - first);
         int cur = 0;
         camera_kernel<<<(n + 127) / 128, 128, 0, st>>>(c, first, n, ctx->rays[cur], ctx->pixel[cur], ctx->rng[cur],
@@ -720,6 +728,19 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
     }
     cudaSetDevice(prev);
     return rc;
+}
+
+int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* sh,
+                     const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
+                     int max_path_len, int rr_start, unsigned long long seed_base, float* image,
+                     long long max_paths_in_flight, long long* stats, void* stream) {
+    if (width <= 0 || height <= 0 || spp <= 0) {
+        set_error(IMBART_ERR_INVALID_ARGUMENT, "imbart_pt_render: invalid argument");
+        return IMBART_ERR_INVALID_ARGUMENT;
+    }
+    return imbart_pt_render_range(ctx, scene, sh, raster_to_world, cam_pos, width, height, spp, max_path_len,
+                                  rr_start, seed_base, image, max_paths_in_flight, 0,
+                                  (long long)width * height * spp, stats, stream);
 }
 
 int imbart_group_by_key(const unsigned char* keys, int n, int* perm, void* stream) {

@@ -15,7 +15,9 @@ camera paths against them. Across G ranks:
      samples) are summed with an all-reduce.
 
 The image equals the single-GPU iteration's up to the order of the float additions. PT
-frames and ray batches need no exchange (the bench runs them as independent replicas).
+frames and ray batches need no exchange (the bench runs them as independent replicas); one
+PT frame can also be split across the ranks by sample ranges (render_frame_split: samples
+are seeded by their index, so the ranges' images summed are the single-GPU frame).
 """
 from __future__ import annotations
 
@@ -75,6 +77,35 @@ def all_gather_light_vertices(local, wave_counts, group=None):
     dist.all_gather(gathered, padded, group=group)
     parts = [gathered[r][:counts[r]] for r in range(world)]
     return assemble_light_vertices(parts, [w.tolist() for w in all_waves])
+
+
+def render_frame_split(pt, spp: int, seed_base: int, width: int | None = None, height: int | None = None,
+                       image=None, group=None, stream=None, device=None):
+    """One path-traced frame split across the ranks of `group`: rank r renders its contiguous
+    share of the frame's width * height * spp samples (PathTracer.render with sample_range)
+    and the ranks' images are summed with an all-reduce, so every rank gets the whole frame —
+    the single-GPU image up to the order of the float additions. Returns the summed image
+    (added to `image` when given); pt.last_stats holds this rank's ray counts. device: where
+    the image lives (default: the path tracer's GPU)."""
+    import torch
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    cam = pt.scene.desc.camera
+    w, h = width or cam.width, height or cam.height
+    dev = torch.device(device) if device is not None else torch.device("cuda", pt.scene.device)
+    part = torch.zeros((h, w, 3), dtype=torch.float32, device=dev)
+    first, count = split_range(w * h * spp, rank, world)
+    if count > 0:
+        pt.render(spp, seed_base, w, h, image=part, stream=stream, sample_range=(first, count))
+    else:
+        pt.last_stats = np.zeros(3, np.int64)
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+    dist.all_reduce(part, group=group)
+    if image is None:
+        return part
+    image += part
+    return image
 
 
 class DistributedVcmIntegrator:

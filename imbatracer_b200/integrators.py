@@ -225,10 +225,12 @@ class PathTracer:
         self.last_stats = np.zeros(3, np.int64)
 
     def render(self, spp: int, seed_base: int, width: int | None = None, height: int | None = None, image=None,
-               stream=None, cam: G.Camera | None = None, stats: bool = True):
+               stream=None, cam: G.Camera | None = None, stats: bool = True, sample_range=None):
         """Adds one frame to `image` (a new zeroed image when None) on `stream`. With stats,
         last_stats holds the frame's closest-hit rays, shadow rays and wavefronts (one
-        synchronization at the end); without, a graph-driven frame returns unsynchronized."""
+        synchronization at the end); without, a graph-driven frame returns unsynchronized.
+        sample_range (first, count): only those of the frame's width * height * spp samples
+        (imbart_pt_render_range), seeded as in the whole frame."""
         import torch
         cam = cam or self.scene.desc.camera
         w = width or cam.width
@@ -240,11 +242,20 @@ class PathTracer:
             image = torch.zeros((h, w, 3), dtype=torch.float32, device=dev)
         st = None if stream is None else stream.cuda_stream
         out = np.zeros(3, np.int64)
-        N.check(N.load().imbart_pt_render(self.ctx, self.scene.trace_scene.handle, self.scene.shading, N.ptr(r2w),
-                                          N.ptr(pos), w, h, spp, self.max_path_len, self.rr_start,
-                                          seed_base & (2 ** 64 - 1), N.ptr(image), self.max_paths,
-                                          N.ptr(out) if stats else None, st),
-                "imbart_pt_render")
+        if sample_range is None:
+            N.check(N.load().imbart_pt_render(self.ctx, self.scene.trace_scene.handle, self.scene.shading, N.ptr(r2w),
+                                              N.ptr(pos), w, h, spp, self.max_path_len, self.rr_start,
+                                              seed_base & (2 ** 64 - 1), N.ptr(image), self.max_paths,
+                                              N.ptr(out) if stats else None, st),
+                    "imbart_pt_render")
+        else:
+            first, count = (int(v) for v in sample_range)
+            N.check(N.load().imbart_pt_render_range(self.ctx, self.scene.trace_scene.handle, self.scene.shading,
+                                                    N.ptr(r2w), N.ptr(pos), w, h, spp, self.max_path_len,
+                                                    self.rr_start, seed_base & (2 ** 64 - 1), N.ptr(image),
+                                                    self.max_paths, first, count, N.ptr(out) if stats else None,
+                                                    st),
+                    "imbart_pt_render_range")
         if stats:
             self.last_stats = out
         return image

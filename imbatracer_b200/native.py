@@ -164,6 +164,8 @@ _SIGNATURES = {
     "imbart_pt_create": (P, [I]),
     "imbart_pt_destroy": (None, [P]),
     "imbart_pt_render": (I, [P, P, P, P, P, I, I, I, I, I, C.c_uint64, P, C.c_longlong, P, P]),
+    "imbart_pt_render_range": (I, [P, P, P, P, P, I, I, I, I, I, C.c_uint64, P, C.c_longlong, C.c_longlong,
+                                   C.c_longlong, P, P]),
     "imbart_pt_set_profile": (I, [P, P]),
     "imbart_pt_set_graphs": (I, [P, I]),
     "imbart_group_by_key": (I, [P, I, P, P]),

@@ -435,6 +435,17 @@ int imbart_pt_render(imbart_pt_context* ctx, const imbart_scene* scene, const im
                      int max_path_len, int rr_start, unsigned long long seed_base, float* image,
                      long long max_paths_in_flight, long long* stats, void* stream);
 
+/* The samples [first_sample, first_sample + n_samples) of the same frame (sample indices 0 ..
+ * width*height*spp - 1, seeded as in the whole frame): disjoint ranges rendered into images
+ * that are then summed give the whole frame's image (up to the order of float additions), so
+ * one frame can be split across devices (imbatracer_b200.distributed.render_frame_split).
+ * imbart_pt_render is the range [0, width*height*spp). */
+int imbart_pt_render_range(imbart_pt_context* ctx, const imbart_scene* scene, const imbart_shading* shading,
+                           const float* raster_to_world, const float* cam_pos, int width, int height, int spp,
+                           int max_path_len, int rr_start, unsigned long long seed_base, float* image,
+                           long long max_paths_in_flight, long long first_sample, long long n_samples,
+                           long long* stats, void* stream);
+
 /* Measurement of the traversal launches inside imbart_pt_render (for roofline reporting). */
 typedef struct {
     int events;                 /* in: time every traversal launch with CUDA events on the stream */

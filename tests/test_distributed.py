@@ -65,9 +65,43 @@ def _gloo_worker(rank, world, port, result_dir):
         g = D.all_gather_light_vertices(fake_cache(rank, waves), waves)
         assert [tuple(int(x) for x in row[:3]) for row in g.tolist()] == \
             [(0, w, i) for w in range(4) for i in range(WAVES[0][w])]
+        # A frame split by sample ranges: every sample lands once in the summed image.
+        pt = FakePathTracer()
+        img = D.render_frame_split(pt, 3, 7, device="cpu")
+        assert torch.equal(img, FakePathTracer.whole(3)), img
+        assert pt.ranges[0][0] == (0 if rank == 0 else pt.ranges[0][0]) and len(pt.ranges) == 1
         open(os.path.join(result_dir, f"ok{rank}"), "w").write("ok")
     finally:
         dist.destroy_process_group()
+
+
+class FakePathTracer:
+    """Stands in for PathTracer on the CPU: render() adds 1 + sample index to the sample's
+    pixel (sample index // spp) for every sample of its range."""
+
+    class scene:
+        class desc:
+            class camera:
+                width, height = 5, 4
+
+    def __init__(self):
+        self.ranges = []
+
+    def render(self, spp, seed_base, w, h, image=None, stream=None, sample_range=None):
+        first, count = sample_range
+        self.ranges.append((first, count))
+        for i in range(first, first + count):
+            image.view(-1, 3)[i // spp] += 1.0 + i
+        self.last_stats = np.zeros(3, np.int64)
+        return image
+
+    @staticmethod
+    def whole(spp):
+        import torch
+        img = torch.zeros((4, 5, 3), dtype=torch.float32)
+        for i in range(4 * 5 * spp):
+            img.view(-1, 3)[i // spp] += 1.0 + i
+        return img
 
 
 def test_two_gloo_ranks(tmp_path):
@@ -146,5 +180,67 @@ def test_distributed_integrator_on_one_nccl_rank(cuda):
         assert b.sum() > 0 and np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / den <= 1e-5
         dv.close()
         vi.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ranks,graphs,paths", [(2, 2, 0), (3, 2, 5000), (3, 0, 0)])
+def test_frame_split_by_sample_ranges_equals_the_frame(cuda, ranks, graphs, paths):
+    """A path-traced frame split into `ranks` contiguous sample ranges (emulated ranks rendered
+    one after another on this GPU, as render_frame_split does on each rank) sums to the
+    single-GPU frame up to float summation order, with the same closest-hit and shadow ray
+    counts; with the bounce loop as CUDA graphs (2) and driven from the host (0), and with a
+    wavefront smaller than a range (several ranges per rank)."""
+    import torch
+    from imbatracer_b200 import native as N
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    from tests.test_pt import small_mixed_scene
+    d = small_mixed_scene()
+    gs = GpuScene(d)
+    pt = PathTracer(gs, max_path_len=6)
+    if paths:
+        pt.max_paths = paths
+    N.check(N.load().imbart_pt_set_graphs(pt.ctx, graphs), "imbart_pt_set_graphs")
+    w, h, spp = 48, 32, 4
+    whole = pt.render(spp, 21, w, h)
+    whole_stats = pt.last_stats.copy()
+    split = torch.zeros_like(whole)
+    stats = np.zeros(3, np.int64)
+    for r in range(ranks):
+        first, count = D.split_range(w * h * spp, r, ranks)
+        pt.render(spp, 21, w, h, image=split, sample_range=(first, count))
+        stats += pt.last_stats
+    torch.cuda.synchronize()
+    a, b = split.cpu().numpy().astype(np.float64), whole.cpu().numpy().astype(np.float64)
+    assert b.sum() > 0
+    assert np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)) <= 1e-6
+    assert stats[0] == whole_stats[0] and stats[1] == whole_stats[1]
+    with pytest.raises(N.ImbartError):
+        pt.render(spp, 21, w, h, sample_range=(w * h * spp - 10, 11))   # past the frame's samples
+    N.load().imbart_clear_error()
+    pt.close()
+    gs.close()
+
+
+@pytest.mark.gpu
+def test_render_frame_split_on_one_nccl_rank(cuda):
+    import torch
+    import torch.distributed as dist
+    from imbatracer_b200.integrators import GpuScene, PathTracer
+    from tests.test_pt import small_mixed_scene
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        gs = GpuScene(small_mixed_scene())
+        pt = PathTracer(gs, max_path_len=6)
+        a = D.render_frame_split(pt, 2, 33, 40, 24)
+        b = pt.render(2, 33, 40, 24)
+        torch.cuda.synchronize()
+        a, b = a.cpu().numpy().astype(np.float64), b.cpu().numpy().astype(np.float64)
+        assert b.sum() > 0 and np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)) <= 1e-6
+        pt.close()
+        gs.close()
     finally:
         dist.destroy_process_group()
